@@ -1,0 +1,447 @@
+#!/usr/bin/env python
+"""ns/day of the 23,958-atom PME water box (LangevinMiddle + SETTLE, 2 fs) on B200.
+
+One bench step is one segment of `--segment` MD steps (default 200) run back to back through
+Context.step, as in production; L2 is flushed (256 MiB write) between timed segments, outside
+the timed region.  Timing uses CUDA events on the Context's own stream; multi-GPU runs are
+independent replicas (no collective on the data path) timed as the max over ranks.
+
+--impl reference times the reference algorithm's CPU implementation (the f64 oracle port of
+openmm-rs's NonbondedForce/PME/LangevinMiddle/SHAKE path, all host threads) on the same
+workload, one MD step per bench step.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "openmm-rs_b200"))
+
+WORKLOAD = "water-23958"
+DT_PS = 0.002
+METRIC = "ns/day @24k-atom PME water box (1 B200) + force RMS rel err vs FP64"
+# Algorithmic FP32 work per in-cutoff pair of the mixed-precision PME pair kernel, FMA = 2,
+# MUFU (rsqrt, exp2, rcp) = 1: delta 3, r^2 5, rsqrt 1, 1/r^2 1, LJ 14, Ewald (r, exp,
+# erfc fit with 7 FMAs, force) 30, f/r sum 1, force vector 3, i/j accumulation 6 + 3 = 71.
+FLOPS_PER_PAIR = 71
+# HBM bytes per particle of one integrator launch: read x, v, fixed-point F, rebuild
+# reference (4 x 24) plus per-molecule index (16/3), write x, v (2 x 24).
+INTEGRATE_BYTES_PER_ATOM = 96 + 16 / 3 + 48
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--segment", type=int, default=200, help="MD steps per bench step")
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--precision", choices=["mixed", "double"], default="mixed")
+    p.add_argument("--skip-extras", action="store_true",
+                   help="skip the FP64-form, roofline and CPU-baseline legs")
+    p.add_argument("--no-equilibrate", action="store_true",
+                   help="start from the lattice (short runs for profiler captures)")
+    return p.parse_args()
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+def ns_per_day(md_steps, seconds):
+    return md_steps * DT_PS / 1000.0 / seconds * 86400.0
+
+
+def measured_peaks():
+    try:
+        return json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except Exception:
+        return {}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id):
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+               "-lms", "200"]
+        if gpu_id:
+            cmd += ["-i", gpu_id]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.file.seek(0)
+        rows = [r.split(",") for r in self.file.read().strip().splitlines() if r.strip()]
+        os.unlink(self.file.name)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except (ValueError, IndexError):
+                continue
+            for k, name in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].strip().lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+_EQUILIBRATED = {}
+
+
+EQUILIBRATION_STEPS = 2000
+
+
+def equilibrate(seed, device, steps=None):
+    """Untimed: the jittered-lattice start releases ~27 MJ/mol while it relaxes, so the box is
+    first brought to 300 K with a strongly coupled bath (20/ps, 4 ps)."""
+    import ommb200
+    from ommb200 import synth, systems
+
+    steps = EQUILIBRATION_STEPS if steps is None else steps
+    if seed not in _EQUILIBRATED:
+        w = synth.water_preset(WORKLOAD)
+        ctx = ommb200.Context(systems.water_system(w), systems.langevin(friction=20.0, seed=seed),
+                              precision="mixed", device=device)
+        ctx.set_positions(w.positions)
+        ctx.set_velocities_to_temperature(300.0, seed=seed)
+        if steps:
+            ctx.step(steps)
+        st = ctx.get_state(positions=True, velocities=True)
+        ctx.close()
+        _EQUILIBRATED[seed] = (w, st.positions, st.velocities)
+    return _EQUILIBRATED[seed]
+
+
+def build_context(precision, seed, device):
+    import ommb200
+    from ommb200 import systems
+
+    w, x, v = equilibrate(seed, device)
+    ctx = ommb200.Context(systems.water_system(w), systems.langevin(seed=seed),
+                          precision=precision, device=device)
+    ctx.set_positions(x)
+    ctx.set_velocities(v)
+    return w, ctx
+
+
+def time_segments(ctx, torch, segments, md_steps, flush):
+    """Device time (ms) of `segments` Context.step(md_steps) calls, flushing L2 between."""
+    stream = torch.cuda.ExternalStream(ctx.stream_handle())
+    total = 0.0
+    for _ in range(segments):
+        flush.zero_()
+        torch.cuda.synchronize()
+        start = torch.cuda.Event(enable_timing=True)
+        stop = torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        ctx.step(md_steps)
+        stop.record(stream)
+        stop.synchronize()
+        total += start.elapsed_time(stop)
+    return total
+
+
+def time_e2e(ctx, torch, n_atoms, segments, md_steps, flush):
+    """End to end through the public API: pinned host inputs uploaded, MD segment, positions,
+    velocities and energies read back, every bench step."""
+    stream = torch.cuda.ExternalStream(ctx.stream_handle())
+    st = ctx.get_state(positions=True, velocities=True)
+    pos = torch.from_numpy(st.positions.copy()).pin_memory()
+    vel = torch.from_numpy(st.velocities.copy()).pin_memory()
+    total = 0.0
+    for _ in range(segments):
+        flush.zero_()
+        torch.cuda.synchronize()
+        start = torch.cuda.Event(enable_timing=True)
+        stop = torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        ctx.set_positions_from_pointer(pos.data_ptr())
+        ctx.set_velocities_from_pointer(vel.data_ptr())
+        ctx.step(md_steps)
+        ctx.get_state_into(pos.data_ptr(), vel.data_ptr(), energy=True)
+        stop.record(stream)
+        stop.synchronize()
+        total += start.elapsed_time(stop)
+    h2d = 2 * 24 * n_atoms
+    d2h = 2 * 24 * n_atoms + 8
+    return total, h2d, d2h
+
+
+def kernel_profile(ctx, md_steps):
+    """Per-kernel device time from CUDA events recorded around every launch on the Context's
+    stream (non-graph launch path), over `md_steps` MD steps."""
+    ctx.set_profiling(True)
+    ctx.step(md_steps)
+    times = ctx.kernel_times()
+    ctx.set_profiling(False)
+    return times
+
+
+def cpu_baseline(w, x0, threads, gpu_forces):
+    """The oracle port of the reference path timed on the host: force evaluation (all given
+    threads) + LangevinMiddle/SHAKE steps of the same box from positions `x0`, bounded to
+    ~10 s of CPU work.  Its first force evaluation is also the FP64 reference for the GPU
+    forces computed at `x0`."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import numpy as np
+
+    import oracle as O
+
+    t0 = time.perf_counter()
+    f, e = O.nonbonded(x0, w.charges(), w.sigmas(), w.epsilons(), w.exceptions(),
+                       method="PME", cutoff=0.9, ewald_tolerance=5e-4, box=w.box,
+                       threads=threads)
+    first = time.perf_counter() - t0
+    err = None
+    if gpu_forces is not None:
+        err = float(np.sqrt(((gpu_forces - f) ** 2).sum() / (f ** 2).sum()))
+    x, v = x0.copy(), np.zeros_like(x0)
+    steps, spent = 0, 0.0
+    budget = 10.0
+    while spent < budget and steps < 50:
+        t0 = time.perf_counter()
+        f, _ = O.nonbonded(x, w.charges(), w.sigmas(), w.epsilons(), w.exceptions(),
+                           method="PME", cutoff=0.9, ewald_tolerance=5e-4, box=w.box,
+                           threads=threads)
+        rc, x, v = O.lfmiddle_step(x, v, f, w.masses(), DT_PS, 300.0, 1.0,
+                                   O.gaussian_noise(1, 0, steps, w.n_atoms),
+                                   constraints=w.constraints(), tolerance=1e-5, mode=0)
+        spent += time.perf_counter() - t0
+        steps += 1
+        if rc != 0:
+            break
+    return {"value": ns_per_day(steps, spent), "unit": "ns/day", "cores": threads,
+            "kind": "port",
+            "sample": f"{steps} MD steps of the {w.n_atoms}-atom box (f64 oracle: PME force "
+                      f"evaluation + LangevinMiddle/SHAKE), {spent:.1f} s; first force "
+                      f"evaluation {first:.2f} s", "energy": e}, err
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import numpy as np
+
+    import oracle as O
+    from ommb200 import synth
+
+    w = synth.water_preset(WORKLOAD)
+    threads = O.max_threads()
+    x, v = w.positions.copy(), np.zeros_like(w.positions)
+
+    def md_step(k):
+        nonlocal x, v
+        f, _ = O.nonbonded(x, w.charges(), w.sigmas(), w.epsilons(), w.exceptions(),
+                           method="PME", cutoff=0.9, ewald_tolerance=5e-4, box=w.box,
+                           threads=threads)
+        rc, x, v = O.lfmiddle_step(x, v, f, w.masses(), DT_PS, 300.0, 1.0,
+                                   O.gaussian_noise(1, 0, k, w.n_atoms),
+                                   constraints=w.constraints(), tolerance=1e-5, mode=0)
+        if rc != 0:
+            raise RuntimeError(f"reference constraint solver failed ({rc})")
+
+    for k in range(args.warmup):
+        md_step(k)
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        md_step(args.warmup + k)
+    secs = time.perf_counter() - t0
+    value = ns_per_day(args.steps, secs)
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "ns/day",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * secs / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n_atoms": w.n_atoms, "box_nm": 6.2, "dt_ps": DT_PS,
+                   "method": "PME cutoff 0.9 nm tol 5e-4 grid 56^3",
+                   "md_steps_per_bench_step": 1, "threads": threads},
+        "cpu_baseline": {"value": value, "unit": "ns/day", "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} MD steps, f64 oracle port of the reference "
+                                   "CPU path (PME + LangevinMiddle/SHAKE)"},
+        "e2e": {"value": value, "unit": "ns/day", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    global EQUILIBRATION_STEPS
+    if args.no_equilibrate:
+        EQUILIBRATION_STEPS = 0
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import numpy as np
+    import torch
+
+    import ommb200
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    seed = 1000 + rank
+    w, ctx = build_context(args.precision, seed, local)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{local}")
+    st0 = ctx.get_state(positions=True, forces=True, energy=True)
+    x0, gpu_forces, e_gpu = st0.positions, st0.forces, st0.potential_energy
+    time_segments(ctx, torch, args.warmup, args.segment, flush)
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        pass
+    barrier()
+    sampler = ClockSampler(uuid)
+    ms = time_segments(ctx, torch, args.steps, args.segment, flush)
+    clocks = sampler.stop()
+    barrier()
+    e2e_ms, h2d, d2h = time_e2e(ctx, torch, w.n_atoms, args.steps, args.segment, flush)
+    barrier()
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([ms, e2e_ms], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, e2e_ms = float(t[0]), float(t[1])
+    md_steps = args.steps * args.segment
+    value = world * ns_per_day(md_steps, ms / 1000.0)
+    e2e_value = world * ns_per_day(md_steps, e2e_ms / 1000.0)
+
+    extras = {}
+    roofline = None
+    cpu = None
+    launches = None
+    if rank == 0 and not args.skip_extras:
+        prof_steps = 100
+        times = kernel_profile(ctx, prof_steps)
+        pairs = len(ctx.debug_pair_list())
+        pair_ms, pair_n = times.get("pair", (0.0, 1))
+        t_pair = pair_ms / max(pair_n, 1) / 1000.0
+        fp32_peak = ommb200.measure_fp32_peak(local)
+        achieved = pairs * FLOPS_PER_PAIR / t_pair / 1e12 if t_pair > 0 else None
+        roofline = {"bound": "fp32", "kernel": "pair_kernel<float, Ewald>",
+                    "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                    "frac": (achieved / fp32_peak) if achieved else None,
+                    "peak_source": "measured FP32 FMA throughput of this GPU "
+                                   "(ommb200_measure_fp32_peak); MEASURED_PEAKS.json has no "
+                                   "FP32 figure",
+                    "algorithmic": f"{pairs} in-cutoff pairs x {FLOPS_PER_PAIR} flops per launch",
+                    "avg_launch_ms": 1000.0 * t_pair,
+                    "traffic": None}
+        peaks = measured_peaks()
+        hbm = peaks.get("hbm_gbs")
+        integ_ms, integ_n = times.get("integrate", (0.0, 1))
+        if integ_ms > 0 and hbm:
+            gbs = w.n_atoms * INTEGRATE_BYTES_PER_ATOM / (integ_ms / integ_n / 1000.0) / 1e9
+            extras["integrate_roofline"] = {"bound": "hbm", "achieved": gbs, "peak": hbm,
+                                            "unit": "GB/s", "frac": gbs / hbm,
+                                            "note": "of measured; latency-bound at this size"}
+        per_step = {k: (v[0] / v[1], v[1] / prof_steps) for k, v in times.items()}
+        extras["kernel_ms_per_md_step"] = {k: round(v[0] * v[1], 5) for k, v in per_step.items()}
+        # our kernels per MD step: rebuild 9, pack 2, pair 1, PME spread/convert/convolve/
+        # gather 4, exceptions 1, integrate 1; plus one counter kernel per graph launch
+        per_md = 9 + 2 + 1 + 4 + 1 + 1
+        launches = md_steps * per_md + args.steps * (args.segment // 20)
+        extras["pairs_in_cutoff"] = pairs
+        # FP64-on-GPU form of the same kernels
+        _, ctx64 = build_context("double", seed, local)
+        time_segments(ctx64, torch, 1, args.segment, flush)
+        n64 = max(2, args.steps // 4)
+        ms64 = time_segments(ctx64, torch, n64, args.segment, flush)
+        v64 = ns_per_day(n64 * args.segment, ms64 / 1000.0)
+        ctx64.close()
+        extras["fp64_form"] = {"value": v64, "unit": "ns/day", "mixed_over_fp64": value / world / v64}
+        if world == 1:
+            threads = os.cpu_count() or 1
+            cpu, err = cpu_baseline(w, x0, threads, gpu_forces)
+            extras["force_rms_rel_err_vs_fp64_oracle"] = err
+            extras["energy_rel_err_vs_fp64_oracle"] = abs(e_gpu - cpu.pop("energy")) / abs(e_gpu)
+            extras["host_cpu"] = {"nproc": os.cpu_count(), "model": _cpu_model()}
+    out = {
+        "metric": METRIC, "value": value, "unit": "ns/day", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "ms_per_md_step": ms / md_steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp32" if args.precision == "mixed" else "fp64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n_atoms": w.n_atoms, "box_nm": 6.2,
+                   "method": "PME cutoff 0.9 nm, Ewald tol 5e-4, grid 56^3, order 5",
+                   "integrator": "LangevinMiddle 300 K, 1/ps, 2 fs, SETTLE",
+                   "precision": args.precision + " (FP32 pair/spline math, int64 fixed-point "
+                                "forces, FP64 integration and constraints)",
+                   "md_steps_per_bench_step": args.segment,
+                   "l2": "flushed (256 MiB write) between timed bench steps; MD steps inside a "
+                         "bench step run back to back",
+                   "parallelism": f"replicas x{world}"},
+        "e2e": {"value": e2e_value, "unit": "ns/day", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "clocks": clocks,
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+    }
+    out.update(extras)
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def _cpu_model():
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
+if __name__ == "__main__":
+    main()

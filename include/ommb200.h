@@ -1,0 +1,213 @@
+/*
+ * ommb200 -- C ABI of the B200-native force and integration engine for the openmm-rs hot
+ * path: NonbondedForce (PME, LJ with cutoff and switching, no-cutoff), GBSAOBCForce,
+ * HarmonicBond/AngleForce and LangevinMiddleIntegrator with SETTLE, driven through a
+ * Context with step / getState.
+ *
+ * Every entry point returns an int status (OMMB200_OK or a negative OMMB200_ERR_* code) and
+ * never aborts; ommb200_last_error() gives the message of the calling thread's last failure.
+ * Handles are opaque; a Context takes ownership of the System and Integrator passed to it
+ * (as openmm-core's Context::new moves them in, context.rs:83-87) and a System takes
+ * ownership of each Force added to it (system.rs:201-204).  Host arrays are copied in/out.
+ * A Context is not thread-safe; use one per host thread.  All reference citations are
+ * relative to mogura-rs/openmm-rs/crates/openmm-core/src.
+ */
+#ifndef OMMB200_H
+#define OMMB200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (constraints.rs:12-21 ConstraintError; asserts become INVALID_ARG) ---- */
+#define OMMB200_OK 0
+#define OMMB200_ERR_INVALID_ARG (-1)
+#define OMMB200_ERR_CONSTRAINT (-2)
+#define OMMB200_ERR_NONFINITE (-3)
+#define OMMB200_ERR_NLIST_OVERFLOW (-4)
+#define OMMB200_ERR_TIMEOUT (-5)
+#define OMMB200_ERR_CUDA (-6)
+#define OMMB200_ERR_UNSUPPORTED (-7)
+#define OMMB200_ERR_OUT_OF_MEMORY (-8)
+
+/* NonbondedMethod (forces/nonbonded.rs:19-33) */
+#define OMMB200_NO_CUTOFF 0
+#define OMMB200_CUTOFF_NON_PERIODIC 1
+#define OMMB200_CUTOFF_PERIODIC 2
+#define OMMB200_EWALD 3 /* accepted by the setter, rejected at Context creation */
+#define OMMB200_PME 4
+#define OMMB200_LJPME 5 /* accepted by the setter, rejected at Context creation */
+
+/* GBSAOBCMethod (forces/gbsa_obc.rs:11-17) */
+#define OMMB200_GBSA_NO_CUTOFF 0
+#define OMMB200_GBSA_CUTOFF_NON_PERIODIC 1
+#define OMMB200_GBSA_CUTOFF_PERIODIC 2
+
+/* arithmetic of the force kernels */
+#define OMMB200_PRECISION_MIXED 0  /* FP32 pair/spline math, 64-bit fixed-point accumulation */
+#define OMMB200_PRECISION_DOUBLE 1 /* the same kernels entirely in FP64 */
+
+/* getState flags (state.rs:7-14) plus the virial, which the reference lacks */
+#define OMMB200_STATE_POSITIONS 1
+#define OMMB200_STATE_VELOCITIES 2
+#define OMMB200_STATE_FORCES 4
+#define OMMB200_STATE_ENERGY 8
+#define OMMB200_STATE_VIRIAL 16
+
+typedef struct ommb200_system ommb200_system;
+typedef struct ommb200_force ommb200_force;
+typedef struct ommb200_integrator ommb200_integrator;
+typedef struct ommb200_context ommb200_context;
+
+typedef struct {
+  int precision;              /* OMMB200_PRECISION_* (default MIXED) */
+  int device;                 /* CUDA device ordinal (default 0) */
+  int use_cuda_graph;         /* capture the step in a CUDA graph (default 1) */
+  double neighbor_skin;       /* Verlet skin in nm; <= 0 picks the tuned default */
+  int steps_per_graph;        /* steps captured per graph launch; <= 0 picks the default */
+} ommb200_options;
+
+typedef struct {
+  double time;                /* ps */
+  int64_t step_count;
+  double potential_energy;    /* kJ/mol, valid if OMMB200_STATE_ENERGY was requested */
+  double kinetic_energy;      /* kJ/mol (context.rs:1107-1163, LFMiddle offset 0) */
+  double box[9];              /* periodic box rows a, b, c in nm */
+  double virial[9];           /* -dU/d(strain), kJ/mol, if OMMB200_STATE_VIRIAL */
+} ommb200_state_info;
+
+/* ---- library ---- */
+const char* ommb200_last_error(void);
+const char* ommb200_version(void);
+void ommb200_default_options(ommb200_options* out);
+
+/* ---- System (system.rs:43-233) ---- */
+int ommb200_system_create(ommb200_system** out);                       /* System::new */
+int ommb200_system_destroy(ommb200_system* system);
+int ommb200_system_add_particle(ommb200_system* s, double mass, int* index); /* system.rs:64-72 */
+int ommb200_system_num_particles(const ommb200_system* s, int* out);
+int ommb200_system_add_constraint(ommb200_system* s, int p1, int p2, double distance,
+                                  int* index);                          /* add_constraint */
+int ommb200_system_set_default_periodic_box_vectors(ommb200_system* s, const double a[3],
+                                                    const double b[3], const double c[3]);
+int ommb200_system_add_force(ommb200_system* s, ommb200_force* force, int* index); /* add_force */
+
+/* ---- forces: common (forces/mod.rs:142-246 force_group / name) ---- */
+int ommb200_force_destroy(ommb200_force* force); /* only for forces not added to a System */
+int ommb200_force_set_group(ommb200_force* force, int group);
+int ommb200_force_get_group(const ommb200_force* force, int* group);
+
+/* ---- NonbondedForce (forces/nonbonded.rs:122-658) ---- */
+int ommb200_nonbonded_create(ommb200_force** out);                          /* new, 122-159 */
+int ommb200_nonbonded_add_particle(ommb200_force* f, double charge, double sigma,
+                                   double epsilon, int* index);             /* 162-173 */
+int ommb200_nonbonded_set_particle_parameters(ommb200_force* f, int index, double charge,
+                                              double sigma, double epsilon); /* 175-184 */
+int ommb200_nonbonded_get_particle_parameters(const ommb200_force* f, int index,
+                                              double* charge, double* sigma, double* epsilon);
+int ommb200_nonbonded_num_particles(const ommb200_force* f, int* out);
+int ommb200_nonbonded_add_exception(ommb200_force* f, int p1, int p2, double charge_prod,
+                                    double sigma, double epsilon, int* index); /* 195-214 */
+int ommb200_nonbonded_num_exceptions(const ommb200_force* f, int* out);
+int ommb200_nonbonded_create_exceptions_from_bonds(ommb200_force* f, int n_bonds,
+                                                   const int* bonds /* 2*n_bonds */,
+                                                   double coulomb14_scale,
+                                                   double lj14_scale); /* 434-500 */
+int ommb200_nonbonded_set_method(ommb200_force* f, int method);           /* 502-504 */
+int ommb200_nonbonded_set_cutoff_distance(ommb200_force* f, double cutoff); /* 521-528 */
+int ommb200_nonbonded_set_reaction_field_dielectric(ommb200_force* f, double eps); /* 534-540 */
+int ommb200_nonbonded_set_ewald_error_tolerance(ommb200_force* f, double tol); /* 546-552 */
+int ommb200_nonbonded_set_exceptions_use_periodic_boundary_conditions(ommb200_force* f,
+                                                                      int periodic); /* 558 */
+int ommb200_nonbonded_set_use_dispersion_correction(ommb200_force* f, int enabled); /* 572 */
+int ommb200_nonbonded_set_use_switching_function(ommb200_force* f, int enabled);  /* 578 */
+int ommb200_nonbonded_set_switching_distance(ommb200_force* f, double distance);  /* 585 */
+int ommb200_nonbonded_set_pme_parameters(ommb200_force* f, double alpha, int nx, int ny,
+                                         int nz);                              /* 597-611 */
+int ommb200_nonbonded_set_reciprocal_space_force_group(ommb200_force* f, int group); /* 111 */
+int ommb200_nonbonded_set_include_direct_space(ommb200_force* f, int enabled);      /* 123 */
+
+/* ---- GBSAOBCForce (forces/gbsa_obc.rs:61-133) ---- */
+int ommb200_gbsa_obc_create(ommb200_force** out);
+int ommb200_gbsa_obc_add_particle(ommb200_force* f, double charge, double radius,
+                                  double scaling_factor, int* index);
+int ommb200_gbsa_obc_set_particle_parameters(ommb200_force* f, int index, double charge,
+                                             double radius, double scaling_factor);
+int ommb200_gbsa_obc_set_method(ommb200_force* f, int method);
+int ommb200_gbsa_obc_set_cutoff_distance(ommb200_force* f, double cutoff);
+int ommb200_gbsa_obc_set_solvent_dielectric(ommb200_force* f, double value);
+int ommb200_gbsa_obc_set_solute_dielectric(ommb200_force* f, double value);
+int ommb200_gbsa_obc_set_surface_area_energy(ommb200_force* f, double value);
+
+/* ---- HarmonicBondForce (forces/harmonic_bond.rs) / HarmonicAngleForce ---- */
+int ommb200_harmonic_bond_create(ommb200_force** out);
+int ommb200_harmonic_bond_add_bond(ommb200_force* f, int p1, int p2, double length, double k,
+                                   int* index);
+int ommb200_harmonic_bond_set_uses_pbc(ommb200_force* f, int use_pbc);
+int ommb200_harmonic_angle_create(ommb200_force** out);
+int ommb200_harmonic_angle_add_angle(ommb200_force* f, int p1, int p2, int p3, double angle,
+                                     double k, int* index);
+int ommb200_harmonic_angle_set_uses_pbc(ommb200_force* f, int use_pbc);
+
+/* ---- LangevinMiddleIntegrator (integrators/langevin.rs:14-102) ---- */
+int ommb200_langevin_middle_create(double temperature, double friction, double step_size,
+                                   ommb200_integrator** out);              /* new, 44-67 */
+int ommb200_integrator_destroy(ommb200_integrator* integrator); /* if not owned by a Context */
+int ommb200_integrator_set_random_number_seed(ommb200_integrator* i, int seed);     /* 33-35 */
+int ommb200_integrator_set_constraint_tolerance(ommb200_integrator* i, double tol); /* 73-79 */
+int ommb200_integrator_set_temperature(ommb200_integrator* i, double t);            /* 83-89 */
+int ommb200_integrator_set_friction(ommb200_integrator* i, double f);              /* 90-96 */
+int ommb200_integrator_set_step_size(ommb200_integrator* i, double dt);            /* 97-102 */
+int ommb200_integrator_set_integration_force_groups(ommb200_integrator* i, uint32_t groups);
+
+/* ---- Context (context.rs:83-1163) ---- */
+/* Context::new (83-161): takes ownership of system and integrator (also on failure). */
+int ommb200_context_create(ommb200_system* system, ommb200_integrator* integrator,
+                           const ommb200_options* options, ommb200_context** out);
+int ommb200_context_destroy(ommb200_context* ctx);
+int ommb200_context_num_particles(const ommb200_context* ctx, int* out);
+int ommb200_context_set_positions(ommb200_context* ctx, const double* positions, int n); /* 163 */
+int ommb200_context_set_velocities(ommb200_context* ctx, const double* velocities, int n);
+/* set_velocities_to_temperature (182-223): Maxwell-Boltzmann draw, half-step force offset,
+ * velocity constraints at tolerance 1e-5. */
+int ommb200_context_set_velocities_to_temperature(ommb200_context* ctx, double temperature,
+                                                  int seed);
+int ommb200_context_set_periodic_box_vectors(ommb200_context* ctx, const double a[3],
+                                             const double b[3], const double c[3]); /* 241 */
+int ommb200_context_set_time(ommb200_context* ctx, double time);
+int ommb200_context_set_step_count(ommb200_context* ctx, int64_t steps);
+int ommb200_context_apply_constraints(ommb200_context* ctx, double tolerance);  /* 767-776 */
+int ommb200_context_apply_velocity_constraints(ommb200_context* ctx, double tolerance);
+/* try_step (800-805): returns OMMB200_ERR_CONSTRAINT / _NONFINITE on failure. */
+int ommb200_context_step(ommb200_context* ctx, int steps);
+/* try_get_state_options (1041-1105): any of the output arrays (3*N doubles) may be NULL. */
+int ommb200_context_get_state(ommb200_context* ctx, int flags, uint32_t groups,
+                              double* positions, double* velocities, double* forces,
+                              ommb200_state_info* info);
+/* PME parameters frozen at Context creation (nonbonded.rs:1078-1106). */
+int ommb200_context_get_pme_parameters(const ommb200_context* ctx, double* alpha, int* nx,
+                                       int* ny, int* nz);
+
+/* ---- diagnostics (no reference counterpart) ---- */
+/* The interacting nonbonded pair set at the current positions, as evaluated by the pair
+ * kernel itself: (i, j) with i < j in original particle indices, unsorted.  Writes up to
+ * max_pairs pairs and the total count. */
+int ommb200_context_debug_pair_list(ommb200_context* ctx, int64_t max_pairs, int32_t* pairs,
+                                    int64_t* count);
+/* Per-kernel device time of the last step() call in ms, summed over launches; names are
+ * written as a ';'-separated list.  Only filled when profiling was enabled. */
+int ommb200_context_set_profiling(ommb200_context* ctx, int enabled);
+int ommb200_context_kernel_times(ommb200_context* ctx, int max_entries, char* names,
+                                 int names_len, double* ms, int* launches, int* count);
+/* The cudaStream_t every kernel of this Context is launched on (for CUDA-event timing). */
+int ommb200_context_get_stream(ommb200_context* ctx, void** stream);
+/* Measured FP32 FMA throughput of the device (TFLOP/s, FMA = 2 flops): the roofline
+ * denominator of the FP32 pair kernel. */
+int ommb200_measure_fp32_peak(int device, double* tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OMMB200_H */

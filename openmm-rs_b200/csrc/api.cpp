@@ -1,0 +1,584 @@
+// extern "C" boundary: every entry point validates its arguments, catches every exception
+// and returns an OMMB200_* status; nothing aborts the caller.
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "../../include/ommb200.h"
+#include "engine.h"
+#include "model.h"
+
+using namespace ommb200;
+
+struct ommb200_context {
+  std::unique_ptr<Engine> engine;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+void require(bool ok, const char* msg) {
+  if (!ok) throw Error(OMMB200_ERR_INVALID_ARG, msg);
+}
+
+template <class F>
+int guarded(F&& fn) {
+  try {
+    fn();
+    return OMMB200_OK;
+  } catch (const Error& e) {
+    set_error(e.what());
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    set_error("host allocation failed");
+    return OMMB200_ERR_OUT_OF_MEMORY;
+  } catch (const std::exception& e) {
+    set_error(e.what());
+    return OMMB200_ERR_CUDA;
+  } catch (...) {
+    set_error("unknown failure");
+    return OMMB200_ERR_CUDA;
+  }
+}
+
+ForceDef* as_force(ommb200_force* f) { return reinterpret_cast<ForceDef*>(f); }
+const ForceDef* as_force(const ommb200_force* f) { return reinterpret_cast<const ForceDef*>(f); }
+
+template <class T, ForceKind K>
+T* force_of(ommb200_force* f) {
+  require(f != nullptr, "null force handle");
+  ForceDef* d = as_force(f);
+  require(d->kind == K, "force handle has the wrong type for this call");
+  return static_cast<T*>(d);
+}
+template <class T, ForceKind K>
+const T* force_of(const ommb200_force* f) {
+  require(f != nullptr, "null force handle");
+  const ForceDef* d = as_force(f);
+  require(d->kind == K, "force handle has the wrong type for this call");
+  return static_cast<const T*>(d);
+}
+
+NonbondedDef* nbf(ommb200_force* f) { return force_of<NonbondedDef, kNonbonded>(f); }
+const NonbondedDef* nbf(const ommb200_force* f) { return force_of<NonbondedDef, kNonbonded>(f); }
+GbsaObcDef* gbf(ommb200_force* f) { return force_of<GbsaObcDef, kGbsaObc>(f); }
+
+SystemDef* sysdef(ommb200_system* s) { return reinterpret_cast<SystemDef*>(s); }
+const SystemDef* sysdef(const ommb200_system* s) { return reinterpret_cast<const SystemDef*>(s); }
+IntegratorDef* integdef(ommb200_integrator* i) { return reinterpret_cast<IntegratorDef*>(i); }
+
+void set_out(int* out, int v) {
+  if (out) *out = v;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* ommb200_last_error(void) { return g_last_error.c_str(); }
+const char* ommb200_version(void) { return "ommb200 0.1 (sm_100a)"; }
+
+void ommb200_default_options(ommb200_options* out) {
+  if (!out) return;
+  out->precision = OMMB200_PRECISION_MIXED;
+  out->device = 0;
+  out->use_cuda_graph = 1;
+  out->neighbor_skin = 0.0;
+  out->steps_per_graph = 0;
+}
+
+// ---- System -----------------------------------------------------------------------------
+int ommb200_system_create(ommb200_system** out) {
+  return guarded([&] {
+    require(out != nullptr, "null output pointer");
+    *out = reinterpret_cast<ommb200_system*>(new SystemDef());
+  });
+}
+int ommb200_system_destroy(ommb200_system* s) {
+  return guarded([&] { delete sysdef(s); });
+}
+int ommb200_system_add_particle(ommb200_system* s, double mass, int* index) {
+  return guarded([&] {
+    require(s != nullptr, "null system handle");
+    set_out(index, sysdef(s)->add_particle(mass));
+  });
+}
+int ommb200_system_num_particles(const ommb200_system* s, int* out) {
+  return guarded([&] {
+    require(s && out, "null argument");
+    *out = (int)sysdef(s)->masses.size();
+  });
+}
+int ommb200_system_add_constraint(ommb200_system* s, int p1, int p2, double distance, int* index) {
+  return guarded([&] {
+    require(s != nullptr, "null system handle");
+    set_out(index, sysdef(s)->add_constraint(p1, p2, distance));
+  });
+}
+int ommb200_system_set_default_periodic_box_vectors(ommb200_system* s, const double a[3],
+                                                    const double b[3], const double c[3]) {
+  return guarded([&] {
+    require(s && a && b && c, "null argument");
+    sysdef(s)->set_default_box(a, b, c);
+  });
+}
+int ommb200_system_add_force(ommb200_system* s, ommb200_force* force, int* index) {
+  return guarded([&] {
+    require(s && force, "null argument");
+    ForceDef* f = as_force(force);
+    require(!f->owned_by_system, "force already belongs to a System");
+    f->owned_by_system = true;
+    sysdef(s)->forces.emplace_back(f);
+    set_out(index, (int)sysdef(s)->forces.size() - 1);
+  });
+}
+
+// ---- forces: common ---------------------------------------------------------------------
+int ommb200_force_destroy(ommb200_force* force) {
+  return guarded([&] {
+    if (!force) return;
+    require(!as_force(force)->owned_by_system, "force is owned by a System");
+    delete as_force(force);
+  });
+}
+int ommb200_force_set_group(ommb200_force* force, int group) {
+  return guarded([&] {
+    require(force != nullptr, "null force handle");
+    require(group >= 0 && group < 32, "force group must be between 0 and 31");
+    as_force(force)->force_group = group;
+  });
+}
+int ommb200_force_get_group(const ommb200_force* force, int* group) {
+  return guarded([&] {
+    require(force && group, "null argument");
+    *group = as_force(force)->force_group;
+  });
+}
+
+// ---- NonbondedForce ---------------------------------------------------------------------
+int ommb200_nonbonded_create(ommb200_force** out) {
+  return guarded([&] {
+    require(out != nullptr, "null output pointer");
+    *out = reinterpret_cast<ommb200_force*>(static_cast<ForceDef*>(new NonbondedDef()));
+  });
+}
+int ommb200_nonbonded_add_particle(ommb200_force* f, double q, double s, double e, int* index) {
+  return guarded([&] { set_out(index, nbf(f)->add_particle(q, s, e)); });
+}
+int ommb200_nonbonded_set_particle_parameters(ommb200_force* f, int index, double q, double s,
+                                              double e) {
+  return guarded([&] {
+    NonbondedDef* d = nbf(f);
+    require(index >= 0 && index < (int)d->charge.size(), "particle index out of range");
+    require(std::isfinite(q) && std::isfinite(s) && std::isfinite(e) && s >= 0.0 && e >= 0.0,
+            "nonbonded parameters must be finite with nonnegative sigma and epsilon");
+    d->charge[index] = q;
+    d->sigma[index] = s;
+    d->epsilon[index] = e;
+  });
+}
+int ommb200_nonbonded_get_particle_parameters(const ommb200_force* f, int index, double* q,
+                                              double* s, double* e) {
+  return guarded([&] {
+    const NonbondedDef* d = nbf(f);
+    require(index >= 0 && index < (int)d->charge.size(), "particle index out of range");
+    if (q) *q = d->charge[index];
+    if (s) *s = d->sigma[index];
+    if (e) *e = d->epsilon[index];
+  });
+}
+int ommb200_nonbonded_num_particles(const ommb200_force* f, int* out) {
+  return guarded([&] {
+    require(out != nullptr, "null output pointer");
+    *out = (int)nbf(f)->charge.size();
+  });
+}
+int ommb200_nonbonded_add_exception(ommb200_force* f, int p1, int p2, double qq, double s,
+                                    double e, int* index) {
+  return guarded([&] { set_out(index, nbf(f)->add_exception(p1, p2, qq, s, e)); });
+}
+int ommb200_nonbonded_num_exceptions(const ommb200_force* f, int* out) {
+  return guarded([&] {
+    require(out != nullptr, "null output pointer");
+    *out = (int)nbf(f)->exceptions.size();
+  });
+}
+int ommb200_nonbonded_create_exceptions_from_bonds(ommb200_force* f, int n_bonds, const int* bonds,
+                                                   double coulomb14, double lj14) {
+  return guarded([&] {
+    require(n_bonds >= 0 && (n_bonds == 0 || bonds), "invalid bond list");
+    std::vector<std::pair<int, int>> b(n_bonds);
+    for (int i = 0; i < n_bonds; ++i) b[i] = {bonds[2 * i], bonds[2 * i + 1]};
+    nbf(f)->create_exceptions_from_bonds(b, coulomb14, lj14);
+  });
+}
+int ommb200_nonbonded_set_method(ommb200_force* f, int method) {
+  return guarded([&] {
+    require(method >= OMMB200_NO_CUTOFF && method <= OMMB200_LJPME, "unknown nonbonded method");
+    nbf(f)->method = method;
+  });
+}
+int ommb200_nonbonded_set_cutoff_distance(ommb200_force* f, double cutoff) {
+  return guarded([&] {
+    require(std::isfinite(cutoff) && cutoff > 0.0, "cutoff must be positive and finite");
+    nbf(f)->cutoff = cutoff;
+  });
+}
+int ommb200_nonbonded_set_reaction_field_dielectric(ommb200_force* f, double eps) {
+  return guarded([&] {
+    require(!std::isnan(eps) && eps >= 1.0, "reaction field dielectric must be at least one");
+    nbf(f)->reaction_field_dielectric = eps;
+  });
+}
+int ommb200_nonbonded_set_ewald_error_tolerance(ommb200_force* f, double tol) {
+  return guarded([&] {
+    require(std::isfinite(tol) && tol > 0.0 && tol < 0.5, "Ewald tolerance must be between zero and one half");
+    nbf(f)->ewald_error_tolerance = tol;
+  });
+}
+int ommb200_nonbonded_set_exceptions_use_periodic_boundary_conditions(ommb200_force* f, int periodic) {
+  return guarded([&] { nbf(f)->exceptions_use_pbc = periodic != 0; });
+}
+int ommb200_nonbonded_set_use_dispersion_correction(ommb200_force* f, int enabled) {
+  return guarded([&] { nbf(f)->use_dispersion_correction = enabled != 0; });
+}
+int ommb200_nonbonded_set_use_switching_function(ommb200_force* f, int enabled) {
+  return guarded([&] { nbf(f)->use_switching = enabled != 0; });
+}
+int ommb200_nonbonded_set_switching_distance(ommb200_force* f, double distance) {
+  return guarded([&] {
+    require(std::isfinite(distance) && distance >= 0.0, "switching distance must be nonnegative and finite");
+    nbf(f)->switching_distance = distance;
+  });
+}
+int ommb200_nonbonded_set_pme_parameters(ommb200_force* f, double alpha, int nx, int ny, int nz) {
+  return guarded([&] {
+    require(std::isfinite(alpha) && alpha >= 0.0, "PME alpha must be nonnegative and finite");
+    require(alpha == 0.0 || (nx >= 5 && ny >= 5 && nz >= 5), "PME grid dimensions must be at least five");
+    NonbondedDef* d = nbf(f);
+    d->pme_alpha = alpha;
+    d->pme_grid = {alpha == 0.0 ? 0 : nx, alpha == 0.0 ? 0 : ny, alpha == 0.0 ? 0 : nz};
+  });
+}
+int ommb200_nonbonded_set_reciprocal_space_force_group(ommb200_force* f, int group) {
+  return guarded([&] {
+    require(group >= -1 && group < 32, "reciprocal force group must be between -1 and 31");
+    nbf(f)->reciprocal_force_group = group;
+  });
+}
+int ommb200_nonbonded_set_include_direct_space(ommb200_force* f, int enabled) {
+  return guarded([&] { nbf(f)->include_direct_space = enabled != 0; });
+}
+
+// ---- GBSAOBCForce -----------------------------------------------------------------------
+int ommb200_gbsa_obc_create(ommb200_force** out) {
+  return guarded([&] {
+    require(out != nullptr, "null output pointer");
+    *out = reinterpret_cast<ommb200_force*>(static_cast<ForceDef*>(new GbsaObcDef()));
+  });
+}
+int ommb200_gbsa_obc_add_particle(ommb200_force* f, double q, double radius, double scale, int* index) {
+  return guarded([&] {
+    GbsaObcDef* d = gbf(f);
+    d->charge.push_back(q);
+    d->radius.push_back(radius);
+    d->scale.push_back(scale);
+    set_out(index, (int)d->charge.size() - 1);
+  });
+}
+int ommb200_gbsa_obc_set_particle_parameters(ommb200_force* f, int index, double q, double radius,
+                                             double scale) {
+  return guarded([&] {
+    GbsaObcDef* d = gbf(f);
+    require(index >= 0 && index < (int)d->charge.size(), "particle index out of range");
+    d->charge[index] = q;
+    d->radius[index] = radius;
+    d->scale[index] = scale;
+  });
+}
+int ommb200_gbsa_obc_set_method(ommb200_force* f, int method) {
+  return guarded([&] {
+    require(method >= 0 && method <= 2, "unknown GBSA method");
+    gbf(f)->method = method;
+  });
+}
+int ommb200_gbsa_obc_set_cutoff_distance(ommb200_force* f, double cutoff) {
+  return guarded([&] { gbf(f)->cutoff = cutoff; });
+}
+int ommb200_gbsa_obc_set_solvent_dielectric(ommb200_force* f, double value) {
+  return guarded([&] { gbf(f)->solvent_dielectric = value; });
+}
+int ommb200_gbsa_obc_set_solute_dielectric(ommb200_force* f, double value) {
+  return guarded([&] { gbf(f)->solute_dielectric = value; });
+}
+int ommb200_gbsa_obc_set_surface_area_energy(ommb200_force* f, double value) {
+  return guarded([&] { gbf(f)->surface_area_energy = value; });
+}
+
+// ---- bonded -----------------------------------------------------------------------------
+int ommb200_harmonic_bond_create(ommb200_force** out) {
+  return guarded([&] {
+    require(out != nullptr, "null output pointer");
+    *out = reinterpret_cast<ommb200_force*>(static_cast<ForceDef*>(new HarmonicBondDef()));
+  });
+}
+int ommb200_harmonic_bond_add_bond(ommb200_force* f, int p1, int p2, double length, double k, int* index) {
+  return guarded([&] {
+    auto* d = force_of<HarmonicBondDef, kHarmonicBond>(f);
+    d->bonds.push_back({p1, p2, length, k});
+    set_out(index, (int)d->bonds.size() - 1);
+  });
+}
+int ommb200_harmonic_bond_set_uses_pbc(ommb200_force* f, int use_pbc) {
+  return guarded([&] { force_of<HarmonicBondDef, kHarmonicBond>(f)->use_pbc = use_pbc != 0; });
+}
+int ommb200_harmonic_angle_create(ommb200_force** out) {
+  return guarded([&] {
+    require(out != nullptr, "null output pointer");
+    *out = reinterpret_cast<ommb200_force*>(static_cast<ForceDef*>(new HarmonicAngleDef()));
+  });
+}
+int ommb200_harmonic_angle_add_angle(ommb200_force* f, int p1, int p2, int p3, double angle,
+                                     double k, int* index) {
+  return guarded([&] {
+    auto* d = force_of<HarmonicAngleDef, kHarmonicAngle>(f);
+    d->angles.push_back({p1, p2, p3, angle, k});
+    set_out(index, (int)d->angles.size() - 1);
+  });
+}
+int ommb200_harmonic_angle_set_uses_pbc(ommb200_force* f, int use_pbc) {
+  return guarded([&] { force_of<HarmonicAngleDef, kHarmonicAngle>(f)->use_pbc = use_pbc != 0; });
+}
+
+// ---- LangevinMiddleIntegrator -----------------------------------------------------------
+int ommb200_langevin_middle_create(double temperature, double friction, double step_size,
+                                   ommb200_integrator** out) {
+  return guarded([&] {
+    require(out != nullptr, "null output pointer");
+    require(std::isfinite(temperature) && temperature >= 0.0, "temperature must be nonnegative and finite");
+    require(std::isfinite(friction) && friction >= 0.0, "friction must be nonnegative and finite");
+    require(std::isfinite(step_size) && step_size > 0.0, "step size must be positive and finite");
+    auto* i = new IntegratorDef();
+    i->temperature = temperature;
+    i->friction = friction;
+    i->step_size = step_size;
+    *out = reinterpret_cast<ommb200_integrator*>(i);
+  });
+}
+int ommb200_integrator_destroy(ommb200_integrator* i) {
+  return guarded([&] {
+    if (!i) return;
+    require(!integdef(i)->owned_by_context, "integrator is owned by a Context");
+    delete integdef(i);
+  });
+}
+int ommb200_integrator_set_random_number_seed(ommb200_integrator* i, int seed) {
+  return guarded([&] {
+    require(i != nullptr, "null integrator handle");
+    integdef(i)->random_seed = seed;
+  });
+}
+int ommb200_integrator_set_constraint_tolerance(ommb200_integrator* i, double tol) {
+  return guarded([&] {
+    require(i != nullptr, "null integrator handle");
+    require(std::isfinite(tol) && tol > 0.0 && tol < 1.0, "constraint tolerance must be between zero and one");
+    integdef(i)->constraint_tolerance = tol;
+  });
+}
+int ommb200_integrator_set_temperature(ommb200_integrator* i, double t) {
+  return guarded([&] {
+    require(i != nullptr, "null integrator handle");
+    require(std::isfinite(t) && t >= 0.0, "temperature must be nonnegative and finite");
+    integdef(i)->temperature = t;
+  });
+}
+int ommb200_integrator_set_friction(ommb200_integrator* i, double f) {
+  return guarded([&] {
+    require(i != nullptr, "null integrator handle");
+    require(std::isfinite(f) && f >= 0.0, "friction must be nonnegative and finite");
+    integdef(i)->friction = f;
+  });
+}
+int ommb200_integrator_set_step_size(ommb200_integrator* i, double dt) {
+  return guarded([&] {
+    require(i != nullptr, "null integrator handle");
+    require(std::isfinite(dt) && dt > 0.0, "step size must be positive and finite");
+    integdef(i)->step_size = dt;
+  });
+}
+int ommb200_integrator_set_integration_force_groups(ommb200_integrator* i, uint32_t groups) {
+  return guarded([&] {
+    require(i != nullptr, "null integrator handle");
+    integdef(i)->integration_force_groups = groups;
+  });
+}
+
+// ---- Context ----------------------------------------------------------------------------
+int ommb200_context_create(ommb200_system* system, ommb200_integrator* integrator,
+                           const ommb200_options* options, ommb200_context** out) {
+  std::unique_ptr<SystemDef> sys(sysdef(system));
+  std::unique_ptr<IntegratorDef> integ(integdef(integrator));
+  return guarded([&] {
+    require(out != nullptr, "null output pointer");
+    *out = nullptr;
+    require(sys != nullptr && integ != nullptr, "null system or integrator handle");
+    integ->owned_by_context = true;
+    ommb200_options o;
+    ommb200_default_options(&o);
+    if (options) o = *options;
+    require(o.precision == OMMB200_PRECISION_MIXED || o.precision == OMMB200_PRECISION_DOUBLE,
+            "unknown precision");
+    EngineOptions eo;
+    eo.precision = o.precision;
+    eo.device = o.device;
+    eo.use_graph = o.use_cuda_graph != 0;
+    eo.skin = o.neighbor_skin;
+    eo.steps_per_graph = o.steps_per_graph;
+    auto ctx = std::make_unique<ommb200_context>();
+    ctx->engine = std::make_unique<Engine>(std::move(sys), std::move(integ), eo);
+    *out = ctx.release();
+  });
+}
+int ommb200_context_destroy(ommb200_context* ctx) {
+  return guarded([&] { delete ctx; });
+}
+
+#define OMMB200_CTX                                   \
+  require(ctx != nullptr && ctx->engine, "null context handle"); \
+  Engine& E = *ctx->engine
+
+int ommb200_context_num_particles(const ommb200_context* ctx, int* out) {
+  return guarded([&] {
+    require(ctx && ctx->engine && out, "null argument");
+    *out = ctx->engine->num_particles();
+  });
+}
+int ommb200_context_set_positions(ommb200_context* ctx, const double* positions, int n) {
+  return guarded([&] {
+    OMMB200_CTX;
+    require(positions != nullptr && n == E.num_particles(), "positions must have shape [N, 3]");
+    E.set_positions(positions);
+  });
+}
+int ommb200_context_set_velocities(ommb200_context* ctx, const double* velocities, int n) {
+  return guarded([&] {
+    OMMB200_CTX;
+    require(velocities != nullptr && n == E.num_particles(), "velocities must have shape [N, 3]");
+    E.set_velocities(velocities);
+  });
+}
+int ommb200_context_set_velocities_to_temperature(ommb200_context* ctx, double temperature, int seed) {
+  return guarded([&] {
+    OMMB200_CTX;
+    E.set_velocities_to_temperature(temperature, seed);
+  });
+}
+int ommb200_context_set_periodic_box_vectors(ommb200_context* ctx, const double a[3],
+                                             const double b[3], const double c[3]) {
+  return guarded([&] {
+    OMMB200_CTX;
+    require(a && b && c, "null box vector");
+    const double box[9] = {a[0], a[1], a[2], b[0], b[1], b[2], c[0], c[1], c[2]};
+    E.set_box(box);
+  });
+}
+int ommb200_context_set_time(ommb200_context* ctx, double time) {
+  return guarded([&] {
+    OMMB200_CTX;
+    E.set_time(time);
+  });
+}
+int ommb200_context_set_step_count(ommb200_context* ctx, int64_t steps) {
+  return guarded([&] {
+    OMMB200_CTX;
+    E.set_step_count(steps);
+  });
+}
+int ommb200_context_apply_constraints(ommb200_context* ctx, double tolerance) {
+  return guarded([&] {
+    OMMB200_CTX;
+    E.apply_constraints(tolerance);
+  });
+}
+int ommb200_context_apply_velocity_constraints(ommb200_context* ctx, double tolerance) {
+  return guarded([&] {
+    OMMB200_CTX;
+    E.apply_velocity_constraints(tolerance);
+  });
+}
+int ommb200_context_step(ommb200_context* ctx, int steps) {
+  return guarded([&] {
+    OMMB200_CTX;
+    require(steps >= 0, "step count must be nonnegative");
+    E.step(steps);
+  });
+}
+int ommb200_context_get_state(ommb200_context* ctx, int flags, uint32_t groups, double* positions,
+                              double* velocities, double* forces, ommb200_state_info* info) {
+  return guarded([&] {
+    OMMB200_CTX;
+    E.get_state(flags, groups, (flags & OMMB200_STATE_POSITIONS) ? positions : nullptr,
+                (flags & OMMB200_STATE_VELOCITIES) ? velocities : nullptr,
+                (flags & OMMB200_STATE_FORCES) ? forces : nullptr, info);
+  });
+}
+int ommb200_context_get_pme_parameters(const ommb200_context* ctx, double* alpha, int* nx, int* ny,
+                                       int* nz) {
+  return guarded([&] {
+    require(ctx && ctx->engine && alpha && nx && ny && nz, "null argument");
+    ctx->engine->pme_parameters(alpha, nx, ny, nz);
+  });
+}
+int ommb200_context_debug_pair_list(ommb200_context* ctx, int64_t max_pairs, int32_t* pairs,
+                                    int64_t* count) {
+  return guarded([&] {
+    OMMB200_CTX;
+    require(max_pairs >= 0 && count != nullptr, "invalid arguments");
+    *count = E.debug_pair_list(max_pairs, pairs);
+  });
+}
+int ommb200_context_set_profiling(ommb200_context* ctx, int enabled) {
+  return guarded([&] {
+    OMMB200_CTX;
+    E.set_profiling(enabled != 0);
+  });
+}
+int ommb200_context_kernel_times(ommb200_context* ctx, int max_entries, char* names, int names_len,
+                                 double* ms, int* launches, int* count) {
+  return guarded([&] {
+    OMMB200_CTX;
+    require(count != nullptr, "null count pointer");
+    auto t = E.kernel_times();
+    *count = (int)t.size();
+    std::string joined;
+    for (int i = 0; i < (int)t.size() && i < max_entries; ++i) {
+      if (ms) ms[i] = t[i].ms;
+      if (launches) launches[i] = t[i].launches;
+      if (i) joined += ';';
+      joined += t[i].name;
+    }
+    if (names && names_len > 0) {
+      std::strncpy(names, joined.c_str(), names_len - 1);
+      names[names_len - 1] = '\0';
+    }
+  });
+}
+int ommb200_context_get_stream(ommb200_context* ctx, void** stream) {
+  return guarded([&] {
+    OMMB200_CTX;
+    require(stream != nullptr, "null output pointer");
+    *stream = (void*)E.stream();
+  });
+}
+int ommb200_measure_fp32_peak(int device, double* tflops) {
+  return guarded([&] {
+    require(tflops != nullptr, "null output pointer");
+    *tflops = measure_fp32_peak(device);
+  });
+}
+
+}  // extern "C"

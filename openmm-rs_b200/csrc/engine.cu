@@ -1,0 +1,1157 @@
+// Context engine: buffers, the per-step launch sequence and its CUDA graph, getState.
+#include "engine.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <numeric>
+#include <random>
+#include <functional>
+#include <set>
+
+namespace ommb200 {
+
+#define OMMB200_CK(call)                                                                    \
+  do {                                                                                      \
+    cudaError_t e_ = (call);                                                                \
+    if (e_ != cudaSuccess)                                                                  \
+      throw Error(OMMB200_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));     \
+  } while (0)
+#define OMMB200_CKFFT(call)                                                                 \
+  do {                                                                                      \
+    cufftResult r_ = (call);                                                                \
+    if (r_ != CUFFT_SUCCESS)                                                                \
+      throw Error(OMMB200_ERR_CUDA, std::string(#call) + ": cuFFT status " +                 \
+                                        std::to_string((int)r_));                           \
+  } while (0)
+
+DeviceArena::~DeviceArena() {
+  for (void* p : ptrs_) cudaFree(p);
+}
+
+void* DeviceArena::alloc_bytes(size_t bytes) {
+  void* p = nullptr;
+  cudaError_t e = cudaMalloc(&p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    throw Error(e == cudaErrorMemoryAllocation ? OMMB200_ERR_OUT_OF_MEMORY : OMMB200_ERR_CUDA,
+                std::string("device allocation of ") + std::to_string(bytes) +
+                    " bytes failed: " + cudaGetErrorString(e));
+  }
+  ptrs_.push_back(p);
+  OMMB200_CK(cudaMemset(p, 0, bytes));
+  return p;
+}
+
+namespace {
+
+void require(bool ok, const std::string& msg, int code = OMMB200_ERR_INVALID_ARG) {
+  if (!ok) throw Error(code, msg);
+}
+
+Box<double> make_box(const double b[9]) {
+  Box<double> r;
+  r.ax = b[0];
+  r.bx = b[3];
+  r.by = b[4];
+  r.cx = b[6];
+  r.cy = b[7];
+  r.cz = b[8];
+  r.inv_ax = 1.0 / r.ax;
+  r.inv_by = 1.0 / r.by;
+  r.inv_cz = 1.0 / r.cz;
+  return r;
+}
+
+template <class Real>
+Box<Real> cast_box(const Box<double>& b) {
+  Box<Real> r;
+  r.ax = (Real)b.ax;
+  r.bx = (Real)b.bx;
+  r.by = (Real)b.by;
+  r.cx = (Real)b.cx;
+  r.cy = (Real)b.cy;
+  r.cz = (Real)b.cz;
+  r.inv_ax = (Real)b.inv_ax;
+  r.inv_by = (Real)b.inv_by;
+  r.inv_cz = (Real)b.inv_cz;
+  return r;
+}
+
+// pme.rs:176-199
+void reciprocal_box(const double* bv, double recip[3][3], double* volume) {
+  auto cross = [](const double* a, const double* b, double* o) {
+    o[0] = a[1] * b[2] - a[2] * b[1];
+    o[1] = a[2] * b[0] - a[0] * b[2];
+    o[2] = a[0] * b[1] - a[1] * b[0];
+  };
+  double bc[3], ca[3], ab[3];
+  cross(bv + 3, bv + 6, bc);
+  cross(bv + 6, bv, ca);
+  cross(bv, bv + 3, ab);
+  const double v = bv[0] * bc[0] + bv[1] * bc[1] + bv[2] * bc[2];
+  for (int i = 0; i < 3; ++i) {
+    recip[0][i] = bc[i] / v;
+    recip[1][i] = ca[i] / v;
+    recip[2][i] = ab[i] / v;
+  }
+  *volume = v;
+}
+
+// pme.rs:151-174 (host copy, used for the B-spline moduli)
+void spline5_host(double f, double w[5]) {
+  w[0] = 1.0 - f;
+  w[1] = f;
+  w[2] = w[3] = w[4] = 0.0;
+  for (int order = 3; order <= 5; ++order) {
+    const double den = order - 1;
+    w[order - 1] = f * w[order - 2] / den;
+    for (int i = order - 2; i >= 1; --i)
+      w[i] = ((f + (order - 1 - i)) * w[i - 1] + ((i + 1) - f) * w[i]) / den;
+    w[0] *= (1.0 - f) / den;
+  }
+}
+
+// pme.rs:240-259
+std::vector<double> bspline_moduli(int n) {
+  double w[5];
+  spline5_host(0.0, w);
+  std::vector<double> v(n);
+  for (int k = 0; k < n; ++k) {
+    double re = 0.0, im = 0.0;
+    for (int i = 0; i < 5; ++i) {
+      const double ang = 2.0 * kPiD * (double)k * (double)i / (double)n;
+      re += w[i] * std::cos(ang);
+      im += w[i] * std::sin(ang);
+    }
+    v[k] = re * re + im * im;
+  }
+  for (int k = 0; k < n; ++k)
+    if (v[k] < 1e-7) v[k] = 0.5 * (v[(k + n - 1) % n] + v[(k + 1) % n]);
+  return v;
+}
+
+// nonbonded.rs:660-719 (no parameter offsets): E_disp = C / V.
+double dispersion_coefficient(const NonbondedDef& nb) {
+  double moments[13] = {0}, diagonal[13] = {0};
+  for (size_t i = 0; i < nb.sigma.size(); ++i) {
+    double power = 1.0;
+    for (int k = 0; k <= 12; ++k) {
+      moments[k] += std::sqrt(nb.epsilon[i]) * power;
+      diagonal[k] += nb.epsilon[i] * power;
+      power *= nb.sigma[i];
+    }
+  }
+  auto pair_moment = [&](int power) {
+    double coefficient = 1.0, sum = 0.0;
+    for (int k = 0; k <= power; ++k) {
+      sum += coefficient * moments[k] * moments[power - k];
+      coefficient *= (double)(power - k) / (double)(k + 1);
+    }
+    return sum / std::pow(2.0, power) + diagonal[power];
+  };
+  const double rc = nb.cutoff, rs = nb.switching_distance;
+  auto integral = [&](int power) {
+    const double tail = std::pow(rc, 3 - power) / (double)(power - 3);
+    if (!nb.use_switching) return tail;
+    auto f = [&](double r) {
+      const double t = (r - rs) / (rc - rs);
+      return t * t * t * (10.0 + t * (-15.0 + 6.0 * t)) * std::pow(r, 2 - power);
+    };
+    // adaptive Simpson, nonbonded.rs:1290-1336
+    struct S {
+      static double rec(const decltype(f)& fn, double a, double b, double fa, double fm, double fb,
+                        double est, double tol, int depth) {
+        const double m = 0.5 * (a + b);
+        const double fl = fn(0.5 * (a + m)), fr = fn(0.5 * (m + b));
+        const double left = (m - a) / 6.0 * (fa + 4.0 * fl + fm);
+        const double right = (b - m) / 6.0 * (fm + 4.0 * fr + fb);
+        const double diff = left + right - est;
+        if (depth == 0 || std::fabs(diff) <= 15.0 * tol) return left + right + diff / 15.0;
+        return rec(fn, a, m, fa, fl, fm, left, 0.5 * tol, depth - 1) +
+               rec(fn, m, b, fm, fr, fb, right, 0.5 * tol, depth - 1);
+      }
+    };
+    const double fa = f(rs), fm = f(0.5 * (rs + rc)), fb = f(rc);
+    const double est = (rc - rs) / 6.0 * (fa + 4.0 * fm + fb);
+    return tail + S::rec(f, rs, rc, fa, fm, fb, est, 1e-11 * std::max(std::fabs(est), 1e-12), 20);
+  };
+  const double nn = (double)nb.sigma.size();
+  return 8.0 * kPiD * nn / (nn + 1.0) *
+         (pair_moment(12) * integral(12) - pair_moment(6) * integral(6));
+}
+
+}  // namespace
+
+Engine::Engine(std::unique_ptr<SystemDef> system, std::unique_ptr<IntegratorDef> integrator,
+               const EngineOptions& options)
+    : sys_(std::move(system)), integ_(std::move(integrator)), opt_(options) {
+  n_ = (int)sys_->masses.size();
+  require(n_ > 0, "cannot create a context for a system with no particles");
+  dp_ = opt_.precision == OMMB200_PRECISION_DOUBLE;
+  std::copy(sys_->box, sys_->box + 9, box_);
+  int devices = 0;
+  OMMB200_CK(cudaGetDeviceCount(&devices));
+  require(opt_.device >= 0 && opt_.device < devices, "CUDA device ordinal out of range");
+  OMMB200_CK(cudaSetDevice(opt_.device));
+  OMMB200_CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  if (integ_->random_seed != 0) {
+    seed_ = (uint32_t)integ_->random_seed;
+  } else {
+    std::random_device rd;
+    seed_ = ((uint64_t)rd() << 32) | rd();
+  }
+  host_masses_ = sys_->masses;
+  pos_ = mem_.alloc<double>(3 * (size_t)n_);
+  vel_ = mem_.alloc<double>(3 * (size_t)n_);
+  scratch3_ = mem_.alloc<double>(3 * (size_t)n_);
+  inv_mass_ = mem_.alloc<double>(n_);
+  force_ = mem_.alloc<long long>(3 * (size_t)n_);
+  energy_ = mem_.alloc<long long>(8);
+  status_ = mem_.alloc<int>(1);
+  rebuild_ = mem_.alloc<int>(1);
+  rng_step_ = mem_.alloc<unsigned long long>(1);
+  std::vector<double> im(n_);
+  for (int i = 0; i < n_; ++i) im[i] = host_masses_[i] == 0.0 ? 0.0 : 1.0 / host_masses_[i];
+  OMMB200_CK(cudaMemcpy(inv_mass_, im.data(), sizeof(double) * n_, cudaMemcpyHostToDevice));
+
+  const NonbondedDef* nb = nullptr;
+  for (auto& f : sys_->forces) {
+    switch (f->kind) {
+      case kNonbonded:
+        require(nb == nullptr, "only one NonbondedForce per System is supported",
+                OMMB200_ERR_UNSUPPORTED);
+        nb = static_cast<const NonbondedDef*>(f.get());
+        break;
+      case kGbsaObc:
+        throw Error(OMMB200_ERR_UNSUPPORTED, "GBSAOBCForce is not yet available in this engine");
+      default:
+        break;
+    }
+    require(f->force_group >= 0 && f->force_group < 32, "force group must be in 0..31");
+  }
+  if (nb) setup_nonbonded(*nb);
+  setup_bonded();
+  setup_integrator();
+  update_box_dependents();
+  const int one = 1;
+  OMMB200_CK(cudaMemcpy(rebuild_, &one, sizeof(int), cudaMemcpyHostToDevice));
+}
+
+Engine::~Engine() {
+  destroy_graph();
+  if (fft_ready_) {
+    cufftDestroy(fft_fwd_);
+    cufftDestroy(fft_inv_);
+  }
+  for (auto& p : pending_) {
+    cudaEventDestroy(p.start);
+    cudaEventDestroy(p.stop);
+  }
+  for (auto e : event_pool_) cudaEventDestroy(e);
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+// nonbonded.rs:1055-1107 (initialize) + device layout.
+void Engine::setup_nonbonded(const NonbondedDef& nb) {
+  nb_ = &nb;
+  require((int)nb.charge.size() == n_, "NonbondedForce must have one parameter record per particle");
+  require(nb.method != kEwald && nb.method != kLJPME,
+          "NonbondedForce methods Ewald and LJPME are not engine methods; use PME",
+          OMMB200_ERR_UNSUPPORTED);
+  require(nb.method >= kNoCutoff && nb.method <= kLJPME, "unknown nonbonded method");
+  std::set<std::pair<int, int>> seen;
+  for (auto& e : nb.exceptions) {
+    require(e.p1 >= 0 && e.p1 < n_ && e.p2 >= 0 && e.p2 < n_, "exception particle index out of range");
+    require(seen.insert({std::min(e.p1, e.p2), std::max(e.p1, e.p2)}).second, "duplicate exception pair");
+  }
+  if (nb.use_switching)
+    require(nb.switching_distance >= 0.0 && nb.switching_distance < nb.cutoff,
+            "switching distance must be between zero and cutoff");
+  nb_periodic_ = nb.periodic();
+  nb_pme_ = nb.method == kPME;
+  elec_ = nb_pme_ ? kElecEwald : (nb.method == kNoCutoff ? kElecCoulomb : kElecReactionField);
+  if (nb_periodic_) {
+    validate_box(box_);
+    for (int a = 0; a < 3; ++a)
+      require(nb.cutoff <= 0.5 * box_[4 * a], "cutoff must not exceed half the periodic box size");
+  }
+  if (nb_pme_) {
+    nb.effective_pme_parameters(box_, &alpha_, grid_);
+    for (int a = 0; a < 3; ++a) require(grid_[a] >= 5, "PME grid dimensions must be at least five");
+  }
+
+  // per-particle parameters
+  const double sk = std::sqrt(kOne4PiEps0);
+  std::vector<double> qs(n_), hs(n_), se(n_);
+  for (int i = 0; i < n_; ++i) {
+    qs[i] = nb.charge[i] * sk;
+    hs[i] = 0.5 * nb.sigma[i];
+    se[i] = std::sqrt(nb.epsilon[i]);
+  }
+  qscaled_ = mem_.alloc<double>(n_);
+  charge_ = mem_.alloc<double>(n_);
+  half_sigma_ = mem_.alloc<double>(n_);
+  sqrt_eps_ = mem_.alloc<double>(n_);
+  OMMB200_CK(cudaMemcpy(qscaled_, qs.data(), 8 * n_, cudaMemcpyHostToDevice));
+  OMMB200_CK(cudaMemcpy(charge_, nb.charge.data(), 8 * n_, cudaMemcpyHostToDevice));
+  OMMB200_CK(cudaMemcpy(half_sigma_, hs.data(), 8 * n_, cudaMemcpyHostToDevice));
+  OMMB200_CK(cudaMemcpy(sqrt_eps_, se.data(), 8 * n_, cudaMemcpyHostToDevice));
+
+  // exceptions: excluded from the pair kernel, evaluated in f64 (nonbonded.rs:995-1036)
+  n_exceptions_ = (int)nb.exceptions.size();
+  std::vector<int2> ep(std::max(n_exceptions_, 1));
+  std::vector<double4> epar(std::max(n_exceptions_, 1));
+  std::vector<std::vector<int>> partners(n_);
+  for (int k = 0; k < n_exceptions_; ++k) {
+    const auto& e = nb.exceptions[k];
+    ep[k] = make_int2(e.p1, e.p2);
+    epar[k] = make_double4(e.charge_prod * kOne4PiEps0, e.sigma, e.epsilon,
+                           nb.charge[e.p1] * nb.charge[e.p2] * kOne4PiEps0);
+    partners[e.p1].push_back(e.p2);
+    partners[e.p2].push_back(e.p1);
+  }
+  exc_pairs_ = mem_.alloc<int2>(ep.size());
+  exc_params_ = mem_.alloc<double4>(epar.size());
+  OMMB200_CK(cudaMemcpy(exc_pairs_, ep.data(), sizeof(int2) * ep.size(), cudaMemcpyHostToDevice));
+  OMMB200_CK(cudaMemcpy(exc_params_, epar.data(), sizeof(double4) * epar.size(), cudaMemcpyHostToDevice));
+  std::vector<int> xs(n_ + 1, 0), xl;
+  for (int i = 0; i < n_; ++i) {
+    xs[i] = (int)xl.size();
+    xl.insert(xl.end(), partners[i].begin(), partners[i].end());
+  }
+  xs[n_] = (int)xl.size();
+  int* excl_start = mem_.alloc<int>(n_ + 1);
+  int* excl_list = mem_.alloc<int>(std::max<size_t>(xl.size(), 1));
+  OMMB200_CK(cudaMemcpy(excl_start, xs.data(), 4 * (n_ + 1), cudaMemcpyHostToDevice));
+  if (!xl.empty())
+    OMMB200_CK(cudaMemcpy(excl_list, xl.data(), 4 * xl.size(), cudaMemcpyHostToDevice));
+
+  // slots and tiles
+  n_blocks_ = (n_ + 31) / 32;
+  n_slots_ = 32 * n_blocks_;
+  NlistArgs& a = nl_;
+  a = NlistArgs{};
+  a.n_atoms = n_;
+  a.n_blocks = n_blocks_;
+  a.pos = pos_;
+  a.excl_start = excl_start;
+  a.excl_list = excl_list;
+  a.rebuild = rebuild_;
+  a.status = status_;
+  a.periodic = nb_periodic_;
+  a.cutoff = nb.cutoff;
+  a.sorted_atom = mem_.alloc<int>(n_slots_);
+  a.atom_slot = mem_.alloc<int>(n_);
+  a.image = mem_.alloc<int>(3 * (size_t)n_);
+  a.block_center = mem_.alloc<double>(3 * (size_t)n_blocks_);
+  a.block_half = mem_.alloc<double>(3 * (size_t)n_blocks_);
+  a.n_tiles = mem_.alloc<int>(1);
+  a.n_masks = mem_.alloc<int>(1);
+  std::vector<int> sorted(n_slots_, -1);
+  for (int i = 0; i < n_; ++i) sorted[i] = i;
+  OMMB200_CK(cudaMemcpy(a.sorted_atom, sorted.data(), 4 * n_slots_, cudaMemcpyHostToDevice));
+  OMMB200_CK(cudaMemcpy(a.atom_slot, sorted.data(), 4 * n_, cudaMemcpyHostToDevice));
+  const long long all_pairs = (long long)n_blocks_ * (n_blocks_ + 1) / 2;
+  if (nb_periodic_) {
+    skin_ = opt_.skin > 0.0 ? opt_.skin : 0.1;
+    a.skin = skin_;
+    double recip[3][3], vol;
+    reciprocal_box(box_, recip, &vol);
+    const double density = n_ / vol;
+    const double edge = std::cbrt(4.0 / density);  // ~32 particles per 2x2x2 voxels
+    int maxv = 1;
+    for (int d = 0; d < 3; ++d) {
+      a.n_vox[d] = std::max(1, std::min(1024, (int)std::floor(box_[4 * d] / edge)));
+      maxv = std::max(maxv, a.n_vox[d]);
+    }
+    int bits = 0;
+    while ((1 << bits) < maxv) ++bits;
+    a.morton_bits = bits;
+    a.n_keys = 1 << (3 * bits);
+    a.pos_ref = mem_.alloc<double>(3 * (size_t)n_);
+    a.key = mem_.alloc<int>(n_);
+    a.key_count = mem_.alloc<int>(a.n_keys);
+    a.key_start = mem_.alloc<int>(a.n_keys + 1);
+    a.key_cursor = mem_.alloc<int>(a.n_keys);
+    a.scratch_atoms = mem_.alloc<int>(n_);
+    const double bvol = 32.0 / density;
+    const double reach = nb.cutoff + skin_ + std::sqrt(3.0) * std::cbrt(bvol);
+    const double per_block = 0.5 * (4.0 / 3.0) * kPiD * reach * reach * reach / bvol + 1.0;
+    a.tile_capacity = (int)std::min<long long>(all_pairs, std::max<long long>(4096, (long long)(3.0 * n_blocks_ * per_block)));
+    // a masked tile holds an exclusion or a padding slot: at most one per exception plus
+    // one per block, so this pool cannot overflow
+    a.mask_capacity = (int)std::min<long long>(a.tile_capacity, (long long)n_exceptions_ + n_blocks_ + 64);
+  } else {
+    a.tile_capacity = (int)all_pairs;
+    a.mask_capacity = (int)all_pairs;
+  }
+  a.tiles = mem_.alloc<int4>(a.tile_capacity);
+  a.tile_shift = mem_.alloc_bytes((dp_ ? 32 : 16) * (size_t)a.tile_capacity);
+  a.masks = mem_.alloc<uint32_t>(32 * (size_t)a.mask_capacity);
+  posq_ = mem_.alloc_bytes((dp_ ? 32 : 16) * (size_t)n_slots_);
+  ljp_ = mem_.alloc_bytes((dp_ ? 16 : 8) * (size_t)n_slots_);
+  if (!nb_periodic_) build_static_tiles();
+  int dev_sms = 148;
+  cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, opt_.device);
+  pair_grid_ = dev_sms * 8;
+
+  if (nb_pme_) {
+    const long long g = (long long)grid_[0] * grid_[1] * grid_[2];
+    const long long gk = (long long)grid_[0] * grid_[1] * (grid_[2] / 2 + 1);
+    const size_t rs = dp_ ? 8 : 4;
+    pme_fixed_ = mem_.alloc<long long>(g);
+    pme_real_ = mem_.alloc_bytes(rs * g);
+    pme_k_ = mem_.alloc_bytes(2 * rs * gk);
+    influence_ = mem_.alloc_bytes(rs * gk);
+    moduli_ = mem_.alloc<double>(grid_[0] + grid_[1] + grid_[2]);
+    OMMB200_CKFFT(cufftPlan3d(&fft_fwd_, grid_[0], grid_[1], grid_[2], dp_ ? CUFFT_D2Z : CUFFT_R2C));
+    OMMB200_CKFFT(cufftPlan3d(&fft_inv_, grid_[0], grid_[1], grid_[2], dp_ ? CUFFT_Z2D : CUFFT_C2R));
+    fft_ready_ = true;
+    OMMB200_CKFFT(cufftSetStream(fft_fwd_, stream_));
+    OMMB200_CKFFT(cufftSetStream(fft_inv_, stream_));
+    std::vector<double> mod;
+    for (int d = 0; d < 3; ++d) {
+      auto m = bspline_moduli(grid_[d]);
+      mod.insert(mod.end(), m.begin(), m.end());
+    }
+    OMMB200_CK(cudaMemcpy(moduli_, mod.data(), 8 * mod.size(), cudaMemcpyHostToDevice));
+  }
+  if (nb_periodic_ && nb.use_dispersion_correction) dispersion_coeff_ = dispersion_coefficient(nb);
+  double q2 = 0.0;
+  for (double q : nb.charge) q2 += q * q;
+  self_energy_ = nb_pme_ ? -kOne4PiEps0 * alpha_ / std::sqrt(kPiD) * q2 : 0.0;
+}
+
+// Identity slot order and every block pair as a tile: non-periodic methods, built once.
+void Engine::build_static_tiles() {
+  NlistArgs& a = nl_;
+  std::vector<int4> tiles;
+  std::vector<uint32_t> masks;
+  std::vector<std::vector<int>> partners(n_);
+  for (auto& e : nb_->exceptions) {
+    partners[e.p1].push_back(e.p2);
+    partners[e.p2].push_back(e.p1);
+  }
+  for (int I = 0; I < n_blocks_; ++I)
+    for (int J = I; J < n_blocks_; ++J) {
+      uint32_t m[32];
+      bool any = false;
+      for (int l = 0; l < 32; ++l) {
+        const int ai = 32 * I + l;
+        uint32_t v = 0;
+        for (int k = 0; k < 32; ++k)
+          if (32 * J + k >= n_) v |= 1u << k;
+        if (ai >= n_) {
+          v = 0xffffffffu;
+        } else {
+          for (int p : partners[ai])
+            if (p / 32 == J) v |= 1u << (p % 32);
+        }
+        m[l] = v;
+        any = any || v != 0;
+      }
+      int slot = -1, flags = 0;
+      if (any) {
+        slot = (int)(masks.size() / 32);
+        masks.insert(masks.end(), m, m + 32);
+        flags = kTileHasMask;
+      }
+      tiles.push_back(make_int4(I, J, flags, slot));
+    }
+  const int nt = (int)tiles.size(), nm = (int)(masks.size() / 32);
+  OMMB200_CK(cudaMemcpy(a.tiles, tiles.data(), sizeof(int4) * nt, cudaMemcpyHostToDevice));
+  if (nm) OMMB200_CK(cudaMemcpy(a.masks, masks.data(), 4 * masks.size(), cudaMemcpyHostToDevice));
+  OMMB200_CK(cudaMemcpy(a.n_tiles, &nt, 4, cudaMemcpyHostToDevice));
+  OMMB200_CK(cudaMemcpy(a.n_masks, &nm, 4, cudaMemcpyHostToDevice));
+}
+
+void Engine::setup_bonded() {
+  for (auto& f : sys_->forces) {
+    if (f->kind == kHarmonicBond) {
+      auto* b = static_cast<const HarmonicBondDef*>(f.get());
+      if (b->bonds.empty()) continue;
+      std::vector<int2> idx;
+      std::vector<double2> prm;
+      for (auto& x : b->bonds) {
+        require(x.p1 >= 0 && x.p1 < n_ && x.p2 >= 0 && x.p2 < n_, "bonded particle index out of range");
+        idx.push_back(make_int2(x.p1, x.p2));
+        prm.push_back(make_double2(x.length, x.k));
+      }
+      BondedLaunch L{};
+      L.group = f->force_group;
+      L.args.n_bonds = (int)idx.size();
+      int2* di = mem_.alloc<int2>(idx.size());
+      double2* dp = mem_.alloc<double2>(prm.size());
+      OMMB200_CK(cudaMemcpy(di, idx.data(), sizeof(int2) * idx.size(), cudaMemcpyHostToDevice));
+      OMMB200_CK(cudaMemcpy(dp, prm.data(), sizeof(double2) * prm.size(), cudaMemcpyHostToDevice));
+      L.args.bonds = di;
+      L.args.bond_params = dp;
+      L.args.bond_pbc = b->use_pbc;
+      bonded_.push_back(L);
+    } else if (f->kind == kHarmonicAngle) {
+      auto* g = static_cast<const HarmonicAngleDef*>(f.get());
+      if (g->angles.empty()) continue;
+      std::vector<int4> idx;
+      std::vector<double2> prm;
+      for (auto& x : g->angles) {
+        require(x.p1 >= 0 && x.p1 < n_ && x.p2 >= 0 && x.p2 < n_ && x.p3 >= 0 && x.p3 < n_,
+                "bonded particle index out of range");
+        idx.push_back(make_int4(x.p1, x.p2, x.p3, 0));
+        prm.push_back(make_double2(x.angle, x.k));
+      }
+      BondedLaunch L{};
+      L.group = f->force_group;
+      L.args.n_angles = (int)idx.size();
+      int4* di = mem_.alloc<int4>(idx.size());
+      double2* dp = mem_.alloc<double2>(prm.size());
+      OMMB200_CK(cudaMemcpy(di, idx.data(), sizeof(int4) * idx.size(), cudaMemcpyHostToDevice));
+      OMMB200_CK(cudaMemcpy(dp, prm.data(), sizeof(double2) * prm.size(), cudaMemcpyHostToDevice));
+      L.args.angles = di;
+      L.args.angle_params = dp;
+      L.args.angle_pbc = g->use_pbc;
+      bonded_.push_back(L);
+    }
+  }
+  for (auto& L : bonded_) {
+    L.args.pos = pos_;
+    L.args.force = force_;
+    L.args.energy = energy_;
+    L.args.n_atoms_for_force = n_;
+  }
+}
+
+// constraints.rs:35-75 validation, then SETTLE waters / free particles / SHAKE clusters.
+void Engine::setup_integrator() {
+  const IntegratorDef& it = *integ_;
+  require(std::isfinite(it.temperature) && it.temperature >= 0.0, "temperature must be nonnegative and finite");
+  require(std::isfinite(it.friction) && it.friction >= 0.0, "friction must be nonnegative and finite");
+  require(std::isfinite(it.step_size) && it.step_size > 0.0, "step size must be positive and finite");
+  std::set<std::pair<int, int>> seen;
+  std::vector<ConstraintDef> active;
+  for (auto& c : sys_->constraints) {
+    require(c.p1 >= 0 && c.p1 < n_ && c.p2 >= 0 && c.p2 < n_ && c.p1 != c.p2,
+            "constraint particle indices must be distinct and valid", OMMB200_ERR_CONSTRAINT);
+    require(std::isfinite(c.distance) && c.distance > 0.0,
+            "constraint distance must be positive and finite", OMMB200_ERR_CONSTRAINT);
+    require(seen.insert({std::min(c.p1, c.p2), std::max(c.p1, c.p2)}).second,
+            "duplicate constraint between the same particles", OMMB200_ERR_CONSTRAINT);
+    require((host_masses_[c.p1] == 0.0) == (host_masses_[c.p2] == 0.0),
+            "a constraint cannot connect a massive and massless particle", OMMB200_ERR_CONSTRAINT);
+    if (host_masses_[c.p1] != 0.0) active.push_back(c);
+  }
+  // connected components of the constraint graph
+  std::vector<int> parent(n_);
+  std::iota(parent.begin(), parent.end(), 0);
+  std::function<int(int)> root = [&](int x) {
+    while (parent[x] != x) x = parent[x] = parent[parent[x]];
+    return x;
+  };
+  for (auto& c : active) parent[root(c.p1)] = root(c.p2);
+  std::map<int, std::vector<int>> comp_cons;
+  std::map<int, std::set<int>> comp_atoms;
+  for (size_t k = 0; k < active.size(); ++k) {
+    const int r = root(active[k].p1);
+    comp_cons[r].push_back((int)k);
+    comp_atoms[r].insert(active[k].p1);
+    comp_atoms[r].insert(active[k].p2);
+  }
+  std::vector<int4> waters;
+  std::vector<int> free_atoms, cstart{0}, astart{0}, catoms;
+  std::vector<int2> cpairs;
+  std::vector<double> cd2;
+  bool have_geom = false;
+  auto same = [](double a, double b) { return std::fabs(a - b) <= 1e-12 * std::max(std::fabs(a), std::fabs(b)); };
+  for (auto& kv : comp_cons) {
+    const auto& cons = kv.second;
+    const auto& atoms = comp_atoms[kv.first];
+    bool is_water = false;
+    if (cons.size() == 3 && atoms.size() == 3) {
+      // the oxygen is the atom in two constraints of equal length
+      for (int o : atoms) {
+        std::vector<int> hs;
+        std::vector<double> d_oh;
+        double d_hh = -1.0;
+        for (int k : cons) {
+          const auto& c = active[k];
+          if (c.p1 == o || c.p2 == o) {
+            hs.push_back(c.p1 == o ? c.p2 : c.p1);
+            d_oh.push_back(c.distance);
+          } else {
+            d_hh = c.distance;
+          }
+        }
+        if (hs.size() != 2 || d_hh <= 0.0 || !same(d_oh[0], d_oh[1])) continue;
+        if (!same(host_masses_[hs[0]], host_masses_[hs[1]])) continue;
+        if (!(d_hh < 2.0 * d_oh[0])) continue;
+        WaterGeometry g{d_oh[0], d_hh, host_masses_[o], host_masses_[hs[0]]};
+        if (!have_geom) {
+          geom_ = g;
+          have_geom = true;
+        }
+        if (same(g.d_oh, geom_.d_oh) && same(g.d_hh, geom_.d_hh) && same(g.m_o, geom_.m_o) &&
+            same(g.m_h, geom_.m_h)) {
+          waters.push_back(make_int4(o, hs[0], hs[1], 0));
+          is_water = true;
+        }
+        break;
+      }
+    }
+    if (is_water) continue;
+    for (int k : cons) {
+      cpairs.push_back(make_int2(active[k].p1, active[k].p2));
+      cd2.push_back(active[k].distance * active[k].distance);
+    }
+    cstart.push_back((int)cpairs.size());
+    catoms.insert(catoms.end(), atoms.begin(), atoms.end());
+    astart.push_back((int)catoms.size());
+  }
+  std::vector<char> constrained(n_, 0);
+  for (auto& c : active) constrained[c.p1] = constrained[c.p2] = 1;
+  for (int i = 0; i < n_; ++i)
+    if (!constrained[i] && host_masses_[i] != 0.0) free_atoms.push_back(i);
+  n_water_ = (int)waters.size();
+  n_free_ = (int)free_atoms.size();
+  n_clusters_ = (int)cstart.size() - 1;
+  water_ = mem_.alloc<int4>(waters.size());
+  free_atoms_ = mem_.alloc<int>(free_atoms.size());
+  cluster_start_ = mem_.alloc<int>(cstart.size());
+  cluster_pairs_ = mem_.alloc<int2>(cpairs.size());
+  cluster_dist2_ = mem_.alloc<double>(cd2.size());
+  cluster_atom_start_ = mem_.alloc<int>(astart.size());
+  cluster_atoms_ = mem_.alloc<int>(catoms.size());
+  auto up = [](void* d, const void* h, size_t bytes) {
+    if (bytes) OMMB200_CK(cudaMemcpy(d, h, bytes, cudaMemcpyHostToDevice));
+  };
+  up(water_, waters.data(), sizeof(int4) * waters.size());
+  up(free_atoms_, free_atoms.data(), 4 * free_atoms.size());
+  up(cluster_start_, cstart.data(), 4 * cstart.size());
+  up(cluster_pairs_, cpairs.data(), sizeof(int2) * cpairs.size());
+  up(cluster_dist2_, cd2.data(), 8 * cd2.size());
+  up(cluster_atom_start_, astart.data(), 4 * astart.size());
+  up(cluster_atoms_, catoms.data(), 4 * catoms.size());
+}
+
+void Engine::update_box_dependents() {
+  reciprocal_box(box_, recip_, &volume_);
+  nl_.box = make_box(box_);
+  for (auto& L : bonded_) L.args.box = make_box(box_);
+  if (!nb_) return;
+  if (nb_pme_) {
+    const int nx = grid_[0], ny = grid_[1], nz = grid_[2], nzh = nz / 2 + 1;
+    std::vector<double> mod[3] = {bspline_moduli(nx), bspline_moduli(ny), bspline_moduli(nz)};
+    auto freq = [](int k, int n) { return k < (n + 1) / 2 ? (double)k : (double)(k - n); };
+    const double pa = kPiD * kPiD / (alpha_ * alpha_);
+    auto G = [&](int x, int y, int z) {
+      const double m[3] = {freq(x, nx), freq(y, ny), freq(z, nz)};
+      double k2 = 0.0;
+      for (int c = 0; c < 3; ++c) {
+        const double kc = m[0] * recip_[0][c] + m[1] * recip_[1][c] + m[2] * recip_[2][c];
+        k2 += kc * kc;
+      }
+      return kOne4PiEps0 * std::exp(-pa * k2) / (kPiD * volume_ * k2 * mod[0][x] * mod[1][y] * mod[2][z]);
+    };
+    const size_t gk = (size_t)nx * ny * nzh;
+    std::vector<double> infl(gk, 0.0);
+    for (int x = 0; x < nx; ++x)
+      for (int y = 0; y < ny; ++y)
+        for (int z = 0; z < nzh; ++z) {
+          if (x == 0 && y == 0 && z == 0) continue;
+          infl[((size_t)x * ny + y) * nzh + z] =
+              0.5 * (G(x, y, z) + G((nx - x) % nx, (ny - y) % ny, (nz - z) % nz));
+        }
+    if (dp_) {
+      OMMB200_CK(cudaMemcpy(influence_, infl.data(), 8 * gk, cudaMemcpyHostToDevice));
+    } else {
+      std::vector<float> f(infl.begin(), infl.end());
+      OMMB200_CK(cudaMemcpy(influence_, f.data(), 4 * gk, cudaMemcpyHostToDevice));
+    }
+    double qt = 0.0;
+    for (double q : nb_->charge) qt += q;
+    plasma_energy_ = kOne4PiEps0 * kPiD * qt * qt / (2.0 * alpha_ * alpha_ * volume_);
+  }
+}
+
+void Engine::destroy_graph() {
+  if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+  if (graph_) cudaGraphDestroy(graph_);
+  graph_exec_ = nullptr;
+  graph_ = nullptr;
+  graph_steps_ = 0;
+}
+
+void Engine::sync() { OMMB200_CK(cudaStreamSynchronize(stream_)); }
+
+void Engine::check_status() {
+  int st = 0;
+  OMMB200_CK(cudaMemcpy(&st, status_, sizeof(int), cudaMemcpyDeviceToHost));
+  if (st == 0) return;
+  const int zero = 0;
+  OMMB200_CK(cudaMemcpy(status_, &zero, sizeof(int), cudaMemcpyHostToDevice));
+  switch (st) {
+    case kStatusConstraint:
+      throw Error(OMMB200_ERR_CONSTRAINT, "constraint projection failed (no rigid solution or no convergence in 1000 iterations)");
+    case kStatusNonfinite:
+      throw Error(OMMB200_ERR_NONFINITE, "a position or velocity became nonfinite");
+    case kStatusTileOverflow:
+      throw Error(OMMB200_ERR_NLIST_OVERFLOW, "neighbour tile list exceeded its capacity");
+    default:
+      throw Error(OMMB200_ERR_CUDA, "device reported status " + std::to_string(st));
+  }
+}
+
+void Engine::prof_begin(const char* name) {
+  if (!profiling_) return;
+  if (event_pool_.size() < 2) {
+    for (int k = 0; k < 64; ++k) {
+      cudaEvent_t e;
+      OMMB200_CK(cudaEventCreate(&e));
+      event_pool_.push_back(e);
+    }
+  }
+  current_prof_ = name;
+  current_start_ = event_pool_.back();
+  event_pool_.pop_back();
+  OMMB200_CK(cudaEventRecord(current_start_, stream_));
+}
+
+void Engine::prof_end() {
+  if (!profiling_ || !current_start_) return;
+  cudaEvent_t stop = event_pool_.back();
+  event_pool_.pop_back();
+  OMMB200_CK(cudaEventRecord(stop, stream_));
+  pending_.push_back({current_prof_, current_start_, stop});
+  current_start_ = nullptr;
+}
+
+void Engine::harvest_profile() {
+  for (auto& p : pending_) {
+    float ms = 0.f;
+    OMMB200_CK(cudaEventElapsedTime(&ms, p.start, p.stop));
+    auto it = std::find_if(kernel_times_.begin(), kernel_times_.end(),
+                           [&](const KernelTime& k) { return k.name == p.name; });
+    if (it == kernel_times_.end()) kernel_times_.push_back({p.name, (double)ms, 1});
+    else {
+      it->ms += ms;
+      it->launches += 1;
+    }
+    event_pool_.push_back(p.start);
+    event_pool_.push_back(p.stop);
+  }
+  pending_.clear();
+}
+
+void Engine::set_profiling(bool enabled) {
+  profiling_ = enabled;
+  kernel_times_.clear();
+}
+
+template <class Real>
+void Engine::enqueue_nonbonded(bool energy, bool direct, bool reciprocal, bool dump) {
+  const NonbondedDef& nb = *nb_;
+  if (nb_periodic_) {
+    prof_begin("nlist_rebuild");
+    launch_nlist_rebuild(nl_, dp_, stream_);
+    prof_end();
+  }
+  if (direct) {
+    prof_begin("pack");
+    launch_pack<Real>(n_slots_, nl_.sorted_atom, pos_, nl_.image, nl_.block_center, qscaled_,
+                      posq_, nl_.box, stream_);
+    launch_pack_params<Real>(n_slots_, nl_.sorted_atom, half_sigma_, sqrt_eps_, ljp_, stream_);
+    prof_end();
+    PairArgs<Real> p{};
+    p.n_atoms = n_;
+    p.sorted_atom = nl_.sorted_atom;
+    p.pos = pos_;
+    p.posq = posq_;
+    p.ljp = ljp_;
+    p.tiles = nl_.tiles;
+    p.tile_shift = nl_.tile_shift;
+    p.masks = nl_.masks;
+    p.n_tiles = nl_.n_tiles;
+    p.tile_capacity = nl_.tile_capacity;
+    p.force = force_;
+    p.energy = energy_;
+    p.box = cast_box<Real>(nl_.box);
+    p.box_exact = nl_.box;
+    p.periodic = nb_periodic_;
+    p.use_cutoff = nb.method != kNoCutoff;
+    const double rc = nb.cutoff;
+    p.cutoff2 = (Real)(rc * rc);
+    p.cutoff2_exact = rc * rc;
+    p.band = (Real)(rc * rc * (dp_ ? 1e-10 : 1e-4));
+    p.alpha = (Real)alpha_;
+    p.alpha2 = (Real)(alpha_ * alpha_);
+    p.two_alpha_sqrtpi = (Real)(2.0 * alpha_ / std::sqrt(kPiD));
+    if (elec_ == kElecReactionField) {
+      const double eps = nb.reaction_field_dielectric, rc3 = rc * rc * rc;
+      double krf, crf;
+      if (std::isinf(eps)) {
+        krf = 0.5 / rc3;
+        crf = 1.5 / rc;
+      } else {
+        krf = (eps - 1.0) / (2.0 * eps + 1.0) / rc3;
+        crf = (3.0 * eps) / (2.0 * eps + 1.0) / rc;
+      }
+      p.krf = (Real)krf;
+      p.crf = (Real)crf;
+    }
+    p.use_switching = (nb.method != kNoCutoff) && nb.use_switching;
+    if (p.use_switching) {
+      p.switch_r = (Real)nb.switching_distance;
+      p.switch_inv_width = (Real)(1.0 / (rc - nb.switching_distance));
+    }
+    p.pair_dump = dump_pairs_;
+    p.pair_count = dump_count_;
+    p.pair_capacity = dump_capacity_;
+    prof_begin("pair");
+    launch_pair<Real>(p, elec_, energy, dump, pair_grid_, stream_);
+    prof_end();
+  }
+  if (reciprocal && nb_pme_) {
+    PmeArgs<Real> m{};
+    m.n_atoms = n_;
+    m.order = nl_.sorted_atom;
+    m.n_order = n_slots_;
+    m.pos = pos_;
+    m.charge = charge_;
+    m.nx = grid_[0];
+    m.ny = grid_[1];
+    m.nz = grid_[2];
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) m.recip[r][c] = recip_[r][c];
+    m.grid_fixed = pme_fixed_;
+    m.grid_real = static_cast<Real*>(pme_real_);
+    m.grid_k = pme_k_;
+    m.influence = static_cast<const Real*>(influence_);
+    m.moduli = moduli_;
+    m.force = force_;
+    m.energy = energy_;
+    m.alpha = alpha_;
+    m.volume = volume_;
+    prof_begin("pme_spread");
+    launch_pme_spread<Real>(m, stream_);
+    prof_end();
+    prof_begin("pme_convert");
+    launch_pme_convert<Real>(m, stream_);
+    prof_end();
+    prof_begin("pme_fft_forward");
+    if (dp_)
+      OMMB200_CKFFT(cufftExecD2Z(fft_fwd_, (cufftDoubleReal*)pme_real_, (cufftDoubleComplex*)pme_k_));
+    else
+      OMMB200_CKFFT(cufftExecR2C(fft_fwd_, (cufftReal*)pme_real_, (cufftComplex*)pme_k_));
+    prof_end();
+    prof_begin("pme_convolve");
+    launch_pme_convolve<Real>(m, energy, stream_);
+    prof_end();
+    prof_begin("pme_fft_inverse");
+    if (dp_)
+      OMMB200_CKFFT(cufftExecZ2D(fft_inv_, (cufftDoubleComplex*)pme_k_, (cufftDoubleReal*)pme_real_));
+    else
+      OMMB200_CKFFT(cufftExecC2R(fft_inv_, (cufftComplex*)pme_k_, (cufftReal*)pme_real_));
+    prof_end();
+    prof_begin("pme_gather");
+    launch_pme_gather<Real>(m, stream_);
+    prof_end();
+  }
+  if (direct && n_exceptions_) {
+    ExceptionArgs e{};
+    e.n = n_exceptions_;
+    e.pairs = exc_pairs_;
+    e.params = exc_params_;
+    e.pos = pos_;
+    e.force = force_;
+    e.energy = energy_;
+    e.box = nl_.box;
+    e.use_pbc = nb_periodic_ && nb.exceptions_use_pbc;
+    e.ewald = nb_pme_;
+    e.alpha = alpha_;
+    e.n_atoms_for_force = n_;
+    prof_begin("exceptions");
+    launch_exceptions(e, energy, stream_);
+    prof_end();
+  }
+}
+
+void Engine::compute_forces(bool energy, uint32_t groups) {
+  prof_begin("zero_forces");
+  OMMB200_CK(cudaMemsetAsync(force_, 0, sizeof(long long) * 3 * (size_t)n_, stream_));
+  prof_end();
+  if (nb_) {
+    const int g = nb_->force_group;
+    const int rg = nb_->reciprocal_force_group < 0 ? g : nb_->reciprocal_force_group;
+    const bool direct = nb_->include_direct_space && ((groups >> g) & 1u);
+    const bool recip = nb_pme_ && ((groups >> rg) & 1u);
+    if (dp_)
+      enqueue_nonbonded<double>(energy, direct, recip, dump_mode_);
+    else
+      enqueue_nonbonded<float>(energy, direct, recip, dump_mode_);
+  }
+  for (auto& L : bonded_) {
+    if (!((groups >> L.group) & 1u)) continue;
+    prof_begin("bonded");
+    launch_bonded(L.args, energy, stream_);
+    prof_end();
+  }
+}
+
+IntegrateArgs Engine::integrate_args(int step_offset) const {
+  IntegrateArgs a{};
+  a.n_atoms = n_;
+  a.n_water = n_water_;
+  a.water = water_;
+  a.geom = geom_;
+  a.n_free = n_free_;
+  a.free_atoms = free_atoms_;
+  a.n_clusters = n_clusters_;
+  a.cluster_start = cluster_start_;
+  a.cluster_pairs = cluster_pairs_;
+  a.cluster_dist2 = cluster_dist2_;
+  a.cluster_atom_start = cluster_atom_start_;
+  a.cluster_atoms = cluster_atoms_;
+  a.pos = pos_;
+  a.vel = vel_;
+  a.scratch = scratch3_;
+  a.force = force_;
+  a.inv_mass = inv_mass_;
+  a.dt = integ_->step_size;
+  a.decay = std::exp(-integ_->friction * integ_->step_size);
+  a.noise_var = kBoltzmann * integ_->temperature * -std::expm1(-2.0 * integ_->friction * integ_->step_size);
+  a.tolerance = integ_->constraint_tolerance;
+  a.seed = seed_;
+  a.rng_step = rng_step_;
+  a.step_offset = step_offset;
+  a.pos_ref = nb_periodic_ ? nl_.pos_ref : nullptr;
+  a.half_skin2 = 0.25 * skin_ * skin_;
+  a.rebuild = rebuild_;
+  a.status = status_;
+  return a;
+}
+
+void Engine::enqueue_step(int step_offset) {
+  compute_forces(false, integ_->integration_force_groups);
+  prof_begin("integrate");
+  launch_integrate(integrate_args(step_offset), stream_);
+  prof_end();
+}
+
+void Engine::run_graph_steps(int launches) {
+  const int k = graph_steps_;
+  if (!graph_exec_) {
+    OMMB200_CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+    try {
+      for (int s = 0; s < k; ++s) enqueue_step(s);
+      launch_advance_counter(rng_step_, k, stream_);
+    } catch (...) {
+      cudaGraph_t g = nullptr;
+      cudaStreamEndCapture(stream_, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    OMMB200_CK(cudaStreamEndCapture(stream_, &graph_));
+    OMMB200_CK(cudaGraphInstantiate(&graph_exec_, graph_, 0));
+  }
+  for (int i = 0; i < launches; ++i) OMMB200_CK(cudaGraphLaunch(graph_exec_, stream_));
+}
+
+void Engine::step(int steps) {
+  if (steps <= 0) return;
+  const int k = opt_.steps_per_graph > 0 ? opt_.steps_per_graph : 20;
+  int remaining = steps;
+  if (opt_.use_graph && !profiling_ && steps >= k) {
+    if (graph_steps_ != k) destroy_graph();
+    graph_steps_ = k;
+    run_graph_steps(steps / k);
+    remaining = steps % k;
+  }
+  for (int s = 0; s < remaining; ++s) {
+    enqueue_step(0);
+    launch_advance_counter(rng_step_, 1, stream_);
+  }
+  OMMB200_CK(cudaGetLastError());
+  sync();
+  harvest_profile();
+  time_ += steps * integ_->step_size;
+  step_count_ += steps;
+  check_status();
+}
+
+void Engine::set_positions(const double* xyz) {
+  for (size_t i = 0; i < 3 * (size_t)n_; ++i)
+    require(std::isfinite(xyz[i]), "particle positions must be finite");  // neighbors.rs:107-110
+  OMMB200_CK(cudaMemcpyAsync(pos_, xyz, sizeof(double) * 3 * (size_t)n_, cudaMemcpyHostToDevice, stream_));
+  const int one = 1;
+  OMMB200_CK(cudaMemcpyAsync(rebuild_, &one, sizeof(int), cudaMemcpyHostToDevice, stream_));
+  sync();
+}
+
+void Engine::set_velocities(const double* v) {
+  OMMB200_CK(cudaMemcpyAsync(vel_, v, sizeof(double) * 3 * (size_t)n_, cudaMemcpyHostToDevice, stream_));
+  sync();
+}
+
+// context.rs:182-223
+void Engine::set_velocities_to_temperature(double temperature, int seed) {
+  require(std::isfinite(temperature) && temperature >= 0.0, "temperature must be nonnegative and finite");
+  const uint64_t key = seed != 0 ? (uint64_t)(uint32_t)seed : seed_;
+  std::vector<double> v(3 * (size_t)n_, 0.0);
+  const uint64_t draw = velocity_draws_++;
+  for (int i = 0; i < n_; ++i) {
+    if (host_masses_[i] == 0.0) continue;
+    uint32_t c[4] = {(uint32_t)i, (uint32_t)draw, (uint32_t)(draw >> 32), 1u};
+    philox4x32_10(c, (uint32_t)key, (uint32_t)(key >> 32));
+    const double s = 2.3283064365386962890625e-10;
+    const double u0 = (c[0] + 0.5) * s, u1 = (c[1] + 0.5) * s, u2 = (c[2] + 0.5) * s, u3 = (c[3] + 0.5) * s;
+    const double m0 = std::sqrt(-2.0 * std::log(u0)), m1 = std::sqrt(-2.0 * std::log(u2));
+    const double scale = std::sqrt(kBoltzmann * temperature / host_masses_[i]);
+    v[3 * i] = scale * m0 * std::cos(2.0 * kPiD * u1);
+    v[3 * i + 1] = scale * m0 * std::sin(2.0 * kPiD * u1);
+    v[3 * i + 2] = scale * m1 * std::cos(2.0 * kPiD * u3);
+  }
+  // LFMiddle velocity_time_offset = dt/2 (langevin.rs:204-206): v -= F/m * dt/2
+  const double offset = 0.5 * integ_->step_size;
+  compute_forces(false, 0xffffffffu);
+  std::vector<long long> f(3 * (size_t)n_);
+  OMMB200_CK(cudaMemcpyAsync(f.data(), force_, 8 * f.size(), cudaMemcpyDeviceToHost, stream_));
+  sync();
+  check_status();
+  for (int i = 0; i < n_; ++i) {
+    if (host_masses_[i] == 0.0) continue;
+    for (int c = 0; c < 3; ++c) v[3 * i + c] -= (double)f[(size_t)c * n_ + i] * kForceScaleInv / host_masses_[i] * offset;
+  }
+  set_velocities(v.data());
+  apply_velocity_constraints(1e-5);
+}
+
+void Engine::set_box(const double b[9]) {
+  validate_box(b);
+  if (nb_ && nb_periodic_)
+    for (int a = 0; a < 3; ++a)
+      require(nb_->cutoff <= 0.5 * b[4 * a], "cutoff must not exceed half the periodic box size");
+  std::copy(b, b + 9, box_);
+  destroy_graph();
+  update_box_dependents();
+  const int one = 1;
+  OMMB200_CK(cudaMemcpy(rebuild_, &one, sizeof(int), cudaMemcpyHostToDevice));
+}
+
+void Engine::apply_constraints(double tolerance) {
+  require(std::isfinite(tolerance) && tolerance > 0.0 && tolerance < 1.0,
+          "constraint tolerance must be finite and between zero and one", OMMB200_ERR_CONSTRAINT);
+  OMMB200_CK(cudaMemcpyAsync(scratch3_, pos_, 24 * (size_t)n_, cudaMemcpyDeviceToDevice, stream_));
+  IntegrateArgs a = integrate_args(0);
+  a.tolerance = tolerance;
+  launch_constrain_positions(a, scratch3_, stream_);
+  const int one = 1;
+  OMMB200_CK(cudaMemcpyAsync(rebuild_, &one, sizeof(int), cudaMemcpyHostToDevice, stream_));
+  sync();
+  check_status();
+}
+
+void Engine::apply_velocity_constraints(double tolerance) {
+  require(std::isfinite(tolerance) && tolerance > 0.0 && tolerance < 1.0,
+          "constraint tolerance must be finite and between zero and one", OMMB200_ERR_CONSTRAINT);
+  IntegrateArgs a = integrate_args(0);
+  a.tolerance = tolerance;
+  launch_constrain_velocities(a, stream_);
+  sync();
+  check_status();
+}
+
+void Engine::get_state(int flags, uint32_t groups, double* pos, double* vel, double* forces,
+                       ommb200_state_info* info) {
+  const bool need_forces = flags & (OMMB200_STATE_FORCES | OMMB200_STATE_ENERGY | OMMB200_STATE_VIRIAL);
+  const bool need_energy = flags & (OMMB200_STATE_ENERGY | OMMB200_STATE_VIRIAL);
+  long long e[8] = {0};
+  if (need_forces) {
+    OMMB200_CK(cudaMemsetAsync(energy_, 0, 8 * sizeof(long long), stream_));
+    compute_forces(need_energy, groups);
+    if (forces) {
+      std::vector<long long> f(3 * (size_t)n_);
+      OMMB200_CK(cudaMemcpyAsync(f.data(), force_, 8 * f.size(), cudaMemcpyDeviceToHost, stream_));
+      sync();
+      for (int i = 0; i < n_; ++i)
+        for (int c = 0; c < 3; ++c) forces[3 * i + c] = (double)f[(size_t)c * n_ + i] * kForceScaleInv;
+    }
+    OMMB200_CK(cudaMemcpyAsync(e, energy_, sizeof(e), cudaMemcpyDeviceToHost, stream_));
+    sync();
+    harvest_profile();
+    check_status();
+  }
+  std::vector<double> vtmp;
+  double* vout = vel;
+  if (!vout && info) {
+    vtmp.resize(3 * (size_t)n_);
+    vout = vtmp.data();
+  }
+  if (pos) OMMB200_CK(cudaMemcpyAsync(pos, pos_, 24 * (size_t)n_, cudaMemcpyDeviceToHost, stream_));
+  if (vout) OMMB200_CK(cudaMemcpyAsync(vout, vel_, 24 * (size_t)n_, cudaMemcpyDeviceToHost, stream_));
+  sync();
+  if (!info) return;
+  info->time = time_;
+  info->step_count = step_count_;
+  std::copy(box_, box_ + 9, info->box);
+  double ke = 0.0;
+  for (int i = 0; i < n_; ++i)
+    ke += host_masses_[i] * (vout[3 * i] * vout[3 * i] + vout[3 * i + 1] * vout[3 * i + 1] + vout[3 * i + 2] * vout[3 * i + 2]);
+  info->kinetic_energy = 0.5 * ke;
+  double pe = (double)e[0] * kEnergyScaleInv;
+  double w[6];
+  for (int c = 0; c < 6; ++c) w[c] = (double)e[1 + c] * kEnergyScaleInv;
+  if (need_energy && nb_) {
+    const int g = nb_->force_group;
+    const int rg = nb_->reciprocal_force_group < 0 ? g : nb_->reciprocal_force_group;
+    const bool direct = nb_->include_direct_space && ((groups >> g) & 1u);
+    const bool recip = nb_pme_ && ((groups >> rg) & 1u);
+    if (recip) {
+      pe += self_energy_ - plasma_energy_;
+      for (int c = 0; c < 3; ++c) w[c] -= plasma_energy_;
+    }
+    if (direct && nb_periodic_ && nb_->use_dispersion_correction) {
+      const double ed = dispersion_coeff_ / volume_;
+      pe += ed;
+      for (int c = 0; c < 3; ++c) w[c] += ed;
+    }
+  }
+  info->potential_energy = need_energy ? pe : 0.0;
+  const double vir[9] = {w[0], w[3], w[4], w[3], w[1], w[5], w[4], w[5], w[2]};
+  std::copy(vir, vir + 9, info->virial);
+}
+
+void Engine::pme_parameters(double* alpha, int* nx, int* ny, int* nz) const {
+  *alpha = alpha_;
+  *nx = grid_[0];
+  *ny = grid_[1];
+  *nz = grid_[2];
+}
+
+int64_t Engine::debug_pair_list(int64_t max_pairs, int32_t* pairs) {
+  require(nb_ != nullptr, "the System has no NonbondedForce");
+  if (max_pairs > dump_capacity_) {
+    dump_pairs_ = mem_.alloc<int32_t>(2 * (size_t)std::max<int64_t>(max_pairs, 1));
+    dump_capacity_ = max_pairs;
+  }
+  if (!dump_count_) dump_count_ = mem_.alloc<unsigned long long>(1);
+  OMMB200_CK(cudaMemsetAsync(dump_count_, 0, 8, stream_));
+  dump_mode_ = true;
+  try {
+    compute_forces(false, 0xffffffffu);
+  } catch (...) {
+    dump_mode_ = false;
+    throw;
+  }
+  dump_mode_ = false;
+  unsigned long long count = 0;
+  OMMB200_CK(cudaMemcpyAsync(&count, dump_count_, 8, cudaMemcpyDeviceToHost, stream_));
+  sync();
+  const int64_t take = std::min<int64_t>((int64_t)count, max_pairs);
+  if (take > 0 && pairs)
+    OMMB200_CK(cudaMemcpy(pairs, dump_pairs_, 8 * (size_t)take, cudaMemcpyDeviceToHost));
+  harvest_profile();
+  check_status();
+  return (int64_t)count;
+}
+
+}  // namespace ommb200

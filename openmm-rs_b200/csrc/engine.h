@@ -1,0 +1,188 @@
+// The Context engine: device-resident state of one System plus the launch sequence of an MD
+// step (context.rs:878-928 try_step_once: forces, then the integrator) and of getState.
+#pragma once
+
+#include <cufft.h>
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/ommb200.h"
+#include "kernels.h"
+#include "model.h"
+
+namespace ommb200 {
+
+// Owns every device allocation of an Engine; memory is zeroed on allocation.
+double measure_fp32_peak(int device);  // diagnostics.cu
+
+class DeviceArena {
+ public:
+  ~DeviceArena();
+  void* alloc_bytes(size_t bytes);
+  template <class T>
+  T* alloc(size_t count) {
+    return static_cast<T*>(alloc_bytes(sizeof(T) * (count ? count : 1)));
+  }
+
+ private:
+  std::vector<void*> ptrs_;
+};
+
+struct EngineOptions {
+  int precision = OMMB200_PRECISION_MIXED;
+  int device = 0;
+  bool use_graph = true;
+  double skin = 0.0;
+  int steps_per_graph = 0;
+};
+
+class Engine {
+ public:
+  Engine(std::unique_ptr<SystemDef> system, std::unique_ptr<IntegratorDef> integrator,
+         const EngineOptions& options);
+  ~Engine();
+  Engine(const Engine&) = delete;
+  Engine& operator=(const Engine&) = delete;
+
+  int num_particles() const { return n_; }
+  void set_positions(const double* xyz);
+  void set_velocities(const double* v);
+  void set_velocities_to_temperature(double temperature, int seed);
+  void set_box(const double box[9]);
+  void set_time(double t) { time_ = t; }
+  void set_step_count(int64_t s) { step_count_ = s; }
+  void apply_constraints(double tolerance);
+  void apply_velocity_constraints(double tolerance);
+  void step(int steps);
+  void get_state(int flags, uint32_t groups, double* pos, double* vel, double* forces,
+                 ommb200_state_info* info);
+  void pme_parameters(double* alpha, int* nx, int* ny, int* nz) const;
+  int64_t debug_pair_list(int64_t max_pairs, int32_t* pairs);
+  void set_profiling(bool enabled);
+  struct KernelTime {
+    std::string name;
+    double ms;
+    int launches;
+  };
+  std::vector<KernelTime> kernel_times() const { return kernel_times_; }
+  cudaStream_t stream() const { return stream_; }
+
+ private:
+  void setup_nonbonded(const NonbondedDef& nb);
+  void setup_bonded();
+  void setup_integrator();
+  void update_box_dependents();
+  void build_static_tiles();
+  void compute_forces(bool energy, uint32_t groups);
+  void enqueue_step(int step_offset);
+  void run_graph_steps(int graph_launches);
+  void check_status();
+  void sync();
+  void destroy_graph();
+  template <class Real>
+  void enqueue_nonbonded(bool energy, bool direct, bool reciprocal, bool dump);
+  void prof_begin(const char* name);
+  void prof_end();
+  void harvest_profile();
+  IntegrateArgs integrate_args(int step_offset) const;
+
+  std::unique_ptr<SystemDef> sys_;
+  std::unique_ptr<IntegratorDef> integ_;
+  EngineOptions opt_;
+  bool dp_ = false;
+  int n_ = 0;
+  double box_[9];
+  double time_ = 0.0;
+  int64_t step_count_ = 0;
+  uint64_t seed_ = 0;
+  uint64_t velocity_draws_ = 0;
+  cudaStream_t stream_ = nullptr;
+  DeviceArena mem_;
+
+  // state
+  double* pos_ = nullptr;
+  double* vel_ = nullptr;
+  double* inv_mass_ = nullptr;
+  double* scratch3_ = nullptr;
+  long long* force_ = nullptr;
+  long long* energy_ = nullptr;  // [7]
+  int* status_ = nullptr;
+  int* rebuild_ = nullptr;
+  unsigned long long* rng_step_ = nullptr;
+  std::vector<double> host_masses_;
+
+  // nonbonded
+  const NonbondedDef* nb_ = nullptr;
+  bool nb_periodic_ = false;
+  bool nb_pme_ = false;
+  int elec_ = kElecCoulomb;
+  int n_blocks_ = 0, n_slots_ = 0;
+  NlistArgs nl_{};
+  double* qscaled_ = nullptr;
+  double* charge_ = nullptr;
+  double* half_sigma_ = nullptr;
+  double* sqrt_eps_ = nullptr;
+  void* posq_ = nullptr;
+  void* ljp_ = nullptr;
+  bool params_packed_ = false;
+  double alpha_ = 0.0;
+  int grid_[3] = {0, 0, 0};
+  double recip_[3][3];
+  double volume_ = 0.0;
+  double self_energy_ = 0.0, plasma_energy_ = 0.0, dispersion_coeff_ = 0.0;
+  long long* pme_fixed_ = nullptr;
+  void* pme_real_ = nullptr;
+  void* pme_k_ = nullptr;
+  void* influence_ = nullptr;
+  double* moduli_ = nullptr;
+  cufftHandle fft_fwd_ = 0, fft_inv_ = 0;
+  bool fft_ready_ = false;
+  int n_exceptions_ = 0;
+  int2* exc_pairs_ = nullptr;
+  double4* exc_params_ = nullptr;
+  int32_t* dump_pairs_ = nullptr;
+  unsigned long long* dump_count_ = nullptr;
+  long long dump_capacity_ = 0;
+  bool dump_mode_ = false;
+  int pair_grid_ = 0;
+
+  // bonded terms, one launch per force
+  struct BondedLaunch {
+    BondedArgs args;
+    int group;
+  };
+  std::vector<BondedLaunch> bonded_;
+
+  // integrator
+  int n_water_ = 0, n_free_ = 0, n_clusters_ = 0;
+  int4* water_ = nullptr;
+  WaterGeometry geom_{};
+  int* free_atoms_ = nullptr;
+  int* cluster_start_ = nullptr;
+  int2* cluster_pairs_ = nullptr;
+  double* cluster_dist2_ = nullptr;
+  int* cluster_atom_start_ = nullptr;
+  int* cluster_atoms_ = nullptr;
+  double skin_ = 0.0;
+
+  // graph
+  cudaGraph_t graph_ = nullptr;
+  cudaGraphExec_t graph_exec_ = nullptr;
+  int graph_steps_ = 0;
+
+  // profiling
+  bool profiling_ = false;
+  struct PendingEvent {
+    std::string name;
+    cudaEvent_t start, stop;
+  };
+  std::vector<PendingEvent> pending_;
+  std::vector<cudaEvent_t> event_pool_;
+  std::vector<KernelTime> kernel_times_;
+  std::string current_prof_;
+  cudaEvent_t current_start_ = nullptr;
+};
+
+}  // namespace ommb200

@@ -1,0 +1,207 @@
+// Argument blocks and launchers of the engine's CUDA kernels.  Every launcher enqueues on the
+// given stream and never synchronizes, so a whole MD step can be captured in a CUDA graph.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cufft.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace ommb200 {
+
+// ---- neighbour tiles -------------------------------------------------------------------
+// A tile is a pair of 32-slot blocks (I <= J) of the spatially sorted particle order.
+enum TileFlags : int {
+  kTileHasMask = 1,    // exclusion/padding mask stored at masks[32 * mask_slot]
+  kTilePairImage = 2,  // apply the minimum image per pair (small boxes)
+};
+
+struct NlistArgs {
+  int n_atoms;        // particles of the system
+  int n_blocks;       // ceil(n_atoms / 32)
+  const double* pos;  // [3N] master positions
+  double* pos_ref;    // [3N] positions at the last rebuild
+  int* image;         // [3N] lattice image n of each particle at the last rebuild
+  int* key;           // [N] Morton key of the particle's voxel
+  int* key_count;     // [n_keys] particles per voxel (zero between rebuilds)
+  int* key_start;     // [n_keys + 1] exclusive scan
+  int* key_cursor;    // [n_keys] scatter cursor (zero between rebuilds)
+  int* scratch_atoms; // [N] unordered scatter
+  int* sorted_atom;   // [32 * n_blocks] particle in each slot, -1 for padding
+  int* atom_slot;     // [N] inverse of sorted_atom
+  double* block_center;  // [3 * n_blocks]
+  double* block_half;    // [3 * n_blocks] half extents of the block's bounding box
+  int4* tiles;           // [tile_capacity] (I, J, flags, mask_slot)
+  void* tile_shift;      // [tile_capacity] float4 / double4 centre offset of J relative to I
+  uint32_t* masks;       // [32 * mask_capacity]
+  int* n_tiles;          // device counter
+  int* n_masks;          // device counter
+  int tile_capacity, mask_capacity;
+  const int* excl_start;  // [N + 1] CSR of excluded partners (both directions)
+  const int* excl_list;
+  int* rebuild;           // nonzero: rebuild before the next force evaluation
+  int* status;
+  Box<double> box;
+  int periodic;
+  double cutoff;      // interaction cutoff (nm)
+  double skin;        // Verlet skin (nm)
+  int n_vox[3];       // voxel grid of the sort
+  int morton_bits;
+  int n_keys;
+};
+
+void launch_nlist_rebuild(const NlistArgs& a, bool double_shift, cudaStream_t s);
+// Static list of all block pairs (non-periodic methods); built once.
+void build_all_pairs_tiles(const NlistArgs& a, bool double_shift, cudaStream_t s);
+
+// ---- nonbonded pair kernel -------------------------------------------------------------
+enum ElecKind : int { kElecEwald = 0, kElecReactionField = 1, kElecCoulomb = 2 };
+
+template <class Real>
+struct PairArgs {
+  int n_atoms;
+  const int* sorted_atom;
+  const double* pos;
+  const void* posq;     // [slots] float4/double4: block-local xyz, q * sqrt(ke)
+  const void* ljp;      // [slots] float2/double2: sigma / 2, sqrt(epsilon)
+  const int4* tiles;
+  const void* tile_shift;
+  const uint32_t* masks;
+  const int* n_tiles;
+  int tile_capacity;
+  long long* force;     // [3][N] fixed point
+  long long* energy;    // [7]: energy, virial xx yy zz xy xz yz (fixed point)
+  Box<Real> box;
+  Box<double> box_exact;
+  int periodic;
+  int use_cutoff;
+  Real cutoff2;
+  double cutoff2_exact;
+  Real band;            // |r2 - rc2| below this is decided in f64 by the reference formula
+  Real alpha, alpha2, two_alpha_sqrtpi;
+  Real krf, crf;
+  int use_switching;
+  Real switch_r, switch_inv_width;
+  int32_t* pair_dump;   // diagnostics
+  unsigned long long* pair_count;
+  long long pair_capacity;
+};
+
+template <class Real>
+void launch_pair(const PairArgs<Real>& a, int elec, bool energy, bool dump, int grid,
+                 cudaStream_t s);
+
+// Per-step packing of block-local coordinates into the sorted slots.
+template <class Real>
+void launch_pack(int n_slots, const int* sorted_atom, const double* pos, const int* image,
+                 const double* block_center, const double* qscaled, void* posq,
+                 const Box<double>& box, cudaStream_t s);
+template <class Real>
+void launch_pack_params(int n_slots, const int* sorted_atom, const double* half_sigma,
+                        const double* sqrt_eps, void* ljp, cudaStream_t s);
+
+// ---- PME -------------------------------------------------------------------------------
+template <class Real>
+struct PmeArgs {
+  int n_atoms;
+  const int* order;     // particle visiting order (sorted slots) or nullptr
+  int n_order;
+  const double* pos;
+  const double* charge;
+  int nx, ny, nz;
+  double recip[3][3];
+  long long* grid_fixed;  // [nx*ny*nz]
+  Real* grid_real;        // [nx*ny*nz]
+  void* grid_k;           // [nx*ny*(nz/2+1)] complex
+  const Real* influence;  // [nx*ny*(nz/2+1)]
+  const double* moduli;   // [nx + ny + nz] B-spline moduli |b(m)|^2 (pme.rs:240-259)
+  long long* force;
+  long long* energy;
+  double alpha, volume;
+};
+
+template <class Real>
+void launch_pme_spread(const PmeArgs<Real>& a, cudaStream_t s);
+template <class Real>
+void launch_pme_convert(const PmeArgs<Real>& a, cudaStream_t s);
+template <class Real>
+void launch_pme_convolve(const PmeArgs<Real>& a, bool energy, cudaStream_t s);
+template <class Real>
+void launch_pme_gather(const PmeArgs<Real>& a, cudaStream_t s);
+
+// ---- exceptions and bonded terms (exceptions always in f64) ------------------------------
+struct ExceptionArgs {
+  int n;
+  const int2* pairs;
+  const double4* params;  // (charge_prod * ke, sigma, epsilon, q_i q_j * ke)
+  const double* pos;
+  long long* force;
+  long long* energy;
+  Box<double> box;
+  int use_pbc;
+  int ewald;
+  double alpha;
+  int n_atoms_for_force;  // row stride of the [3][N] force array
+};
+void launch_exceptions(const ExceptionArgs& a, bool energy, cudaStream_t s);
+
+struct BondedArgs {
+  int n_bonds;
+  const int2* bonds;
+  const double2* bond_params;  // (length, k)
+  int bond_pbc;
+  int n_angles;
+  const int4* angles;
+  const double2* angle_params;  // (theta0, k)
+  int angle_pbc;
+  const double* pos;
+  long long* force;
+  long long* energy;
+  Box<double> box;
+  int n_atoms_for_force;
+};
+void launch_bonded(const BondedArgs& a, bool energy, cudaStream_t s);
+
+// ---- integration -----------------------------------------------------------------------
+struct WaterGeometry {
+  double d_oh, d_hh, m_o, m_h;
+};
+
+struct IntegrateArgs {
+  int n_atoms;
+  int n_water;
+  const int4* water;  // (O, H1, H2, unused)
+  WaterGeometry geom;
+  int n_free;
+  const int* free_atoms;
+  int n_clusters;
+  const int* cluster_start;       // [n_clusters + 1] into the constraint arrays
+  const int2* cluster_pairs;      // constraint particle pairs
+  const double* cluster_dist2;    // squared distances
+  const int* cluster_atom_start;  // [n_clusters + 1] into cluster_atoms
+  const int* cluster_atoms;
+  double* pos;
+  double* vel;
+  double* scratch;                // [3N] SHAKE reference / proposal buffer
+  const long long* force;
+  const double* inv_mass;
+  double dt, decay, noise_var;    // noise_var = kT (1 - decay^2)
+  double tolerance;
+  uint64_t seed;
+  const unsigned long long* rng_step;
+  int step_offset;
+  const double* pos_ref;          // neighbour-list reference positions (may be null)
+  double half_skin2;
+  int* rebuild;
+  int* status;
+};
+void launch_integrate(const IntegrateArgs& a, cudaStream_t s);
+void launch_advance_counter(unsigned long long* counter, int by, cudaStream_t s);
+
+// Velocity / position constraint projections used outside the step (apply_constraints,
+// set_velocities_to_temperature).
+void launch_constrain_positions(const IntegrateArgs& a, const double* reference, cudaStream_t s);
+void launch_constrain_velocities(const IntegrateArgs& a, cudaStream_t s);
+
+}  // namespace ommb200
