@@ -27,9 +27,9 @@ WORKLOAD = "water-23958"
 DT_PS = 0.002
 METRIC = "ns/day @24k-atom PME water box (1 B200) + force RMS rel err vs FP64"
 # Algorithmic FP32 work per in-cutoff pair of the mixed-precision PME pair kernel, FMA = 2,
-# MUFU (rsqrt, exp2, rcp) = 1: delta 3, r^2 5, rsqrt 1, 1/r^2 1, LJ 14, Ewald (r, exp,
-# erfc fit with 7 FMAs, force) 30, f/r sum 1, force vector 3, i/j accumulation 6 + 3 = 71.
-FLOPS_PER_PAIR = 71
+# MUFU (rsqrt, exp2, rcp) = 1: delta 3, r^2 5, rsqrt + 1/r^2 2, LJ 11, Ewald (r, exp2,
+# erfc fit with 7 FMAs, force) 28, f/r sum 1, i and j force accumulation 6 + 6 = 62.
+FLOPS_PER_PAIR = 62
 # HBM bytes per particle of one integrator launch: read x, v, fixed-point F, rebuild
 # reference (4 x 24) plus per-molecule index (16/3), write x, v (2 x 24).
 INTEGRATE_BYTES_PER_ATOM = 96 + 16 / 3 + 48
@@ -386,6 +386,11 @@ def main():
         per_md = 9 + 2 + 1 + 4 + 1 + 1
         launches = md_steps * per_md + args.steps * (args.segment // 20)
         extras["pairs_in_cutoff"] = pairs
+        nl = ctx.nlist_stats()
+        nl["pair_efficiency"] = pairs / max(1, nl["tiles"] * 1024)
+        steps_on_ctx = (args.warmup + 2 * args.steps) * args.segment + prof_steps
+        nl["md_steps_per_rebuild"] = steps_on_ctx / max(1, nl["rebuilds"])
+        extras["nlist"] = nl
         # FP64-on-GPU form of the same kernels
         _, ctx64 = build_context("double", seed, local)
         time_segments(ctx64, torch, 1, args.segment, flush)

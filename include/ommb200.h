@@ -201,6 +201,10 @@ int ommb200_context_debug_pair_list(ommb200_context* ctx, int64_t max_pairs, int
 int ommb200_context_set_profiling(ommb200_context* ctx, int enabled);
 int ommb200_context_kernel_times(ommb200_context* ctx, int max_entries, char* names,
                                  int names_len, double* ms, int* launches, int* count);
+/* Neighbour-list state after the last force evaluation: tiles (32 x 32 pair blocks) in use,
+ * 32-slot particle blocks in use, tiles carrying exclusion masks, and list rebuilds so far. */
+int ommb200_context_nlist_stats(ommb200_context* ctx, int* tiles, int* blocks, int* masked,
+                                int64_t* rebuilds);
 /* The cudaStream_t every kernel of this Context is launched on (for CUDA-event timing). */
 int ommb200_context_get_stream(ommb200_context* ctx, void** stream);
 /* Measured FP32 FMA throughput of the device (TFLOP/s, FMA = 2 flops): the roofline

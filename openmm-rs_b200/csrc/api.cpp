@@ -567,6 +567,13 @@ int ommb200_context_kernel_times(ommb200_context* ctx, int max_entries, char* na
     }
   });
 }
+int ommb200_context_nlist_stats(ommb200_context* ctx, int* tiles, int* blocks, int* masked,
+                                int64_t* rebuilds) {
+  return guarded([&] {
+    OMMB200_CTX;
+    E.nlist_stats(tiles, blocks, masked, rebuilds);
+  });
+}
 int ommb200_context_get_stream(ommb200_context* ctx, void** stream) {
   return guarded([&] {
     OMMB200_CTX;

@@ -19,9 +19,9 @@ constexpr double kBoltzmann = 1.380649e-23 * 6.02214076e23 / 1000.0;
 // is associative, so the sum is independent of launch order and bit-identical run to run.
 constexpr double kForceScale = 4294967296.0;        // 2^32
 constexpr double kForceScaleInv = 1.0 / 4294967296.0;
-// Energies and virials accumulate in units of 2^-26 kJ/mol (range +-1.4e11 kJ/mol).
-constexpr double kEnergyScale = 67108864.0;          // 2^26
-constexpr double kEnergyScaleInv = 1.0 / 67108864.0;
+// Energies and virials accumulate in units of 2^-32 kJ/mol (range +-2.1e9 kJ/mol).
+constexpr double kEnergyScale = 4294967296.0;        // 2^32
+constexpr double kEnergyScaleInv = 1.0 / 4294967296.0;
 // PME charge grid: units of 2^-40 e (a grid point can hold up to 8.4e6 e).
 constexpr double kGridScale = 1099511627776.0;  // 2^40
 constexpr double kGridScaleInv = 1.0 / 1099511627776.0;

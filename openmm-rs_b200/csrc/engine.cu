@@ -288,7 +288,7 @@ void Engine::setup_nonbonded(const NonbondedDef& nb) {
   for (int i = 0; i < n_; ++i) {
     qs[i] = nb.charge[i] * sk;
     hs[i] = 0.5 * nb.sigma[i];
-    se[i] = std::sqrt(nb.epsilon[i]);
+    se[i] = 2.0 * std::sqrt(nb.epsilon[i]);  // pair product = 4 sqrt(eps_i eps_j)
   }
   qscaled_ = mem_.alloc<double>(n_);
   charge_ = mem_.alloc<double>(n_);
@@ -329,12 +329,9 @@ void Engine::setup_nonbonded(const NonbondedDef& nb) {
     OMMB200_CK(cudaMemcpy(excl_list, xl.data(), 4 * xl.size(), cudaMemcpyHostToDevice));
 
   // slots and tiles
-  n_blocks_ = (n_ + 31) / 32;
-  n_slots_ = 32 * n_blocks_;
   NlistArgs& a = nl_;
   a = NlistArgs{};
   a.n_atoms = n_;
-  a.n_blocks = n_blocks_;
   a.pos = pos_;
   a.excl_start = excl_start;
   a.excl_list = excl_list;
@@ -342,53 +339,67 @@ void Engine::setup_nonbonded(const NonbondedDef& nb) {
   a.status = status_;
   a.periodic = nb_periodic_;
   a.cutoff = nb.cutoff;
-  a.sorted_atom = mem_.alloc<int>(n_slots_);
-  a.atom_slot = mem_.alloc<int>(n_);
-  a.image = mem_.alloc<int>(3 * (size_t)n_);
-  a.block_center = mem_.alloc<double>(3 * (size_t)n_blocks_);
-  a.block_half = mem_.alloc<double>(3 * (size_t)n_blocks_);
+  a.min_width = std::min(box_[0], std::min(box_[4], box_[8]));
+  a.n_blocks = mem_.alloc<int>(1);
+  a.rebuild_count = mem_.alloc<unsigned long long>(1);
   a.n_tiles = mem_.alloc<int>(1);
   a.n_masks = mem_.alloc<int>(1);
-  std::vector<int> sorted(n_slots_, -1);
-  for (int i = 0; i < n_; ++i) sorted[i] = i;
-  OMMB200_CK(cudaMemcpy(a.sorted_atom, sorted.data(), 4 * n_slots_, cudaMemcpyHostToDevice));
-  OMMB200_CK(cudaMemcpy(a.atom_slot, sorted.data(), 4 * n_, cudaMemcpyHostToDevice));
-  const long long all_pairs = (long long)n_blocks_ * (n_blocks_ + 1) / 2;
   if (nb_periodic_) {
     skin_ = opt_.skin > 0.0 ? opt_.skin : 0.1;
     a.skin = skin_;
     double recip[3][3], vol;
     reciprocal_box(box_, recip, &vol);
     const double density = n_ / vol;
-    const double edge = std::cbrt(4.0 / density);  // ~32 particles per 2x2x2 voxels
-    int maxv = 1;
-    for (int d = 0; d < 3; ++d) {
-      a.n_vox[d] = std::max(1, std::min(1024, (int)std::floor(box_[4 * d] / edge)));
-      maxv = std::max(maxv, a.n_vox[d]);
-    }
-    int bits = 0;
-    while ((1 << bits) < maxv) ++bits;
-    a.morton_bits = bits;
-    a.n_keys = 1 << (3 * bits);
+    // x-y columns ~0.62 nm wide: z-sorted blocks of 32 become ~0.6 x 0.6 x 0.8 nm bricks.
+    // Tall boxes get narrower columns so a column stays within the per-column sort's
+    // shared-memory capacity (4096 keys).
+    const double width = std::min(0.62, std::sqrt(1500.0 / (density * box_[8])));
+    for (int d = 0; d < 2; ++d)
+      a.n_col[d] = std::max(1, std::min(4096, (int)std::floor(box_[4 * d] / width)));
+    a.n_cols = a.n_col[0] * a.n_col[1];
+    const double col_area = (box_[0] / a.n_col[0]) * (box_[4] / a.n_col[1]);
+    const double expected = density * col_area * box_[8];
+    a.col_max = std::max(64, (int)std::min(4096.0, 2.5 * expected + 64));
+    a.slot_capacity = ((n_ + 31 * a.n_cols) + 31) / 32 * 32;
     a.pos_ref = mem_.alloc<double>(3 * (size_t)n_);
-    a.key = mem_.alloc<int>(n_);
-    a.key_count = mem_.alloc<int>(a.n_keys);
-    a.key_start = mem_.alloc<int>(a.n_keys + 1);
-    a.key_cursor = mem_.alloc<int>(a.n_keys);
+    a.column = mem_.alloc<int>(n_);
+    a.zkey = mem_.alloc<float>(n_);
+    a.col_count = mem_.alloc<int>(a.n_cols);
+    a.col_start = mem_.alloc<int>(a.n_cols + 1);
+    a.col_scatter = mem_.alloc<int>(a.n_cols + 1);
+    a.col_cursor = mem_.alloc<int>(a.n_cols);
     a.scratch_atoms = mem_.alloc<int>(n_);
-    const double bvol = 32.0 / density;
-    const double reach = nb.cutoff + skin_ + std::sqrt(3.0) * std::cbrt(bvol);
-    const double per_block = 0.5 * (4.0 / 3.0) * kPiD * reach * reach * reach / bvol + 1.0;
-    a.tile_capacity = (int)std::min<long long>(all_pairs, std::max<long long>(4096, (long long)(3.0 * n_blocks_ * per_block)));
-    // a masked tile holds an exclusion or a padding slot: at most one per exception plus
-    // one per block, so this pool cannot overflow
-    a.mask_capacity = (int)std::min<long long>(a.tile_capacity, (long long)n_exceptions_ + n_blocks_ + 64);
+    const long long blocks = a.slot_capacity / 32;
+    const double reach = nb.cutoff + skin_;
+    const double wx = box_[0] / a.n_col[0], wy = box_[4] / a.n_col[1];
+    const double hz = 32.0 / (density * wx * wy);
+    const double gathered = density * (wx + 2 * reach) * (wy + 2 * reach) * (hz + 2 * reach) / 2.0;
+    const long long per_block = (long long)(1.5 * gathered / 32.0) + 8;
+    const bool small_box = a.min_width < 2.0 * (reach + 2.0);
+    const long long all_pairs = blocks * (blocks + 1) / 2 + blocks;
+    a.tile_capacity = (int)std::min<long long>(all_pairs, small_box ? all_pairs : blocks * per_block);
+    // a masked tile holds an exclusion or a padding slot: at most one per exception plus two
+    // per block (self tile, last partial neighbour tile), so this pool cannot overflow
+    a.mask_capacity = (int)std::min<long long>(a.tile_capacity, (long long)n_exceptions_ + 2 * blocks + 64);
   } else {
-    a.tile_capacity = (int)all_pairs;
-    a.mask_capacity = (int)all_pairs;
+    a.slot_capacity = (n_ + 31) / 32 * 32;
+    const long long blocks = a.slot_capacity / 32;
+    a.tile_capacity = (int)(blocks * (blocks + 1) / 2);
+    a.mask_capacity = a.tile_capacity;
   }
+  n_slots_ = a.slot_capacity;
+  n_blocks_ = n_slots_ / 32;
+  a.sorted_atom = mem_.alloc<int>(n_slots_);
+  a.atom_slot = mem_.alloc<int>(n_);
+  a.image = mem_.alloc<int>(3 * (size_t)n_);
+  a.block_center = mem_.alloc<double>(3 * (size_t)n_blocks_);
+  a.block_half = mem_.alloc<double>(3 * (size_t)n_blocks_);
+  std::vector<int> sorted(n_slots_, -1);
+  for (int i = 0; i < n_; ++i) sorted[i] = i;
+  OMMB200_CK(cudaMemcpy(a.sorted_atom, sorted.data(), 4 * n_slots_, cudaMemcpyHostToDevice));
+  OMMB200_CK(cudaMemcpy(a.atom_slot, sorted.data(), 4 * n_, cudaMemcpyHostToDevice));
   a.tiles = mem_.alloc<int4>(a.tile_capacity);
-  a.tile_shift = mem_.alloc_bytes((dp_ ? 32 : 16) * (size_t)a.tile_capacity);
+  a.entries = mem_.alloc_bytes((size_t)(dp_ ? 32 : 16) * 32 * (size_t)a.tile_capacity);
   a.masks = mem_.alloc<uint32_t>(32 * (size_t)a.mask_capacity);
   posq_ = mem_.alloc_bytes((dp_ ? 32 : 16) * (size_t)n_slots_);
   ljp_ = mem_.alloc_bytes((dp_ ? 16 : 8) * (size_t)n_slots_);
@@ -429,6 +440,8 @@ void Engine::build_static_tiles() {
   NlistArgs& a = nl_;
   std::vector<int4> tiles;
   std::vector<uint32_t> masks;
+  std::vector<float4> entry_f;
+  std::vector<double4> entry_d;
   std::vector<std::vector<int>> partners(n_);
   for (auto& e : nb_->exceptions) {
     partners[e.p1].push_back(e.p2);
@@ -452,19 +465,36 @@ void Engine::build_static_tiles() {
         m[l] = v;
         any = any || v != 0;
       }
-      int slot = -1, flags = 0;
+      int slot = -1, flags = I == J ? kTileSelf : 0;
       if (any) {
         slot = (int)(masks.size() / 32);
         masks.insert(masks.end(), m, m + 32);
-        flags = kTileHasMask;
+        flags |= kTileHasMask;
       }
-      tiles.push_back(make_int4(I, J, flags, slot));
+      tiles.push_back(make_int4(I, flags, slot, 0));
+      // entries: the 32 slots of block J in its own (shared, unshifted) frame
+      for (int k = 0; k < 32; ++k) {
+        const int s = 32 * J + k < n_ ? 32 * J + k : -1;
+        if (dp_) {
+          entry_d.push_back(make_double4(0.0, 0.0, 0.0, (double)s));
+        } else {
+          float4 e = make_float4(0.f, 0.f, 0.f, 0.f);
+          std::memcpy(&e.w, &s, sizeof(int));
+          entry_f.push_back(e);
+        }
+      }
     }
   const int nt = (int)tiles.size(), nm = (int)(masks.size() / 32);
+  const int nb = n_blocks_;
   OMMB200_CK(cudaMemcpy(a.tiles, tiles.data(), sizeof(int4) * nt, cudaMemcpyHostToDevice));
+  if (dp_)
+    OMMB200_CK(cudaMemcpy(a.entries, entry_d.data(), sizeof(double4) * entry_d.size(), cudaMemcpyHostToDevice));
+  else
+    OMMB200_CK(cudaMemcpy(a.entries, entry_f.data(), sizeof(float4) * entry_f.size(), cudaMemcpyHostToDevice));
   if (nm) OMMB200_CK(cudaMemcpy(a.masks, masks.data(), 4 * masks.size(), cudaMemcpyHostToDevice));
   OMMB200_CK(cudaMemcpy(a.n_tiles, &nt, 4, cudaMemcpyHostToDevice));
   OMMB200_CK(cudaMemcpy(a.n_masks, &nm, 4, cudaMemcpyHostToDevice));
+  OMMB200_CK(cudaMemcpy(a.n_blocks, &nb, 4, cudaMemcpyHostToDevice));
 }
 
 void Engine::setup_bonded() {
@@ -758,8 +788,7 @@ void Engine::enqueue_nonbonded(bool energy, bool direct, bool reciprocal, bool d
   if (direct) {
     prof_begin("pack");
     launch_pack<Real>(n_slots_, nl_.sorted_atom, pos_, nl_.image, nl_.block_center, qscaled_,
-                      posq_, nl_.box, stream_);
-    launch_pack_params<Real>(n_slots_, nl_.sorted_atom, half_sigma_, sqrt_eps_, ljp_, stream_);
+                      half_sigma_, sqrt_eps_, posq_, ljp_, nl_.box, stream_);
     prof_end();
     PairArgs<Real> p{};
     p.n_atoms = n_;
@@ -768,7 +797,7 @@ void Engine::enqueue_nonbonded(bool energy, bool direct, bool reciprocal, bool d
     p.posq = posq_;
     p.ljp = ljp_;
     p.tiles = nl_.tiles;
-    p.tile_shift = nl_.tile_shift;
+    p.entries = nl_.entries;
     p.masks = nl_.masks;
     p.n_tiles = nl_.n_tiles;
     p.tile_capacity = nl_.tile_capacity;
@@ -783,7 +812,8 @@ void Engine::enqueue_nonbonded(bool energy, bool direct, bool reciprocal, bool d
     p.cutoff2_exact = rc * rc;
     p.band = (Real)(rc * rc * (dp_ ? 1e-10 : 1e-4));
     p.alpha = (Real)alpha_;
-    p.alpha2 = (Real)(alpha_ * alpha_);
+    // the FP32 kernel evaluates exp(-alpha^2 r^2) as exp2(-alpha^2 log2(e) r^2)
+    p.exp_scale = (Real)(-alpha_ * alpha_ * (dp_ ? 1.0 : 1.4426950408889634));
     p.two_alpha_sqrtpi = (Real)(2.0 * alpha_ / std::sqrt(kPiD));
     if (elec_ == kElecReactionField) {
       const double eps = nb.reaction_field_dielectric, rc3 = rc * rc * rc;
@@ -1118,6 +1148,22 @@ void Engine::get_state(int flags, uint32_t groups, double* pos, double* vel, dou
   info->potential_energy = need_energy ? pe : 0.0;
   const double vir[9] = {w[0], w[3], w[4], w[3], w[1], w[5], w[4], w[5], w[2]};
   std::copy(vir, vir + 9, info->virial);
+}
+
+void Engine::nlist_stats(int* tiles, int* blocks, int* masked, int64_t* rebuilds) {
+  int v[3] = {0, 0, 0};
+  unsigned long long r = 0;
+  if (nb_) {
+    OMMB200_CK(cudaMemcpyAsync(&v[0], nl_.n_tiles, 4, cudaMemcpyDeviceToHost, stream_));
+    OMMB200_CK(cudaMemcpyAsync(&v[1], nl_.n_blocks, 4, cudaMemcpyDeviceToHost, stream_));
+    OMMB200_CK(cudaMemcpyAsync(&v[2], nl_.n_masks, 4, cudaMemcpyDeviceToHost, stream_));
+    OMMB200_CK(cudaMemcpyAsync(&r, nl_.rebuild_count, 8, cudaMemcpyDeviceToHost, stream_));
+    sync();
+  }
+  if (tiles) *tiles = v[0];
+  if (blocks) *blocks = v[1];
+  if (masked) *masked = v[2];
+  if (rebuilds) *rebuilds = (int64_t)r;
 }
 
 void Engine::pme_parameters(double* alpha, int* nx, int* ny, int* nz) const {

@@ -59,6 +59,7 @@ class Engine {
   void get_state(int flags, uint32_t groups, double* pos, double* vel, double* forces,
                  ommb200_state_info* info);
   void pme_parameters(double* alpha, int* nx, int* ny, int* nz) const;
+  void nlist_stats(int* tiles, int* blocks, int* masked, int64_t* rebuilds);
   int64_t debug_pair_list(int64_t max_pairs, int32_t* pairs);
   void set_profiling(bool enabled);
   struct KernelTime {
@@ -123,7 +124,7 @@ class Engine {
   double* qscaled_ = nullptr;
   double* charge_ = nullptr;
   double* half_sigma_ = nullptr;
-  double* sqrt_eps_ = nullptr;
+  double* sqrt_eps_ = nullptr;  // 2 sqrt(epsilon)
   void* posq_ = nullptr;
   void* ljp_ = nullptr;
   bool params_packed_ = false;

@@ -11,29 +11,36 @@
 namespace ommb200 {
 
 // ---- neighbour tiles -------------------------------------------------------------------
-// A tile is a pair of 32-slot blocks (I <= J) of the spatially sorted particle order.
+// Particles live in 32-slot blocks of a spatially sorted order.  A tile pairs the 32 slots
+// of block I with 32 "entries": either block I itself (self tile) or up to 32 j-particles
+// gathered from blocks J > I, each entry carrying the offset of its block's frame from I's.
 enum TileFlags : int {
   kTileHasMask = 1,    // exclusion/padding mask stored at masks[32 * mask_slot]
   kTilePairImage = 2,  // apply the minimum image per pair (small boxes)
+  kTileSelf = 4,       // entries are block I itself; each pair is seen twice
 };
 
 struct NlistArgs {
   int n_atoms;        // particles of the system
-  int n_blocks;       // ceil(n_atoms / 32)
+  int slot_capacity;  // multiple of 32: N + 31 * columns
   const double* pos;  // [3N] master positions
   double* pos_ref;    // [3N] positions at the last rebuild
   int* image;         // [3N] lattice image n of each particle at the last rebuild
-  int* key;           // [N] Morton key of the particle's voxel
-  int* key_count;     // [n_keys] particles per voxel (zero between rebuilds)
-  int* key_start;     // [n_keys + 1] exclusive scan
-  int* key_cursor;    // [n_keys] scatter cursor (zero between rebuilds)
+  int* column;        // [N] x-y column of each particle
+  float* zkey;        // [N] wrapped z of each particle
+  int* col_count;     // [n_cols] particles per column (zero between rebuilds)
+  int* col_start;     // [n_cols + 1] first slot of each column (columns padded to blocks)
+  int* col_scatter;   // [n_cols + 1] unpadded prefix, for the scatter
+  int* col_cursor;    // [n_cols] scatter cursor (zero between rebuilds)
   int* scratch_atoms; // [N] unordered scatter
-  int* sorted_atom;   // [32 * n_blocks] particle in each slot, -1 for padding
+  int* n_blocks;      // device: blocks in use after the last rebuild
+  int* sorted_atom;   // [slot_capacity] particle in each slot, -1 for padding
   int* atom_slot;     // [N] inverse of sorted_atom
-  double* block_center;  // [3 * n_blocks]
-  double* block_half;    // [3 * n_blocks] half extents of the block's bounding box
-  int4* tiles;           // [tile_capacity] (I, J, flags, mask_slot)
-  void* tile_shift;      // [tile_capacity] float4 / double4 centre offset of J relative to I
+  double* block_center;  // [3 * slot_capacity / 32]
+  double* block_half;    // [3 * slot_capacity / 32] half extents of the bounding box
+  int4* tiles;           // [tile_capacity] (I, flags, mask_slot, 0)
+  void* entries;         // [32 * tile_capacity] float4/double4: shift xyz, slot (as int bits
+                         //   for float4, as a double for double4); slot -1 = padding
   uint32_t* masks;       // [32 * mask_capacity]
   int* n_tiles;          // device counter
   int* n_masks;          // device counter
@@ -41,19 +48,19 @@ struct NlistArgs {
   const int* excl_start;  // [N + 1] CSR of excluded partners (both directions)
   const int* excl_list;
   int* rebuild;           // nonzero: rebuild before the next force evaluation
+  unsigned long long* rebuild_count;
   int* status;
   Box<double> box;
   int periodic;
   double cutoff;      // interaction cutoff (nm)
   double skin;        // Verlet skin (nm)
-  int n_vox[3];       // voxel grid of the sort
-  int morton_bits;
-  int n_keys;
+  double min_width;   // shortest lattice vector bound: min(ax, by, cz)
+  int n_col[2];       // x-y column grid of the sort
+  int n_cols;
+  int col_max;        // largest column the per-column sort accepts
 };
 
-void launch_nlist_rebuild(const NlistArgs& a, bool double_shift, cudaStream_t s);
-// Static list of all block pairs (non-periodic methods); built once.
-void build_all_pairs_tiles(const NlistArgs& a, bool double_shift, cudaStream_t s);
+void launch_nlist_rebuild(const NlistArgs& a, bool double_entries, cudaStream_t s);
 
 // ---- nonbonded pair kernel -------------------------------------------------------------
 enum ElecKind : int { kElecEwald = 0, kElecReactionField = 1, kElecCoulomb = 2 };
@@ -64,9 +71,9 @@ struct PairArgs {
   const int* sorted_atom;
   const double* pos;
   const void* posq;     // [slots] float4/double4: block-local xyz, q * sqrt(ke)
-  const void* ljp;      // [slots] float2/double2: sigma / 2, sqrt(epsilon)
+  const void* ljp;      // [slots] float2/double2: sigma / 2, 2 sqrt(epsilon)
   const int4* tiles;
-  const void* tile_shift;
+  const void* entries;
   const uint32_t* masks;
   const int* n_tiles;
   int tile_capacity;
@@ -79,7 +86,8 @@ struct PairArgs {
   Real cutoff2;
   double cutoff2_exact;
   Real band;            // |r2 - rc2| below this is decided in f64 by the reference formula
-  Real alpha, alpha2, two_alpha_sqrtpi;
+  Real alpha, two_alpha_sqrtpi;
+  Real exp_scale;       // -alpha^2 (times log2 e in the FP32 form, which uses exp2)
   Real krf, crf;
   int use_switching;
   Real switch_r, switch_inv_width;
@@ -92,14 +100,12 @@ template <class Real>
 void launch_pair(const PairArgs<Real>& a, int elec, bool energy, bool dump, int grid,
                  cudaStream_t s);
 
-// Per-step packing of block-local coordinates into the sorted slots.
+// Per-step packing of block-local coordinates and LJ parameters into the sorted slots.
 template <class Real>
 void launch_pack(int n_slots, const int* sorted_atom, const double* pos, const int* image,
-                 const double* block_center, const double* qscaled, void* posq,
-                 const Box<double>& box, cudaStream_t s);
-template <class Real>
-void launch_pack_params(int n_slots, const int* sorted_atom, const double* half_sigma,
-                        const double* sqrt_eps, void* ljp, cudaStream_t s);
+                 const double* block_center, const double* qscaled, const double* half_sigma,
+                 const double* two_sqrt_eps, void* posq, void* ljp, const Box<double>& box,
+                 cudaStream_t s);
 
 // ---- PME -------------------------------------------------------------------------------
 template <class Real>

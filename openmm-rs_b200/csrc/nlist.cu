@@ -2,31 +2,32 @@
 //
 // The reference enumerates candidate pairs from a linked-list cell grid rebuilt at every
 // evaluation (forces/neighbors.rs:96-181) and tests each pair against r^2 < rc^2
-// (forces/nonbonded.rs:862).  Here particles are sorted into 32-slot blocks along a Morton
-// curve of small voxels, block bounding boxes are computed, and every block pair whose boxes
-// come within cutoff + skin becomes a tile.  The list is rebuilt only when some particle has
-// moved more than skin/2 since the last rebuild (the integrator raises `rebuild`), so every
-// pair inside the cutoff at any step in between is covered by a tile; the pair kernel applies
-// the reference's exact cutoff test, which makes the interacting pair set the reference's.
+// (forces/nonbonded.rs:862).  Here the list is rebuilt only when some particle has moved
+// more than skin/2 since the last rebuild (the integrator raises `rebuild`), so every pair
+// inside the cutoff at any step in between is covered; the pair kernel applies the
+// reference's exact cutoff test, which makes the interacting pair set the reference's.
+//
+// Sort: particles are binned into x-y columns about 0.62 nm wide and ordered by z inside
+// each column; every column starts on a 32-slot block boundary, so a block is a compact
+// ~0.6 x 0.6 x 0.7 nm brick.  Ties are broken by particle index, so the slot order (and with
+// it every force sum) is deterministic.
+//
+// Tiles: for every block I, one self tile, then the particles of blocks J > I that lie within
+// cutoff + skin of I's bounding box, packed 32 at a time into neighbour tiles.  Each entry
+// stores the offset of its block's frame from I's frame, so the pair kernel works in small
+// block-local coordinates.  Block pairs too close to a periodic image of themselves are kept
+// whole and flagged for a per-pair minimum image.
 //
 // Every kernel returns at once unless `rebuild` is set, so the sequence can sit in a CUDA
-// graph that is replayed every step.  The sort is a stable counting sort (ties broken by
-// particle index), so the slot order, and with it every force sum, is deterministic.
+// graph that is replayed every step.
 #include "kernels.h"
 
 namespace ommb200 {
 namespace {
 
-__device__ __forceinline__ uint32_t spread_bits(uint32_t v) {
-  v &= 0x3ffu;
-  v = (v | (v << 16)) & 0x030000FFu;
-  v = (v | (v << 8)) & 0x0300F00Fu;
-  v = (v | (v << 4)) & 0x030C30C3u;
-  v = (v | (v << 2)) & 0x09249249u;
-  return v;
-}
+constexpr unsigned kFull = 0xffffffffu;
 
-__global__ void nl_keys(NlistArgs a) {
+__global__ void nl_columns(NlistArgs a) {
   if (*a.rebuild == 0) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i == 0) {
@@ -51,59 +52,109 @@ __global__ void nl_keys(NlistArgs a) {
   a.image[3 * i] = (int)n0;
   a.image[3 * i + 1] = (int)n1;
   a.image[3 * i + 2] = (int)n2;
-  const int vx = min(max((int)(x * b.inv_ax * a.n_vox[0]), 0), a.n_vox[0] - 1);
-  const int vy = min(max((int)(y * b.inv_by * a.n_vox[1]), 0), a.n_vox[1] - 1);
-  const int vz = min(max((int)(z * b.inv_cz * a.n_vox[2]), 0), a.n_vox[2] - 1);
-  const int key = (int)(spread_bits(vx) | (spread_bits(vy) << 1) | (spread_bits(vz) << 2));
-  a.key[i] = key;
-  atomicAdd(&a.key_count[key], 1);
+  const int cx = min(max((int)(x * b.inv_ax * a.n_col[0]), 0), a.n_col[0] - 1);
+  const int cy = min(max((int)(y * b.inv_by * a.n_col[1]), 0), a.n_col[1] - 1);
+  const int col = cy * a.n_col[0] + cx;
+  a.column[i] = col;
+  a.zkey[i] = fmaxf((float)z, 0.0f);
+  atomicAdd(&a.col_count[col], 1);
 }
 
-// Single-CTA exclusive scan of the voxel counts.
-__global__ void __launch_bounds__(1024) nl_scan(NlistArgs a) {
+// Single-CTA scan over the columns: padded slot starts, unpadded scatter starts, block count.
+__global__ void __launch_bounds__(1024) nl_col_scan(NlistArgs a) {
   if (*a.rebuild == 0) return;
-  __shared__ int partial[1024];
+  __shared__ int ps[1024], pu[1024];
   const int t = threadIdx.x;
-  const int chunk = (a.n_keys + 1023) / 1024;
-  const int lo = min(t * chunk, a.n_keys), hi = min(lo + chunk, a.n_keys);
-  int sum = 0;
-  for (int k = lo; k < hi; ++k) sum += a.key_count[k];
-  partial[t] = sum;
+  const int chunk = (a.n_cols + 1023) / 1024;
+  const int lo = min(t * chunk, a.n_cols), hi = min(lo + chunk, a.n_cols);
+  int sp = 0, su = 0;
+  for (int c = lo; c < hi; ++c) {
+    const int n = a.col_count[c];
+    if (n > a.col_max) report_status(a.status, kStatusTileOverflow);
+    sp += (n + 31) & ~31;
+    su += n;
+  }
+  ps[t] = sp;
+  pu[t] = su;
   __syncthreads();
   for (int off = 1; off < 1024; off <<= 1) {
-    int v = t >= off ? partial[t - off] : 0;
+    const int vp = t >= off ? ps[t - off] : 0, vu = t >= off ? pu[t - off] : 0;
     __syncthreads();
-    partial[t] += v;
+    ps[t] += vp;
+    pu[t] += vu;
     __syncthreads();
   }
-  int run = partial[t] - sum;
-  for (int k = lo; k < hi; ++k) {
-    a.key_start[k] = run;
-    run += a.key_count[k];
+  int rp = ps[t] - sp, ru = pu[t] - su;
+  for (int c = lo; c < hi; ++c) {
+    a.col_start[c] = rp;
+    a.col_scatter[c] = ru;
+    const int n = a.col_count[c];
+    rp += (n + 31) & ~31;
+    ru += n;
   }
-  if (t == 1023) a.key_start[a.n_keys] = partial[1023];
+  const int total = min(ps[1023], a.slot_capacity);
+  if (t == 0) {
+    a.col_start[a.n_cols] = total;
+    a.col_scatter[a.n_cols] = pu[1023];
+    *a.n_blocks = total / 32;
+  }
+  for (int s = total + t; s < a.slot_capacity; s += 1024) a.sorted_atom[s] = -1;
 }
 
-__global__ void nl_scatter(NlistArgs a) {
+__global__ void nl_col_scatter(NlistArgs a) {
   if (*a.rebuild == 0) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.n_atoms) return;
-  const int key = a.key[i];
-  const int slot = a.key_start[key] + atomicAdd(&a.key_cursor[key], 1);
-  a.scratch_atoms[slot] = i;
+  const int c = a.column[i];
+  a.scratch_atoms[a.col_scatter[c] + atomicAdd(&a.col_cursor[c], 1)] = i;
 }
 
-// Stable order inside each voxel: rank = number of voxel members with a smaller index.
-__global__ void nl_order(NlistArgs a) {
+// One CTA per column: bitonic sort of (z, particle) keys in shared memory.
+__global__ void __launch_bounds__(256) nl_col_sort(NlistArgs a) {
   if (*a.rebuild == 0) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.n_atoms) return;
-  const int key = a.key[i];
-  const int s0 = a.key_start[key], c = a.key_count[key];
-  int rank = 0;
-  for (int k = 0; k < c; ++k) rank += a.scratch_atoms[s0 + k] < i;
-  a.sorted_atom[s0 + rank] = i;
-  a.atom_slot[i] = s0 + rank;
+  extern __shared__ unsigned long long keys[];
+  const int c = blockIdx.x;
+  const int n = a.col_count[c];
+  if (n > a.col_max || n == 0) return;
+  int m = 1;
+  while (m < n) m <<= 1;
+  const int s0 = a.col_scatter[c];
+  for (int k = threadIdx.x; k < m; k += blockDim.x) {
+    if (k < n) {
+      const int atom = a.scratch_atoms[s0 + k];
+      keys[k] = ((unsigned long long)__float_as_uint(a.zkey[atom]) << 32) | (unsigned)atom;
+    } else {
+      keys[k] = ~0ull;
+    }
+  }
+  __syncthreads();
+  for (int size = 2; size <= m; size <<= 1)
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int k = threadIdx.x; k < m; k += blockDim.x) {
+        const int j = k ^ stride;
+        if (j > k) {
+          const bool up = (k & size) == 0;
+          const unsigned long long x = keys[k], y = keys[j];
+          if ((x > y) == up) {
+            keys[k] = y;
+            keys[j] = x;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  const int base = a.col_start[c];
+  const int padded = (n + 31) & ~31;
+  for (int k = threadIdx.x; k < padded; k += blockDim.x) {
+    if (base + k >= a.slot_capacity) break;
+    if (k < n) {
+      const int atom = (int)(keys[k] & 0xffffffffu);
+      a.sorted_atom[base + k] = atom;
+      a.atom_slot[atom] = base + k;
+    } else {
+      a.sorted_atom[base + k] = -1;
+    }
+  }
 }
 
 // One warp per block: bounding box of the wrapped rebuild positions.
@@ -111,7 +162,7 @@ __global__ void nl_bounds(NlistArgs a) {
   if (*a.rebuild == 0) return;
   const int lane = threadIdx.x & 31;
   const int blk = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (blk >= a.n_blocks) return;
+  if (blk >= *a.n_blocks) return;
   const int atom = a.sorted_atom[32 * blk + lane];
   double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
   if (atom >= 0) {
@@ -124,144 +175,255 @@ __global__ void nl_bounds(NlistArgs a) {
   }
   for (int off = 16; off > 0; off >>= 1)
     for (int d = 0; d < 3; ++d) {
-      lo[d] = fmin(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], off));
-      hi[d] = fmax(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], off));
+      lo[d] = fmin(lo[d], __shfl_xor_sync(kFull, lo[d], off));
+      hi[d] = fmax(hi[d], __shfl_xor_sync(kFull, hi[d], off));
     }
   if (lane == 0)
     for (int d = 0; d < 3; ++d) {
-      a.block_center[3 * blk + d] = 0.5 * (lo[d] + hi[d]);
-      a.block_half[3 * blk + d] = 0.5 * (hi[d] - lo[d]);
+      const bool empty = lo[d] > hi[d];
+      a.block_center[3 * blk + d] = empty ? 0.0 : 0.5 * (lo[d] + hi[d]);
+      a.block_half[3 * blk + d] = empty ? 0.0 : 0.5 * (hi[d] - lo[d]);
     }
 }
 
 __device__ __forceinline__ double box_gap2(const double d[3], const double* hi, const double* hj) {
   double s = 0.0;
   for (int k = 0; k < 3; ++k) {
-    double g = fabs(d[k]) - hi[k] - hj[k];
+    double g = fabs(d[k]) - hi[k] - (hj ? hj[k] : 0.0);
     g = g > 0.0 ? g : 0.0;
     s += g * g;
   }
   return s;
 }
 
-// One thread per block pair (I <= J).
-template <bool kDoubleShift>
-__global__ void nl_tiles(NlistArgs a) {
-  if (*a.rebuild == 0) return;
-  const long long nb = a.n_blocks;
-  const long long total = nb * (nb + 1) / 2;
-  for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < total;
-       p += (long long)gridDim.x * blockDim.x) {
-    // row I holds pairs (I, I..nb-1); rows start at I*nb - I(I-1)/2
-    long long I = (long long)((2.0 * nb + 1.0 - sqrt((2.0 * nb + 1.0) * (2.0 * nb + 1.0) - 8.0 * p)) * 0.5);
-    if (I < 0) I = 0;
-    if (I >= nb) I = nb - 1;
-    while (I > 0 && I * nb - I * (I - 1) / 2 > p) --I;
-    while (I + 1 < nb && (I + 1) * nb - (I + 1) * I / 2 <= p) ++I;
-    const long long J = I + (p - (I * nb - I * (I - 1) / 2));
-    const double* ci = a.block_center + 3 * I;
-    const double* cj = a.block_center + 3 * J;
-    const double* hi = a.block_half + 3 * I;
-    const double* hj = a.block_half + 3 * J;
-    double d[3] = {cj[0] - ci[0], cj[1] - ci[1], cj[2] - ci[2]};
-    const Box<double>& b = a.box;
-    if (a.periodic) min_image_fast(d[0], d[1], d[2], b);
-    const double reach = a.cutoff + a.skin;
-    const double ri = sqrt(hi[0] * hi[0] + hi[1] * hi[1] + hi[2] * hi[2]);
-    const double rj = sqrt(hj[0] * hj[0] + hj[1] * hj[1] + hj[2] * hj[2]);
-    bool safe = true;
-    double best = box_gap2(d, hi, hj);
-    if (a.periodic) {
-      const double need = reach + ri + rj;
-      for (int m0 = -1; m0 <= 1; ++m0)
-        for (int m1 = -1; m1 <= 1; ++m1)
-          for (int m2 = -1; m2 <= 1; ++m2) {
-            if (m0 == 0 && m1 == 0 && m2 == 0) continue;
-            const double e[3] = {d[0] + m0 * b.ax + m1 * b.bx + m2 * b.cx,
-                                 d[1] + m1 * b.by + m2 * b.cy, d[2] + m2 * b.cz};
-            if (e[0] * e[0] + e[1] * e[1] + e[2] * e[2] < need * need) safe = false;
-            best = fmin(best, box_gap2(e, hi, hj));
-          }
-    }
-    const double gap2 = safe ? box_gap2(d, hi, hj) : best;
-    if (I != J && gap2 >= reach * reach) continue;
-    const int t = atomicAdd(a.n_tiles, 1);
-    if (t >= a.tile_capacity) {
-      report_status(a.status, kStatusTileOverflow);
-      continue;
-    }
-    a.tiles[t] = make_int4((int)I, (int)J, safe ? 0 : kTilePairImage, -1);
-    if (kDoubleShift)
-      reinterpret_cast<double4*>(a.tile_shift)[t] = make_double4(d[0], d[1], d[2], 0.0);
-    else
-      reinterpret_cast<float4*>(a.tile_shift)[t] =
-          make_float4((float)d[0], (float)d[1], (float)d[2], 0.0f);
+// Mask of lane l over 32 entry slots: bit k set when entry k is padding or an exclusion
+// partner of the lane's particle; all bits when the lane itself is padding.
+__device__ __forceinline__ uint32_t entry_mask(const NlistArgs& a, int ai, const int* slots) {
+  if (ai < 0) return kFull;
+  uint32_t m = 0;
+  for (int k = 0; k < 32; ++k)
+    if (slots[k] < 0) m |= 1u << k;
+  for (int e = a.excl_start[ai]; e < a.excl_start[ai + 1]; ++e) {
+    const int sp = a.atom_slot[a.excl_list[e]];
+    for (int k = 0; k < 32; ++k)
+      if (slots[k] == sp) m |= 1u << k;
   }
+  return m;
 }
 
-// One warp per tile: exclusion and padding masks (bit m of lane l: skip pair (l, m)).
-__global__ void nl_masks(NlistArgs a) {
-  if (*a.rebuild == 0) return;
-  const int lane = threadIdx.x & 31;
-  const int nt = min(*a.n_tiles, a.tile_capacity);
-  for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < nt;
-       t += (gridDim.x * blockDim.x) >> 5) {
-    const int4 tile = a.tiles[t];
-    const int ai = a.sorted_atom[32 * tile.x + lane];
-    const int aj = a.sorted_atom[32 * tile.y + lane];
-    uint32_t mask = __ballot_sync(0xffffffffu, aj < 0);
-    if (ai < 0) {
-      mask = 0xffffffffu;
+// Reserve a tile (and a mask slot if any lane needs one) and write its header and masks.
+__device__ __forceinline__ int commit_tile(const NlistArgs& a, int I, int flags, uint32_t mask,
+                                           int lane) {
+  int t = 0;
+  if (lane == 0) t = atomicAdd(a.n_tiles, 1);
+  t = __shfl_sync(kFull, t, 0);
+  if (t >= a.tile_capacity) {
+    if (lane == 0) report_status(a.status, kStatusTileOverflow);
+    return -1;
+  }
+  int slot = -1;
+  if (__any_sync(kFull, mask != 0)) {
+    if (lane == 0) slot = atomicAdd(a.n_masks, 1);
+    slot = __shfl_sync(kFull, slot, 0);
+    if (slot < a.mask_capacity) {
+      a.masks[32 * slot + lane] = mask;
+      flags |= kTileHasMask;
     } else {
-      for (int k = a.excl_start[ai]; k < a.excl_start[ai + 1]; ++k) {
-        const int s = a.atom_slot[a.excl_list[k]];
-        if ((s >> 5) == tile.y) mask |= 1u << (s & 31);
+      if (lane == 0) report_status(a.status, kStatusTileOverflow);
+      slot = -1;
+    }
+  }
+  if (lane == 0) a.tiles[t] = make_int4(I, flags, slot, 0);
+  return t;
+}
+
+template <bool kDouble>
+__device__ __forceinline__ void write_entry(const NlistArgs& a, int t, int lane, int slot,
+                                            const double* sh) {
+  if (kDouble)
+    reinterpret_cast<double4*>(a.entries)[32 * t + lane] =
+        make_double4(sh[0], sh[1], sh[2], (double)slot);
+  else
+    reinterpret_cast<float4*>(a.entries)[32 * t + lane] =
+        make_float4((float)sh[0], (float)sh[1], (float)sh[2], __int_as_float(slot));
+}
+
+constexpr int kListWarps = 4;
+
+// One warp per block I: self tile, then neighbour tiles of up to 32 gathered particles.
+template <bool kDouble>
+__global__ void __launch_bounds__(32 * kListWarps) nl_lists(NlistArgs a) {
+  if (*a.rebuild == 0) return;
+  __shared__ int s_slot[kListWarps][64];
+  __shared__ int s_flag[kListWarps][64];
+  __shared__ double s_shift[kListWarps][64][3];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int nb = *a.n_blocks;
+  const double reach = a.cutoff + a.skin;
+  const double reach2 = reach * reach;
+  const int warps = gridDim.x * kListWarps;
+  for (int I = blockIdx.x * kListWarps + w; I < nb; I += warps) {
+    const double ci[3] = {a.block_center[3 * I], a.block_center[3 * I + 1], a.block_center[3 * I + 2]};
+    const double hi[3] = {a.block_half[3 * I], a.block_half[3 * I + 1], a.block_half[3 * I + 2]};
+    const double ri = sqrt(hi[0] * hi[0] + hi[1] * hi[1] + hi[2] * hi[2]);
+    const int ai = a.sorted_atom[32 * I + lane];
+    // self tile
+    {
+      s_slot[w][lane] = ai < 0 ? -1 : 32 * I + lane;
+      __syncwarp();
+      uint32_t m = entry_mask(a, ai, s_slot[w]);
+      const bool image = a.periodic && a.min_width < reach + 2.0 * ri;
+      commit_tile(a, I, kTileSelf | (image ? kTilePairImage : 0), m, lane);
+      __syncwarp();
+    }
+    int pending = 0;
+    auto flush = [&](int count) {
+      const int slot = lane < count ? s_slot[w][lane] : -1;
+      const int f = __reduce_or_sync(kFull, lane < count ? s_flag[w][lane] : 0);
+      if (lane >= count) s_slot[w][lane] = -1;
+      __syncwarp();
+      const uint32_t m = entry_mask(a, ai, s_slot[w]);
+      const int t = commit_tile(a, I, f, m, lane);
+      double sh[3] = {0.0, 0.0, 0.0};
+      if (lane < count)
+        for (int d = 0; d < 3; ++d) sh[d] = s_shift[w][lane][d];
+      if (t >= 0) write_entry<kDouble>(a, t, lane, slot, sh);
+      __syncwarp();
+    };
+    for (int base = I + 1; base < nb; base += 32) {
+      const int J = base + lane;
+      bool cand = false, unsafe = false;
+      double d[3] = {0.0, 0.0, 0.0};
+      if (J < nb) {
+        const double* cj = a.block_center + 3 * J;
+        const double* hj = a.block_half + 3 * J;
+        d[0] = cj[0] - ci[0];
+        d[1] = cj[1] - ci[1];
+        d[2] = cj[2] - ci[2];
+        double gap2 = 0.0;
+        if (a.periodic) {
+          min_image_fast(d[0], d[1], d[2], a.box);
+          const double rj = sqrt(hj[0] * hj[0] + hj[1] * hj[1] + hj[2] * hj[2]);
+          const double dist = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+          // every other image is at least min_width - |d| away (reduced box); when that is
+          // not enough to rule the other images out, all 27 images are tested
+          unsafe = a.min_width - dist < reach + ri + rj;
+        }
+        gap2 = box_gap2(d, hi, hj);
+        if (unsafe) {
+          const Box<double>& b = a.box;
+          for (int m0 = -1; m0 <= 1; ++m0)
+            for (int m1 = -1; m1 <= 1; ++m1)
+              for (int m2 = -1; m2 <= 1; ++m2) {
+                const double e[3] = {d[0] + m0 * b.ax + m1 * b.bx + m2 * b.cx,
+                                     d[1] + m1 * b.by + m2 * b.cy, d[2] + m2 * b.cz};
+                gap2 = fmin(gap2, box_gap2(e, hi, hj));
+              }
+        }
+        cand = gap2 < reach2;
+      }
+      unsigned cm = __ballot_sync(kFull, cand);
+      while (cm) {
+        const int src = __ffs(cm) - 1;
+        cm &= cm - 1;
+        const int Jc = base + src;
+        const double s0 = __shfl_sync(kFull, d[0], src), s1 = __shfl_sync(kFull, d[1], src),
+                     s2 = __shfl_sync(kFull, d[2], src);
+        const bool un = __shfl_sync(kFull, unsafe, src);
+        const int aj = a.sorted_atom[32 * Jc + lane];
+        bool in = false;
+        if (aj >= 0) {
+          const Box<double>& b = a.box;
+          const double n0 = a.image[3 * aj], n1 = a.image[3 * aj + 1], n2 = a.image[3 * aj + 2];
+          const double* cj = a.block_center + 3 * Jc;
+          double rel[3] = {a.pos_ref[3 * aj] - (n0 * b.ax + n1 * b.bx + n2 * b.cx) - cj[0] + s0,
+                           a.pos_ref[3 * aj + 1] - (n1 * b.by + n2 * b.cy) - cj[1] + s1,
+                           a.pos_ref[3 * aj + 2] - n2 * b.cz - cj[2] + s2};
+          if (un) {
+            // conservative: the nearest image of the particle to I's centre, against a
+            // sphere that contains I's box
+            min_image_fast(rel[0], rel[1], rel[2], b);
+            const double r = sqrt(rel[0] * rel[0] + rel[1] * rel[1] + rel[2] * rel[2]);
+            in = r < reach + ri + 1e-6;
+          } else {
+            in = box_gap2(rel, hi, nullptr) < reach2;
+          }
+        }
+        const unsigned im = __ballot_sync(kFull, in);
+        if (in) {
+          const int p = pending + __popc(im & ((1u << lane) - 1u));
+          s_slot[w][p] = 32 * Jc + lane;
+          s_flag[w][p] = un ? kTilePairImage : 0;
+          s_shift[w][p][0] = s0;
+          s_shift[w][p][1] = s1;
+          s_shift[w][p][2] = s2;
+        }
+        pending += __popc(im);
+        __syncwarp();
+        if (pending >= 32) {
+          flush(32);
+          const int rest = pending - 32;
+          int sl = 0, fl = 0;
+          double sh0 = 0.0, sh1 = 0.0, sh2 = 0.0;
+          if (lane < rest) {
+            sl = s_slot[w][32 + lane];
+            fl = s_flag[w][32 + lane];
+            sh0 = s_shift[w][32 + lane][0];
+            sh1 = s_shift[w][32 + lane][1];
+            sh2 = s_shift[w][32 + lane][2];
+          }
+          __syncwarp();
+          if (lane < rest) {
+            s_slot[w][lane] = sl;
+            s_flag[w][lane] = fl;
+            s_shift[w][lane][0] = sh0;
+            s_shift[w][lane][1] = sh1;
+            s_shift[w][lane][2] = sh2;
+          }
+          pending = rest;
+          __syncwarp();
+        }
       }
     }
-    if (__any_sync(0xffffffffu, mask != 0)) {
-      int slot = 0;
-      if (lane == 0) slot = atomicAdd(a.n_masks, 1);
-      slot = __shfl_sync(0xffffffffu, slot, 0);
-      if (slot < a.mask_capacity) {
-        a.masks[32 * slot + lane] = mask;
-        if (lane == 0) a.tiles[t] = make_int4(tile.x, tile.y, tile.z | kTileHasMask, slot);
-      } else if (lane == 0) {
-        report_status(a.status, kStatusTileOverflow);
-      }
-    }
+    if (pending > 0) flush(pending);
   }
 }
 
 __global__ void nl_finish(NlistArgs a) {
   if (*a.rebuild == 0) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  for (int k = i; k < a.n_keys; k += gridDim.x * blockDim.x) {
-    a.key_count[k] = 0;
-    a.key_cursor[k] = 0;
+  for (int k = i; k < a.n_cols; k += gridDim.x * blockDim.x) {
+    a.col_count[k] = 0;
+    a.col_cursor[k] = 0;
   }
 }
 
-__global__ void nl_clear_flag(int* rebuild) { *rebuild = 0; }
+__global__ void nl_clear_flag(NlistArgs a) {
+  if (*a.rebuild == 0) return;
+  *a.rebuild = 0;
+  *a.rebuild_count += 1;
+}
 
 }  // namespace
 
-void launch_nlist_rebuild(const NlistArgs& a, bool double_shift, cudaStream_t s) {
+void launch_nlist_rebuild(const NlistArgs& a, bool double_entries, cudaStream_t s) {
   const int tb = 256;
   const int ga = ceil_div(a.n_atoms, tb);
-  nl_keys<<<ga, tb, 0, s>>>(a);
-  nl_scan<<<1, 1024, 0, s>>>(a);
-  nl_scatter<<<ga, tb, 0, s>>>(a);
-  nl_order<<<ga, tb, 0, s>>>(a);
-  nl_bounds<<<ceil_div((long long)a.n_blocks * 32, tb), tb, 0, s>>>(a);
-  const long long pairs = (long long)a.n_blocks * (a.n_blocks + 1) / 2;
-  const int gt = (int)std::min<long long>((pairs + tb - 1) / tb, 148LL * 64);
-  if (double_shift)
-    nl_tiles<true><<<gt, tb, 0, s>>>(a);
+  const int block_cap = a.slot_capacity / 32;
+  nl_columns<<<ga, tb, 0, s>>>(a);
+  nl_col_scan<<<1, 1024, 0, s>>>(a);
+  nl_col_scatter<<<ga, tb, 0, s>>>(a);
+  int m = 1;
+  while (m < a.col_max) m <<= 1;
+  nl_col_sort<<<a.n_cols, 256, sizeof(unsigned long long) * m, s>>>(a);
+  nl_bounds<<<ceil_div((long long)block_cap * 32, tb), tb, 0, s>>>(a);
+  const int gl = ceil_div(block_cap, kListWarps);
+  if (double_entries)
+    nl_lists<true><<<gl, 32 * kListWarps, 0, s>>>(a);
   else
-    nl_tiles<false><<<gt, tb, 0, s>>>(a);
-  nl_masks<<<148 * 8, tb, 0, s>>>(a);
-  nl_finish<<<std::min(ceil_div(a.n_keys, tb), 148 * 4), tb, 0, s>>>(a);
-  nl_clear_flag<<<1, 1, 0, s>>>(a.rebuild);
+    nl_lists<false><<<gl, 32 * kListWarps, 0, s>>>(a);
+  nl_finish<<<std::max(1, std::min(ceil_div(a.n_cols, tb), 148 * 4)), tb, 0, s>>>(a);
+  nl_clear_flag<<<1, 1, 0, s>>>(a);
 }
 
 }  // namespace ommb200

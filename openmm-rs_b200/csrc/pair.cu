@@ -2,12 +2,13 @@
 // Ewald-screened, reaction-field or bare Coulomb, following forces/nonbonded.rs:842-924 and
 // the pair functions at nonbonded.rs:1194-1288.
 //
-// One warp evaluates one 32x32 tile.  Lane l owns i-particle l of block I; the j-particles
-// of block J start in lane l and rotate one lane per step (warp shuffles) together with the
-// force they accumulate, so after 32 steps every (i, j) pair was seen once and each j-force
-// is back in its own lane.  Diagonal tiles (I == J) read partners by shuffle and keep only
-// i-forces, visiting each pair twice at half energy.  Forces are summed in `Real` within the
-// tile and committed as 64-bit fixed point, which makes the total independent of tile order.
+// One warp evaluates one tile: lane l owns i-particle l of block I; the tile's 32 j-entries
+// are staged in shared memory and lane l visits entry (l + k) mod 32 at step k, so every
+// (i, j) pair is seen once in 32 steps with conflict-free shared-memory reads.  The force on
+// each j-entry travels with the entry: it is rotated one lane per step by a warp shuffle and
+// is back in lane j after 32 steps.  Self tiles (entries = block I) visit each pair from both
+// sides and keep only i-forces, at half energy.  Forces are summed in `Real` within a tile and
+// committed as 64-bit fixed point, so the total does not depend on tile order.
 //
 // Pair membership reproduces the reference exactly: pairs whose squared distance falls
 // within `band` of rc^2 are re-decided from the f64 master positions with the reference's
@@ -30,16 +31,41 @@ struct V4<double> {
   using T2 = double2;
 };
 
-__device__ __forceinline__ float rsqrt_r(float x) { return rsqrtf(x); }
+// Approximate SFU forms for the FP32 kernel; exact library forms for the FP64 kernel.
+__device__ __forceinline__ float rsqrt_r(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
 __device__ __forceinline__ double rsqrt_r(double x) { return rsqrt(x); }
-__device__ __forceinline__ float exp_r(float x) { return __expf(x); }
-__device__ __forceinline__ double exp_r(double x) { return exp(x); }
-__device__ __forceinline__ float erfc_r(float x, float ex) { return erfc_fit(x, ex); }
-__device__ __forceinline__ double erfc_r(double x, double) { return erfc(x); }
+__device__ __forceinline__ float rcp_r(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float exp2_r(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// erfc(x) = exp(-x^2) P(1 / (1 + 0.46 x)), own least-squares fit (csrc/fit_erfc.py).
+__device__ __forceinline__ float erfc_poly(float x) {
+  const float t = rcp_r(fmaf(0.46f, x, 1.0f));
+  float p = 0.10014041224442242f;
+  p = fmaf(p, t, -0.504550213499043f);
+  p = fmaf(p, t, 0.8277608617691994f);
+  p = fmaf(p, t, -0.35775472734883446f);
+  p = fmaf(p, t, 0.4707476000236329f);
+  p = fmaf(p, t, 0.1949991373822864f);
+  p = fmaf(p, t, 0.2692933367874065f);
+  p = fmaf(p, t, -0.0006363939510855f);
+  return p;
+}
 
 // The reference's cutoff decision for particles a, b (original indices).
-__device__ __noinline__ bool exact_inside(const double* pos, int a, int b, int periodic,
-                                          const Box<double>& box, double rc2) {
+__device__ __forceinline__ bool exact_inside(const double* pos, int a, int b, int periodic,
+                                             const Box<double>& box, double rc2) {
   const int i = a < b ? a : b, j = a < b ? b : a;
   double dx = __dsub_rn(pos[3 * j], pos[3 * i]);
   double dy = __dsub_rn(pos[3 * j + 1], pos[3 * i + 1]);
@@ -49,163 +75,171 @@ __device__ __noinline__ bool exact_inside(const double* pos, int a, int b, int p
   return r2 < rc2;
 }
 
-template <class Real, int kElec, bool kEnergy>
-struct PairResult {
-  Real f_over_r;  // dE/dr / r
-  Real energy;
-};
-
-template <class Real, int kElec, bool kEnergy>
-__device__ __forceinline__ PairResult<Real, kElec, kEnergy> pair_terms(
-    const PairArgs<Real>& a, Real r2, Real qq, Real sig, Real eps) {
+// dE/dr / r and E of one pair; `eps4` = 4 sqrt(eps_i eps_j), `sig` = (sigma_i + sigma_j) / 2.
+template <class Real, int kElec, bool kEnergy, bool kSwitch>
+__device__ __forceinline__ void pair_terms(const PairArgs<Real>& a, Real r2, Real qq, Real sig,
+                                           Real eps4, Real& f_over_r, Real& energy) {
   const Real inv_r = rsqrt_r(r2);
   const Real inv_r2 = inv_r * inv_r;
   // LJ 12-6 (nonbonded.rs:1203-1214)
   const Real s2 = sig * sig * inv_r2;
   const Real s6 = s2 * s2 * s2;
-  const Real eps4 = Real(4) * eps;
-  Real f_lj = eps4 * (Real(6) * s6 - Real(12) * s6 * s6) * inv_r2;
-  Real e_lj = eps4 * (s6 * s6 - s6);
-  if (eps == Real(0)) {
+  Real f_lj = eps4 * s6 * fma(Real(-12), s6, Real(6)) * inv_r2;
+  Real e_lj = kEnergy ? eps4 * s6 * (s6 - Real(1)) : Real(0);
+  if (eps4 == Real(0)) {
     f_lj = Real(0);
     e_lj = Real(0);
   }
   // switching (nonbonded.rs:888-900)
-  if (a.use_switching) {
+  if (kSwitch) {
     const Real r = r2 * inv_r;
     if (r > a.switch_r) {
+      const Real e_full = eps4 * s6 * (s6 - Real(1));
       const Real t = (r - a.switch_r) * a.switch_inv_width;
       const Real sw = Real(1) + t * t * t * (Real(-10) + t * (Real(15) - Real(6) * t));
       const Real dsw = Real(-30) * t * t * (Real(1) - t) * (Real(1) - t) * a.switch_inv_width;
-      f_lj = sw * f_lj + e_lj * dsw * inv_r;
-      e_lj *= sw;
+      f_lj = sw * f_lj + (eps4 == Real(0) ? Real(0) : e_full) * dsw * inv_r;
+      e_lj = kEnergy ? e_lj * sw : Real(0);
     }
   }
-  Real f_el, e_el;
+  Real f_el, e_el = Real(0);
   if (kElec == kElecEwald) {
     // screened_coulomb (nonbonded.rs:1263-1273)
     const Real r = r2 * inv_r;
-    const Real ex = exp_r(-a.alpha2 * r2);
-    const Real ec = erfc_r(a.alpha * r, ex);
-    e_el = qq * ec * inv_r;
-    f_el = -qq * (ec * inv_r + a.two_alpha_sqrtpi * ex) * inv_r2;
+    Real ex, ec;
+    if constexpr (sizeof(Real) == 4) {
+      ex = exp2_r(a.exp_scale * r2);
+      ec = ex * erfc_poly(a.alpha * r);
+    } else {
+      ex = exp(a.exp_scale * r2);
+      ec = erfc(a.alpha * r);
+    }
+    f_el = -qq * fma(ec, inv_r, a.two_alpha_sqrtpi * ex) * inv_r2;
+    if (kEnergy) e_el = qq * ec * inv_r;
   } else if (kElec == kElecReactionField) {
     // reaction_field (nonbonded.rs:1222-1243)
-    e_el = qq * (inv_r + a.krf * r2 - a.crf);
     f_el = qq * (Real(2) * a.krf - inv_r * inv_r2);
+    if (kEnergy) e_el = qq * (inv_r + a.krf * r2 - a.crf);
   } else {
     // coulomb_pair (nonbonded.rs:1186-1192)
-    e_el = qq * inv_r;
     f_el = -qq * inv_r * inv_r2;
+    if (kEnergy) e_el = qq * inv_r;
   }
-  PairResult<Real, kElec, kEnergy> res;
-  res.f_over_r = f_lj + f_el;
-  res.energy = kEnergy ? e_lj + e_el : Real(0);
-  return res;
+  f_over_r = f_lj + f_el;
+  energy = e_lj + e_el;
 }
 
-template <class Real, int kElec, bool kEnergy, bool kDump>
-__global__ void __launch_bounds__(128) pair_kernel(const PairArgs<Real> a) {
+constexpr int kPairWarps = 4;
+
+template <class Real, int kElec, bool kEnergy, bool kDump, bool kSwitch>
+__global__ void __launch_bounds__(32 * kPairWarps) pair_kernel(const PairArgs<Real> a) {
   using T4 = typename V4<Real>::T4;
   using T2 = typename V4<Real>::T2;
-  const unsigned FULL = 0xffffffffu;
-  const int lane = threadIdx.x & 31;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  constexpr unsigned FULL = 0xffffffffu;
+  __shared__ T4 s_pos[kPairWarps][32];
+  __shared__ T2 s_lj[kPairWarps][32];
+  __shared__ int s_atom[kPairWarps][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int warp = blockIdx.x * kPairWarps + w;
+  const int nwarps = gridDim.x * kPairWarps;
   const int nt = min(*a.n_tiles, a.tile_capacity);
   const T4* posq = reinterpret_cast<const T4*>(a.posq);
   const T2* ljp = reinterpret_cast<const T2*>(a.ljp);
-  const T4* shifts = reinterpret_cast<const T4*>(a.tile_shift);
+  const T4* entries = reinterpret_cast<const T4*>(a.entries);
   long long e_fixed = 0;
   long long w_fixed[6] = {0, 0, 0, 0, 0, 0};
 
   for (int t = warp; t < nt; t += nwarps) {
     const int4 tile = a.tiles[t];
-    const int I = tile.x, J = tile.y;
-    const int si = 32 * I + lane, sj = 32 * J + lane;
+    const int I = tile.x;
+    const bool self = (tile.y & kTileSelf) != 0;
+    const bool pair_image = (tile.y & kTilePairImage) != 0;
+    const int si = 32 * I + lane;
     const T4 pi = posq[si];
     const T2 li = ljp[si];
-    T4 pj = posq[sj];
-    T2 lj = ljp[sj];
-    const T4 sh = shifts[t];
-    pj.x += sh.x;
-    pj.y += sh.y;
-    pj.z += sh.z;
-    const uint32_t excl = (tile.z & kTileHasMask) ? a.masks[32 * tile.w + lane] : 0u;
-    const bool pair_image = (tile.z & kTilePairImage) != 0;
     const int ai = a.sorted_atom[si];
+    const uint32_t excl = (tile.y & kTileHasMask) ? a.masks[32 * tile.z + lane] : 0u;
+    int aj = ai;
+    if (self) {
+      s_pos[w][lane] = pi;
+      s_lj[w][lane] = li;
+    } else {
+      const T4 e = entries[32 * t + lane];
+      int slot;
+      if constexpr (sizeof(Real) == 4) slot = __float_as_int(e.w);
+      else slot = (int)e.w;
+      T4 pj;
+      T2 lj;
+      if (slot >= 0) {
+        pj = posq[slot];
+        lj = ljp[slot];
+        aj = a.sorted_atom[slot];
+      } else {
+        pj.x = pj.y = pj.z = pj.w = Real(0);
+        lj.x = lj.y = Real(0);
+        aj = -1;
+      }
+      pj.x += e.x;
+      pj.y += e.y;
+      pj.z += e.z;
+      s_pos[w][lane] = pj;
+      s_lj[w][lane] = lj;
+    }
+    s_atom[w][lane] = aj;
+    __syncwarp();
     Real fix = 0, fiy = 0, fiz = 0, fjx = 0, fjy = 0, fjz = 0;
     double e_tile = 0.0;
     double w_tile[6] = {0, 0, 0, 0, 0, 0};
-    const bool diag = (I == J);
-    for (int k = diag ? 1 : 0; k < 32; ++k) {
+#pragma unroll 4
+    for (int k = self ? 1 : 0; k < 32; ++k) {
       const int jl = (lane + k) & 31;
-      Real xj, yj, zj, qj, sj_, ej;
-      if (diag) {
-        xj = __shfl_sync(FULL, pj.x, jl);
-        yj = __shfl_sync(FULL, pj.y, jl);
-        zj = __shfl_sync(FULL, pj.z, jl);
-        qj = __shfl_sync(FULL, pj.w, jl);
-        sj_ = __shfl_sync(FULL, lj.x, jl);
-        ej = __shfl_sync(FULL, lj.y, jl);
-      } else {
-        xj = pj.x;
-        yj = pj.y;
-        zj = pj.z;
-        qj = pj.w;
-        sj_ = lj.x;
-        ej = lj.y;
-      }
-      Real dx = xj - pi.x, dy = yj - pi.y, dz = zj - pi.z;
+      const T4 pj = s_pos[w][jl];
+      const T2 lj = s_lj[w][jl];
+      Real dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
       if (pair_image) min_image_fast(dx, dy, dz, a.box);
       Real r2 = dx * dx + dy * dy + dz * dz;
       bool use = ((excl >> jl) & 1u) == 0u;
-      if (a.use_cutoff && use) {
+      if (a.use_cutoff) {
         bool inside = r2 < a.cutoff2;
-        if (fabs(r2 - a.cutoff2) < a.band) {
-          const int aj = a.sorted_atom[32 * J + jl];
-          inside = ai >= 0 && aj >= 0 &&
-                   exact_inside(a.pos, ai, aj, a.periodic, a.box_exact, a.cutoff2_exact);
+        if (fabs(r2 - a.cutoff2) < a.band && use) {
+          const int b = s_atom[w][jl];
+          inside = ai >= 0 && b >= 0 &&
+                   exact_inside(a.pos, ai, b, a.periodic, a.box_exact, a.cutoff2_exact);
         }
-        use = inside;
+        use = use && inside;
       }
-      const int aj_dump = kDump ? a.sorted_atom[32 * J + jl] : 0;
-      if (kDump && use && ai >= 0 && aj_dump >= 0 && (!diag || ai < aj_dump)) {
-        const int aj = aj_dump;
-        const unsigned long long slot = atomicAdd(a.pair_count, 1ull);
-        if ((long long)slot < a.pair_capacity) {
-          a.pair_dump[2 * slot] = ai < aj ? ai : aj;
-          a.pair_dump[2 * slot + 1] = ai < aj ? aj : ai;
+      if (kDump && use) {
+        const int b = s_atom[w][jl];
+        if (ai >= 0 && b >= 0 && (!self || ai < b)) {
+          const unsigned long long slot = atomicAdd(a.pair_count, 1ull);
+          if ((long long)slot < a.pair_capacity) {
+            a.pair_dump[2 * slot] = ai < b ? ai : b;
+            a.pair_dump[2 * slot + 1] = ai < b ? b : ai;
+          }
         }
       }
-      if (!use) r2 = Real(1);
-      const auto res = pair_terms<Real, kElec, kEnergy>(a, r2, pi.w * qj, li.x + sj_, li.y * ej);
-      const Real fo = use ? res.f_over_r : Real(0);
-      const Real fx = fo * dx, fy = fo * dy, fz = fo * dz;
-      fix += fx;
-      fiy += fy;
-      fiz += fz;
+      Real fo, en;
+      pair_terms<Real, kElec, kEnergy, kSwitch>(a, use ? r2 : Real(1), pi.w * pj.w, li.x + lj.x,
+                                                li.y * lj.y, fo, en);
+      fo = use ? fo : Real(0);
+      fix = fma(fo, dx, fix);
+      fiy = fma(fo, dy, fiy);
+      fiz = fma(fo, dz, fiz);
       if (kEnergy && use) {
-        const double scale = diag ? 0.5 : 1.0;
-        e_tile += scale * (double)res.energy;
-        w_tile[0] -= scale * (double)(fx * dx);
-        w_tile[1] -= scale * (double)(fy * dy);
-        w_tile[2] -= scale * (double)(fz * dz);
-        w_tile[3] -= scale * (double)(fx * dy);
-        w_tile[4] -= scale * (double)(fx * dz);
-        w_tile[5] -= scale * (double)(fy * dz);
+        const double scale = self ? 0.5 : 1.0;
+        e_tile += scale * (double)en;
+        w_tile[0] -= scale * (double)(fo * dx * dx);
+        w_tile[1] -= scale * (double)(fo * dy * dy);
+        w_tile[2] -= scale * (double)(fo * dz * dz);
+        w_tile[3] -= scale * (double)(fo * dx * dy);
+        w_tile[4] -= scale * (double)(fo * dx * dz);
+        w_tile[5] -= scale * (double)(fo * dy * dz);
       }
-      if (!diag) {
-        fjx -= fx;
-        fjy -= fy;
-        fjz -= fz;
+      if (!self) {
+        fjx = fma(-fo, dx, fjx);
+        fjy = fma(-fo, dy, fjy);
+        fjz = fma(-fo, dz, fjz);
         const int src = (lane + 1) & 31;
-        pj.x = __shfl_sync(FULL, pj.x, src);
-        pj.y = __shfl_sync(FULL, pj.y, src);
-        pj.z = __shfl_sync(FULL, pj.z, src);
-        pj.w = __shfl_sync(FULL, pj.w, src);
-        lj.x = __shfl_sync(FULL, lj.x, src);
-        lj.y = __shfl_sync(FULL, lj.y, src);
         fjx = __shfl_sync(FULL, fjx, src);
         fjy = __shfl_sync(FULL, fjy, src);
         fjz = __shfl_sync(FULL, fjz, src);
@@ -217,24 +251,24 @@ __global__ void __launch_bounds__(128) pair_kernel(const PairArgs<Real> a) {
       add_fixed(a.force + a.n_atoms + ai, to_fixed(fiy, fscale));
       add_fixed(a.force + 2 * a.n_atoms + ai, to_fixed(fiz, fscale));
     }
-    if (!diag) {
-      const int aj = a.sorted_atom[sj];
-      if (aj >= 0) {
-        add_fixed(a.force + aj, to_fixed(fjx, fscale));
-        add_fixed(a.force + a.n_atoms + aj, to_fixed(fjy, fscale));
-        add_fixed(a.force + 2 * a.n_atoms + aj, to_fixed(fjz, fscale));
-      }
+    if (!self && aj >= 0) {
+      add_fixed(a.force + aj, to_fixed(fjx, fscale));
+      add_fixed(a.force + a.n_atoms + aj, to_fixed(fjy, fscale));
+      add_fixed(a.force + 2 * a.n_atoms + aj, to_fixed(fjz, fscale));
     }
     if (kEnergy) {
+      // one fixed-point rounding per tile: reduce the tile's partial sums across the warp in
+      // f64 first (a fixed order, so the result stays deterministic)
+      for (int off = 16; off > 0; off >>= 1) {
+        e_tile += __shfl_xor_sync(FULL, e_tile, off);
+        for (int c = 0; c < 6; ++c) w_tile[c] += __shfl_xor_sync(FULL, w_tile[c], off);
+      }
       e_fixed += to_fixed(e_tile, kEnergyScale);
       for (int c = 0; c < 6; ++c) w_fixed[c] += to_fixed(w_tile[c], kEnergyScale);
     }
+    __syncwarp();
   }
   if (kEnergy) {
-    for (int off = 16; off > 0; off >>= 1) {
-      e_fixed += __shfl_xor_sync(FULL, e_fixed, off);
-      for (int c = 0; c < 6; ++c) w_fixed[c] += __shfl_xor_sync(FULL, w_fixed[c], off);
-    }
     if (lane == 0) {
       add_fixed(a.energy, e_fixed);
       for (int c = 0; c < 6; ++c) add_fixed(a.energy + 1 + c, w_fixed[c]);
@@ -245,13 +279,17 @@ __global__ void __launch_bounds__(128) pair_kernel(const PairArgs<Real> a) {
 template <class Real>
 __global__ void pack_kernel(int n_slots, const int* sorted_atom, const double* pos,
                             const int* image, const double* block_center, const double* qscaled,
-                            typename V4<Real>::T4* posq, Box<double> b) {
+                            const double* half_sigma, const double* two_sqrt_eps,
+                            typename V4<Real>::T4* posq, typename V4<Real>::T2* ljp,
+                            Box<double> b) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n_slots) return;
   const int a = sorted_atom[s];
   typename V4<Real>::T4 out;
+  typename V4<Real>::T2 lj;
   if (a < 0) {
     out.x = out.y = out.z = out.w = Real(0);
+    lj.x = lj.y = Real(0);
   } else {
     const double n0 = image[3 * a], n1 = image[3 * a + 1], n2 = image[3 * a + 2];
     const double* c = block_center + 3 * (s >> 5);
@@ -259,20 +297,11 @@ __global__ void pack_kernel(int n_slots, const int* sorted_atom, const double* p
     out.y = (Real)(pos[3 * a + 1] - (n1 * b.by + n2 * b.cy) - c[1]);
     out.z = (Real)(pos[3 * a + 2] - n2 * b.cz - c[2]);
     out.w = (Real)qscaled[a];
+    lj.x = (Real)half_sigma[a];
+    lj.y = (Real)two_sqrt_eps[a];
   }
   posq[s] = out;
-}
-
-template <class Real>
-__global__ void pack_params_kernel(int n_slots, const int* sorted_atom, const double* half_sigma,
-                                   const double* sqrt_eps, typename V4<Real>::T2* ljp) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= n_slots) return;
-  const int a = sorted_atom[s];
-  typename V4<Real>::T2 out;
-  out.x = a < 0 ? Real(0) : (Real)half_sigma[a];
-  out.y = a < 0 ? Real(0) : (Real)sqrt_eps[a];
-  ljp[s] = out;
+  ljp[s] = lj;
 }
 
 }  // namespace
@@ -280,50 +309,50 @@ __global__ void pack_params_kernel(int n_slots, const int* sorted_atom, const do
 template <class Real>
 void launch_pair(const PairArgs<Real>& a, int elec, bool energy, bool dump, int grid,
                  cudaStream_t s) {
-#define OMMB200_PAIR(E, EN, D) pair_kernel<Real, E, EN, D><<<grid, 128, 0, s>>>(a)
+#define OMMB200_PAIR(E, EN, D, SW) pair_kernel<Real, E, EN, D, SW><<<grid, 32 * kPairWarps, 0, s>>>(a)
+#define OMMB200_PAIR_SW(E, EN, D)     \
+  if (a.use_switching)                \
+    OMMB200_PAIR(E, EN, D, true);     \
+  else                                \
+    OMMB200_PAIR(E, EN, D, false)
+#define OMMB200_PAIR_E(EN, D)                                      \
+  if (elec == kElecEwald) {                                        \
+    OMMB200_PAIR_SW(kElecEwald, EN, D);                            \
+  } else if (elec == kElecReactionField) {                         \
+    OMMB200_PAIR_SW(kElecReactionField, EN, D);                    \
+  } else {                                                         \
+    OMMB200_PAIR_SW(kElecCoulomb, EN, D);                          \
+  }
   if (dump) {
-    if (elec == kElecEwald) OMMB200_PAIR(kElecEwald, false, true);
-    else if (elec == kElecReactionField) OMMB200_PAIR(kElecReactionField, false, true);
-    else OMMB200_PAIR(kElecCoulomb, false, true);
-    return;
-  }
-  if (energy) {
-    if (elec == kElecEwald) OMMB200_PAIR(kElecEwald, true, false);
-    else if (elec == kElecReactionField) OMMB200_PAIR(kElecReactionField, true, false);
-    else OMMB200_PAIR(kElecCoulomb, true, false);
+    OMMB200_PAIR_E(false, true)
+  } else if (energy) {
+    OMMB200_PAIR_E(true, false)
   } else {
-    if (elec == kElecEwald) OMMB200_PAIR(kElecEwald, false, false);
-    else if (elec == kElecReactionField) OMMB200_PAIR(kElecReactionField, false, false);
-    else OMMB200_PAIR(kElecCoulomb, false, false);
+    OMMB200_PAIR_E(false, false)
   }
+#undef OMMB200_PAIR_E
+#undef OMMB200_PAIR_SW
 #undef OMMB200_PAIR
 }
 
 template <class Real>
 void launch_pack(int n_slots, const int* sorted_atom, const double* pos, const int* image,
-                 const double* block_center, const double* qscaled, void* posq,
-                 const Box<double>& box, cudaStream_t s) {
+                 const double* block_center, const double* qscaled, const double* half_sigma,
+                 const double* two_sqrt_eps, void* posq, void* ljp, const Box<double>& box,
+                 cudaStream_t s) {
   pack_kernel<Real><<<ceil_div(n_slots, 256), 256, 0, s>>>(
-      n_slots, sorted_atom, pos, image, block_center, qscaled,
-      reinterpret_cast<typename V4<Real>::T4*>(posq), box);
-}
-
-template <class Real>
-void launch_pack_params(int n_slots, const int* sorted_atom, const double* half_sigma,
-                        const double* sqrt_eps, void* ljp, cudaStream_t s) {
-  pack_params_kernel<Real><<<ceil_div(n_slots, 256), 256, 0, s>>>(
-      n_slots, sorted_atom, half_sigma, sqrt_eps, reinterpret_cast<typename V4<Real>::T2*>(ljp));
+      n_slots, sorted_atom, pos, image, block_center, qscaled, half_sigma, two_sqrt_eps,
+      reinterpret_cast<typename V4<Real>::T4*>(posq), reinterpret_cast<typename V4<Real>::T2*>(ljp),
+      box);
 }
 
 template void launch_pair<float>(const PairArgs<float>&, int, bool, bool, int, cudaStream_t);
 template void launch_pair<double>(const PairArgs<double>&, int, bool, bool, int, cudaStream_t);
 template void launch_pack<float>(int, const int*, const double*, const int*, const double*,
-                                 const double*, void*, const Box<double>&, cudaStream_t);
+                                 const double*, const double*, const double*, void*, void*,
+                                 const Box<double>&, cudaStream_t);
 template void launch_pack<double>(int, const int*, const double*, const int*, const double*,
-                                  const double*, void*, const Box<double>&, cudaStream_t);
-template void launch_pack_params<float>(int, const int*, const double*, const double*, void*,
-                                        cudaStream_t);
-template void launch_pack_params<double>(int, const int*, const double*, const double*, void*,
-                                         cudaStream_t);
+                                  const double*, const double*, const double*, void*, void*,
+                                  const Box<double>&, cudaStream_t);
 
 }  // namespace ommb200

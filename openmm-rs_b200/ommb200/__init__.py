@@ -535,6 +535,14 @@ class Context:
     def set_profiling(self, enabled: bool) -> None:
         _check(library().ommb200_context_set_profiling(self._h, int(enabled)))
 
+    def nlist_stats(self) -> dict:
+        """Neighbour-list state: tiles, blocks and masked tiles in use, rebuilds so far."""
+        t, b, m, r = C.c_int(), C.c_int(), C.c_int(), C.c_int64()
+        _check(library().ommb200_context_nlist_stats(self._h, C.byref(t), C.byref(b), C.byref(m),
+                                                     C.byref(r)))
+        return {"tiles": t.value, "blocks": b.value, "masked_tiles": m.value,
+                "rebuilds": r.value}
+
     def stream_handle(self) -> int:
         """cudaStream_t (as an integer) that every kernel of this Context runs on."""
         s = C.c_void_p()
