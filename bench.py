@@ -147,7 +147,12 @@ def build_context(precision, seed, device):
                           precision=precision, device=device)
     ctx.set_positions(x)
     ctx.set_velocities(v)
+    TUNED[precision] = ctx.autotune(200) if TUNE else None
     return w, ctx
+
+
+TUNE = True
+TUNED = {}
 
 
 def time_segments(ctx, torch, segments, md_steps, flush):
@@ -294,9 +299,10 @@ def run_reference(args):
 
 def main():
     args = parse()
-    global EQUILIBRATION_STEPS
+    global EQUILIBRATION_STEPS, TUNE
     if args.no_equilibrate:
         EQUILIBRATION_STEPS = 0
+        TUNE = False
     if args.impl == "reference":
         run_reference(args)
         return
@@ -419,7 +425,8 @@ def main():
                    "md_steps_per_bench_step": args.segment,
                    "l2": "flushed (256 MiB write) between timed bench steps; MD steps inside a "
                          "bench step run back to back",
-                   "parallelism": f"replicas x{world}"},
+                   "parallelism": f"replicas x{world}",
+                   "autotuned": TUNED.get(args.precision)},
         "e2e": {"value": e2e_value, "unit": "ns/day", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,

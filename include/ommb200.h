@@ -186,6 +186,12 @@ int ommb200_context_step(ommb200_context* ctx, int steps);
 int ommb200_context_get_state(ommb200_context* ctx, int flags, uint32_t groups,
                               double* positions, double* velocities, double* forces,
                               ommb200_state_info* info);
+/* Autotuner (no reference counterpart): times trial_steps MD steps from the current state
+ * for each candidate Verlet skin (which sets the neighbour-list rebuild interval) and
+ * pair-kernel grid, keeps the fastest and restores positions, velocities and the random
+ * stream, so the trajectory is unchanged.  Outputs may be NULL. */
+int ommb200_context_autotune(ommb200_context* ctx, int trial_steps, double* skin,
+                             int* pair_ctas_per_sm, double* ms_per_step);
 /* PME parameters frozen at Context creation (nonbonded.rs:1078-1106). */
 int ommb200_context_get_pme_parameters(const ommb200_context* ctx, double* alpha, int* nx,
                                        int* ny, int* nz);

@@ -567,6 +567,13 @@ int ommb200_context_kernel_times(ommb200_context* ctx, int max_entries, char* na
     }
   });
 }
+int ommb200_context_autotune(ommb200_context* ctx, int trial_steps, double* skin,
+                             int* pair_ctas_per_sm, double* ms_per_step) {
+  return guarded([&] {
+    OMMB200_CTX;
+    E.autotune(trial_steps, skin, pair_ctas_per_sm, ms_per_step);
+  });
+}
 int ommb200_context_nlist_stats(ommb200_context* ctx, int* tiles, int* blocks, int* masked,
                                 int64_t* rebuilds) {
   return guarded([&] {

@@ -196,6 +196,9 @@ Engine::Engine(std::unique_ptr<SystemDef> system, std::unique_ptr<IntegratorDef>
   require(opt_.device >= 0 && opt_.device < devices, "CUDA device ordinal out of range");
   OMMB200_CK(cudaSetDevice(opt_.device));
   OMMB200_CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+  OMMB200_CK(cudaStreamCreateWithFlags(&pme_stream_, cudaStreamNonBlocking));
+  OMMB200_CK(cudaEventCreateWithFlags(&fork_ev_, cudaEventDisableTiming));
+  OMMB200_CK(cudaEventCreateWithFlags(&join_ev_, cudaEventDisableTiming));
   if (integ_->random_seed != 0) {
     seed_ = (uint32_t)integ_->random_seed;
   } else {
@@ -250,6 +253,9 @@ Engine::~Engine() {
     cudaEventDestroy(p.stop);
   }
   for (auto e : event_pool_) cudaEventDestroy(e);
+  if (fork_ev_) cudaEventDestroy(fork_ev_);
+  if (join_ev_) cudaEventDestroy(join_ev_);
+  if (pme_stream_) cudaStreamDestroy(pme_stream_);
   if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -370,7 +376,8 @@ void Engine::setup_nonbonded(const NonbondedDef& nb) {
     a.col_cursor = mem_.alloc<int>(a.n_cols);
     a.scratch_atoms = mem_.alloc<int>(n_);
     const long long blocks = a.slot_capacity / 32;
-    const double reach = nb.cutoff + skin_;
+    // sized for the largest skin the autotuner may pick
+    const double reach = nb.cutoff + std::max(skin_, kMaxTunedSkin);
     const double wx = box_[0] / a.n_col[0], wy = box_[4] / a.n_col[1];
     const double hz = 32.0 / (density * wx * wy);
     const double gathered = density * (wx + 2 * reach) * (wy + 2 * reach) * (hz + 2 * reach) / 2.0;
@@ -406,6 +413,7 @@ void Engine::setup_nonbonded(const NonbondedDef& nb) {
   if (!nb_periodic_) build_static_tiles();
   int dev_sms = 148;
   cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, opt_.device);
+  sm_count_ = dev_sms;
   pair_grid_ = dev_sms * 8;
 
   if (nb_pme_) {
@@ -785,6 +793,14 @@ void Engine::enqueue_nonbonded(bool energy, bool direct, bool reciprocal, bool d
     launch_nlist_rebuild(nl_, dp_, stream_);
     prof_end();
   }
+  // fork: PME on its own stream (serialised on the main stream while profiling, so that
+  // per-kernel events time one kernel at a time)
+  const bool pme = reciprocal && nb_pme_;
+  cudaStream_t ps = (pme && !profiling_) ? pme_stream_ : stream_;
+  if (ps != stream_) {
+    OMMB200_CK(cudaEventRecord(fork_ev_, stream_));
+    OMMB200_CK(cudaStreamWaitEvent(ps, fork_ev_, 0));
+  }
   if (direct) {
     prof_begin("pack");
     launch_pack<Real>(n_slots_, nl_.sorted_atom, pos_, nl_.image, nl_.block_center, qscaled_,
@@ -862,11 +878,13 @@ void Engine::enqueue_nonbonded(bool energy, bool direct, bool reciprocal, bool d
     m.alpha = alpha_;
     m.volume = volume_;
     prof_begin("pme_spread");
-    launch_pme_spread<Real>(m, stream_);
+    launch_pme_spread<Real>(m, ps);
     prof_end();
     prof_begin("pme_convert");
-    launch_pme_convert<Real>(m, stream_);
+    launch_pme_convert<Real>(m, ps);
     prof_end();
+    OMMB200_CKFFT(cufftSetStream(fft_fwd_, ps));
+    OMMB200_CKFFT(cufftSetStream(fft_inv_, ps));
     prof_begin("pme_fft_forward");
     if (dp_)
       OMMB200_CKFFT(cufftExecD2Z(fft_fwd_, (cufftDoubleReal*)pme_real_, (cufftDoubleComplex*)pme_k_));
@@ -874,7 +892,7 @@ void Engine::enqueue_nonbonded(bool energy, bool direct, bool reciprocal, bool d
       OMMB200_CKFFT(cufftExecR2C(fft_fwd_, (cufftReal*)pme_real_, (cufftComplex*)pme_k_));
     prof_end();
     prof_begin("pme_convolve");
-    launch_pme_convolve<Real>(m, energy, stream_);
+    launch_pme_convolve<Real>(m, energy, ps);
     prof_end();
     prof_begin("pme_fft_inverse");
     if (dp_)
@@ -883,7 +901,7 @@ void Engine::enqueue_nonbonded(bool energy, bool direct, bool reciprocal, bool d
       OMMB200_CKFFT(cufftExecC2R(fft_inv_, (cufftComplex*)pme_k_, (cufftReal*)pme_real_));
     prof_end();
     prof_begin("pme_gather");
-    launch_pme_gather<Real>(m, stream_);
+    launch_pme_gather<Real>(m, ps);
     prof_end();
   }
   if (direct && n_exceptions_) {
@@ -902,6 +920,10 @@ void Engine::enqueue_nonbonded(bool energy, bool direct, bool reciprocal, bool d
     prof_begin("exceptions");
     launch_exceptions(e, energy, stream_);
     prof_end();
+  }
+  if (ps != stream_) {  // join
+    OMMB200_CK(cudaEventRecord(join_ev_, ps));
+    OMMB200_CK(cudaStreamWaitEvent(stream_, join_ev_, 0));
   }
 }
 
@@ -1148,6 +1170,88 @@ void Engine::get_state(int flags, uint32_t groups, double* pos, double* vel, dou
   info->potential_energy = need_energy ? pe : 0.0;
   const double vir[9] = {w[0], w[3], w[4], w[3], w[1], w[5], w[4], w[5], w[2]};
   std::copy(vir, vir + 9, info->virial);
+}
+
+void Engine::autotune(int trial_steps, double* skin_out, int* ctas_out, double* ms_out) {
+  require(trial_steps > 0, "autotune needs a positive number of trial steps");
+  const size_t bytes = 24 * (size_t)n_;
+  double* save_x = mem_.alloc<double>(3 * (size_t)n_);
+  double* save_v = mem_.alloc<double>(3 * (size_t)n_);
+  unsigned long long rng = 0;
+  OMMB200_CK(cudaMemcpyAsync(save_x, pos_, bytes, cudaMemcpyDeviceToDevice, stream_));
+  OMMB200_CK(cudaMemcpyAsync(save_v, vel_, bytes, cudaMemcpyDeviceToDevice, stream_));
+  OMMB200_CK(cudaMemcpyAsync(&rng, rng_step_, 8, cudaMemcpyDeviceToHost, stream_));
+  sync();
+  const double time0 = time_;
+  const int64_t steps0 = step_count_;
+  const bool prof = profiling_;
+  profiling_ = false;
+  cudaEvent_t t0, t1;
+  OMMB200_CK(cudaEventCreate(&t0));
+  OMMB200_CK(cudaEventCreate(&t1));
+  auto restore = [&]() {
+    OMMB200_CK(cudaMemcpyAsync(pos_, save_x, bytes, cudaMemcpyDeviceToDevice, stream_));
+    OMMB200_CK(cudaMemcpyAsync(vel_, save_v, bytes, cudaMemcpyDeviceToDevice, stream_));
+    OMMB200_CK(cudaMemcpyAsync(rng_step_, &rng, 8, cudaMemcpyHostToDevice, stream_));
+    const int one = 1;
+    OMMB200_CK(cudaMemcpyAsync(rebuild_, &one, sizeof(int), cudaMemcpyHostToDevice, stream_));
+    sync();
+    time_ = time0;
+    step_count_ = steps0;
+  };
+  auto trial = [&](double skin, int ctas) {
+    skin_ = skin;
+    nl_.skin = skin;
+    pair_grid_ = sm_count_ * ctas;
+    destroy_graph();
+    restore();
+    step(std::min(trial_steps, 40));  // warm-up, builds the graph
+    OMMB200_CK(cudaEventRecord(t0, stream_));
+    step(trial_steps);
+    OMMB200_CK(cudaEventRecord(t1, stream_));
+    OMMB200_CK(cudaEventSynchronize(t1));
+    float ms = 0.f;
+    OMMB200_CK(cudaEventElapsedTime(&ms, t0, t1));
+    return (double)ms / trial_steps;
+  };
+  double best_skin = skin_, best_ms = 1e30;
+  int best_ctas = pair_grid_ / std::max(1, sm_count_);
+  try {
+    if (nb_ && nb_periodic_) {
+      for (double s : kTunedSkins) {
+        const double ms = trial(s, best_ctas);
+        if (ms < best_ms) {
+          best_ms = ms;
+          best_skin = s;
+        }
+      }
+    }
+    if (nb_) {
+      for (int c : kTunedPairCtasPerSm) {
+        const double ms = trial(best_skin, c);
+        if (ms < best_ms) {
+          best_ms = ms;
+          best_ctas = c;
+        }
+      }
+    }
+  } catch (...) {
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    profiling_ = prof;
+    throw;
+  }
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  skin_ = best_skin;
+  nl_.skin = best_skin;
+  pair_grid_ = sm_count_ * best_ctas;
+  destroy_graph();
+  restore();
+  profiling_ = prof;
+  if (skin_out) *skin_out = best_skin;
+  if (ctas_out) *ctas_out = best_ctas;
+  if (ms_out) *ms_out = best_ms;
 }
 
 void Engine::nlist_stats(int* tiles, int* blocks, int* masked, int64_t* rebuilds) {

@@ -17,6 +17,11 @@ namespace ommb200 {
 // Owns every device allocation of an Engine; memory is zeroed on allocation.
 double measure_fp32_peak(int device);  // diagnostics.cu
 
+// Verlet skins and pair-kernel CTAs per SM the autotuner tries.
+constexpr double kTunedSkins[] = {0.06, 0.08, 0.1, 0.13, 0.16, 0.2};
+constexpr double kMaxTunedSkin = 0.2;
+constexpr int kTunedPairCtasPerSm[] = {4, 6, 8, 12};
+
 class DeviceArena {
  public:
   ~DeviceArena();
@@ -60,6 +65,10 @@ class Engine {
                  ommb200_state_info* info);
   void pme_parameters(double* alpha, int* nx, int* ny, int* nz) const;
   void nlist_stats(int* tiles, int* blocks, int* masked, int64_t* rebuilds);
+  // Times `trial_steps` MD steps for each candidate skin and pair-kernel grid from the
+  // current state, keeps the fastest, and restores the state (positions, velocities, RNG
+  // counter), so the trajectory is the same as without tuning.
+  void autotune(int trial_steps, double* skin, int* pair_ctas_per_sm, double* ms_per_step);
   int64_t debug_pair_list(int64_t max_pairs, int32_t* pairs);
   void set_profiling(bool enabled);
   struct KernelTime {
@@ -100,6 +109,10 @@ class Engine {
   uint64_t seed_ = 0;
   uint64_t velocity_draws_ = 0;
   cudaStream_t stream_ = nullptr;
+  // PME runs on its own stream, forked after the neighbour-list rebuild and joined before
+  // the integrator, so it overlaps the real-space pair kernel (also inside the CUDA graph).
+  cudaStream_t pme_stream_ = nullptr;
+  cudaEvent_t fork_ev_ = nullptr, join_ev_ = nullptr;
   DeviceArena mem_;
 
   // state
@@ -148,6 +161,7 @@ class Engine {
   long long dump_capacity_ = 0;
   bool dump_mode_ = false;
   int pair_grid_ = 0;
+  int sm_count_ = 148;
 
   // bonded terms, one launch per force
   struct BondedLaunch {

@@ -535,6 +535,14 @@ class Context:
     def set_profiling(self, enabled: bool) -> None:
         _check(library().ommb200_context_set_profiling(self._h, int(enabled)))
 
+    def autotune(self, trial_steps: int = 200) -> dict:
+        """Pick the Verlet skin and pair-kernel grid by timing `trial_steps` MD steps per
+        candidate; the state is restored afterwards."""
+        skin, ctas, ms = C.c_double(), C.c_int(), C.c_double()
+        _check(library().ommb200_context_autotune(self._h, int(trial_steps), C.byref(skin),
+                                                  C.byref(ctas), C.byref(ms)))
+        return {"skin_nm": skin.value, "pair_ctas_per_sm": ctas.value, "ms_per_step": ms.value}
+
     def nlist_stats(self) -> dict:
         """Neighbour-list state: tiles, blocks and masked tiles in use, rebuilds so far."""
         t, b, m, r = C.c_int(), C.c_int(), C.c_int(), C.c_int64()

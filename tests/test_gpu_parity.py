@@ -300,6 +300,25 @@ def equilibrated_water(name="water-1944", steps=3000):
     return w, st.positions, st.velocities
 
 
+def test_autotune_keeps_the_trajectory():
+    w = water("water-1944")
+    out = []
+    for tune in (False, True):
+        ctx = make_context(w, "mixed", seed=21)
+        ctx.set_velocities_to_temperature(300.0, seed=6)
+        if tune:
+            t = ctx.autotune(40)
+            assert 0.05 < t["skin_nm"] <= 0.2 and t["pair_ctas_per_sm"] in (4, 6, 8, 12)
+        ctx.step(30)
+        st = ctx.get_state(positions=True, velocities=True)
+        out.append((st.positions, st.velocities, st.step_count))
+    # the skin changes how pairs are grouped into tiles (so float summation order), never
+    # which pairs interact or the random stream: the trajectories agree to rounding
+    assert np.abs(out[0][0] - out[1][0]).max() < 1e-6
+    assert np.abs(out[0][1] - out[1][1]).max() < 1e-3
+    assert out[0][2] == out[1][2] == 30
+
+
 def test_thermostat_temperature():
     w, x, v = equilibrated_water()
     ctx = ommb200.Context(systems.water_system(w), systems.langevin(friction=5.0, seed=8),
