@@ -196,6 +196,22 @@ int ommb200_context_autotune(ommb200_context* ctx, int trial_steps, double* skin
 int ommb200_context_get_pme_parameters(const ommb200_context* ctx, double* alpha, int* nx,
                                        int* ny, int* nz);
 
+/* ---- allocation-free force evaluation (no counterpart in the reference) ----
+ * For callers that must not allocate device memory: code inside another framework's memory
+ * pool, a plugin that may only use the buffers it is handed, or a stream being captured into a
+ * CUDA graph.  Evaluates NonbondedForce forces and energy of a non-periodic system without
+ * exceptions (method OMMB200_NO_CUTOFF or OMMB200_CUTOFF_NON_PERIODIC) with the Context's
+ * mixed-precision arithmetic.  All pointers are device pointers on the current device:
+ * positions[3n], charges[n], sigmas[n], epsilons[n] in; forces[3n] and energy[1] out.  Work is
+ * enqueued on `stream` (a cudaStream_t; NULL = legacy default stream) and not synchronised.
+ * n is at most 8192: the scratch is a 384 KiB static device array that every GPU loading the
+ * library keeps until exit.  The first call on a device looks up that array's address; make it
+ * before any stream capture.  Calls share the array, so calls that overlap on the GPU race. */
+int ommb200_nonbonded_forces_noalloc(int n, const double* positions, const double* charges,
+                                     const double* sigmas, const double* epsilons, int method,
+                                     double cutoff, double reaction_field_dielectric,
+                                     double* forces, double* energy, void* stream);
+
 /* ---- diagnostics (no reference counterpart) ---- */
 /* The interacting nonbonded pair set at the current positions, as evaluated by the pair
  * kernel itself: (i, j) with i < j in original particle indices, unsorted.  Writes up to

@@ -588,6 +588,15 @@ int ommb200_context_get_stream(ommb200_context* ctx, void** stream) {
     *stream = (void*)E.stream();
   });
 }
+int ommb200_nonbonded_forces_noalloc(int n, const double* positions, const double* charges,
+                                     const double* sigmas, const double* epsilons, int method,
+                                     double cutoff, double reaction_field_dielectric,
+                                     double* forces, double* energy, void* stream) {
+  return guarded([&] {
+    nonbonded_forces_noalloc(n, positions, charges, sigmas, epsilons, method, cutoff,
+                             reaction_field_dielectric, forces, energy, (cudaStream_t)stream);
+  });
+}
 int ommb200_measure_fp32_peak(int device, double* tflops) {
   return guarded([&] {
     require(tflops != nullptr, "null output pointer");

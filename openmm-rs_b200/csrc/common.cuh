@@ -112,7 +112,9 @@ __device__ __forceinline__ float erfc_fit(float x, float expmx2) {
 // ------------------------------------------------------------------------------------------
 __host__ __device__ __forceinline__ void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
   const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u, W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#ifdef __CUDA_ARCH__
 #pragma unroll
+#endif
   for (int r = 0; r < 10; ++r) {
     const uint64_t p0 = (uint64_t)M0 * c[0];
     const uint64_t p1 = (uint64_t)M1 * c[2];

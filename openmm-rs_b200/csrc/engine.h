@@ -16,6 +16,10 @@ namespace ommb200 {
 
 // Owns every device allocation of an Engine; memory is zeroed on allocation.
 double measure_fp32_peak(int device);  // diagnostics.cu
+// noalloc.cu: NonbondedForce forces with scratch in a static device array (no allocation)
+void nonbonded_forces_noalloc(int n, const double* pos, const double* q, const double* sigma,
+                              const double* eps, int method, double cutoff, double rf_dielectric,
+                              double* forces, double* energy, cudaStream_t stream);
 
 // Verlet skins and pair-kernel CTAs per SM the autotuner tries.
 constexpr double kTunedSkins[] = {0.06, 0.08, 0.1, 0.13, 0.16, 0.2};

@@ -14,120 +14,10 @@
 // within `band` of rc^2 are re-decided from the f64 master positions with the reference's
 // minimum-image and r^2 < rc^2 arithmetic (explicitly rounded, no fused multiply-add).
 #include "kernels.h"
+#include "pair_math.cuh"
 
 namespace ommb200 {
 namespace {
-
-template <class Real>
-struct V4;
-template <>
-struct V4<float> {
-  using T4 = float4;
-  using T2 = float2;
-};
-template <>
-struct V4<double> {
-  using T4 = double4;
-  using T2 = double2;
-};
-
-// Approximate SFU forms for the FP32 kernel; exact library forms for the FP64 kernel.
-__device__ __forceinline__ float rsqrt_r(float x) {
-  float y;
-  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-  return y;
-}
-__device__ __forceinline__ double rsqrt_r(double x) { return rsqrt(x); }
-__device__ __forceinline__ float rcp_r(float x) {
-  float y;
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-  return y;
-}
-__device__ __forceinline__ float exp2_r(float x) {
-  float y;
-  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-  return y;
-}
-
-// erfc(x) = exp(-x^2) P(1 / (1 + 0.46 x)), own least-squares fit (csrc/fit_erfc.py).
-__device__ __forceinline__ float erfc_poly(float x) {
-  const float t = rcp_r(fmaf(0.46f, x, 1.0f));
-  float p = 0.10014041224442242f;
-  p = fmaf(p, t, -0.504550213499043f);
-  p = fmaf(p, t, 0.8277608617691994f);
-  p = fmaf(p, t, -0.35775472734883446f);
-  p = fmaf(p, t, 0.4707476000236329f);
-  p = fmaf(p, t, 0.1949991373822864f);
-  p = fmaf(p, t, 0.2692933367874065f);
-  p = fmaf(p, t, -0.0006363939510855f);
-  return p;
-}
-
-// The reference's cutoff decision for particles a, b (original indices).
-__device__ __forceinline__ bool exact_inside(const double* pos, int a, int b, int periodic,
-                                             const Box<double>& box, double rc2) {
-  const int i = a < b ? a : b, j = a < b ? b : a;
-  double dx = __dsub_rn(pos[3 * j], pos[3 * i]);
-  double dy = __dsub_rn(pos[3 * j + 1], pos[3 * i + 1]);
-  double dz = __dsub_rn(pos[3 * j + 2], pos[3 * i + 2]);
-  if (periodic) min_image_exact(dx, dy, dz, box);
-  const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
-  return r2 < rc2;
-}
-
-// dE/dr / r and E of one pair; `eps4` = 4 sqrt(eps_i eps_j), `sig` = (sigma_i + sigma_j) / 2.
-template <class Real, int kElec, bool kEnergy, bool kSwitch>
-__device__ __forceinline__ void pair_terms(const PairArgs<Real>& a, Real r2, Real qq, Real sig,
-                                           Real eps4, Real& f_over_r, Real& energy) {
-  const Real inv_r = rsqrt_r(r2);
-  const Real inv_r2 = inv_r * inv_r;
-  // LJ 12-6 (nonbonded.rs:1203-1214)
-  const Real s2 = sig * sig * inv_r2;
-  const Real s6 = s2 * s2 * s2;
-  Real f_lj = eps4 * s6 * fma(Real(-12), s6, Real(6)) * inv_r2;
-  Real e_lj = kEnergy ? eps4 * s6 * (s6 - Real(1)) : Real(0);
-  if (eps4 == Real(0)) {
-    f_lj = Real(0);
-    e_lj = Real(0);
-  }
-  // switching (nonbonded.rs:888-900)
-  if (kSwitch) {
-    const Real r = r2 * inv_r;
-    if (r > a.switch_r) {
-      const Real e_full = eps4 * s6 * (s6 - Real(1));
-      const Real t = (r - a.switch_r) * a.switch_inv_width;
-      const Real sw = Real(1) + t * t * t * (Real(-10) + t * (Real(15) - Real(6) * t));
-      const Real dsw = Real(-30) * t * t * (Real(1) - t) * (Real(1) - t) * a.switch_inv_width;
-      f_lj = sw * f_lj + (eps4 == Real(0) ? Real(0) : e_full) * dsw * inv_r;
-      e_lj = kEnergy ? e_lj * sw : Real(0);
-    }
-  }
-  Real f_el, e_el = Real(0);
-  if (kElec == kElecEwald) {
-    // screened_coulomb (nonbonded.rs:1263-1273)
-    const Real r = r2 * inv_r;
-    Real ex, ec;
-    if constexpr (sizeof(Real) == 4) {
-      ex = exp2_r(a.exp_scale * r2);
-      ec = ex * erfc_poly(a.alpha * r);
-    } else {
-      ex = exp(a.exp_scale * r2);
-      ec = erfc(a.alpha * r);
-    }
-    f_el = -qq * fma(ec, inv_r, a.two_alpha_sqrtpi * ex) * inv_r2;
-    if (kEnergy) e_el = qq * ec * inv_r;
-  } else if (kElec == kElecReactionField) {
-    // reaction_field (nonbonded.rs:1222-1243)
-    f_el = qq * (Real(2) * a.krf - inv_r * inv_r2);
-    if (kEnergy) e_el = qq * (inv_r + a.krf * r2 - a.crf);
-  } else {
-    // coulomb_pair (nonbonded.rs:1186-1192)
-    f_el = -qq * inv_r * inv_r2;
-    if (kEnergy) e_el = qq * inv_r;
-  }
-  f_over_r = f_lj + f_el;
-  energy = e_lj + e_el;
-}
 
 constexpr int kPairWarps = 4;
 
