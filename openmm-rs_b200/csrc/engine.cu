@@ -228,13 +228,17 @@ Engine::Engine(std::unique_ptr<SystemDef> system, std::unique_ptr<IntegratorDef>
         nb = static_cast<const NonbondedDef*>(f.get());
         break;
       case kGbsaObc:
-        throw Error(OMMB200_ERR_UNSUPPORTED, "GBSAOBCForce is not yet available in this engine");
+        require(gb_def_ == nullptr, "only one GBSAOBCForce per System is supported",
+                OMMB200_ERR_UNSUPPORTED);
+        gb_def_ = static_cast<const GbsaObcDef*>(f.get());
+        break;
       default:
         break;
     }
     require(f->force_group >= 0 && f->force_group < 32, "force group must be in 0..31");
   }
   if (nb) setup_nonbonded(*nb);
+  if (gb_def_) setup_gbsa(*gb_def_);
   setup_bonded();
   setup_integrator();
   update_box_dependents();
@@ -560,6 +564,82 @@ void Engine::setup_bonded() {
   }
 }
 
+// gbsa_obc.rs:313-343 (initialize) + device layout: identity slot order, one segment, every
+// block pair of the segment as a tile.
+void Engine::setup_gbsa(const GbsaObcDef& g) {
+  require((int)g.charge.size() == n_, "GBSA particle count must match System");
+  for (int i = 0; i < n_; ++i) {
+    require(std::isfinite(g.charge[i]), "GBSA charges must be finite");
+    require(std::isfinite(g.radius[i]) && g.radius[i] > 0.0, "GBSA radii must be positive and finite");
+    require(std::isfinite(g.scale[i]) && g.scale[i] > 0.0,
+            "GBSA scaling factors must be positive and finite");
+  }
+  require(std::isfinite(g.solvent_dielectric) && std::isfinite(g.solute_dielectric) &&
+              std::isfinite(g.surface_area_energy),
+          "GBSA global settings must be finite");
+  if (g.method != 0) require(std::isfinite(g.cutoff) && g.cutoff > 0.0, "GBSA cutoff must be positive and finite");
+  if (g.method == 2) {
+    validate_box(box_);
+    for (int a = 0; a < 3; ++a)
+      require(box_[4 * a] >= 2.0 * g.cutoff, "GBSA cutoff exceeds half a periodic box width");
+  }
+  GbArgs& a = gb_;
+  a = GbArgs{};
+  a.n_atoms = n_;
+  const int blocks = (n_ + 31) / 32;
+  a.n_slots = 32 * blocks;
+  std::vector<int> slot_atom(a.n_slots, -1), seg_block(blocks, 0), seg_atom(n_, 0);
+  for (int i = 0; i < n_; ++i) slot_atom[i] = i;
+  std::vector<int2> tiles;
+  for (int I = 0; I < blocks; ++I)
+    for (int J = I; J < blocks; ++J) tiles.push_back(make_int2(I, J));
+  a.n_tiles = (int)tiles.size();
+  int2* dt = mem_.alloc<int2>(tiles.size());
+  int* dsa = mem_.alloc<int>(a.n_slots);
+  int* dsb = mem_.alloc<int>(blocks);
+  int* dsat = mem_.alloc<int>(n_);
+  OMMB200_CK(cudaMemcpy(dt, tiles.data(), sizeof(int2) * tiles.size(), cudaMemcpyHostToDevice));
+  OMMB200_CK(cudaMemcpy(dsa, slot_atom.data(), 4 * slot_atom.size(), cudaMemcpyHostToDevice));
+  OMMB200_CK(cudaMemcpy(dsb, seg_block.data(), 4 * seg_block.size(), cudaMemcpyHostToDevice));
+  OMMB200_CK(cudaMemcpy(dsat, seg_atom.data(), 4 * seg_atom.size(), cudaMemcpyHostToDevice));
+  a.tiles = dt;
+  a.slot_atom = dsa;
+  a.block_segment = dsb;
+  a.atom_segment = dsat;
+  double* q = mem_.alloc<double>(n_);
+  double* r = mem_.alloc<double>(n_);
+  double* s = mem_.alloc<double>(n_);
+  OMMB200_CK(cudaMemcpy(q, g.charge.data(), 8 * n_, cudaMemcpyHostToDevice));
+  OMMB200_CK(cudaMemcpy(r, g.radius.data(), 8 * n_, cudaMemcpyHostToDevice));
+  OMMB200_CK(cudaMemcpy(s, g.scale.data(), 8 * n_, cudaMemcpyHostToDevice));
+  a.pos = pos_;
+  a.charge = q;
+  a.radius = r;
+  a.scale = s;
+  // gbsa_obc.rs:214-218
+  a.prefactor = (g.solute_dielectric != 0.0 && g.solvent_dielectric != 0.0)
+                    ? -kOne4PiEps0 * (1.0 / g.solute_dielectric - 1.0 / g.solvent_dielectric)
+                    : 0.0;
+  a.prefactor_sign = a.prefactor < 0.0 ? -1.0 : (a.prefactor > 0.0 ? 1.0 : 0.0);
+  a.charge_scale = std::sqrt(std::fabs(a.prefactor));
+  a.surface = 4.0 * kPiD * g.surface_area_energy;
+  a.periodic = g.method == 2;
+  a.use_cutoff = g.method != 0;
+  a.cutoff = g.cutoff;
+  const size_t rs = dp_ ? 8 : 4;
+  a.posq = mem_.alloc_bytes(4 * rs * a.n_slots);
+  a.params = mem_.alloc_bytes(2 * rs * a.n_slots);
+  a.born_slot = mem_.alloc_bytes(rs * a.n_slots);
+  a.dedr_slot = mem_.alloc_bytes(rs * a.n_slots);
+  a.born_sum = mem_.alloc<long long>(n_);
+  a.dedr_sum = mem_.alloc<long long>(n_);
+  a.born_radius = mem_.alloc<double>(n_);
+  a.chain = mem_.alloc<double>(n_);
+  a.dedr_self = mem_.alloc<double>(n_);
+  a.force = force_;
+  a.energy = energy_;
+}
+
 // constraints.rs:35-75 validation, then SETTLE waters / free particles / SHAKE clusters.
 void Engine::setup_integrator() {
   const IntegratorDef& it = *integ_;
@@ -675,6 +755,8 @@ void Engine::update_box_dependents() {
   reciprocal_box(box_, recip_, &volume_);
   nl_.box = make_box(box_);
   for (auto& L : bonded_) L.args.box = make_box(box_);
+  gb_.boxd = make_box(box_);
+  gb_.boxf = cast_box<float>(gb_.boxd);
   if (!nb_) return;
   if (nb_pme_) {
     const int nx = grid_[0], ny = grid_[1], nz = grid_[2], nzh = nz / 2 + 1;
@@ -940,6 +1022,14 @@ void Engine::compute_forces(bool energy, uint32_t groups) {
       enqueue_nonbonded<double>(energy, direct, recip, dump_mode_);
     else
       enqueue_nonbonded<float>(energy, direct, recip, dump_mode_);
+  }
+  if (gb_def_ && ((groups >> gb_def_->force_group) & 1u)) {
+    prof_begin("gbsa");
+    if (dp_)
+      launch_gbsa<double>(gb_, energy, stream_);
+    else
+      launch_gbsa<float>(gb_, energy, stream_);
+    prof_end();
   }
   for (auto& L : bonded_) {
     if (!((groups >> L.group) & 1u)) continue;

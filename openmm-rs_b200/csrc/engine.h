@@ -86,6 +86,7 @@ class Engine {
  private:
   void setup_nonbonded(const NonbondedDef& nb);
   void setup_bonded();
+  void setup_gbsa(const GbsaObcDef& gb);
   void setup_integrator();
   void update_box_dependents();
   void build_static_tiles();
@@ -166,6 +167,10 @@ class Engine {
   bool dump_mode_ = false;
   int pair_grid_ = 0;
   int sm_count_ = 148;
+
+  // GBSAOBCForce
+  const GbsaObcDef* gb_def_ = nullptr;
+  GbArgs gb_{};
 
   // bonded terms, one launch per force
   struct BondedLaunch {

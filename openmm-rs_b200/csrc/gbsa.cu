@@ -1,0 +1,286 @@
+// GBSAOBCForce (forces/gbsa_obc.rs:184-309): OBC-II Born radii from the HCT descreening
+// integral, generalized-Born pair energy, ACE surface term.
+//
+// Three pair passes over 32 x 32 tiles of particle blocks, separated by per-particle f64
+// kernels:
+//   pass 1  I_i = sum_j H(r_ij; rho_i - 0.009, s_j (rho_j - 0.009))    (both directions)
+//   radii   R_i = 1 / (1/(rho_i - 0.009) - tanh(psi - 0.8 psi^2 + 4.85 psi^3) / rho_i),
+//           self and ACE energies, dE/dR_i from them
+//   pass 2  GB pair energy, radial forces, dE/dR_i += dE_ij/dR_i
+//   chain   dE/dR_i *= R_i^2 dR_i/dI_i
+//   pass 3  forces from the descreening gradient
+// The pair arithmetic runs in `Real` (FP32 in the mixed form); every sum over pairs is
+// committed in 64-bit fixed point (descreening sums in 2^-40 nm^-1, dE/dR in 2^-32 kJ/mol/nm,
+// forces in 2^-32 kJ/mol/nm), so results are bit-identical run to run.
+//
+// Tiles pair blocks of the same segment (one segment per independent system in a batch), so
+// many systems of uneven size run in the same launches.
+#include "kernels.h"
+#include "pair_math.cuh"
+
+namespace ommb200 {
+namespace {
+
+constexpr double kDielectricOffset = 0.009;  // gbsa_obc.rs:8
+constexpr double kProbeRadius = 0.14;        // gbsa_obc.rs:9
+constexpr double kBornScale = 1099511627776.0;  // 2^40
+constexpr double kBornScaleInv = 1.0 / 1099511627776.0;
+
+__device__ __forceinline__ float log_r(float x) { return logf(x); }
+__device__ __forceinline__ double log_r(double x) { return log(x); }
+__device__ __forceinline__ float exp_gb(float x) { return expf(x); }
+__device__ __forceinline__ double exp_gb(double x) { return exp(x); }
+__device__ __forceinline__ float sqrt_r(float x) { return sqrtf(x); }
+__device__ __forceinline__ double sqrt_r(double x) { return sqrt(x); }
+
+// gbsa_obc.rs:278-295; `radius` = rho_i - 0.009, `scaled` = s_j (rho_j - 0.009)
+template <class Real>
+__device__ __forceinline__ Real descreening(Real radius, Real scaled, Real r) {
+  if (radius >= r + scaled) return Real(0);
+  const Real lower = Real(1) / fmax(radius, fabs(r - scaled));
+  const Real upper = Real(1) / (r + scaled);
+  const Real inverse = Real(1) / r;
+  Real value = lower - upper + Real(0.25) * r * (upper * upper - lower * lower) +
+               Real(0.5) * inverse * log_r(upper / lower) +
+               Real(0.25) * scaled * scaled * inverse * (lower * lower - upper * upper);
+  if (radius < scaled - r) value += Real(2) * (Real(1) / radius - lower);
+  return value;
+}
+
+// gbsa_obc.rs:297-309
+template <class Real>
+__device__ __forceinline__ Real descreening_gradient(Real radius, Real scaled, Real r) {
+  if (radius >= r + scaled) return Real(0);
+  const Real lower = Real(1) / fmax(radius, fabs(r - scaled));
+  const Real upper = Real(1) / (r + scaled);
+  const Real inverse = Real(1) / r;
+  return (Real(0.125) * (Real(1) + scaled * scaled * inverse * inverse) *
+              (lower * lower - upper * upper) +
+          Real(0.25) * log_r(upper / lower) * inverse * inverse) *
+         inverse;
+}
+
+template <class Real, int kPass, bool kEnergy>
+__global__ void __launch_bounds__(128) gb_pass(const GbArgs a) {
+  using T4 = typename V4<Real>::T4;
+  using T2 = typename V4<Real>::T2;
+  constexpr unsigned FULL = 0xffffffffu;
+  __shared__ T4 s_pos[4][32];
+  __shared__ T2 s_par[4][32];
+  __shared__ Real s_aux[4][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const T4* posq = reinterpret_cast<const T4*>(a.posq);
+  const T2* par = reinterpret_cast<const T2*>(a.params);
+  const Real* born = reinterpret_cast<const Real*>(a.born_slot);
+  const Real* dedr = reinterpret_cast<const Real*>(a.dedr_slot);
+  for (int t = blockIdx.x * 4 + w; t < a.n_tiles; t += gridDim.x * 4) {
+    const int2 tile = a.tiles[t];
+    const int I = tile.x, J = tile.y;
+    const bool self = I == J;
+    const int si = 32 * I + lane, sj = 32 * J + lane;
+    const int ai = a.slot_atom[si], aj = a.slot_atom[sj];
+    const T4 pi = posq[si];
+    const T2 qi = par[si];  // (offset radius, scaled radius)
+    Real ri_aux = Real(0);
+    if (kPass == 2) ri_aux = born[si];
+    if (kPass == 3) ri_aux = dedr[si];
+    s_pos[w][lane] = posq[sj];
+    s_par[w][lane] = par[sj];
+    s_aux[w][lane] = kPass == 2 ? born[sj] : (kPass == 3 ? dedr[sj] : Real(0));
+    __syncwarp();
+    Real acc_i = 0, acc_j = 0;  // pass 1: descreening sums; pass 2: dE/dR
+    Real fix = 0, fiy = 0, fiz = 0, fjx = 0, fjy = 0, fjz = 0;
+    double e_tile = 0.0;
+    for (int k = self ? 1 : 0; k < 32; ++k) {
+      const int jl = (lane + k) & 31;
+      const T4 pj = s_pos[w][jl];
+      const T2 qj = s_par[w][jl];
+      const Real rj_aux = s_aux[w][jl];
+      const int bj = a.slot_atom[32 * J + jl];
+      Real dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
+      if (a.periodic) {
+        if constexpr (sizeof(Real) == 4) min_image_fast(dx, dy, dz, a.boxf);
+        else min_image_fast(dx, dy, dz, a.boxd);
+      }
+      const Real r2 = dx * dx + dy * dy + dz * dz;
+      bool use = ai >= 0 && bj >= 0;
+      const Real r = sqrt_r(use ? r2 : Real(1));
+      if (a.use_cutoff) use = use && r <= (Real)a.cutoff;  // gbsa_obc.rs:169 (<=)
+      Real fo = 0;
+      if (kPass == 1) {
+        if (use) {
+          acc_i += descreening<Real>(qi.x, qj.y, r);
+          if (!self) acc_j += descreening<Real>(qj.x, qi.y, r);
+        }
+      } else if (kPass == 2) {
+        if (use) {
+          const Real product = ri_aux * rj_aux;
+          const Real d = r2 / (Real(4) * product);
+          const Real ex = exp_gb(-d);
+          const Real den2 = r2 + product * ex;
+          // prefactor q_i q_j, with q stored as q sqrt|prefactor|
+          const Real coefficient = (Real)a.prefactor_sign * pi.w * pj.w;
+          const Real pe = coefficient / sqrt_r(den2);
+          fo = -pe * (Real(1) - Real(0.25) * ex) / den2;
+          const Real bd = Real(-0.5) * pe * ex * (Real(1) + d) / den2;
+          acc_i += bd * rj_aux;
+          if (!self) acc_j += bd * ri_aux;
+          if (kEnergy) {
+            const double e = a.use_cutoff ? (double)pe - (double)coefficient / a.cutoff : (double)pe;
+            e_tile += (self ? 0.5 : 1.0) * e;
+          }
+        }
+      } else {
+        if (use)
+          fo = -(ri_aux * descreening_gradient<Real>(qi.x, qj.y, r) +
+                 rj_aux * descreening_gradient<Real>(qj.x, qi.y, r));
+      }
+      if (kPass != 1) {
+        // self tiles visit each pair from both sides; each visit moves only its own lane
+        fix = fma(fo, dx, fix);
+        fiy = fma(fo, dy, fiy);
+        fiz = fma(fo, dz, fiz);
+      }
+      if (!self) {
+        const int src = (lane + 1) & 31;
+        if (kPass != 1) {
+          fjx = fma(-fo, dx, fjx);
+          fjy = fma(-fo, dy, fjy);
+          fjz = fma(-fo, dz, fjz);
+          fjx = __shfl_sync(FULL, fjx, src);
+          fjy = __shfl_sync(FULL, fjy, src);
+          fjz = __shfl_sync(FULL, fjz, src);
+        }
+        if (kPass != 3) acc_j = __shfl_sync(FULL, acc_j, src);
+      }
+    }
+    if (kPass == 1) {
+      if (ai >= 0) add_fixed(a.born_sum + ai, to_fixed((double)acc_i, kBornScale));
+      if (!self && aj >= 0) add_fixed(a.born_sum + aj, to_fixed((double)acc_j, kBornScale));
+    } else {
+      const Real fs = Real(kForceScale);
+      if (ai >= 0) {
+        add_fixed(a.force + ai, to_fixed(fix, fs));
+        add_fixed(a.force + a.n_atoms + ai, to_fixed(fiy, fs));
+        add_fixed(a.force + 2 * a.n_atoms + ai, to_fixed(fiz, fs));
+      }
+      if (!self && aj >= 0) {
+        add_fixed(a.force + aj, to_fixed(fjx, fs));
+        add_fixed(a.force + a.n_atoms + aj, to_fixed(fjy, fs));
+        add_fixed(a.force + 2 * a.n_atoms + aj, to_fixed(fjz, fs));
+      }
+      if (kPass == 2) {
+        if (ai >= 0) add_fixed(a.dedr_sum + ai, to_fixed((double)acc_i, kForceScale));
+        if (!self && aj >= 0) add_fixed(a.dedr_sum + aj, to_fixed((double)acc_j, kForceScale));
+      }
+    }
+    if (kEnergy && kPass == 2) {
+      for (int off = 16; off > 0; off >>= 1) e_tile += __shfl_xor_sync(FULL, e_tile, off);
+      const long long ef = to_fixed(e_tile, kEnergyScale);
+      if (lane == 0 && ef) add_fixed(a.energy + 8 * a.block_segment[I], ef);
+    }
+    __syncwarp();
+  }
+}
+
+// gbsa_obc.rs:214-237: radii, chain factor, self + ACE energies, dE/dR from them.
+template <class Real, bool kEnergy>
+__global__ void gb_radii(const GbArgs a) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.n_slots) return;
+  const int atom = a.slot_atom[s];
+  Real* born = reinterpret_cast<Real*>(a.born_slot);
+  if (atom < 0) {
+    born[s] = Real(1);
+    return;
+  }
+  const double rho = a.radius[atom];
+  const double offset = rho - kDielectricOffset;
+  const double integral = (double)a.born_sum[atom] * kBornScaleInv;
+  const double psi = 0.5 * offset * integral;
+  const double t = tanh(psi - 0.8 * psi * psi + 4.85 * psi * psi * psi);
+  const double R = 1.0 / (1.0 / offset - t / rho);
+  a.chain[atom] = offset * (1.0 - 1.6 * psi + 14.55 * psi * psi) * (1.0 - t * t) / rho;
+  a.born_radius[atom] = R;
+  born[s] = (Real)R;
+  const double q = a.charge[atom];
+  const double self_energy = 0.5 * a.prefactor * q * q / fabs(R);
+  double dedr = -self_energy / R;
+  double e = self_energy;
+  if (R > 0.0) {
+    const double ratio = rho / R;
+    const double r2 = ratio * ratio;
+    const double area = a.surface * (rho + kProbeRadius) * (rho + kProbeRadius) * r2 * r2 * r2;
+    e += area;
+    dedr -= 6.0 * area / R;
+  }
+  a.dedr_self[atom] = dedr;
+  if (kEnergy) add_fixed(a.energy + 8 * a.atom_segment[atom], to_fixed(e, kEnergyScale));
+}
+
+// gbsa_obc.rs:261-263
+template <class Real>
+__global__ void gb_chain(const GbArgs a) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.n_slots) return;
+  const int atom = a.slot_atom[s];
+  Real* dedr = reinterpret_cast<Real*>(a.dedr_slot);
+  if (atom < 0) {
+    dedr[s] = Real(0);
+    return;
+  }
+  const double R = a.born_radius[atom];
+  const double total = a.dedr_self[atom] + (double)a.dedr_sum[atom] * kForceScaleInv;
+  dedr[s] = (Real)(total * R * R * a.chain[atom]);
+}
+
+template <class Real>
+__global__ void gb_pack(const GbArgs a) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.n_slots) return;
+  const int atom = a.slot_atom[s];
+  typename V4<Real>::T4 p;
+  typename V4<Real>::T2 q;
+  if (atom < 0) {
+    p.x = p.y = p.z = p.w = Real(0);
+    q.x = q.y = Real(0);
+  } else {
+    p.x = (Real)a.pos[3 * atom];
+    p.y = (Real)a.pos[3 * atom + 1];
+    p.z = (Real)a.pos[3 * atom + 2];
+    p.w = (Real)(a.charge[atom] * a.charge_scale);
+    a.born_sum[atom] = 0;
+    a.dedr_sum[atom] = 0;
+    const double offset = a.radius[atom] - kDielectricOffset;
+    q.x = (Real)offset;
+    q.y = (Real)(offset * a.scale[atom]);
+  }
+  reinterpret_cast<typename V4<Real>::T4*>(a.posq)[s] = p;
+  reinterpret_cast<typename V4<Real>::T2*>(a.params)[s] = q;
+}
+
+}  // namespace
+
+template <class Real>
+void launch_gbsa(const GbArgs& a, bool energy, cudaStream_t s) {
+  const int tb = 256;
+  const int gs = ceil_div(a.n_slots, tb);
+  const int gt = (int)std::min<long long>((a.n_tiles + 3) / 4, 148LL * 16);
+  gb_pack<Real><<<gs, tb, 0, s>>>(a);
+  gb_pass<Real, 1, false><<<gt, 128, 0, s>>>(a);
+  if (energy)
+    gb_radii<Real, true><<<gs, tb, 0, s>>>(a);
+  else
+    gb_radii<Real, false><<<gs, tb, 0, s>>>(a);
+  if (energy)
+    gb_pass<Real, 2, true><<<gt, 128, 0, s>>>(a);
+  else
+    gb_pass<Real, 2, false><<<gt, 128, 0, s>>>(a);
+  gb_chain<Real><<<gs, tb, 0, s>>>(a);
+  gb_pass<Real, 3, false><<<gt, 128, 0, s>>>(a);
+}
+
+template void launch_gbsa<float>(const GbArgs&, bool, cudaStream_t);
+template void launch_gbsa<double>(const GbArgs&, bool, cudaStream_t);
+
+}  // namespace ommb200

@@ -136,6 +136,42 @@ void launch_pme_convolve(const PmeArgs<Real>& a, bool energy, cudaStream_t s);
 template <class Real>
 void launch_pme_gather(const PmeArgs<Real>& a, cudaStream_t s);
 
+// ---- GBSAOBCForce --------------------------------------------------------------------------
+// Particles in segment-padded slot order (one segment per independent system); tiles pair
+// 32-slot blocks of the same segment.  energy[8 * segment] receives each segment's energy.
+struct GbArgs {
+  int n_atoms, n_slots, n_tiles;
+  const int2* tiles;          // (I, J), I <= J
+  const int* slot_atom;       // [n_slots], -1 = padding
+  const int* block_segment;   // [n_slots / 32]
+  const int* atom_segment;    // [n_atoms]
+  const double* pos;
+  const double* charge;
+  const double* radius;
+  const double* scale;
+  double prefactor;           // -ke (1/eps_solute - 1/eps_solvent), gbsa_obc.rs:214-218
+  double prefactor_sign;      // sign of the prefactor; charges are packed as q sqrt|prefactor|
+  double charge_scale;        // sqrt|prefactor|
+  double surface;             // 4 pi * surface-area energy
+  int periodic, use_cutoff;
+  double cutoff;
+  Box<double> boxd;
+  Box<float> boxf;
+  void* posq;                 // [n_slots] Real4: x, y, z, q sqrt|prefactor|
+  void* params;               // [n_slots] Real2: rho - 0.009, s (rho - 0.009)
+  void* born_slot;            // [n_slots] Real: Born radius
+  void* dedr_slot;            // [n_slots] Real: dE/dR R^2 chain
+  long long* born_sum;        // [n_atoms] descreening sums, 2^-40
+  long long* dedr_sum;        // [n_atoms] pair dE/dR sums, 2^-32
+  double* born_radius;        // [n_atoms]
+  double* chain;              // [n_atoms]
+  double* dedr_self;          // [n_atoms]
+  long long* force;
+  long long* energy;
+};
+template <class Real>
+void launch_gbsa(const GbArgs& a, bool energy, cudaStream_t s);
+
 // ---- exceptions and bonded terms (exceptions always in f64) ------------------------------
 struct ExceptionArgs {
   int n;

@@ -3,7 +3,7 @@ from __future__ import annotations
 
 import numpy as np
 
-from . import HarmonicAngleForce, HarmonicBondForce, LangevinMiddleIntegrator, NonbondedForce, System
+from . import GBSAOBCForce, HarmonicAngleForce, HarmonicBondForce, LangevinMiddleIntegrator, NonbondedForce, System
 from .synth import D_HH, D_OH, WaterBox
 
 
@@ -42,9 +42,10 @@ def langevin(temperature=300.0, friction=1.0, step_size=0.002, seed=1234):
     return integ
 
 
-def chain_system(chain, coulomb14=1.0, lj14=1.0) -> System:
+def chain_system(chain, coulomb14=1.0, lj14=1.0, gbsa=True, solvent_dielectric=78.5,
+                 solute_dielectric=1.0, surface_area_energy=2.25936) -> System:
     """One implicit-solvent chain: NoCutoff NonbondedForce with 1-2/1-3 exclusions and 1-4
-    exceptions, harmonic bonds and angles (GBSAOBCForce is added by the caller)."""
+    exceptions, harmonic bonds and angles, and (by default) a NoCutoff GBSAOBCForce."""
     system = System()
     for _ in range(chain.n_atoms):
         system.add_particle(chain.mass)
@@ -63,6 +64,14 @@ def chain_system(chain, coulomb14=1.0, lj14=1.0) -> System:
     for i, j, k, th, kt in chain.angles():
         ha.add_angle(i, j, k, th, kt)
     system.add_force(ha)
+    if gbsa:
+        gb = GBSAOBCForce()
+        gb.set_solvent_dielectric(solvent_dielectric)
+        gb.set_solute_dielectric(solute_dielectric)
+        gb.set_surface_area_energy(surface_area_energy)
+        for q, r in zip(chain.charges, chain.radii):
+            gb.add_particle(float(q), float(r), chain.gb_scale)
+        system.add_force(gb)
     return system
 
 

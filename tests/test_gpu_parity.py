@@ -155,8 +155,8 @@ def test_switching_and_reaction_field_match_oracle():
 def test_no_cutoff_chain_matches_oracle():
     ch = synth.chain(300, seed=3)
     for precision, bound in (("double", 1e-9), ("mixed", 5e-6)):
-        ctx = ommb200.Context(systems.chain_system(ch), systems.langevin(step_size=0.001),
-                              precision=precision)
+        ctx = ommb200.Context(systems.chain_system(ch, gbsa=False),
+                              systems.langevin(step_size=0.001), precision=precision)
         ctx.set_positions(ch.positions)
         st = ctx.get_state(forces=True, energy=True)
         exc = _chain_exceptions(ch)
