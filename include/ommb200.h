@@ -196,6 +196,27 @@ int ommb200_context_autotune(ommb200_context* ctx, int trial_steps, double* skin
 int ommb200_context_get_pme_parameters(const ommb200_context* ctx, double* alpha, int* nx,
                                        int* ny, int* nz);
 
+/* ---- batches of independent systems (no reference counterpart) ----
+ * One Context over n_systems independent Systems: each step() advances all of them with one
+ * set of launches (the reference runs one Context per System).  The Systems must carry the
+ * same force kinds with the same global settings (method, cutoff, dielectrics, switching,
+ * groups) and, when there is more than one, be non-periodic; particle counts may differ.  The
+ * batch's particles are the Systems' particles concatenated in order: positions, velocities
+ * and forces of get_state / set_positions use that order, and every Context call behaves as
+ * for one System whose energy is the sum over the batch.  Particles of different Systems never
+ * interact.  Takes ownership of every System and the integrator (also on failure).  The
+ * random stream is per particle, so a System's trajectory depends on its offset in the batch. */
+int ommb200_context_create_batch(ommb200_system* const* systems, int n_systems,
+                                 ommb200_integrator* integrator, const ommb200_options* options,
+                                 ommb200_context** out);
+int ommb200_context_num_systems(const ommb200_context* ctx, int* out);
+/* First particle and particle count of System `index` within the batch. */
+int ommb200_context_system_range(const ommb200_context* ctx, int index, int* first, int* count);
+/* Potential (of force groups `groups`) and kinetic energy of each System, kJ/mol; arrays of
+ * n_systems doubles, either may be NULL. */
+int ommb200_context_get_system_energies(ommb200_context* ctx, uint32_t groups,
+                                        double* potential, double* kinetic);
+
 /* ---- allocation-free force evaluation (no counterpart in the reference) ----
  * For callers that must not allocate device memory: code inside another framework's memory
  * pool, a plugin that may only use the buffers it is handed, or a stream being captured into a

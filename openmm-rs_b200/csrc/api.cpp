@@ -3,6 +3,7 @@
 #include <cmath>
 #include <cstring>
 #include <new>
+#include <set>
 #include <string>
 
 #include "../../include/ommb200.h"
@@ -418,6 +419,21 @@ int ommb200_integrator_set_integration_force_groups(ommb200_integrator* i, uint3
 }
 
 // ---- Context ----------------------------------------------------------------------------
+static EngineOptions engine_options(const ommb200_options* options) {
+  ommb200_options o;
+  ommb200_default_options(&o);
+  if (options) o = *options;
+  require(o.precision == OMMB200_PRECISION_MIXED || o.precision == OMMB200_PRECISION_DOUBLE,
+          "unknown precision");
+  EngineOptions eo;
+  eo.precision = o.precision;
+  eo.device = o.device;
+  eo.use_graph = o.use_cuda_graph != 0;
+  eo.skin = o.neighbor_skin;
+  eo.steps_per_graph = o.steps_per_graph;
+  return eo;
+}
+
 int ommb200_context_create(ommb200_system* system, ommb200_integrator* integrator,
                            const ommb200_options* options, ommb200_context** out) {
   std::unique_ptr<SystemDef> sys(sysdef(system));
@@ -427,19 +443,37 @@ int ommb200_context_create(ommb200_system* system, ommb200_integrator* integrato
     *out = nullptr;
     require(sys != nullptr && integ != nullptr, "null system or integrator handle");
     integ->owned_by_context = true;
-    ommb200_options o;
-    ommb200_default_options(&o);
-    if (options) o = *options;
-    require(o.precision == OMMB200_PRECISION_MIXED || o.precision == OMMB200_PRECISION_DOUBLE,
-            "unknown precision");
-    EngineOptions eo;
-    eo.precision = o.precision;
-    eo.device = o.device;
-    eo.use_graph = o.use_cuda_graph != 0;
-    eo.skin = o.neighbor_skin;
-    eo.steps_per_graph = o.steps_per_graph;
     auto ctx = std::make_unique<ommb200_context>();
-    ctx->engine = std::make_unique<Engine>(std::move(sys), std::move(integ), eo);
+    ctx->engine = std::make_unique<Engine>(std::move(sys), std::move(integ), engine_options(options));
+    *out = ctx.release();
+  });
+}
+int ommb200_context_create_batch(ommb200_system* const* systems, int n_systems,
+                                 ommb200_integrator* integrator, const ommb200_options* options,
+                                 ommb200_context** out) {
+  std::vector<std::unique_ptr<SystemDef>> defs;
+  std::set<ommb200_system*> seen;
+  bool repeated = false;
+  if (systems)
+    for (int k = 0; k < n_systems; ++k) {
+      const bool fresh = seen.insert(systems[k]).second;
+      repeated = repeated || !fresh;
+      defs.emplace_back(fresh ? sysdef(systems[k]) : nullptr);
+    }
+  std::unique_ptr<IntegratorDef> integ(integdef(integrator));
+  return guarded([&] {
+    require(out != nullptr, "null output pointer");
+    *out = nullptr;
+    require(systems != nullptr && n_systems > 0, "a batch needs at least one System");
+    require(!repeated, "a System handle appears more than once in the batch");
+    for (auto& d : defs) require(d != nullptr, "null system handle");
+    require(integ != nullptr, "null integrator handle");
+    integ->owned_by_context = true;
+    std::vector<Segment> segments;
+    std::unique_ptr<SystemDef> merged = merge_systems(std::move(defs), &segments);
+    auto ctx = std::make_unique<ommb200_context>();
+    ctx->engine = std::make_unique<Engine>(std::move(merged), std::move(integ),
+                                           engine_options(options), segments);
     *out = ctx.release();
   });
 }
@@ -531,6 +565,28 @@ int ommb200_context_get_pme_parameters(const ommb200_context* ctx, double* alpha
   return guarded([&] {
     require(ctx && ctx->engine && alpha && nx && ny && nz, "null argument");
     ctx->engine->pme_parameters(alpha, nx, ny, nz);
+  });
+}
+int ommb200_context_num_systems(const ommb200_context* ctx, int* out) {
+  return guarded([&] {
+    require(ctx && ctx->engine && out, "null argument");
+    *out = ctx->engine->num_segments();
+  });
+}
+int ommb200_context_system_range(const ommb200_context* ctx, int index, int* first, int* count) {
+  return guarded([&] {
+    require(ctx && ctx->engine && first && count, "null argument");
+    require(index >= 0 && index < ctx->engine->num_segments(), "system index out of range");
+    const Segment g = ctx->engine->segment(index);
+    *first = g.first;
+    *count = g.count;
+  });
+}
+int ommb200_context_get_system_energies(ommb200_context* ctx, uint32_t groups, double* potential,
+                                        double* kinetic) {
+  return guarded([&] {
+    OMMB200_CTX;
+    E.segment_energies(groups, potential, kinetic);
   });
 }
 int ommb200_context_debug_pair_list(ommb200_context* ctx, int64_t max_pairs, int32_t* pairs,

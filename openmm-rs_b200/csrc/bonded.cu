@@ -15,7 +15,20 @@ __device__ __forceinline__ void commit_pair(long long* force, int n, int i, int 
   }
 }
 
-__device__ __forceinline__ void reduce_commit(long long* energy, double e, const double w[6]) {
+// `seg`: the term's system in a batch (energy at energy[8 * seg]), or -1 for a single
+// system, whose warp sums are committed once.
+__device__ __forceinline__ void reduce_commit(long long* energy, double e, const double w[6],
+                                              int seg) {
+  if (seg >= 0) {
+    long long* dst = energy + 8 * seg;
+    const long long ef = to_fixed(e, kEnergyScale);
+    if (ef) add_fixed(dst, ef);
+    for (int c = 0; c < 6; ++c) {
+      const long long wf = to_fixed(w[c], kEnergyScale);
+      if (wf) add_fixed(dst + 1 + c, wf);
+    }
+    return;
+  }
   long long ef = to_fixed(e, kEnergyScale);
   long long wf[6];
   for (int c = 0; c < 6; ++c) wf[c] = to_fixed(w[c], kEnergyScale);
@@ -43,8 +56,10 @@ template <bool kEnergy>
 __global__ void exceptions_kernel(const ExceptionArgs a, int n_atoms) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   double en = 0.0, w[6] = {0, 0, 0, 0, 0, 0};
+  int seg = a.atom_segment ? 0 : -1;
   if (e < a.n) {
     const int2 p = a.pairs[e];
+    if (a.atom_segment) seg = a.atom_segment[p.x];
     const double4 prm = a.params[e];
     double d[3] = {a.pos[3 * p.y] - a.pos[3 * p.x], a.pos[3 * p.y + 1] - a.pos[3 * p.x + 1],
                    a.pos[3 * p.y + 2] - a.pos[3 * p.x + 2]};
@@ -82,15 +97,17 @@ __global__ void exceptions_kernel(const ExceptionArgs a, int n_atoms) {
       pair_virial(w, fo, d);
     }
   }
-  if (kEnergy) reduce_commit(a.energy, en, w);
+  if (kEnergy) reduce_commit(a.energy, en, w, seg);
 }
 
 template <bool kEnergy>
 __global__ void bonded_kernel(const BondedArgs a, int n_atoms) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   double en = 0.0, w[6] = {0, 0, 0, 0, 0, 0};
+  int seg = a.atom_segment ? 0 : -1;
   if (t < a.n_bonds) {
     const int2 b = a.bonds[t];
+    if (a.atom_segment) seg = a.atom_segment[b.x];
     const double2 prm = a.bond_params[t];
     double d[3] = {a.pos[3 * b.y] - a.pos[3 * b.x], a.pos[3 * b.y + 1] - a.pos[3 * b.x + 1],
                    a.pos[3 * b.y + 2] - a.pos[3 * b.x + 2]};
@@ -107,6 +124,7 @@ __global__ void bonded_kernel(const BondedArgs a, int n_atoms) {
     const int4 an = a.angles[t - a.n_bonds];
     const double2 prm = a.angle_params[t - a.n_bonds];
     const int i = an.x, j = an.y, k = an.z;
+    if (a.atom_segment) seg = a.atom_segment[j];
     double rji[3] = {a.pos[3 * i] - a.pos[3 * j], a.pos[3 * i + 1] - a.pos[3 * j + 1],
                      a.pos[3 * i + 2] - a.pos[3 * j + 2]};
     double rjk[3] = {a.pos[3 * k] - a.pos[3 * j], a.pos[3 * k + 1] - a.pos[3 * j + 1],
@@ -146,7 +164,7 @@ __global__ void bonded_kernel(const BondedArgs a, int n_atoms) {
     }
     if (kEnergy) en = 0.5 * prm.y * dtheta * dtheta;
   }
-  if (kEnergy) reduce_commit(a.energy, en, w);
+  if (kEnergy) reduce_commit(a.energy, en, w, seg);
 }
 
 }  // namespace

@@ -185,10 +185,12 @@ double dispersion_coefficient(const NonbondedDef& nb) {
 }  // namespace
 
 Engine::Engine(std::unique_ptr<SystemDef> system, std::unique_ptr<IntegratorDef> integrator,
-               const EngineOptions& options)
-    : sys_(std::move(system)), integ_(std::move(integrator)), opt_(options) {
+               const EngineOptions& options, std::vector<Segment> segments)
+    : sys_(std::move(system)), integ_(std::move(integrator)), opt_(options),
+      segments_(std::move(segments)) {
   n_ = (int)sys_->masses.size();
   require(n_ > 0, "cannot create a context for a system with no particles");
+  if (segments_.empty()) segments_.push_back({0, n_});
   dp_ = opt_.precision == OMMB200_PRECISION_DOUBLE;
   std::copy(sys_->box, sys_->box + 9, box_);
   int devices = 0;
@@ -211,7 +213,7 @@ Engine::Engine(std::unique_ptr<SystemDef> system, std::unique_ptr<IntegratorDef>
   scratch3_ = mem_.alloc<double>(3 * (size_t)n_);
   inv_mass_ = mem_.alloc<double>(n_);
   force_ = mem_.alloc<long long>(3 * (size_t)n_);
-  energy_ = mem_.alloc<long long>(8);
+  energy_ = mem_.alloc<long long>(8 * segments_.size());
   status_ = mem_.alloc<int>(1);
   rebuild_ = mem_.alloc<int>(1);
   rng_step_ = mem_.alloc<unsigned long long>(1);
@@ -237,6 +239,7 @@ Engine::Engine(std::unique_ptr<SystemDef> system, std::unique_ptr<IntegratorDef>
     }
     require(f->force_group >= 0 && f->force_group < 32, "force group must be in 0..31");
   }
+  build_static_layout();
   if (nb) setup_nonbonded(*nb);
   if (gb_def_) setup_gbsa(*gb_def_);
   setup_bonded();
@@ -393,9 +396,13 @@ void Engine::setup_nonbonded(const NonbondedDef& nb) {
     // per block (self tile, last partial neighbour tile), so this pool cannot overflow
     a.mask_capacity = (int)std::min<long long>(a.tile_capacity, (long long)n_exceptions_ + 2 * blocks + 64);
   } else {
-    a.slot_capacity = (n_ + 31) / 32 * 32;
-    const long long blocks = a.slot_capacity / 32;
-    a.tile_capacity = (int)(blocks * (blocks + 1) / 2);
+    a.slot_capacity = static_slots_;
+    long long tiles = 0;
+    for (const Segment& g : segments_) {
+      const long long b = (g.count + 31) / 32;
+      tiles += b * (b + 1) / 2;
+    }
+    a.tile_capacity = (int)tiles;
     a.mask_capacity = a.tile_capacity;
   }
   n_slots_ = a.slot_capacity;
@@ -405,10 +412,15 @@ void Engine::setup_nonbonded(const NonbondedDef& nb) {
   a.image = mem_.alloc<int>(3 * (size_t)n_);
   a.block_center = mem_.alloc<double>(3 * (size_t)n_blocks_);
   a.block_half = mem_.alloc<double>(3 * (size_t)n_blocks_);
-  std::vector<int> sorted(n_slots_, -1);
-  for (int i = 0; i < n_; ++i) sorted[i] = i;
-  OMMB200_CK(cudaMemcpy(a.sorted_atom, sorted.data(), 4 * n_slots_, cudaMemcpyHostToDevice));
-  OMMB200_CK(cudaMemcpy(a.atom_slot, sorted.data(), 4 * n_, cudaMemcpyHostToDevice));
+  if (nb_periodic_) {  // replaced by the first rebuild
+    std::vector<int> sorted(n_slots_, -1);
+    for (int i = 0; i < n_; ++i) sorted[i] = i;
+    OMMB200_CK(cudaMemcpy(a.sorted_atom, sorted.data(), 4 * n_slots_, cudaMemcpyHostToDevice));
+    OMMB200_CK(cudaMemcpy(a.atom_slot, sorted.data(), 4 * n_, cudaMemcpyHostToDevice));
+  } else {
+    OMMB200_CK(cudaMemcpy(a.sorted_atom, static_slot_atom_.data(), 4 * n_slots_, cudaMemcpyHostToDevice));
+    OMMB200_CK(cudaMemcpy(a.atom_slot, static_atom_slot_.data(), 4 * n_, cudaMemcpyHostToDevice));
+  }
   a.tiles = mem_.alloc<int4>(a.tile_capacity);
   a.entries = mem_.alloc_bytes((size_t)(dp_ ? 32 : 16) * 32 * (size_t)a.tile_capacity);
   a.masks = mem_.alloc<uint32_t>(32 * (size_t)a.mask_capacity);
@@ -447,7 +459,9 @@ void Engine::setup_nonbonded(const NonbondedDef& nb) {
   self_energy_ = nb_pme_ ? -kOne4PiEps0 * alpha_ / std::sqrt(kPiD) * q2 : 0.0;
 }
 
-// Identity slot order and every block pair as a tile: non-periodic methods, built once.
+// Segment-padded slot order and every block pair within one segment as a tile:
+// non-periodic methods, built once.  Pairs across segments (independent systems of a batch)
+// have no tile, so they never interact.
 void Engine::build_static_tiles() {
   NlistArgs& a = nl_;
   std::vector<int4> tiles;
@@ -460,19 +474,22 @@ void Engine::build_static_tiles() {
     partners[e.p2].push_back(e.p1);
   }
   for (int I = 0; I < n_blocks_; ++I)
-    for (int J = I; J < n_blocks_; ++J) {
+    for (int J = I; J < n_blocks_ && static_block_seg_[J] == static_block_seg_[I]; ++J) {
       uint32_t m[32];
       bool any = false;
+      uint32_t pad = 0;
+      for (int k = 0; k < 32; ++k)
+        if (static_slot_atom_[32 * J + k] < 0) pad |= 1u << k;
       for (int l = 0; l < 32; ++l) {
-        const int ai = 32 * I + l;
-        uint32_t v = 0;
-        for (int k = 0; k < 32; ++k)
-          if (32 * J + k >= n_) v |= 1u << k;
-        if (ai >= n_) {
+        const int ai = static_slot_atom_[32 * I + l];
+        uint32_t v = pad;
+        if (ai < 0) {
           v = 0xffffffffu;
         } else {
-          for (int p : partners[ai])
-            if (p / 32 == J) v |= 1u << (p % 32);
+          for (int p : partners[ai]) {
+            const int sp = static_atom_slot_[p];
+            if (sp / 32 == J) v |= 1u << (sp % 32);
+          }
         }
         m[l] = v;
         any = any || v != 0;
@@ -486,7 +503,7 @@ void Engine::build_static_tiles() {
       tiles.push_back(make_int4(I, flags, slot, 0));
       // entries: the 32 slots of block J in its own (shared, unshifted) frame
       for (int k = 0; k < 32; ++k) {
-        const int s = 32 * J + k < n_ ? 32 * J + k : -1;
+        const int s = static_slot_atom_[32 * J + k] >= 0 ? 32 * J + k : -1;
         if (dp_) {
           entry_d.push_back(make_double4(0.0, 0.0, 0.0, (double)s));
         } else {
@@ -561,11 +578,39 @@ void Engine::setup_bonded() {
     L.args.force = force_;
     L.args.energy = energy_;
     L.args.n_atoms_for_force = n_;
+    L.args.atom_segment = segments_.size() > 1 ? d_atom_segment_ : nullptr;
   }
 }
 
-// gbsa_obc.rs:313-343 (initialize) + device layout: identity slot order, one segment, every
-// block pair of the segment as a tile.
+// Segment-padded slot order: segment s occupies a run of whole 32-slot blocks.
+void Engine::build_static_layout() {
+  static_slot_atom_.clear();
+  static_block_seg_.clear();
+  static_atom_slot_.assign(n_, -1);
+  std::vector<int> atom_seg(n_, 0);
+  for (size_t s = 0; s < segments_.size(); ++s) {
+    const Segment g = segments_[s];
+    require(g.first >= 0 && g.count > 0 && g.first + g.count <= n_, "invalid system range");
+    const int start = (int)static_slot_atom_.size();
+    const int padded = (g.count + 31) / 32 * 32;
+    static_slot_atom_.resize(start + padded, -1);
+    for (int i = 0; i < g.count; ++i) {
+      static_slot_atom_[start + i] = g.first + i;
+      static_atom_slot_[g.first + i] = start + i;
+      atom_seg[g.first + i] = (int)s;
+    }
+    for (int b = 0; b < padded / 32; ++b) static_block_seg_.push_back((int)s);
+  }
+  static_slots_ = (int)static_slot_atom_.size();
+  d_block_segment_ = mem_.alloc<int>(static_block_seg_.size());
+  d_atom_segment_ = mem_.alloc<int>(n_);
+  OMMB200_CK(cudaMemcpy(d_block_segment_, static_block_seg_.data(), 4 * static_block_seg_.size(),
+                        cudaMemcpyHostToDevice));
+  OMMB200_CK(cudaMemcpy(d_atom_segment_, atom_seg.data(), 4 * (size_t)n_, cudaMemcpyHostToDevice));
+}
+
+// gbsa_obc.rs:313-343 (initialize) + device layout: the segment-padded slot order, every
+// block pair of a segment as a tile.
 void Engine::setup_gbsa(const GbsaObcDef& g) {
   require((int)g.charge.size() == n_, "GBSA particle count must match System");
   for (int i = 0; i < n_; ++i) {
@@ -586,26 +631,22 @@ void Engine::setup_gbsa(const GbsaObcDef& g) {
   GbArgs& a = gb_;
   a = GbArgs{};
   a.n_atoms = n_;
-  const int blocks = (n_ + 31) / 32;
-  a.n_slots = 32 * blocks;
-  std::vector<int> slot_atom(a.n_slots, -1), seg_block(blocks, 0), seg_atom(n_, 0);
-  for (int i = 0; i < n_; ++i) slot_atom[i] = i;
+  a.n_slots = static_slots_;
+  const int blocks = static_slots_ / 32;
   std::vector<int2> tiles;
   for (int I = 0; I < blocks; ++I)
-    for (int J = I; J < blocks; ++J) tiles.push_back(make_int2(I, J));
+    for (int J = I; J < blocks && static_block_seg_[J] == static_block_seg_[I]; ++J)
+      tiles.push_back(make_int2(I, J));
   a.n_tiles = (int)tiles.size();
   int2* dt = mem_.alloc<int2>(tiles.size());
   int* dsa = mem_.alloc<int>(a.n_slots);
-  int* dsb = mem_.alloc<int>(blocks);
-  int* dsat = mem_.alloc<int>(n_);
   OMMB200_CK(cudaMemcpy(dt, tiles.data(), sizeof(int2) * tiles.size(), cudaMemcpyHostToDevice));
-  OMMB200_CK(cudaMemcpy(dsa, slot_atom.data(), 4 * slot_atom.size(), cudaMemcpyHostToDevice));
-  OMMB200_CK(cudaMemcpy(dsb, seg_block.data(), 4 * seg_block.size(), cudaMemcpyHostToDevice));
-  OMMB200_CK(cudaMemcpy(dsat, seg_atom.data(), 4 * seg_atom.size(), cudaMemcpyHostToDevice));
+  OMMB200_CK(cudaMemcpy(dsa, static_slot_atom_.data(), 4 * static_slot_atom_.size(),
+                        cudaMemcpyHostToDevice));
   a.tiles = dt;
   a.slot_atom = dsa;
-  a.block_segment = dsb;
-  a.atom_segment = dsat;
+  a.block_segment = d_block_segment_;
+  a.atom_segment = d_atom_segment_;
   double* q = mem_.alloc<double>(n_);
   double* r = mem_.alloc<double>(n_);
   double* s = mem_.alloc<double>(n_);
@@ -901,6 +942,7 @@ void Engine::enqueue_nonbonded(bool energy, bool direct, bool reciprocal, bool d
     p.tile_capacity = nl_.tile_capacity;
     p.force = force_;
     p.energy = energy_;
+    p.block_segment = segments_.size() > 1 ? d_block_segment_ : nullptr;
     p.box = cast_box<Real>(nl_.box);
     p.box_exact = nl_.box;
     p.periodic = nb_periodic_;
@@ -994,6 +1036,7 @@ void Engine::enqueue_nonbonded(bool energy, bool direct, bool reciprocal, bool d
     e.pos = pos_;
     e.force = force_;
     e.energy = energy_;
+    e.atom_segment = segments_.size() > 1 ? d_atom_segment_ : nullptr;
     e.box = nl_.box;
     e.use_pbc = nb_periodic_ && nb.exceptions_use_pbc;
     e.ewald = nb_pme_;
@@ -1202,25 +1245,61 @@ void Engine::apply_velocity_constraints(double tolerance) {
   check_status();
 }
 
+// Forces (into `forces`, may be null) and, with `energy`, the fixed-point energy/virial
+// terms of every segment: [8 * segment + (energy, virial xx yy zz xy xz yz)].
+std::vector<long long> Engine::evaluate(bool energy, uint32_t groups, double* forces) {
+  const size_t nterms = 8 * segments_.size();
+  OMMB200_CK(cudaMemsetAsync(energy_, 0, nterms * sizeof(long long), stream_));
+  compute_forces(energy, groups);
+  if (forces) {
+    std::vector<long long> f(3 * (size_t)n_);
+    OMMB200_CK(cudaMemcpyAsync(f.data(), force_, 8 * f.size(), cudaMemcpyDeviceToHost, stream_));
+    sync();
+    for (int i = 0; i < n_; ++i)
+      for (int c = 0; c < 3; ++c) forces[3 * i + c] = (double)f[(size_t)c * n_ + i] * kForceScaleInv;
+  }
+  std::vector<long long> terms(nterms);
+  OMMB200_CK(cudaMemcpyAsync(terms.data(), energy_, 8 * nterms, cudaMemcpyDeviceToHost, stream_));
+  sync();
+  harvest_profile();
+  check_status();
+  return terms;
+}
+
+void Engine::segment_energies(uint32_t groups, double* potential, double* kinetic) {
+  const int ns = (int)segments_.size();
+  if (ns == 1) {  // one system: the full getState energy, long-range corrections included
+    ommb200_state_info info{};
+    get_state(OMMB200_STATE_ENERGY, groups, nullptr, nullptr, nullptr, &info);
+    if (potential) potential[0] = info.potential_energy;
+    if (kinetic) kinetic[0] = info.kinetic_energy;
+    return;
+  }
+  if (potential) {
+    std::vector<long long> terms = evaluate(true, groups, nullptr);
+    for (int s = 0; s < ns; ++s) potential[s] = (double)terms[8 * s] * kEnergyScaleInv;
+  }
+  if (kinetic) {
+    std::vector<double> v(3 * (size_t)n_);
+    OMMB200_CK(cudaMemcpyAsync(v.data(), vel_, 24 * (size_t)n_, cudaMemcpyDeviceToHost, stream_));
+    sync();
+    for (int s = 0; s < ns; ++s) {
+      double ke = 0.0;
+      for (int i = segments_[s].first; i < segments_[s].first + segments_[s].count; ++i)
+        ke += host_masses_[i] * (v[3 * i] * v[3 * i] + v[3 * i + 1] * v[3 * i + 1] + v[3 * i + 2] * v[3 * i + 2]);
+      kinetic[s] = 0.5 * ke;
+    }
+  }
+}
+
 void Engine::get_state(int flags, uint32_t groups, double* pos, double* vel, double* forces,
                        ommb200_state_info* info) {
   const bool need_forces = flags & (OMMB200_STATE_FORCES | OMMB200_STATE_ENERGY | OMMB200_STATE_VIRIAL);
   const bool need_energy = flags & (OMMB200_STATE_ENERGY | OMMB200_STATE_VIRIAL);
   long long e[8] = {0};
   if (need_forces) {
-    OMMB200_CK(cudaMemsetAsync(energy_, 0, 8 * sizeof(long long), stream_));
-    compute_forces(need_energy, groups);
-    if (forces) {
-      std::vector<long long> f(3 * (size_t)n_);
-      OMMB200_CK(cudaMemcpyAsync(f.data(), force_, 8 * f.size(), cudaMemcpyDeviceToHost, stream_));
-      sync();
-      for (int i = 0; i < n_; ++i)
-        for (int c = 0; c < 3; ++c) forces[3 * i + c] = (double)f[(size_t)c * n_ + i] * kForceScaleInv;
-    }
-    OMMB200_CK(cudaMemcpyAsync(e, energy_, sizeof(e), cudaMemcpyDeviceToHost, stream_));
-    sync();
-    harvest_profile();
-    check_status();
+    std::vector<long long> terms = evaluate(need_energy, groups, forces);
+    for (size_t k = 0; k < terms.size(); ++k) e[k % 8] += terms[k];
   }
   std::vector<double> vtmp;
   double* vout = vel;

@@ -49,8 +49,14 @@ struct EngineOptions {
 
 class Engine {
  public:
+  // `segments`: particle ranges of independent systems merged into `system` (a batch);
+  // empty = one system.
   Engine(std::unique_ptr<SystemDef> system, std::unique_ptr<IntegratorDef> integrator,
-         const EngineOptions& options);
+         const EngineOptions& options, std::vector<Segment> segments = {});
+  int num_segments() const { return (int)segments_.size(); }
+  Segment segment(int s) const { return segments_.at(s); }
+  // Per-system potential and kinetic energy of the included force groups.
+  void segment_energies(uint32_t groups, double* potential, double* kinetic);
   ~Engine();
   Engine(const Engine&) = delete;
   Engine& operator=(const Engine&) = delete;
@@ -87,10 +93,12 @@ class Engine {
   void setup_nonbonded(const NonbondedDef& nb);
   void setup_bonded();
   void setup_gbsa(const GbsaObcDef& gb);
+  void build_static_layout();
   void setup_integrator();
   void update_box_dependents();
   void build_static_tiles();
   void compute_forces(bool energy, uint32_t groups);
+  std::vector<long long> evaluate(bool energy, uint32_t groups, double* forces);
   void enqueue_step(int step_offset);
   void run_graph_steps(int graph_launches);
   void check_status();
@@ -126,7 +134,7 @@ class Engine {
   double* inv_mass_ = nullptr;
   double* scratch3_ = nullptr;
   long long* force_ = nullptr;
-  long long* energy_ = nullptr;  // [7]
+  long long* energy_ = nullptr;  // [8 * segments]: energy, virial (6), unused
   int* status_ = nullptr;
   int* rebuild_ = nullptr;
   unsigned long long* rng_step_ = nullptr;
@@ -167,6 +175,16 @@ class Engine {
   bool dump_mode_ = false;
   int pair_grid_ = 0;
   int sm_count_ = 148;
+
+  // segments (independent systems) and the segment-padded slot order shared by the
+  // non-periodic nonbonded tiles and GBSA: every segment starts on a 32-slot boundary
+  std::vector<Segment> segments_;
+  std::vector<int> static_slot_atom_;   // [static_slots_], -1 = padding
+  std::vector<int> static_atom_slot_;   // [n_]
+  std::vector<int> static_block_seg_;   // [static_slots_ / 32]
+  int static_slots_ = 0;
+  int* d_block_segment_ = nullptr;
+  int* d_atom_segment_ = nullptr;
 
   // GBSAOBCForce
   const GbsaObcDef* gb_def_ = nullptr;

@@ -79,6 +79,7 @@ struct PairArgs {
   int tile_capacity;
   long long* force;     // [3][N] fixed point
   long long* energy;    // [7]: energy, virial xx yy zz xy xz yz (fixed point)
+  const int* block_segment;  // batch: system of each block, energy at energy[8 * system]
   Box<Real> box;
   Box<double> box_exact;
   int periodic;
@@ -185,6 +186,7 @@ struct ExceptionArgs {
   int ewald;
   double alpha;
   int n_atoms_for_force;  // row stride of the [3][N] force array
+  const int* atom_segment;  // batch: system of each particle, energy at energy[8 * system]
 };
 void launch_exceptions(const ExceptionArgs& a, bool energy, cudaStream_t s);
 
@@ -202,6 +204,7 @@ struct BondedArgs {
   long long* energy;
   Box<double> box;
   int n_atoms_for_force;
+  const int* atom_segment;  // batch: system of each particle, energy at energy[8 * system]
 };
 void launch_bonded(const BondedArgs& a, bool energy, cudaStream_t s);
 

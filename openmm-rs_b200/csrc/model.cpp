@@ -11,8 +11,8 @@
 
 namespace ommb200 {
 
-static void require(bool ok, const char* msg) {
-  if (!ok) throw Error(OMMB200_ERR_INVALID_ARG, msg);
+static void require(bool ok, const char* msg, int code = OMMB200_ERR_INVALID_ARG) {
+  if (!ok) throw Error(code, msg);
 }
 
 // nonbonded.rs:1245-1255
@@ -104,6 +104,121 @@ void validate_box(const double b[9]) {
   require(b[0] > 0.0 && b[4] > 0.0 && b[8] > 0.0 && b[0] >= 2.0 * std::fabs(b[3]) &&
               b[0] >= 2.0 * std::fabs(b[6]) && b[4] >= 2.0 * std::fabs(b[7]),
           "periodic box vectors must be in reduced form");
+}
+
+std::unique_ptr<SystemDef> merge_systems(std::vector<std::unique_ptr<SystemDef>> systems,
+                                         std::vector<Segment>* segments) {
+  require(!systems.empty(), "a batch needs at least one System");
+  auto out = std::make_unique<SystemDef>();
+  std::copy(systems[0]->box, systems[0]->box + 9, out->box);
+  NonbondedDef* nb = nullptr;
+  GbsaObcDef* gb = nullptr;
+  HarmonicBondDef* hb = nullptr;
+  HarmonicAngleDef* ha = nullptr;
+  std::vector<int> kinds0;
+  for (size_t k = 0; k < systems.size(); ++k) {
+    SystemDef& s = *systems[k];
+    require(s.masses.size() > 0, "every System of a batch needs particles");
+    const int off = (int)out->masses.size();
+    segments->push_back({off, (int)s.masses.size()});
+    out->masses.insert(out->masses.end(), s.masses.begin(), s.masses.end());
+    for (auto& c : s.constraints) out->constraints.push_back({c.p1 + off, c.p2 + off, c.distance});
+    std::vector<int> kinds;
+    for (auto& f : s.forces) kinds.push_back(f->kind);
+    std::sort(kinds.begin(), kinds.end());
+    kinds.erase(std::unique(kinds.begin(), kinds.end()), kinds.end());
+    if (k == 0) kinds0 = kinds;
+    require(kinds == kinds0, "every System of a batch must carry the same force kinds");
+    for (auto& f : s.forces) {
+      switch (f->kind) {
+        case kNonbonded: {
+          auto* src = static_cast<NonbondedDef*>(f.get());
+          if (!nb) {
+            nb = new NonbondedDef(*src);
+            nb->charge.clear();
+            nb->sigma.clear();
+            nb->epsilon.clear();
+            nb->exceptions.clear();
+            nb->owned_by_system = true;
+            out->forces.emplace_back(nb);
+          }
+          require(src->method == nb->method && src->cutoff == nb->cutoff &&
+                      src->reaction_field_dielectric == nb->reaction_field_dielectric &&
+                      src->use_switching == nb->use_switching &&
+                      src->switching_distance == nb->switching_distance &&
+                      src->force_group == nb->force_group &&
+                      src->include_direct_space == nb->include_direct_space,
+                  "the NonbondedForces of a batch must share their global settings");
+          require((int)src->charge.size() == (int)s.masses.size(),
+                  "NonbondedForce must have one parameter record per particle");
+          nb->charge.insert(nb->charge.end(), src->charge.begin(), src->charge.end());
+          nb->sigma.insert(nb->sigma.end(), src->sigma.begin(), src->sigma.end());
+          nb->epsilon.insert(nb->epsilon.end(), src->epsilon.begin(), src->epsilon.end());
+          for (auto e : src->exceptions) {
+            e.p1 += off;
+            e.p2 += off;
+            nb->exceptions.push_back(e);
+          }
+          break;
+        }
+        case kGbsaObc: {
+          auto* src = static_cast<GbsaObcDef*>(f.get());
+          if (!gb) {
+            gb = new GbsaObcDef(*src);
+            gb->charge.clear();
+            gb->radius.clear();
+            gb->scale.clear();
+            gb->owned_by_system = true;
+            out->forces.emplace_back(gb);
+          }
+          require(src->method == gb->method && src->cutoff == gb->cutoff &&
+                      src->solvent_dielectric == gb->solvent_dielectric &&
+                      src->solute_dielectric == gb->solute_dielectric &&
+                      src->surface_area_energy == gb->surface_area_energy &&
+                      src->force_group == gb->force_group,
+                  "the GBSAOBCForces of a batch must share their global settings");
+          gb->charge.insert(gb->charge.end(), src->charge.begin(), src->charge.end());
+          gb->radius.insert(gb->radius.end(), src->radius.begin(), src->radius.end());
+          gb->scale.insert(gb->scale.end(), src->scale.begin(), src->scale.end());
+          break;
+        }
+        case kHarmonicBond: {
+          auto* src = static_cast<HarmonicBondDef*>(f.get());
+          if (!hb) {
+            hb = new HarmonicBondDef();
+            hb->force_group = src->force_group;
+            hb->use_pbc = src->use_pbc;
+            hb->owned_by_system = true;
+            out->forces.emplace_back(hb);
+          }
+          require(src->force_group == hb->force_group && src->use_pbc == hb->use_pbc,
+                  "the HarmonicBondForces of a batch must share group and periodicity");
+          for (auto b : src->bonds) hb->bonds.push_back({b.p1 + off, b.p2 + off, b.length, b.k});
+          break;
+        }
+        case kHarmonicAngle: {
+          auto* src = static_cast<HarmonicAngleDef*>(f.get());
+          if (!ha) {
+            ha = new HarmonicAngleDef();
+            ha->force_group = src->force_group;
+            ha->use_pbc = src->use_pbc;
+            ha->owned_by_system = true;
+            out->forces.emplace_back(ha);
+          }
+          require(src->force_group == ha->force_group && src->use_pbc == ha->use_pbc,
+                  "the HarmonicAngleForces of a batch must share group and periodicity");
+          for (auto a : src->angles)
+            ha->angles.push_back({a.p1 + off, a.p2 + off, a.p3 + off, a.angle, a.k});
+          break;
+        }
+      }
+    }
+  }
+  if (systems.size() > 1) {
+    if (nb) require(!nb->periodic(), "a batch of several Systems must be non-periodic", OMMB200_ERR_UNSUPPORTED);
+    if (gb) require(gb->method != 2, "a batch of several Systems must be non-periodic", OMMB200_ERR_UNSUPPORTED);
+  }
+  return out;
 }
 
 void SystemDef::set_default_box(const double a[3], const double b[3], const double c[3]) {

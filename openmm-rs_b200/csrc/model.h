@@ -126,4 +126,16 @@ struct IntegratorDef {
 
 void validate_box(const double box[9]);  // system.rs:13-38
 
+// A contiguous particle range of the merged System that came from one input System.
+struct Segment {
+  int first, count;
+};
+
+// Concatenates independent Systems into one, with every force kind merged into a single
+// force whose particles, exceptions, bonds and angles are offset per input System.  The
+// inputs must carry the same force kinds with the same global settings, and must not be
+// periodic when there is more than one.  `segments` receives each input's particle range.
+std::unique_ptr<SystemDef> merge_systems(std::vector<std::unique_ptr<SystemDef>> systems,
+                                         std::vector<Segment>* segments);
+
 }  // namespace ommb200

@@ -153,12 +153,20 @@ __global__ void __launch_bounds__(32 * kPairWarps) pair_kernel(const PairArgs<Re
         e_tile += __shfl_xor_sync(FULL, e_tile, off);
         for (int c = 0; c < 6; ++c) w_tile[c] += __shfl_xor_sync(FULL, w_tile[c], off);
       }
-      e_fixed += to_fixed(e_tile, kEnergyScale);
-      for (int c = 0; c < 6; ++c) w_fixed[c] += to_fixed(w_tile[c], kEnergyScale);
+      if (a.block_segment) {  // a batch: each tile's energy goes to its own system
+        if (lane == 0) {
+          long long* dst = a.energy + 8 * a.block_segment[I];
+          add_fixed(dst, to_fixed(e_tile, kEnergyScale));
+          for (int c = 0; c < 6; ++c) add_fixed(dst + 1 + c, to_fixed(w_tile[c], kEnergyScale));
+        }
+      } else {
+        e_fixed += to_fixed(e_tile, kEnergyScale);
+        for (int c = 0; c < 6; ++c) w_fixed[c] += to_fixed(w_tile[c], kEnergyScale);
+      }
     }
     __syncwarp();
   }
-  if (kEnergy) {
+  if (kEnergy && !a.block_segment) {
     if (lane == 0) {
       add_fixed(a.energy, e_fixed);
       for (int c = 0; c < 6; ++c) add_fixed(a.energy + 1 + c, w_fixed[c]);

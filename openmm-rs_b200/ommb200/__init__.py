@@ -104,6 +104,11 @@ def library() -> C.CDLL:
             "ommb200_integrator_set_step_size": [P, D],
             "ommb200_integrator_set_integration_force_groups": [P, C.c_uint32],
             "ommb200_context_create": [P, P, C.POINTER(Options), C.POINTER(P)],
+            "ommb200_context_create_batch": [C.POINTER(P), I, P, C.POINTER(Options),
+                                             C.POINTER(P)],
+            "ommb200_context_num_systems": [P, C.POINTER(I)],
+            "ommb200_context_system_range": [P, I, C.POINTER(I), C.POINTER(I)],
+            "ommb200_context_get_system_energies": [P, C.c_uint32, C.POINTER(D), C.POINTER(D)],
             "ommb200_context_set_positions": [P, C.POINTER(D), I],
             "ommb200_context_set_velocities": [P, C.POINTER(D), I],
             "ommb200_context_set_velocities_to_temperature": [P, D, I],
@@ -433,6 +438,16 @@ class State:
         return self.kinetic_energy
 
 
+def _options(precision, device, use_cuda_graph, neighbor_skin, steps_per_graph) -> "Options":
+    opt = Options()
+    opt.precision = {"mixed": PRECISION_MIXED, "double": PRECISION_DOUBLE}[precision]
+    opt.device = device
+    opt.use_cuda_graph = int(use_cuda_graph)
+    opt.neighbor_skin = neighbor_skin
+    opt.steps_per_graph = steps_per_graph
+    return opt
+
+
 class Context:
     """context.rs:83-1163.  Takes ownership of `system` and `integrator` (context.rs:83-87)."""
 
@@ -440,12 +455,7 @@ class Context:
                  device: int = 0, use_cuda_graph: bool = True, neighbor_skin: float = 0.0,
                  steps_per_graph: int = 0):
         n = system.num_particles()
-        opt = Options()
-        opt.precision = {"mixed": PRECISION_MIXED, "double": PRECISION_DOUBLE}[precision]
-        opt.device = device
-        opt.use_cuda_graph = int(use_cuda_graph)
-        opt.neighbor_skin = neighbor_skin
-        opt.steps_per_graph = steps_per_graph
+        opt = _options(precision, device, use_cuda_graph, neighbor_skin, steps_per_graph)
         h = C.c_void_p()
         sys_h, int_h = system._take(), integrator._take()
         _check(library().ommb200_context_create(sys_h, int_h, C.byref(opt), C.byref(h)))
@@ -587,3 +597,52 @@ class Context:
                                                       C.byref(count)))
         keys = names.value.decode().split(";") if count.value else []
         return {k: (ms[i], launches[i]) for i, k in enumerate(keys)}
+
+
+class BatchContext(Context):
+    """Many independent Systems advanced by one Context (no reference counterpart: the
+    reference runs one Context per System).  The Systems share their force kinds and global
+    settings and, when there are several, are non-periodic; particle counts may differ.
+    Positions, velocities and forces are the Systems' particles concatenated in order;
+    `split` cuts such an array back into per-System pieces.  Takes ownership of every System
+    and the integrator."""
+
+    def __init__(self, systems, integrator: LangevinMiddleIntegrator, precision="mixed",
+                 device: int = 0, use_cuda_graph: bool = True, neighbor_skin: float = 0.0,
+                 steps_per_graph: int = 0):
+        systems = list(systems)
+        n = sum(s.num_particles() for s in systems)
+        opt = _options(precision, device, use_cuda_graph, neighbor_skin, steps_per_graph)
+        handles = (C.c_void_p * len(systems))(*[s._take() for s in systems])
+        h = C.c_void_p()
+        _check(library().ommb200_context_create_batch(handles, len(systems), integrator._take(),
+                                                      C.byref(opt), C.byref(h)))
+        self._h = h
+        self._n = n
+        self.step_size = integrator.step_size
+        self.precision = precision
+        self._ranges = [self.system_range(k) for k in range(self.num_systems())]
+
+    def num_systems(self) -> int:
+        out = C.c_int()
+        _check(library().ommb200_context_num_systems(self._h, C.byref(out)))
+        return out.value
+
+    def system_range(self, index: int) -> tuple:
+        """(first particle, particle count) of System `index`."""
+        first, count = C.c_int(), C.c_int()
+        _check(library().ommb200_context_system_range(self._h, index, C.byref(first),
+                                                      C.byref(count)))
+        return first.value, count.value
+
+    def split(self, array) -> list:
+        a = np.asarray(array)
+        return [a[f:f + c] for f, c in self._ranges]
+
+    def system_energies(self, groups: int = -1) -> tuple:
+        """(potential, kinetic) energies of every System, kJ/mol, as two arrays."""
+        k = len(self._ranges)
+        pot, kin = np.zeros(k), np.zeros(k)
+        _check(library().ommb200_context_get_system_energies(self._h, groups & 0xffffffff,
+                                                             _dptr(pot), _dptr(kin)))
+        return pot, kin

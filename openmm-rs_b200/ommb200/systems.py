@@ -43,14 +43,19 @@ def langevin(temperature=300.0, friction=1.0, step_size=0.002, seed=1234):
 
 
 def chain_system(chain, coulomb14=1.0, lj14=1.0, gbsa=True, solvent_dielectric=78.5,
-                 solute_dielectric=1.0, surface_area_energy=2.25936) -> System:
-    """One implicit-solvent chain: NoCutoff NonbondedForce with 1-2/1-3 exclusions and 1-4
-    exceptions, harmonic bonds and angles, and (by default) a NoCutoff GBSAOBCForce."""
+                 solute_dielectric=1.0, surface_area_energy=2.25936, cutoff=None) -> System:
+    """One implicit-solvent chain: NonbondedForce with 1-2/1-3 exclusions and 1-4 exceptions,
+    harmonic bonds and angles, and (by default) a GBSAOBCForce; NoCutoff, or
+    CutoffNonPeriodic for both forces when `cutoff` (nm) is given."""
     system = System()
     for _ in range(chain.n_atoms):
         system.add_particle(chain.mass)
     nb = NonbondedForce()
-    nb.set_nonbonded_method("NoCutoff")
+    if cutoff is None:
+        nb.set_nonbonded_method("NoCutoff")
+    else:
+        nb.set_nonbonded_method("CutoffNonPeriodic")
+        nb.set_cutoff_distance(cutoff)
     for q in chain.charges:
         nb.add_particle(float(q), chain.sigma, chain.epsilon)
     bonds = [(i, i + 1) for i in range(chain.n_atoms - 1)]
@@ -66,6 +71,9 @@ def chain_system(chain, coulomb14=1.0, lj14=1.0, gbsa=True, solvent_dielectric=7
     system.add_force(ha)
     if gbsa:
         gb = GBSAOBCForce()
+        if cutoff is not None:
+            gb.set_nonbonded_method(1)
+            gb.set_cutoff_distance(cutoff)
         gb.set_solvent_dielectric(solvent_dielectric)
         gb.set_solute_dielectric(solute_dielectric)
         gb.set_surface_area_energy(surface_area_energy)

@@ -117,3 +117,28 @@ def test_header_status_codes_match_python():
     codes = dict(re.findall(r"#define OMMB200_(ERR_[A-Z_]+) \((-\d+)\)", text))
     for name, value in codes.items():
         assert getattr(ommb200, name) == int(value), name
+
+
+def test_batch_validation_happens_before_the_device():
+    """Batch creation checks its Systems on the host: mismatched force kinds or settings and
+    periodic Systems are refused with their own codes (no GPU is touched)."""
+    chs = [synth.chain(20, seed=1), synth.chain(30, seed=2)]
+    with pytest.raises(ommb200.InvalidArgument):
+        ommb200.BatchContext([systems.chain_system(chs[0]),
+                              systems.chain_system(chs[1], gbsa=False)], systems.langevin())
+    with pytest.raises(ommb200.InvalidArgument):
+        ommb200.BatchContext([systems.chain_system(chs[0]),
+                              systems.chain_system(chs[1], cutoff=1.0)], systems.langevin())
+    w = synth.water_box(8, 1.9, (2, 2, 2), seed=1)
+    with pytest.raises(ommb200.OmmB200Error) as e:
+        ommb200.BatchContext([systems.water_system(w), systems.water_system(w)],
+                             systems.langevin())
+    assert e.value.code == ommb200.ERR_UNSUPPORTED
+    s = systems.chain_system(chs[0])
+    with pytest.raises(ommb200.InvalidArgument):
+        ommb200.BatchContext([s, s], systems.langevin())  # the second take is refused
+    lib = ommb200.library()
+    h = C.c_void_p()
+    integ = systems.langevin()
+    assert lib.ommb200_context_create_batch(None, 0, integ._take(), None, C.byref(h)) == \
+        ommb200.ERR_INVALID_ARG
