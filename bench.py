@@ -47,6 +47,8 @@ def parse():
                    help="skip the FP64-form, roofline and CPU-baseline legs")
     p.add_argument("--no-equilibrate", action="store_true",
                    help="start from the lattice (short runs for profiler captures)")
+    p.add_argument("--workload", choices=["water-23958", "chains-256"], default="water-23958",
+                   help="chains-256: 256 uneven implicit-solvent chains batched in one Context")
     return p.parse_args()
 
 
@@ -303,6 +305,9 @@ def main():
     if args.no_equilibrate:
         EQUILIBRATION_STEPS = 0
         TUNE = False
+    if args.workload == "chains-256":
+        main_chains(args)
+        return
     if args.impl == "reference":
         run_reference(args)
         return
@@ -432,6 +437,209 @@ def main():
         "gpu_launches": launches,
         "clocks": clocks,
         "roofline": roofline,
+        "cpu_baseline": cpu,
+    }
+    out.update(extras)
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+# FP32 work per pair of the Coulomb (NoCutoff) pair kernel: the Ewald count above with the
+# 28-flop screened term replaced by the 2-flop bare Coulomb term.
+FLOPS_PER_PAIR_COULOMB = FLOPS_PER_PAIR - 28 + 2
+CHAIN_DT_PS = 0.001
+
+
+def chain_oracle_step(O, ch, x, v, threads, k):
+    """One f64 oracle MD step of one chain: NonbondedForce (NoCutoff, 1-2/1-3 exclusions, 1-4
+    exceptions), GBSAOBCForce, bonds, angles, then LangevinMiddle."""
+    n = ch.n_atoms
+    excl = sorted({(i, i + 1) for i in range(n - 1)} | {(i, i + 2) for i in range(n - 2)})
+    exc = [(i, j, 0.0, ch.sigma, 0.0) for i, j in excl]
+    exc += [(i, i + 3, ch.charges[i] * ch.charges[i + 3], ch.sigma, ch.epsilon)
+            for i in range(n - 3)]
+    f, _ = O.nonbonded(x, ch.charges, [ch.sigma] * n, [ch.epsilon] * n, exc, method="NoCutoff",
+                       threads=threads)
+    f = f + O.gbsa_obc(x, ch.charges, ch.radii, [ch.gb_scale] * n, solvent_dielectric=78.5,
+                       solute_dielectric=1.0)[0]
+    f = f + O.harmonic_bonds(x, ch.bonds())[0] + O.harmonic_angles(x, ch.angles())[0]
+    import numpy as np
+
+    _, x, v = O.lfmiddle_step(x, v, f, np.full(n, ch.mass), CHAIN_DT_PS, 300.0, 1.0,
+                              O.gaussian_noise(1, 0, k, n), mode=0)
+    return x, v
+
+
+def chains_cpu(chs, threads, budget=10.0):
+    """The oracle's MD step time for the whole batch, extrapolated from chains stepped within
+    `budget` seconds by the batch's sum of n^2 (all terms but the bonded ones are O(n^2))."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import numpy as np
+
+    import oracle as O
+
+    spent, sample_n2, done = 0.0, 0.0, 0
+    for ch in chs:
+        x, v = ch.positions.copy(), np.zeros_like(ch.positions)
+        t0 = time.perf_counter()
+        chain_oracle_step(O, ch, x, v, threads, 0)
+        spent += time.perf_counter() - t0
+        sample_n2 += float(ch.n_atoms) ** 2
+        done += 1
+        if spent > budget:
+            break
+    total_n2 = sum(float(c.n_atoms) ** 2 for c in chs)
+    return spent * total_n2 / sample_n2, done, spent
+
+
+def main_chains(args):
+    """256 independent implicit-solvent chains (200-2,000 atoms each) in one BatchContext:
+    MD steps per second of the whole batch, against one Context per chain stepped in turn
+    (the reference's way to run many systems) and the oracle on the host."""
+    import numpy as np
+    import torch
+
+    import ommb200
+    from ommb200 import synth, systems
+
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        chs = synth.chain_batch(256, 200, 2000, seed=7)
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import oracle as O
+
+        threads = O.max_threads()
+        secs = []
+        for k in range(args.warmup + args.steps):
+            sec, done, spent = chains_cpu(chs, threads, budget=5.0)
+            secs.append(sec)
+        sec = statistics.median(secs[args.warmup:])
+        value = 1.0 / sec
+        print(json.dumps({
+            "impl": "reference", "metric": "MD steps/s of the 256-chain batch", "value": value,
+            "unit": "batch steps/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * sec, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "chains-256", "threads": threads},
+            "cpu_baseline": {"value": value, "unit": "batch steps/s", "cores": threads,
+                             "kind": "port", "sample": f"{done} chains per bench step, "
+                             "extrapolated by sum of n^2"},
+            "e2e": {"value": value, "unit": "batch steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}), flush=True)
+        return
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    chs = synth.chain_batch(256, 200, 2000, seed=7)
+    sizes = np.array([c.n_atoms for c in chs])
+    seed = 1000 + rank
+    ctx = ommb200.BatchContext([systems.chain_system(c) for c in chs],
+                               systems.langevin(step_size=CHAIN_DT_PS, seed=seed),
+                               precision=args.precision, device=local)
+    ctx.set_positions(np.concatenate([c.positions for c in chs]))
+    ctx.set_velocities_to_temperature(300.0, seed=seed)
+    ctx.step(500)  # untimed: relax the random-walk start
+    tuned = ctx.autotune(100)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{local}")
+    seg = args.segment
+    time_segments(ctx, torch, args.warmup, seg, flush)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+    torch.cuda.synchronize()
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        pass
+    sampler = ClockSampler(uuid)
+    ms = time_segments(ctx, torch, args.steps, seg, flush)
+    clocks = sampler.stop()
+    e2e_ms, h2d, d2h = time_e2e(ctx, torch, int(sizes.sum()), args.steps, seg, flush)
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([ms, e2e_ms], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, e2e_ms = float(t[0]), float(t[1])
+    md_steps = args.steps * seg
+    value = world * md_steps / (ms / 1000.0)
+    extras = {}
+    cpu = None
+    if rank == 0 and not args.skip_extras:
+        prof = 20
+        times = kernel_profile(ctx, prof)
+        extras["kernel_ms_per_md_step"] = {k: round(v[0] / prof, 5) for k, v in times.items()}
+        n_excl = int((2 * sizes - 3).sum())
+        pairs = int((sizes * (sizes - 1) // 2).sum()) - n_excl
+        pair_ms, pair_n = times.get("pair", (0.0, 1))
+        t_pair = pair_ms / max(pair_n, 1) / 1000.0
+        fp32_peak = ommb200.measure_fp32_peak(local)
+        achieved = pairs * FLOPS_PER_PAIR_COULOMB / t_pair / 1e12 if t_pair > 0 else None
+        extras["roofline"] = {
+            "bound": "fp32", "kernel": "pair_kernel<float, Coulomb>", "achieved": achieved,
+            "peak": fp32_peak, "unit": "TFLOP/s",
+            "frac": achieved / fp32_peak if achieved else None,
+            "algorithmic": f"{pairs} pairs x {FLOPS_PER_PAIR_COULOMB} flops per launch",
+            "avg_launch_ms": 1000.0 * t_pair, "traffic": None}
+        # one Context per chain, stepped in turn: a sample of the first 32 chains
+        sample = chs[:32]
+        total = 0.0
+        for k, ch in enumerate(sample):
+            one = ommb200.Context(systems.chain_system(ch),
+                                  systems.langevin(step_size=CHAIN_DT_PS, seed=seed),
+                                  precision=args.precision, device=local)
+            one.set_positions(ch.positions)
+            one.set_velocities_to_temperature(300.0, seed=seed)
+            one.step(seg)
+            total += time_segments(one, torch, 1, seg, flush)
+            one.close()
+        per_step_sep = total / seg * len(chs) / len(sample)
+        extras["separate_contexts"] = {
+            "ms_per_batch_step": per_step_sep,
+            "batch_speedup": per_step_sep / (ms / md_steps),
+            "sample": f"{len(sample)} of {len(chs)} chains, each its own Context, scaled by count"}
+        threads = os.cpu_count() or 1
+        sec, done, spent = chains_cpu(chs, threads)
+        cpu = {"value": 1.0 / sec, "unit": "batch steps/s", "cores": threads, "kind": "port",
+               "sample": f"{done} chains, one f64 oracle MD step each in {spent:.1f} s, "
+                         "extrapolated to the batch by sum of n^2"}
+        _, kin = ctx.system_energies()
+        temps = 2.0 * kin / (3 * sizes * 0.008314462618)
+        extras["temperature_k"] = {"mean": float(temps.mean()), "min": float(temps.min()),
+                                   "max": float(temps.max())}
+    out = {
+        "metric": "MD steps/s of the 256-chain batch", "value": value,
+        "unit": "batch steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms / args.steps, "ms_per_md_step": ms / md_steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp32" if args.precision == "mixed" else "fp64", "data": "synthetic",
+        "aggregate_ns_per_day": len(chs) * md_steps * CHAIN_DT_PS / 1000.0 / (ms / 1000.0) * 86400.0,
+        "gb_evaluations_per_s": len(chs) * value,
+        "config": {"workload": "chains-256", "n_systems": len(chs), "n_atoms": int(sizes.sum()),
+                   "sizes": "uniform in [200, 2000], seed 7",
+                   "method": "NoCutoff NonbondedForce + GBSAOBCForce (78.5 / 1), bonds, angles",
+                   "integrator": "LangevinMiddle 300 K, 1/ps, 1 fs",
+                   "md_steps_per_bench_step": seg,
+                   "l2": "flushed (256 MiB write) between timed bench steps",
+                   "parallelism": f"replicas x{world}", "autotuned": tuned},
+        "e2e": {"value": world * md_steps / (e2e_ms / 1000.0), "unit": "batch steps/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "clocks": clocks,
         "cpu_baseline": cpu,
     }
     out.update(extras)

@@ -16,6 +16,8 @@ from __future__ import annotations
 
 from dataclasses import dataclass, field
 
+import math
+
 import numpy as np
 
 D_OH = 0.09572
@@ -153,34 +155,61 @@ class Chain:
 
 
 def chain(n_atoms: int, seed: int, min_contact: float = 0.3, max_tries: int = 200) -> Chain:
-    """Self-avoiding random walk with tetrahedral bond angles and random dihedrals."""
+    """Self-avoiding random walk with tetrahedral bond angles and random dihedrals: monomer i
+    keeps at least `min_contact` from every monomer before i - 3 (checked on a cell grid of
+    that width); a monomer with no valid dihedral after `max_tries` draws backs the walk up
+    five monomers."""
     rng = np.random.default_rng(seed)
     b = 0.153
     theta = np.deg2rad(109.5)
-    pos = np.zeros((n_atoms, 3))
+    cos_t, sin_t = math.cos(theta), math.sin(theta)
+    mc2 = min_contact * min_contact
+    pos = [(0.0, 0.0, 0.0)] * n_atoms
     if n_atoms > 1:
-        pos[1] = [b, 0, 0]
+        pos[1] = (b, 0.0, 0.0)
     if n_atoms > 2:
-        pos[2] = pos[1] + b * np.array([-np.cos(theta), np.sin(theta), 0.0])
+        pos[2] = (b - b * cos_t, b * sin_t, 0.0)
+    cells = {}
+    in_grid = 0  # monomers 0 .. in_grid-1 are on the grid
+
+    def cell(p):
+        return (math.floor(p[0] / min_contact), math.floor(p[1] / min_contact),
+                math.floor(p[2] / min_contact))
+
+    def clear(p, i):
+        for dx in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                for dz in (-1, 0, 1):
+                    for j in cells.get((p[0] + dx, p[1] + dy, p[2] + dz), ()):
+                        q = pos[j]
+                        ex, ey, ez = q[0] - i[0], q[1] - i[1], q[2] - i[2]
+                        if ex * ex + ey * ey + ez * ez < mc2:
+                            return False
+        return True
+
     i = 3
     restarts = 0
     while i < n_atoms:
+        while in_grid < i - 3:
+            cells.setdefault(cell(pos[in_grid]), []).append(in_grid)
+            in_grid += 1
         a, bb, c = pos[i - 3], pos[i - 2], pos[i - 1]
-        bc = c - bb
-        bc /= np.linalg.norm(bc)
-        nrm = np.cross(bb - a, bc)
-        nrm /= np.linalg.norm(nrm)
-        m = np.cross(nrm, bc)
+        bc = (c[0] - bb[0], c[1] - bb[1], c[2] - bb[2])
+        nb = math.sqrt(bc[0] * bc[0] + bc[1] * bc[1] + bc[2] * bc[2])
+        bc = (bc[0] / nb, bc[1] / nb, bc[2] / nb)
+        u = (bb[0] - a[0], bb[1] - a[1], bb[2] - a[2])
+        nrm = (u[1] * bc[2] - u[2] * bc[1], u[2] * bc[0] - u[0] * bc[2], u[0] * bc[1] - u[1] * bc[0])
+        nn = math.sqrt(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2])
+        nrm = (nrm[0] / nn, nrm[1] / nn, nrm[2] / nn)
+        m = (nrm[1] * bc[2] - nrm[2] * bc[1], nrm[2] * bc[0] - nrm[0] * bc[2],
+             nrm[0] * bc[1] - nrm[1] * bc[0])
         placed = False
         for _ in range(max_tries):
             phi = rng.uniform(-np.pi, np.pi)
-            d = np.array([-b * np.cos(theta), b * np.sin(theta) * np.cos(phi),
-                          b * np.sin(theta) * np.sin(phi)])
-            p = c + d[0] * bc + d[1] * m + d[2] * nrm
-            if i > 3:
-                r2 = np.sum((pos[: i - 3] - p) ** 2, axis=1)
-                if r2.min() < min_contact * min_contact:
-                    continue
+            d0, d1, d2 = -b * cos_t, b * sin_t * math.cos(phi), b * sin_t * math.sin(phi)
+            p = tuple(c[k] + d0 * bc[k] + d1 * m[k] + d2 * nrm[k] for k in range(3))
+            if in_grid and not clear(cell(p), p):
+                continue
             pos[i] = p
             placed = True
             break
@@ -189,8 +218,12 @@ def chain(n_atoms: int, seed: int, min_contact: float = 0.3, max_tries: int = 20
         else:  # dead end: back up a few monomers
             restarts += 1
             i = max(3, i - 5)
+            while in_grid > i - 3:
+                in_grid -= 1
+                cells[cell(pos[in_grid])].remove(in_grid)
             if restarts > 100 * n_atoms:
                 raise RuntimeError("self-avoiding walk failed")
+    pos = np.array(pos, dtype=np.float64).reshape(n_atoms, 3)
     pos -= pos.mean(axis=0)
     q = rng.normal(0.0, 0.3, n_atoms)
     q -= q.mean()
