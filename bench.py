@@ -47,8 +47,10 @@ def parse():
                    help="skip the FP64-form, roofline and CPU-baseline legs")
     p.add_argument("--no-equilibrate", action="store_true",
                    help="start from the lattice (short runs for profiler captures)")
-    p.add_argument("--workload", choices=["water-23958", "chains-256"], default="water-23958",
-                   help="chains-256: 256 uneven implicit-solvent chains batched in one Context")
+    p.add_argument("--workload", choices=["water-23958", "water-1065000", "chains-256"],
+                   default="water-23958",
+                   help="water-1065000: the 22 nm box of 355,000 waters; chains-256: 256 uneven "
+                        "implicit-solvent chains batched in one Context")
     return p.parse_args()
 
 
@@ -287,8 +289,9 @@ def run_reference(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000.0 * secs / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "n_atoms": w.n_atoms, "box_nm": 6.2, "dt_ps": DT_PS,
-                   "method": "PME cutoff 0.9 nm tol 5e-4 grid 56^3",
+        "config": {"workload": WORKLOAD, "n_atoms": w.n_atoms, "box_nm": float(w.box[0][0]),
+                   "dt_ps": DT_PS, "method": "PME cutoff 0.9 nm tol 5e-4, grid by the "
+                                             "tolerance rule",
                    "md_steps_per_bench_step": 1, "threads": threads},
         "cpu_baseline": {"value": value, "unit": "ns/day", "cores": threads, "kind": "port",
                          "sample": f"{args.steps} MD steps, f64 oracle port of the reference "
@@ -301,7 +304,9 @@ def run_reference(args):
 
 def main():
     args = parse()
-    global EQUILIBRATION_STEPS, TUNE
+    global EQUILIBRATION_STEPS, TUNE, WORKLOAD
+    if args.workload.startswith("water"):
+        WORKLOAD = args.workload
     if args.no_equilibrate:
         EQUILIBRATION_STEPS = 0
         TUNE = False
@@ -345,9 +350,11 @@ def main():
     except Exception:
         pass
     barrier()
+    rebuilds0 = ctx.nlist_stats()["rebuilds"]
     sampler = ClockSampler(uuid)
     ms = time_segments(ctx, torch, args.steps, args.segment, flush)
     clocks = sampler.stop()
+    rebuilds_timed = ctx.nlist_stats()["rebuilds"] - rebuilds0
     barrier()
     e2e_ms, h2d, d2h = time_e2e(ctx, torch, w.n_atoms, args.steps, args.segment, flush)
     barrier()
@@ -368,7 +375,7 @@ def main():
     if rank == 0 and not args.skip_extras:
         prof_steps = 100
         times = kernel_profile(ctx, prof_steps)
-        pairs = len(ctx.debug_pair_list())
+        pairs = ctx.count_pairs()
         pair_ms, pair_n = times.get("pair", (0.0, 1))
         t_pair = pair_ms / max(pair_n, 1) / 1000.0
         fp32_peak = ommb200.measure_fp32_peak(local)
@@ -399,8 +406,7 @@ def main():
         extras["pairs_in_cutoff"] = pairs
         nl = ctx.nlist_stats()
         nl["pair_efficiency"] = pairs / max(1, nl["tiles"] * 1024)
-        steps_on_ctx = (args.warmup + 2 * args.steps) * args.segment + prof_steps
-        nl["md_steps_per_rebuild"] = steps_on_ctx / max(1, nl["rebuilds"])
+        nl["md_steps_per_rebuild"] = md_steps / max(1, rebuilds_timed)  # timed region only
         extras["nlist"] = nl
         # FP64-on-GPU form of the same kernels
         _, ctx64 = build_context("double", seed, local)
@@ -422,8 +428,9 @@ def main():
         "ms_per_step": ms / args.steps, "ms_per_md_step": ms / md_steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "fp32" if args.precision == "mixed" else "fp64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "n_atoms": w.n_atoms, "box_nm": 6.2,
-                   "method": "PME cutoff 0.9 nm, Ewald tol 5e-4, grid 56^3, order 5",
+        "config": {"workload": WORKLOAD, "n_atoms": w.n_atoms, "box_nm": float(w.box[0][0]),
+                   "method": "PME cutoff 0.9 nm, Ewald tol 5e-4, grid %d^3, order 5"
+                             % ctx.get_pme_parameters()[1][0],
                    "integrator": "LangevinMiddle 300 K, 1/ps, 2 fs, SETTLE",
                    "precision": args.precision + " (FP32 pair/spline math, int64 fixed-point "
                                 "forces, FP64 integration and constraints)",

@@ -290,98 +290,126 @@ __global__ void __launch_bounds__(32 * kListWarps) nl_lists(NlistArgs a) {
       if (t >= 0) write_entry<kDouble>(a, t, lane, slot, sh);
       __syncwarp();
     };
-    for (int base = I + 1; base < nb; base += 32) {
-      const int J = base + lane;
-      bool cand = false, unsafe = false;
-      double d[3] = {0.0, 0.0, 0.0};
-      if (J < nb) {
-        const double* cj = a.block_center + 3 * J;
-        const double* hj = a.block_half + 3 * J;
-        d[0] = cj[0] - ci[0];
-        d[1] = cj[1] - ci[1];
-        d[2] = cj[2] - ci[2];
-        double gap2 = 0.0;
-        if (a.periodic) {
-          min_image_fast(d[0], d[1], d[2], a.box);
-          const double rj = sqrt(hj[0] * hj[0] + hj[1] * hj[1] + hj[2] * hj[2]);
-          const double dist = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
-          // every other image is at least min_width - |d| away (reduced box); when that is
-          // not enough to rule the other images out, all 27 images are tested
-          unsafe = a.min_width - dist < reach + ri + rj;
+    // candidate blocks J in [j0, j1), 32 per pass
+    auto scan = [&](int j0, int j1) {
+      for (int base = j0; base < j1; base += 32) {
+        const int J = base + lane;
+        bool cand = false, unsafe = false;
+        double d[3] = {0.0, 0.0, 0.0};
+        if (J < j1) {
+          const double* cj = a.block_center + 3 * J;
+          const double* hj = a.block_half + 3 * J;
+          d[0] = cj[0] - ci[0];
+          d[1] = cj[1] - ci[1];
+          d[2] = cj[2] - ci[2];
+          double gap2 = 0.0;
+          if (a.periodic) {
+            min_image_fast(d[0], d[1], d[2], a.box);
+            const double rj = sqrt(hj[0] * hj[0] + hj[1] * hj[1] + hj[2] * hj[2]);
+            const double dist = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+            // every other image is at least min_width - |d| away (reduced box); when that is
+            // not enough to rule the other images out, all 27 images are tested
+            unsafe = a.min_width - dist < reach + ri + rj;
+          }
+          gap2 = box_gap2(d, hi, hj);
+          if (unsafe) {
+            const Box<double>& b = a.box;
+            for (int m0 = -1; m0 <= 1; ++m0)
+              for (int m1 = -1; m1 <= 1; ++m1)
+                for (int m2 = -1; m2 <= 1; ++m2) {
+                  const double e[3] = {d[0] + m0 * b.ax + m1 * b.bx + m2 * b.cx,
+                                       d[1] + m1 * b.by + m2 * b.cy, d[2] + m2 * b.cz};
+                  gap2 = fmin(gap2, box_gap2(e, hi, hj));
+                }
+          }
+          cand = gap2 < reach2;
         }
-        gap2 = box_gap2(d, hi, hj);
-        if (unsafe) {
-          const Box<double>& b = a.box;
-          for (int m0 = -1; m0 <= 1; ++m0)
-            for (int m1 = -1; m1 <= 1; ++m1)
-              for (int m2 = -1; m2 <= 1; ++m2) {
-                const double e[3] = {d[0] + m0 * b.ax + m1 * b.bx + m2 * b.cx,
-                                     d[1] + m1 * b.by + m2 * b.cy, d[2] + m2 * b.cz};
-                gap2 = fmin(gap2, box_gap2(e, hi, hj));
-              }
+        unsigned cm = __ballot_sync(kFull, cand);
+        while (cm) {
+          const int src = __ffs(cm) - 1;
+          cm &= cm - 1;
+          const int Jc = base + src;
+          const double s0 = __shfl_sync(kFull, d[0], src), s1 = __shfl_sync(kFull, d[1], src),
+                       s2 = __shfl_sync(kFull, d[2], src);
+          const bool un = __shfl_sync(kFull, unsafe, src);
+          const int aj = a.sorted_atom[32 * Jc + lane];
+          bool in = false;
+          if (aj >= 0) {
+            const Box<double>& b = a.box;
+            const double n0 = a.image[3 * aj], n1 = a.image[3 * aj + 1], n2 = a.image[3 * aj + 2];
+            const double* cj = a.block_center + 3 * Jc;
+            double rel[3] = {a.pos_ref[3 * aj] - (n0 * b.ax + n1 * b.bx + n2 * b.cx) - cj[0] + s0,
+                             a.pos_ref[3 * aj + 1] - (n1 * b.by + n2 * b.cy) - cj[1] + s1,
+                             a.pos_ref[3 * aj + 2] - n2 * b.cz - cj[2] + s2};
+            if (un) {
+              // conservative: the nearest image of the particle to I's centre, against a
+              // sphere that contains I's box
+              min_image_fast(rel[0], rel[1], rel[2], b);
+              const double r = sqrt(rel[0] * rel[0] + rel[1] * rel[1] + rel[2] * rel[2]);
+              in = r < reach + ri + 1e-6;
+            } else {
+              in = box_gap2(rel, hi, nullptr) < reach2;
+            }
+          }
+          const unsigned im = __ballot_sync(kFull, in);
+          if (in) {
+            const int p = pending + __popc(im & ((1u << lane) - 1u));
+            s_slot[w][p] = 32 * Jc + lane;
+            s_flag[w][p] = un ? kTilePairImage : 0;
+            s_shift[w][p][0] = s0;
+            s_shift[w][p][1] = s1;
+            s_shift[w][p][2] = s2;
+          }
+          pending += __popc(im);
+          __syncwarp();
+          if (pending >= 32) {
+            flush(32);
+            const int rest = pending - 32;
+            int sl = 0, fl = 0;
+            double sh0 = 0.0, sh1 = 0.0, sh2 = 0.0;
+            if (lane < rest) {
+              sl = s_slot[w][32 + lane];
+              fl = s_flag[w][32 + lane];
+              sh0 = s_shift[w][32 + lane][0];
+              sh1 = s_shift[w][32 + lane][1];
+              sh2 = s_shift[w][32 + lane][2];
+            }
+            __syncwarp();
+            if (lane < rest) {
+              s_slot[w][lane] = sl;
+              s_flag[w][lane] = fl;
+              s_shift[w][lane][0] = sh0;
+              s_shift[w][lane][1] = sh1;
+              s_shift[w][lane][2] = sh2;
+            }
+            pending = rest;
+            __syncwarp();
+          }
         }
-        cand = gap2 < reach2;
       }
-      unsigned cm = __ballot_sync(kFull, cand);
-      while (cm) {
-        const int src = __ffs(cm) - 1;
-        cm &= cm - 1;
-        const int Jc = base + src;
-        const double s0 = __shfl_sync(kFull, d[0], src), s1 = __shfl_sync(kFull, d[1], src),
-                     s2 = __shfl_sync(kFull, d[2], src);
-        const bool un = __shfl_sync(kFull, unsafe, src);
-        const int aj = a.sorted_atom[32 * Jc + lane];
-        bool in = false;
-        if (aj >= 0) {
-          const Box<double>& b = a.box;
-          const double n0 = a.image[3 * aj], n1 = a.image[3 * aj + 1], n2 = a.image[3 * aj + 2];
-          const double* cj = a.block_center + 3 * Jc;
-          double rel[3] = {a.pos_ref[3 * aj] - (n0 * b.ax + n1 * b.bx + n2 * b.cx) - cj[0] + s0,
-                           a.pos_ref[3 * aj + 1] - (n1 * b.by + n2 * b.cy) - cj[1] + s1,
-                           a.pos_ref[3 * aj + 2] - n2 * b.cz - cj[2] + s2};
-          if (un) {
-            // conservative: the nearest image of the particle to I's centre, against a
-            // sphere that contains I's box
-            min_image_fast(rel[0], rel[1], rel[2], b);
-            const double r = sqrt(rel[0] * rel[0] + rel[1] * rel[1] + rel[2] * rel[2]);
-            in = r < reach + ri + 1e-6;
-          } else {
-            in = box_gap2(rel, hi, nullptr) < reach2;
-          }
-        }
-        const unsigned im = __ballot_sync(kFull, in);
-        if (in) {
-          const int p = pending + __popc(im & ((1u << lane) - 1u));
-          s_slot[w][p] = 32 * Jc + lane;
-          s_flag[w][p] = un ? kTilePairImage : 0;
-          s_shift[w][p][0] = s0;
-          s_shift[w][p][1] = s1;
-          s_shift[w][p][2] = s2;
-        }
-        pending += __popc(im);
-        __syncwarp();
-        if (pending >= 32) {
-          flush(32);
-          const int rest = pending - 32;
-          int sl = 0, fl = 0;
-          double sh0 = 0.0, sh1 = 0.0, sh2 = 0.0;
-          if (lane < rest) {
-            sl = s_slot[w][32 + lane];
-            fl = s_flag[w][32 + lane];
-            sh0 = s_shift[w][32 + lane][0];
-            sh1 = s_shift[w][32 + lane][1];
-            sh2 = s_shift[w][32 + lane][2];
-          }
-          __syncwarp();
-          if (lane < rest) {
-            s_slot[w][lane] = sl;
-            s_flag[w][lane] = fl;
-            s_shift[w][lane][0] = sh0;
-            s_shift[w][lane][1] = sh1;
-            s_shift[w][lane][2] = sh2;
-          }
-          pending = rest;
-          __syncwarp();
+    };
+    const Box<double>& bx = a.box;
+    if (!a.periodic || bx.bx != 0.0 || bx.cx != 0.0 || bx.cy != 0.0 || a.sorted_atom[32 * I] < 0) {
+      scan(I + 1, nb);  // triclinic: every later block is a candidate
+    } else {
+      // rectangular box: blocks lie inside their x-y column, so only columns whose x and y
+      // ranges come within `reach` of I's column can hold candidates (a column k apart is at
+      // least (k - 1) column widths away); the range covers every periodic image
+      const int first = a.sorted_atom[32 * I];
+      const int col = first >= 0 ? a.column[first] : 0;
+      const int nx = a.n_col[0], ny = a.n_col[1];
+      const int kx = (int)floor(reach * nx / bx.ax + 1e-6) + 1;
+      const int ky = (int)floor(reach * ny / bx.by + 1e-6) + 1;
+      const bool all_x = 2 * kx + 1 >= nx, all_y = 2 * ky + 1 >= ny;
+      const int x0 = col % nx, y0 = col / nx;
+      const int ny_iter = all_y ? ny : 2 * ky + 1, nx_iter = all_x ? nx : 2 * kx + 1;
+      for (int oy = 0; oy < ny_iter; ++oy) {
+        const int cy = all_y ? oy : (y0 + oy - ky + ny) % ny;
+        for (int ox = 0; ox < nx_iter; ++ox) {
+          const int cx = all_x ? ox : (x0 + ox - kx + nx) % nx;
+          const int c = cy * nx + cx;
+          const int j0 = max(a.col_start[c] / 32, I + 1), j1 = min(a.col_start[c + 1] / 32, nb);
+          if (j0 < j1) scan(j0, j1);
         }
       }
     }

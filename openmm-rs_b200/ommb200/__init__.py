@@ -542,6 +542,12 @@ class Context:
             self._h, cap, out.ctypes.data_as(C.POINTER(C.c_int32)), C.byref(count)))
         return out[:min(cap, count.value)]
 
+    def count_pairs(self) -> int:
+        """Number of interacting nonbonded pairs at the current positions (pair kernel)."""
+        count = C.c_int64()
+        _check(library().ommb200_context_debug_pair_list(self._h, 0, None, C.byref(count)))
+        return count.value
+
     def set_profiling(self, enabled: bool) -> None:
         _check(library().ommb200_context_set_profiling(self._h, int(enabled)))
 
