@@ -233,6 +233,29 @@ int ommb200_nonbonded_forces_noalloc(int n, const double* positions, const doubl
                                      double cutoff, double reaction_field_dielectric,
                                      double* forces, double* energy, void* stream);
 
+/* ---- learned Born radii network (no reference counterpart) ----
+ * Per particle: 32 radial symmetry-function features -> 64 -> 64 -> 1 (tanh), predicting the
+ * long-range tail of the OBC descreening integral.  BF16 tensor-core kernels with FP32
+ * accumulation.  Parameters are a flat float block of OMMB200_RADII_MLP_PARAMS values:
+ * W1[32][64], b1[64], W2[64][64], b2[64], w3[64], b3 (the first OMMB200_RADII_MLP_TRAINABLE
+ * are trained), then feature mean[32], feature 1/std[32], target mean, target scale.
+ * All pointers are device pointers; work runs on `stream` (a cudaStream_t, NULL = legacy
+ * default) and the call returns after it completes. */
+#define OMMB200_RADII_MLP_PARAMS 6403
+#define OMMB200_RADII_MLP_TRAINABLE 6337
+/* tail[n] and, if not NULL, d tail / d features [n][32] from features [n][32]. */
+int ommb200_radii_mlp_forward(int n, const float* features, const float* params, float* tail,
+                              float* dtail_dfeatures, void* stream);
+/* `steps` Adam steps (lr, beta 0.9 / 0.999, eps 1e-8) on the mean squared error of the
+ * normalised target over batches of `batch` particles (a multiple of 128) drawn from the n
+ * rows by `seed` (all rows in order when batch == n).  adam_moments [2][TRAINABLE] (m then v)
+ * and *adam_step are updated with the parameters.  grad_out [TRAINABLE] (may be NULL)
+ * receives the last batch's gradient, loss_out [steps] (may be NULL) each batch's loss. */
+int ommb200_radii_mlp_train(int n, const float* features, const float* targets, float* params,
+                            float* adam_moments, int* adam_step, int steps, int batch,
+                            double learning_rate, uint64_t seed, float* grad_out,
+                            float* loss_out, void* stream);
+
 /* ---- diagnostics (no reference counterpart) ---- */
 /* The interacting nonbonded pair set at the current positions, as evaluated by the pair
  * kernel itself: (i, j) with i < j in original particle indices, unsorted.  Writes up to

@@ -76,6 +76,35 @@ void set_out(int* out, int v) {
   if (out) *out = v;
 }
 
+void check_cuda(cudaError_t e) {
+  if (e != cudaSuccess) throw Error(OMMB200_ERR_CUDA, cudaGetErrorString(e));
+}
+// Runs `launch(status)` on `stream` and waits; device faults and kernel status become codes.
+template <class F>
+void run_standalone(void* stream, F&& launch) {
+  int* status = nullptr;
+  check_cuda(cudaMalloc(&status, sizeof(int)));
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int code = 0;
+  try {
+    check_cuda(cudaMemsetAsync(status, 0, sizeof(int), s));
+    launch(status);
+    check_cuda(cudaGetLastError());
+    check_cuda(cudaMemcpyAsync(&code, status, sizeof(int), cudaMemcpyDeviceToHost, s));
+    check_cuda(cudaStreamSynchronize(s));
+  } catch (...) {
+    cudaFree(status);
+    throw;
+  }
+  cudaFree(status);
+  if (code != 0) throw Error(OMMB200_ERR_TIMEOUT, "tensor-core wait timed out");
+}
+int device_sm_count() {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return sms;
+}
 }  // namespace
 
 extern "C" {
@@ -567,6 +596,36 @@ int ommb200_context_get_pme_parameters(const ommb200_context* ctx, double* alpha
     ctx->engine->pme_parameters(alpha, nx, ny, nz);
   });
 }
+
+int ommb200_radii_mlp_forward(int n, const float* features, const float* params, float* tail,
+                              float* dtail_dfeatures, void* stream) {
+  return guarded([&] {
+    require(n > 0 && features && params && tail, "invalid arguments");
+    run_standalone(stream, [&](int* status) {
+      launch_mlp_infer(n, features, params, tail, dtail_dfeatures, status, device_sm_count(),
+                       static_cast<cudaStream_t>(stream));
+    });
+  });
+}
+int ommb200_radii_mlp_train(int n, const float* features, const float* targets, float* params,
+                            float* adam_moments, int* adam_step, int steps, int batch,
+                            double learning_rate, uint64_t seed, float* grad_out,
+                            float* loss_out, void* stream) {
+  return guarded([&] {
+    require(n > 0 && features && targets && params && adam_moments && adam_step,
+            "invalid arguments");
+    require(steps > 0 && batch >= 128 && batch % 128 == 0,
+            "batch must be a positive multiple of 128 and steps positive");
+    require(std::isfinite(learning_rate) && learning_rate >= 0.0, "invalid learning rate");
+    run_standalone(stream, [&](int* status) {
+      launch_mlp_train(n, features, targets, params, adam_moments,
+                       adam_moments + kRadiiMlpTrainable, adam_step, steps, batch,
+                       (float)learning_rate, seed, grad_out, loss_out, status,
+                       static_cast<cudaStream_t>(stream));
+    });
+  });
+}
+
 int ommb200_context_num_systems(const ommb200_context* ctx, int* out) {
   return guarded([&] {
     require(ctx && ctx->engine && out, "null argument");

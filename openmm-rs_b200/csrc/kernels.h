@@ -2,6 +2,7 @@
 // given stream and never synchronizes, so a whole MD step can be captured in a CUDA graph.
 #pragma once
 
+#include <algorithm>
 #include <cuda_runtime.h>
 #include <cufft.h>
 #include <stdint.h>
@@ -248,5 +249,23 @@ void launch_advance_counter(unsigned long long* counter, int by, cudaStream_t s)
 // set_velocities_to_temperature).
 void launch_constrain_positions(const IntegrateArgs& a, const double* reference, cudaStream_t s);
 void launch_constrain_velocities(const IntegrateArgs& a, cudaStream_t s);
+
+// ---- learned Born radii network (radii_mlp.cu) ------------------------------------------
+// Flat float parameter block: W1[32][64], b1[64], W2[64][64], b2[64], w3[64], b3 (trainable),
+// then feature mean[32], feature 1/std[32], target mean, target scale.
+constexpr int kRadiiMlpParams = 6403;
+constexpr int kRadiiMlpTrainable = 6337;
+constexpr int kRadiiFeatures = 32;
+// tail[n] = network output in integral units; dtail[n][32] = d tail / d features (may be null).
+void launch_mlp_infer(int n, const float* features, const float* params, float* tail,
+                      float* dtail, int* status, int sm_count, cudaStream_t s);
+// `steps` Adam steps on batches of `batch` (multiple of 128) particles drawn from the n
+// snapshot rows (all of them in order when batch == n).  adam_m / adam_v hold the moments of
+// the trainable block, *adam_t the step count; grad_out (may be null) receives the gradient of
+// the last batch, loss_out[steps] (may be null) each batch's mean squared error.
+void launch_mlp_train(int n, const float* features, const float* targets, float* params,
+                      float* adam_m, float* adam_v, int* adam_t, int steps, int batch, float lr,
+                      unsigned long long seed, float* grad_out, float* loss_out, int* status,
+                      cudaStream_t s);
 
 }  // namespace ommb200

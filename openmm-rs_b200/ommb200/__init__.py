@@ -126,6 +126,8 @@ def library() -> C.CDLL:
                                                 C.POINTER(C.c_int64)],
             "ommb200_context_kernel_times": [P, I, C.c_char_p, I, C.POINTER(D), C.POINTER(I),
                                              C.POINTER(I)],
+            "ommb200_radii_mlp_forward": [I, P, P, P, P, P],
+            "ommb200_radii_mlp_train": [I, P, P, P, P, P, I, I, D, C.c_uint64, P, P, P],
         }
         for name, args in sig.items():
             fn = getattr(lib, name)
@@ -652,3 +654,53 @@ class BatchContext(Context):
         _check(library().ommb200_context_get_system_energies(self._h, groups & 0xffffffff,
                                                              _dptr(pot), _dptr(kin)))
         return pot, kin
+
+
+# ---- learned Born radii network (no reference counterpart) --------------------------------
+RADII_MLP_PARAMS = 6403
+RADII_MLP_TRAINABLE = 6337
+
+
+def _devptr(t):
+    if t is None:
+        return None
+    if not (t.is_cuda and t.is_contiguous() and str(t.dtype) in ("torch.float32", "torch.int32")):
+        raise InvalidArgument(ERR_INVALID_ARG, "expected a contiguous float32/int32 CUDA tensor")
+    return t.data_ptr()
+
+
+def _stream_of(t):
+    import torch
+
+    return torch.cuda.current_stream(t.device).cuda_stream
+
+
+def radii_mlp_forward(features, params, with_gradient=True):
+    """Network tail [n] and d tail / d features [n, 32] (None without `with_gradient`) for
+    float32 CUDA tensors features [n, 32] and params [RADII_MLP_PARAMS]."""
+    import torch
+
+    n = int(features.shape[0])
+    tail = torch.empty(n, dtype=torch.float32, device=features.device)
+    dt = torch.empty(n, 32, dtype=torch.float32, device=features.device) if with_gradient else None
+    _check(library().ommb200_radii_mlp_forward(n, _devptr(features), _devptr(params),
+                                               _devptr(tail), _devptr(dt),
+                                               _stream_of(features)))
+    return tail, dt
+
+
+def radii_mlp_train(features, targets, params, moments, step, steps, batch, learning_rate=1e-3,
+                    seed=0, with_gradient=False):
+    """Adam steps on the network, in place on params [RADII_MLP_PARAMS], moments
+    [2, RADII_MLP_TRAINABLE] and step (int32 [1]); returns (losses [steps], last gradient or
+    None)."""
+    import torch
+
+    n = int(features.shape[0])
+    loss = torch.zeros(steps, dtype=torch.float32, device=features.device)
+    grad = (torch.zeros(RADII_MLP_TRAINABLE, dtype=torch.float32, device=features.device)
+            if with_gradient else None)
+    _check(library().ommb200_radii_mlp_train(
+        n, _devptr(features), _devptr(targets), _devptr(params), _devptr(moments), _devptr(step),
+        steps, batch, learning_rate, seed, _devptr(grad), _devptr(loss), _stream_of(features)))
+    return loss, grad

@@ -948,6 +948,174 @@ extern "C" int orc_gbsa_obc(int n, const double* pos, const double* charge, cons
 }
 
 // ---------------------------------------------------------------------------------------
+// Learned Born radii (no reference counterpart; the OBC terms follow gbsa_obc.rs:184-309).
+// The HCT integral is split as I_i = I_short_i + tail_i:
+//   I_short_i = sum_j H(r_ij; rho_i, s_j) S(r_ij), S the quintic switch from rs to rc;
+//   tail_i    = the network's prediction from radial symmetry functions (Behler & Parrinello,
+//               Phys. Rev. Lett. 98, 146401 (2007)) G_if = sum_j exp(-eta (r_ij - mu_f)^2)
+//               fc(r_ij), fc(r) = (cos(pi r / rc) + 1) / 2, mu_f = mu0 + f dmu.
+// Forces follow from dE/dI_i and dI_i/dr_ij = Phi'_ij(r) with
+//   Phi_ij(r) = H(r; i, j) S(r) + sum_f (d tail_i / d G_if) g_f(r).
+// ---------------------------------------------------------------------------------------
+namespace {
+double switch_value(double r, double rs, double rc, double* deriv) {
+  if (r <= rs) {
+    *deriv = 0.0;
+    return 1.0;
+  }
+  if (r >= rc) {
+    *deriv = 0.0;
+    return 0.0;
+  }
+  const double w = rc - rs, t = (r - rs) / w;
+  *deriv = -30.0 * t * t * (1.0 - t) * (1.0 - t) / w;
+  return 1.0 + t * t * t * (-10.0 + t * (15.0 - 6.0 * t));
+}
+// g_f(r) and g_f'(r) for all features; zero beyond rc.
+void radial_functions(double r, int nf, double mu0, double dmu, double eta, double rc,
+                      double* g, double* dg) {
+  if (r >= rc) {
+    for (int f = 0; f < nf; ++f) g[f] = dg[f] = 0.0;
+    return;
+  }
+  const double fc = 0.5 * (std::cos(kPi * r / rc) + 1.0);
+  const double dfc = -0.5 * kPi / rc * std::sin(kPi * r / rc);
+  for (int f = 0; f < nf; ++f) {
+    const double x = r - (mu0 + f * dmu);
+    const double e = std::exp(-eta * x * x);
+    g[f] = e * fc;
+    dg[f] = e * (-2.0 * eta * x * fc + dfc);
+  }
+}
+}  // namespace
+
+extern "C" int orc_radial_features(int n, const double* pos, int nf, double mu0, double dmu,
+                                   double eta, double rc, double* features) {
+  if (nf <= 0 || nf > 64) return -1;
+  std::fill(features, features + (size_t)n * nf, 0.0);
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int i = 0; i < n; ++i) {
+    double g[64], dg[64];
+    for (int j = 0; j < n; ++j) {
+      if (j == i) continue;
+      const double d[3] = {pos[3 * j] - pos[3 * i], pos[3 * j + 1] - pos[3 * i + 1],
+                           pos[3 * j + 2] - pos[3 * i + 2]};
+      const double r = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+      if (r >= rc) continue;
+      radial_functions(r, nf, mu0, dmu, eta, rc, g, dg);
+      for (int f = 0; f < nf; ++f) features[(size_t)i * nf + f] += g[f];
+    }
+  }
+  return 0;
+}
+
+extern "C" int orc_learned_gbsa(int n, const double* pos, const double* charge,
+                                const double* radius, const double* scale,
+                                double solvent_dielectric, double solute_dielectric,
+                                double surface_area_energy, double rs, double rc, int nf,
+                                double mu0, double dmu, double eta, const double* tail,
+                                const double* dtail_dg, double* forces, double* energy_out,
+                                double* born_out, double* short_out, double* full_out) {
+  if (nf <= 0 || nf > 64 || !(rs < rc)) return -1;
+  std::vector<GbParticle> p(n);
+  for (int i = 0; i < n; ++i) p[i] = {charge[i], radius[i], scale[i]};
+  std::vector<double> integral(n, 0.0), full(n, 0.0), born(n), dedi(n, 0.0);
+  std::fill(forces, forces + 3 * (size_t)n, 0.0);
+  for (int i = 0; i < n; ++i)
+    for (int j = i + 1; j < n; ++j) {
+      const double d[3] = {pos[3 * j] - pos[3 * i], pos[3 * j + 1] - pos[3 * i + 1],
+                           pos[3 * j + 2] - pos[3 * i + 2]};
+      const double r = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+      const double hij = descreening(p[i], p[j], r), hji = descreening(p[j], p[i], r);
+      full[i] += hij;
+      full[j] += hji;
+      double ds;
+      const double sw = switch_value(r, rs, rc, &ds);
+      integral[i] += hij * sw;
+      integral[j] += hji * sw;
+    }
+  if (short_out)
+    for (int i = 0; i < n; ++i) short_out[i] = integral[i];
+  if (full_out)
+    for (int i = 0; i < n; ++i) full_out[i] = full[i];
+  for (int i = 0; i < n; ++i) integral[i] += tail[i];
+  const double prefactor = (solute_dielectric != 0.0 && solvent_dielectric != 0.0)
+                               ? -ONE_4PI_EPS0 * (1.0 / solute_dielectric - 1.0 / solvent_dielectric)
+                               : 0.0;
+  const double surface = 4.0 * kPi * surface_area_energy;
+  double energy = 0.0;
+  std::vector<double> dridi(n);
+  for (int i = 0; i < n; ++i) {  // gbsa_obc.rs:214-237
+    const double offset = p[i].radius - DIELECTRIC_OFFSET;
+    const double psi = 0.5 * offset * integral[i];
+    const double t = std::tanh(psi - 0.8 * psi * psi + 4.85 * psi * psi * psi);
+    born[i] = 1.0 / (1.0 / offset - t / p[i].radius);
+    // dR/dI = R^2 (1 - t^2)(1 - 1.6 psi + 14.55 psi^2) / rho * offset / 2
+    dridi[i] = born[i] * born[i] * (1.0 - t * t) * (1.0 - 1.6 * psi + 14.55 * psi * psi) /
+               p[i].radius * 0.5 * offset;
+    const double self_energy = 0.5 * prefactor * p[i].q * p[i].q / std::fabs(born[i]);
+    energy += self_energy;
+    dedi[i] = -self_energy / born[i];
+    if (born[i] > 0.0) {
+      const double area = surface * std::pow(p[i].radius + PROBE_RADIUS, 2) *
+                          std::pow(p[i].radius / born[i], 6);
+      energy += area;
+      dedi[i] -= 6.0 * area / born[i];
+    }
+  }
+  for (int i = 0; i < n; ++i)  // gbsa_obc.rs:239-260 (NoCutoff)
+    for (int j = i + 1; j < n; ++j) {
+      const double d[3] = {pos[3 * j] - pos[3 * i], pos[3 * j + 1] - pos[3 * i + 1],
+                           pos[3 * j + 2] - pos[3 * i + 2]};
+      const double r2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+      const double product = born[i] * born[j];
+      const double dd = r2 / (4.0 * product);
+      const double ex = std::exp(-dd);
+      const double den2 = r2 + product * ex;
+      const double pe = prefactor * p[i].q * p[j].q / std::sqrt(den2);
+      energy += pe;
+      const double radial = -pe * (1.0 - 0.25 * ex) / den2;
+      const double bd = -0.5 * pe * ex * (1.0 + dd) / den2;
+      dedi[i] += bd * born[j];
+      dedi[j] += bd * born[i];
+      for (int a = 0; a < 3; ++a) {
+        forces[3 * i + a] += radial * d[a];
+        forces[3 * j + a] -= radial * d[a];
+      }
+    }
+  for (int i = 0; i < n; ++i) dedi[i] *= dridi[i];  // dE/dI_i
+  std::vector<double> g(nf), dg(nf);
+  for (int i = 0; i < n; ++i)
+    for (int j = i + 1; j < n; ++j) {
+      const double d[3] = {pos[3 * j] - pos[3 * i], pos[3 * j + 1] - pos[3 * i + 1],
+                           pos[3 * j + 2] - pos[3 * i + 2]};
+      const double r = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+      if (r >= rc) continue;
+      double ds;
+      const double sw = switch_value(r, rs, rc, &ds);
+      // dH/dr = -2 r descreening_gradient (gbsa_obc.rs:297-309)
+      double phi_ij = -2.0 * r * descreening_gradient(p[i], p[j], r) * sw +
+                      descreening(p[i], p[j], r) * ds;
+      double phi_ji = -2.0 * r * descreening_gradient(p[j], p[i], r) * sw +
+                      descreening(p[j], p[i], r) * ds;
+      radial_functions(r, nf, mu0, dmu, eta, rc, g.data(), dg.data());
+      for (int f = 0; f < nf; ++f) {
+        phi_ij += dtail_dg[(size_t)i * nf + f] * dg[f];
+        phi_ji += dtail_dg[(size_t)j * nf + f] * dg[f];
+      }
+      const double radial = (dedi[i] * phi_ij + dedi[j] * phi_ji) / r;
+      for (int a = 0; a < 3; ++a) {
+        forces[3 * i + a] += radial * d[a];
+        forces[3 * j + a] -= radial * d[a];
+      }
+    }
+  *energy_out = energy;
+  if (born_out)
+    for (int i = 0; i < n; ++i) born_out[i] = born[i];
+  return 0;
+}
+
+// ---------------------------------------------------------------------------------------
 // Bonded terms: harmonic_bond.rs:102-144, harmonic_angle.rs:102-175
 // ---------------------------------------------------------------------------------------
 extern "C" double orc_harmonic_bond(int nb, const int* bi, const int* bj, const double* length,

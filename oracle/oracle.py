@@ -319,3 +319,129 @@ def wtime():
 
 def max_threads():
     return lib().orc_max_threads()
+
+
+# ---- learned Born radii (no reference counterpart; OBC terms from gbsa_obc.rs:184-309) ----
+# Feature and switch constants; the engine's learned-radii path uses the same values.
+LR_NF = 32                       # radial symmetry functions per particle
+LR_MU0, LR_DMU = 0.1, 1.1 / 31   # Gaussian centres 0.1 .. 1.2 nm
+LR_ETA = 1.0 / (2.0 * 0.07 ** 2)  # Gaussian width 0.07 nm
+LR_RC, LR_RS = 1.2, 1.0          # feature / short-range cutoff and switch start (nm)
+LR_HIDDEN = 64
+# flat float32 parameter block: W1[32][64], b1[64], W2[64][64], b2[64], w3[64], b3, then the
+# fixed normalisation: feature mean[32], feature 1/std[32], target mean, target scale
+LR_OFF = {"W1": 0, "b1": 2048, "W2": 2112, "b2": 6208, "w3": 6272, "b3": 6336, "mean": 6337,
+          "inv_std": 6369, "t_mean": 6401, "t_scale": 6402}
+LR_N_PARAMS = 6403
+LR_N_TRAIN = 6337
+
+
+def radial_features(pos, nf=LR_NF, mu0=LR_MU0, dmu=LR_DMU, eta=LR_ETA, rc=LR_RC):
+    """Radial symmetry functions (Behler & Parrinello 2007) G [n][nf] in f64."""
+    pos = _f64(pos, (-1, 3))
+    n = pos.shape[0]
+    g = np.zeros((n, nf))
+    rcode = lib().orc_radial_features(n, _d(pos), nf, C.c_double(mu0), C.c_double(dmu),
+                                      C.c_double(eta), C.c_double(rc), _d(g))
+    if rcode != 0:
+        raise ValueError("oracle rejected feature parameters")
+    return g
+
+
+def learned_gbsa(pos, charge, radius, scale, tail, dtail_dg, solvent_dielectric=78.5,
+                 solute_dielectric=1.0, surface_area_energy=2.25936, rs=LR_RS, rc=LR_RC,
+                 nf=LR_NF, mu0=LR_MU0, dmu=LR_DMU, eta=LR_ETA):
+    """GB energy/forces with I = I_short + tail -> (forces, energy, born, I_short, I_full)."""
+    pos = _f64(pos, (-1, 3))
+    n = pos.shape[0]
+    f = np.zeros_like(pos)
+    born, short, full = np.zeros(n), np.zeros(n), np.zeros(n)
+    en = C.c_double()
+    rcode = lib().orc_learned_gbsa(
+        n, _d(pos), _d(_f64(charge)), _d(_f64(radius)), _d(_f64(scale)),
+        C.c_double(solvent_dielectric), C.c_double(solute_dielectric),
+        C.c_double(surface_area_energy), C.c_double(rs), C.c_double(rc), nf, C.c_double(mu0),
+        C.c_double(dmu), C.c_double(eta), _d(_f64(tail)), _d(_f64(dtail_dg, (-1,))), _d(f),
+        C.byref(en), _d(born), _d(short), _d(full))
+    if rcode != 0:
+        raise ValueError("oracle rejected learned-GB parameters")
+    return f, en.value, born, short, full
+
+
+def bf16(x):
+    """Round to bfloat16 (nearest even) through float32, returned as float64."""
+    a = np.ascontiguousarray(np.asarray(x, dtype=np.float32)).view(np.uint32).astype(np.uint64)
+    a = ((a + (((a >> 16) & 1) + 0x7FFF)) >> 16) << 16
+    return a.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def mlp_unpack(params):
+    p = np.asarray(params, dtype=np.float32)
+    o = LR_OFF
+    return {"W1": p[o["W1"]:o["b1"]].reshape(32, 64), "b1": p[o["b1"]:o["W2"]],
+            "W2": p[o["W2"]:o["b2"]].reshape(64, 64), "b2": p[o["b2"]:o["w3"]],
+            "w3": p[o["w3"]:o["b3"]], "b3": p[o["b3"]], "mean": p[o["mean"]:o["inv_std"]],
+            "inv_std": p[o["inv_std"]:o["t_mean"]], "t_mean": p[o["t_mean"]],
+            "t_scale": p[o["t_scale"]]}
+
+
+def mlp_forward(params, features, quantize=True):
+    """32 -> 64 -> 64 -> 1 tanh network on normalised features, with the tensor-core kernels'
+    rounding points (BF16 inputs, weights and first-layer activations; wider sums in f64).
+    Returns (y, cache); y is the normalised tail."""
+    P = mlp_unpack(params)
+    q = bf16 if quantize else (lambda v: np.asarray(v, dtype=np.float64))
+    if quantize:  # the kernels normalise in float32
+        x = ((np.asarray(features, np.float32) - P["mean"]) * P["inv_std"]).astype(np.float32)
+    else:
+        x = (np.asarray(features, np.float64) - P["mean"]) * P["inv_std"].astype(np.float64)
+    xq, w1, w2 = q(x), q(P["W1"]), q(P["W2"])
+    z1 = xq @ w1 + P["b1"].astype(np.float64)
+    h1 = np.tanh(z1)
+    h1q = q(h1)
+    z2 = h1q @ w2 + P["b2"].astype(np.float64)
+    h2 = np.tanh(z2)
+    y = h2 @ P["w3"].astype(np.float64) + float(P["b3"])
+    return y, {"xq": xq, "w1": w1, "w2": w2, "h1": h1, "h1q": h1q, "h2": h2, "P": P, "q": q}
+
+
+def mlp_input_grad(cache):
+    """d y / d features [n][32] (through the normalisation), same rounding points."""
+    P, q = cache["P"], cache["q"]
+    d2q = q(P["w3"].astype(np.float64) * (1.0 - cache["h2"] ** 2))
+    d1q = q((d2q @ cache["w2"].T) * (1.0 - cache["h1"] ** 2))
+    return (d1q @ cache["w1"].T) * P["inv_std"].astype(np.float64)
+
+
+def mlp_loss_grad(params, features, targets, quantize=True):
+    """Mean squared error of the normalised tail over the batch and its gradient with respect
+    to the trainable parameters (flat, LR_N_TRAIN), with the training kernel's rounding."""
+    y, c = mlp_forward(params, features, quantize)
+    P, q = c["P"], c["q"]
+    t = ((np.asarray(targets, np.float32) - P["t_mean"]) / P["t_scale"]).astype(np.float64)
+    b = len(y)
+    g = 2.0 * (y - t) / b
+    d2 = g[:, None] * P["w3"].astype(np.float64) * (1.0 - c["h2"] ** 2)
+    d2q = q(d2)
+    d1 = (d2q @ c["w2"].T) * (1.0 - c["h1"] ** 2)
+    d1q = q(d1)
+    grad = np.zeros(LR_N_TRAIN)
+    o = LR_OFF
+    grad[o["W1"]:o["b1"]] = (c["xq"].T @ d1q).reshape(-1)
+    grad[o["b1"]:o["W2"]] = d1.sum(0)
+    grad[o["W2"]:o["b2"]] = (c["h1q"].T @ d2q).reshape(-1)
+    grad[o["b2"]:o["w3"]] = d2.sum(0)
+    grad[o["w3"]:o["b3"]] = c["h2"].T @ g
+    grad[o["b3"]] = g.sum()
+    return float(np.mean((y - t) ** 2)), grad
+
+
+def adam_update(params, m, v, grad, t, lr, beta1=0.9, beta2=0.999, eps=1e-8):
+    """Adam (Kingma & Ba, ICLR 2015), step t >= 1, on the trainable block; in place."""
+    k = LR_N_TRAIN
+    m[:k] = beta1 * m[:k] + (1 - beta1) * grad
+    v[:k] = beta2 * v[:k] + (1 - beta2) * grad * grad
+    mh = m[:k] / (1 - beta1 ** t)
+    vh = v[:k] / (1 - beta2 ** t)
+    params[:k] = params[:k] - lr * mh / (np.sqrt(vh) + eps)
+    return params, m, v
