@@ -151,6 +151,17 @@ int ommb200_harmonic_angle_add_angle(ommb200_force* f, int p1, int p2, int p3, d
                                      double k, int* index);
 int ommb200_harmonic_angle_set_uses_pbc(ommb200_force* f, int use_pbc);
 
+/* ---- learned Born radii for GBSAOBCForce (no reference counterpart) ----
+ * With learned radii enabled (NoCutoff GBSA only), the O(N^2) descreening passes are replaced
+ * by a switched short-range integral (cutoff 3.0 nm, switch from 2.7 nm) plus a network tail
+ * predicted from 32 radial symmetry functions per particle (cutoff 1.2 nm).  Every judge_interval MD steps the
+ * exact pass runs as judge: that step uses exact radii, the network is trained on the exact
+ * radii (train_steps Adam steps, batches of 4,096 particles, lr 1e-3) and it is used for the
+ * following steps only if its largest per-particle radius relative error was at most
+ * radius_tolerance. */
+int ommb200_gbsa_obc_set_learned_radii(ommb200_force* f, int enabled, int judge_interval,
+                                       double radius_tolerance, int train_steps);
+
 /* ---- LangevinMiddleIntegrator (integrators/langevin.rs:14-102) ---- */
 int ommb200_langevin_middle_create(double temperature, double friction, double step_size,
                                    ommb200_integrator** out);              /* new, 44-67 */
@@ -195,6 +206,21 @@ int ommb200_context_autotune(ommb200_context* ctx, int trial_steps, double* skin
 /* PME parameters frozen at Context creation (nonbonded.rs:1078-1106). */
 int ommb200_context_get_pme_parameters(const ommb200_context* ctx, double* alpha, int* nx,
                                        int* ny, int* nz);
+
+/* Learned-radii state of a Context whose GBSAOBCForce uses learned radii. */
+typedef struct {
+  int64_t judges;            /* exact-pass judgements so far */
+  int64_t learned_steps;     /* MD steps whose radii came from the network */
+  int64_t exact_steps;       /* MD steps whose radii came from the exact pass */
+  int active;                /* the network passed the last judgement */
+  double last_radius_error;  /* largest per-particle radius relative error, last judgement */
+  double last_loss;          /* normalised mean squared error of the last training batch */
+} ommb200_learned_radii_stats;
+int ommb200_context_get_learned_radii_stats(ommb200_context* ctx,
+                                            ommb200_learned_radii_stats* out);
+/* The network parameters (host float [OMMB200_RADII_MLP_PARAMS], layout below). */
+int ommb200_context_get_radii_mlp_params(ommb200_context* ctx, float* params);
+int ommb200_context_set_radii_mlp_params(ommb200_context* ctx, const float* params);
 
 /* ---- batches of independent systems (no reference counterpart) ----
  * One Context over n_systems independent Systems: each step() advances all of them with one

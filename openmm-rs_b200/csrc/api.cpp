@@ -348,6 +348,20 @@ int ommb200_gbsa_obc_set_solute_dielectric(ommb200_force* f, double value) {
 int ommb200_gbsa_obc_set_surface_area_energy(ommb200_force* f, double value) {
   return guarded([&] { gbf(f)->surface_area_energy = value; });
 }
+int ommb200_gbsa_obc_set_learned_radii(ommb200_force* f, int enabled, int judge_interval,
+                                       double radius_tolerance, int train_steps) {
+  return guarded([&] {
+    GbsaObcDef* g = gbf(f);
+    require(judge_interval >= 1, "judge interval must be at least one step");
+    require(std::isfinite(radius_tolerance) && radius_tolerance > 0.0,
+            "radius tolerance must be positive and finite");
+    require(train_steps >= 0, "training steps must be nonnegative");
+    g->learned.enabled = enabled != 0;
+    g->learned.judge_interval = judge_interval;
+    g->learned.radius_tolerance = radius_tolerance;
+    g->learned.train_steps = train_steps;
+  });
+}
 
 // ---- bonded -----------------------------------------------------------------------------
 int ommb200_harmonic_bond_create(ommb200_force** out) {
@@ -626,6 +640,30 @@ int ommb200_radii_mlp_train(int n, const float* features, const float* targets, 
   });
 }
 
+int ommb200_context_get_learned_radii_stats(ommb200_context* ctx,
+                                            ommb200_learned_radii_stats* out) {
+  return guarded([&] {
+    OMMB200_CTX;
+    require(out != nullptr, "null output");
+    E.learned_stats(out);
+  });
+}
+int ommb200_context_get_radii_mlp_params(ommb200_context* ctx, float* params) {
+  return guarded([&] {
+    OMMB200_CTX;
+    require(params != nullptr, "null output");
+    E.learned_params(params);
+  });
+}
+int ommb200_context_set_radii_mlp_params(ommb200_context* ctx, const float* params) {
+  return guarded([&] {
+    OMMB200_CTX;
+    require(params != nullptr, "null input");
+    for (int i = 0; i < OMMB200_RADII_MLP_PARAMS; ++i)
+      require(std::isfinite(params[i]), "network parameters must be finite");
+    E.set_learned_params(params);
+  });
+}
 int ommb200_context_num_systems(const ommb200_context* ctx, int* out) {
   return guarded([&] {
     require(ctx && ctx->engine && out, "null argument");

@@ -197,6 +197,7 @@ Engine::Engine(std::unique_ptr<SystemDef> system, std::unique_ptr<IntegratorDef>
   OMMB200_CK(cudaGetDeviceCount(&devices));
   require(opt_.device >= 0 && opt_.device < devices, "CUDA device ordinal out of range");
   OMMB200_CK(cudaSetDevice(opt_.device));
+  OMMB200_CK(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, opt_.device));
   OMMB200_CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
   OMMB200_CK(cudaStreamCreateWithFlags(&pme_stream_, cudaStreamNonBlocking));
   OMMB200_CK(cudaEventCreateWithFlags(&fork_ev_, cudaEventDisableTiming));
@@ -679,6 +680,136 @@ void Engine::setup_gbsa(const GbsaObcDef& g) {
   a.dedr_self = mem_.alloc<double>(n_);
   a.force = force_;
   a.energy = energy_;
+  if (g.learned.enabled) setup_learned(g.learned);
+}
+
+// Learned radii: per-block short-range lists over the segment-padded blocks, network
+// parameters (deterministic Xavier-normal start from the seed) and training state.
+void Engine::setup_learned(const LearnedRadiiDef& def) {
+  require(gb_def_->method == 0, "learned Born radii need a NoCutoff GBSAOBCForce",
+          OMMB200_ERR_UNSUPPORTED);
+  learned_ = true;
+  LearnedGbArgs& L = lr_;
+  L = LearnedGbArgs{};
+  L.n_atoms = n_;
+  L.n_blocks = static_slots_ / 32;
+  std::vector<int> first(L.n_blocks), count(L.n_blocks);
+  int max_blocks = 1;
+  for (int b = 0; b < L.n_blocks;) {
+    int e = b;
+    while (e < L.n_blocks && static_block_seg_[e] == static_block_seg_[b]) ++e;
+    for (int k = b; k < e; ++k) {
+      first[k] = b;
+      count[k] = e - b;
+    }
+    max_blocks = std::max(max_blocks, e - b);
+    b = e;
+  }
+  L.max_nbr = max_blocks;
+  int* dfirst = mem_.alloc<int>(L.n_blocks);
+  int* dcount = mem_.alloc<int>(L.n_blocks);
+  OMMB200_CK(cudaMemcpy(dfirst, first.data(), 4 * first.size(), cudaMemcpyHostToDevice));
+  OMMB200_CK(cudaMemcpy(dcount, count.data(), 4 * count.size(), cudaMemcpyHostToDevice));
+  L.block_first = dfirst;
+  L.block_count = dcount;
+  L.block_box = mem_.alloc<float4>(2 * (size_t)L.n_blocks);
+  L.nbr = mem_.alloc<int>((size_t)L.n_blocks * L.max_nbr);
+  L.nbr_count = mem_.alloc<int>(L.n_blocks);
+  L.rc = 3.0f;
+  L.rs = 2.7f;
+  L.rf = 1.2f;
+  L.features = mem_.alloc<float>((size_t)n_ * kRadiiFeatures);
+  L.tail = mem_.alloc<float>(n_);
+  L.dtail = mem_.alloc<float>((size_t)n_ * kRadiiFeatures);
+  L.short_sum = mem_.alloc<long long>(n_);
+  L.params = mem_.alloc<float>(kRadiiMlpParams);
+  L.moments = mem_.alloc<float>(2 * kRadiiMlpTrainable);
+  L.adam_t = mem_.alloc<int>(1);
+  L.snap_features = mem_.alloc<float>((size_t)n_ * kRadiiFeatures);
+  L.snap_target = mem_.alloc<float>(n_);
+  L.train_steps = def.train_steps;
+  L.loss = mem_.alloc<float>(std::max(1, def.train_steps));
+  L.batch = def.batch;
+  L.judge_interval = def.judge_interval;
+  L.learning_rate = (float)def.learning_rate;
+  L.tolerance = (float)def.radius_tolerance;
+  L.seed = (unsigned long long)(uint32_t)def.seed * 0x9E3779B97F4A7C15ull + 1ull;
+  L.n_segments = (int)segments_.size();
+  std::vector<int> sf, sc;
+  for (const Segment& g : segments_) {
+    sf.push_back(g.first);
+    sc.push_back(g.count);
+  }
+  int* dsf = mem_.alloc<int>(sf.size());
+  int* dsc = mem_.alloc<int>(sc.size());
+  OMMB200_CK(cudaMemcpy(dsf, sf.data(), 4 * sf.size(), cudaMemcpyHostToDevice));
+  OMMB200_CK(cudaMemcpy(dsc, sc.data(), 4 * sc.size(), cudaMemcpyHostToDevice));
+  L.seg_first = dsf;
+  L.seg_count = dsc;
+  L.seg_offset = mem_.alloc<float>(sf.size());
+  L.state = mem_.alloc<LearnedState>(1);
+  L.step = rng_step_;
+  L.status = status_;
+  // Xavier-normal weights (Box-Muller on a 64-bit LCG stream), zero biases, identity
+  // normalisation until the first judge fixes it
+  std::vector<float> p(kRadiiMlpParams, 0.f);
+  uint64_t st = L.seed;
+  auto uniform = [&]() {
+    st = st * 6364136223846793005ull + 1442695040888963407ull;
+    return ((st >> 11) + 0.5) * (1.0 / 9007199254740992.0);
+  };
+  auto normal = [&]() {
+    const double u = uniform(), v = uniform();
+    return std::sqrt(-2.0 * std::log(u)) * std::cos(2.0 * kPiD * v);
+  };
+  for (int i = 0; i < 32 * 64; ++i) p[i] = (float)(normal() / std::sqrt(32.0));
+  for (int i = 0; i < 64 * 64; ++i) p[2112 + i] = (float)(normal() / std::sqrt(64.0));
+  for (int i = 0; i < 64; ++i) p[6272 + i] = (float)(0.1 * normal() / std::sqrt(64.0));
+  for (int f = 0; f < 32; ++f) p[kRadiiMlpOffInvStd + f] = 1.f;
+  p[kRadiiMlpOffTScale] = 1.f;
+  OMMB200_CK(cudaMemcpy(L.params, p.data(), 4 * p.size(), cudaMemcpyHostToDevice));
+  gb_.use_learned = &L.state->use_learned;
+  gb_.short_sum = L.short_sum;
+  gb_.tail = L.tail;
+  gb_.seg_offset = L.seg_offset;
+}
+
+void Engine::learned_stats(ommb200_learned_radii_stats* out) {
+  *out = ommb200_learned_radii_stats{};
+  if (!learned_) return;
+  LearnedState st{};
+  float loss = 0.f;
+  OMMB200_CK(cudaMemcpyAsync(&st, lr_.state, sizeof(st), cudaMemcpyDeviceToHost, stream_));
+  if (lr_.train_steps > 0)
+    OMMB200_CK(cudaMemcpyAsync(&loss, lr_.loss + lr_.train_steps - 1, 4, cudaMemcpyDeviceToHost,
+                               stream_));
+  sync();
+  out->judges = (int64_t)st.judges;
+  out->learned_steps = (int64_t)st.learned_evals;
+  out->exact_steps = (int64_t)st.exact_evals;
+  out->active = st.active;
+  out->last_radius_error = st.last_error;
+  out->last_loss = loss;
+}
+
+void Engine::learned_params(float* out) {
+  require(learned_, "the Context has no learned Born radii", OMMB200_ERR_UNSUPPORTED);
+  OMMB200_CK(cudaMemcpyAsync(out, lr_.params, 4 * kRadiiMlpParams, cudaMemcpyDeviceToHost, stream_));
+  sync();
+}
+
+// Installs given parameters (normalisation included) and trusts them until the next judge.
+void Engine::set_learned_params(const float* in) {
+  require(learned_, "the Context has no learned Born radii", OMMB200_ERR_UNSUPPORTED);
+  OMMB200_CK(cudaMemcpyAsync(lr_.params, in, 4 * kRadiiMlpParams, cudaMemcpyHostToDevice, stream_));
+  OMMB200_CK(cudaMemsetAsync(lr_.seg_offset, 0, 4 * (size_t)lr_.n_segments, stream_));
+  LearnedState st{};
+  OMMB200_CK(cudaMemcpyAsync(&st, lr_.state, sizeof(st), cudaMemcpyDeviceToHost, stream_));
+  sync();
+  st.initialized = 1;
+  st.active = 1;
+  OMMB200_CK(cudaMemcpyAsync(lr_.state, &st, sizeof(st), cudaMemcpyHostToDevice, stream_));
+  sync();
 }
 
 // constraints.rs:35-75 validation, then SETTLE waters / free particles / SHAKE clusters.
@@ -1052,7 +1183,7 @@ void Engine::enqueue_nonbonded(bool energy, bool direct, bool reciprocal, bool d
   }
 }
 
-void Engine::compute_forces(bool energy, uint32_t groups) {
+void Engine::compute_forces(bool energy, uint32_t groups, bool in_step, int step_offset) {
   prof_begin("zero_forces");
   OMMB200_CK(cudaMemsetAsync(force_, 0, sizeof(long long) * 3 * (size_t)n_, stream_));
   prof_end();
@@ -1068,10 +1199,11 @@ void Engine::compute_forces(bool energy, uint32_t groups) {
   }
   if (gb_def_ && ((groups >> gb_def_->force_group) & 1u)) {
     prof_begin("gbsa");
+    if (learned_) launch_learned_control(lr_, in_step, step_offset, stream_);
     if (dp_)
-      launch_gbsa<double>(gb_, energy, stream_);
+      launch_gbsa<double>(gb_, energy, stream_, learned_ ? &lr_ : nullptr, sm_count_);
     else
-      launch_gbsa<float>(gb_, energy, stream_);
+      launch_gbsa<float>(gb_, energy, stream_, learned_ ? &lr_ : nullptr, sm_count_);
     prof_end();
   }
   for (auto& L : bonded_) {
@@ -1116,7 +1248,7 @@ IntegrateArgs Engine::integrate_args(int step_offset) const {
 }
 
 void Engine::enqueue_step(int step_offset) {
-  compute_forces(false, integ_->integration_force_groups);
+  compute_forces(false, integ_->integration_force_groups, true, step_offset);
   prof_begin("integrate");
   launch_integrate(integrate_args(step_offset), stream_);
   prof_end();
@@ -1350,6 +1482,24 @@ void Engine::autotune(int trial_steps, double* skin_out, int* ctas_out, double* 
   OMMB200_CK(cudaMemcpyAsync(save_x, pos_, bytes, cudaMemcpyDeviceToDevice, stream_));
   OMMB200_CK(cudaMemcpyAsync(save_v, vel_, bytes, cudaMemcpyDeviceToDevice, stream_));
   OMMB200_CK(cudaMemcpyAsync(&rng, rng_step_, 8, cudaMemcpyDeviceToHost, stream_));
+  // learned radii train during the trials: their network and counters are restored too
+  const size_t lr_bytes =
+      4 * (size_t)(kRadiiMlpParams + 2 * kRadiiMlpTrainable + 1 + segments_.size());
+  const size_t off_at = kRadiiMlpParams + 2 * kRadiiMlpTrainable + 1;
+  float* save_lr = learned_ ? mem_.alloc<float>(lr_bytes / 4) : nullptr;
+  LearnedState save_state{};
+  if (learned_) {
+    OMMB200_CK(cudaMemcpyAsync(save_lr, lr_.params, 4 * kRadiiMlpParams, cudaMemcpyDeviceToDevice,
+                               stream_));
+    OMMB200_CK(cudaMemcpyAsync(save_lr + kRadiiMlpParams, lr_.moments, 8 * kRadiiMlpTrainable,
+                               cudaMemcpyDeviceToDevice, stream_));
+    OMMB200_CK(cudaMemcpyAsync(save_lr + kRadiiMlpParams + 2 * kRadiiMlpTrainable, lr_.adam_t, 4,
+                               cudaMemcpyDeviceToDevice, stream_));
+    OMMB200_CK(cudaMemcpyAsync(save_lr + off_at, lr_.seg_offset, 4 * segments_.size(),
+                               cudaMemcpyDeviceToDevice, stream_));
+    OMMB200_CK(cudaMemcpyAsync(&save_state, lr_.state, sizeof(save_state), cudaMemcpyDeviceToHost,
+                               stream_));
+  }
   sync();
   const double time0 = time_;
   const int64_t steps0 = step_count_;
@@ -1364,6 +1514,18 @@ void Engine::autotune(int trial_steps, double* skin_out, int* ctas_out, double* 
     OMMB200_CK(cudaMemcpyAsync(rng_step_, &rng, 8, cudaMemcpyHostToDevice, stream_));
     const int one = 1;
     OMMB200_CK(cudaMemcpyAsync(rebuild_, &one, sizeof(int), cudaMemcpyHostToDevice, stream_));
+    if (learned_) {
+      OMMB200_CK(cudaMemcpyAsync(lr_.params, save_lr, 4 * kRadiiMlpParams,
+                                 cudaMemcpyDeviceToDevice, stream_));
+      OMMB200_CK(cudaMemcpyAsync(lr_.moments, save_lr + kRadiiMlpParams, 8 * kRadiiMlpTrainable,
+                                 cudaMemcpyDeviceToDevice, stream_));
+      OMMB200_CK(cudaMemcpyAsync(lr_.adam_t, save_lr + kRadiiMlpParams + 2 * kRadiiMlpTrainable,
+                                 4, cudaMemcpyDeviceToDevice, stream_));
+      OMMB200_CK(cudaMemcpyAsync(lr_.seg_offset, save_lr + off_at, 4 * segments_.size(),
+                                 cudaMemcpyDeviceToDevice, stream_));
+      OMMB200_CK(cudaMemcpyAsync(lr_.state, &save_state, sizeof(save_state),
+                                 cudaMemcpyHostToDevice, stream_));
+    }
     sync();
     time_ = time0;
     step_count_ = steps0;

@@ -88,6 +88,10 @@ class Engine {
   };
   std::vector<KernelTime> kernel_times() const { return kernel_times_; }
   cudaStream_t stream() const { return stream_; }
+  // learned Born radii: counters of the device control block, last judge error and loss
+  void learned_stats(ommb200_learned_radii_stats* out);
+  void learned_params(float* out);
+  void set_learned_params(const float* in);
 
  private:
   void setup_nonbonded(const NonbondedDef& nb);
@@ -97,7 +101,10 @@ class Engine {
   void setup_integrator();
   void update_box_dependents();
   void build_static_tiles();
-  void compute_forces(bool energy, uint32_t groups);
+  // `in_step`: an MD step's evaluation (the learned radii may judge and train there);
+  // `step_offset`: its position inside the captured group of steps.
+  void compute_forces(bool energy, uint32_t groups, bool in_step = false, int step_offset = 0);
+  void setup_learned(const LearnedRadiiDef& def);
   std::vector<long long> evaluate(bool energy, uint32_t groups, double* forces);
   void enqueue_step(int step_offset);
   void run_graph_steps(int graph_launches);
@@ -189,6 +196,9 @@ class Engine {
   // GBSAOBCForce
   const GbsaObcDef* gb_def_ = nullptr;
   GbArgs gb_{};
+  // learned Born radii
+  bool learned_ = false;
+  LearnedGbArgs lr_{};
 
   // bonded terms, one launch per force
   struct BondedLaunch {

@@ -16,52 +16,17 @@
 // Tiles pair blocks of the same segment (one segment per independent system in a batch), so
 // many systems of uneven size run in the same launches.
 #include "kernels.h"
+#include "gb_math.cuh"
 #include "pair_math.cuh"
 
 namespace ommb200 {
 namespace {
 
-constexpr double kDielectricOffset = 0.009;  // gbsa_obc.rs:8
-constexpr double kProbeRadius = 0.14;        // gbsa_obc.rs:9
-constexpr double kBornScale = 1099511627776.0;  // 2^40
-constexpr double kBornScaleInv = 1.0 / 1099511627776.0;
-
-__device__ __forceinline__ float log_r(float x) { return logf(x); }
-__device__ __forceinline__ double log_r(double x) { return log(x); }
-__device__ __forceinline__ float exp_gb(float x) { return expf(x); }
-__device__ __forceinline__ double exp_gb(double x) { return exp(x); }
-__device__ __forceinline__ float sqrt_r(float x) { return sqrtf(x); }
-__device__ __forceinline__ double sqrt_r(double x) { return sqrt(x); }
-
-// gbsa_obc.rs:278-295; `radius` = rho_i - 0.009, `scaled` = s_j (rho_j - 0.009)
-template <class Real>
-__device__ __forceinline__ Real descreening(Real radius, Real scaled, Real r) {
-  if (radius >= r + scaled) return Real(0);
-  const Real lower = Real(1) / fmax(radius, fabs(r - scaled));
-  const Real upper = Real(1) / (r + scaled);
-  const Real inverse = Real(1) / r;
-  Real value = lower - upper + Real(0.25) * r * (upper * upper - lower * lower) +
-               Real(0.5) * inverse * log_r(upper / lower) +
-               Real(0.25) * scaled * scaled * inverse * (lower * lower - upper * upper);
-  if (radius < scaled - r) value += Real(2) * (Real(1) / radius - lower);
-  return value;
-}
-
-// gbsa_obc.rs:297-309
-template <class Real>
-__device__ __forceinline__ Real descreening_gradient(Real radius, Real scaled, Real r) {
-  if (radius >= r + scaled) return Real(0);
-  const Real lower = Real(1) / fmax(radius, fabs(r - scaled));
-  const Real upper = Real(1) / (r + scaled);
-  const Real inverse = Real(1) / r;
-  return (Real(0.125) * (Real(1) + scaled * scaled * inverse * inverse) *
-              (lower * lower - upper * upper) +
-          Real(0.25) * log_r(upper / lower) * inverse * inverse) *
-         inverse;
-}
+using namespace gb;
 
 template <class Real, int kPass, bool kEnergy>
 __global__ void __launch_bounds__(128) gb_pass(const GbArgs a) {
+  if (kPass != 2 && a.use_learned && *a.use_learned) return;  // the network replaces them
   using T4 = typename V4<Real>::T4;
   using T2 = typename V4<Real>::T2;
   constexpr unsigned FULL = 0xffffffffu;
@@ -196,7 +161,10 @@ __global__ void gb_radii(const GbArgs a) {
   }
   const double rho = a.radius[atom];
   const double offset = rho - kDielectricOffset;
-  const double integral = (double)a.born_sum[atom] * kBornScaleInv;
+  const double integral = (a.use_learned && *a.use_learned)
+                              ? (double)a.short_sum[atom] * kBornScaleInv + (double)a.tail[atom] +
+                                    (double)a.seg_offset[a.atom_segment[atom]]
+                              : (double)a.born_sum[atom] * kBornScaleInv;
   const double psi = 0.5 * offset * integral;
   const double t = tanh(psi - 0.8 * psi * psi + 4.85 * psi * psi * psi);
   const double R = 1.0 / (1.0 / offset - t / rho);
@@ -262,11 +230,13 @@ __global__ void gb_pack(const GbArgs a) {
 }  // namespace
 
 template <class Real>
-void launch_gbsa(const GbArgs& a, bool energy, cudaStream_t s) {
+void launch_gbsa(const GbArgs& a, bool energy, cudaStream_t s, const LearnedGbArgs* learned,
+                 int sm_count) {
   const int tb = 256;
   const int gs = ceil_div(a.n_slots, tb);
-  const int gt = (int)std::min<long long>((a.n_tiles + 3) / 4, 148LL * 16);
+  const int gt = (int)std::min<long long>((a.n_tiles + 3) / 4, (long long)sm_count * 16);
   gb_pack<Real><<<gs, tb, 0, s>>>(a);
+  if (learned) launch_learned_front(*learned, a, sm_count, s);
   gb_pass<Real, 1, false><<<gt, 128, 0, s>>>(a);
   if (energy)
     gb_radii<Real, true><<<gs, tb, 0, s>>>(a);
@@ -278,9 +248,10 @@ void launch_gbsa(const GbArgs& a, bool energy, cudaStream_t s) {
     gb_pass<Real, 2, false><<<gt, 128, 0, s>>>(a);
   gb_chain<Real><<<gs, tb, 0, s>>>(a);
   gb_pass<Real, 3, false><<<gt, 128, 0, s>>>(a);
+  if (learned) launch_learned_back<Real>(*learned, a, sm_count, s);
 }
 
-template void launch_gbsa<float>(const GbArgs&, bool, cudaStream_t);
-template void launch_gbsa<double>(const GbArgs&, bool, cudaStream_t);
+template void launch_gbsa<float>(const GbArgs&, bool, cudaStream_t, const LearnedGbArgs*, int);
+template void launch_gbsa<double>(const GbArgs&, bool, cudaStream_t, const LearnedGbArgs*, int);
 
 }  // namespace ommb200

@@ -170,9 +170,70 @@ struct GbArgs {
   double* dedr_self;          // [n_atoms]
   long long* force;
   long long* energy;
+  // learned radii (null when off): while *use_learned is set the radii come from
+  // I_short + tail and the exact descreening passes 1 and 3 are skipped
+  const int* use_learned;
+  const long long* short_sum;  // [n_atoms] switched short-range integral, 2^-40
+  const float* tail;           // [n_atoms] network tail
+  const float* seg_offset;     // [segments] tail offset per system
 };
+
+// ---- learned Born radii (learned_gb.cu) -----------------------------------------------------
+// Device control block of the learned-radii path.
+struct LearnedState {
+  int use_learned;  // this evaluation takes its radii from the network
+  int judge;        // this evaluation judges the network against the exact pass
+  int need;         // use_learned | judge: features and network run
+  int active;       // the network passed the last judge
+  int initialized;  // feature / target normalisation fixed
+  int pad;
+  unsigned long long judges, learned_evals, exact_evals;
+  unsigned int max_err_bits;  // judge scratch: largest radius relative error (float bits)
+  float last_error;           // largest per-particle radius relative error at the last judge
+};
+struct LearnedGbArgs {
+  int n_atoms, n_blocks, max_nbr;
+  const int* block_first;   // [n_blocks] first block of the block's segment
+  const int* block_count;   // [n_blocks] blocks of that segment
+  float4* block_box;        // [n_blocks][2] centre, half extents
+  int* nbr;                 // [n_blocks][max_nbr] blocks of the segment within rc
+  int* nbr_count;           // [n_blocks]
+  float rc, rs;             // short-range integral cutoff and switch start (nm)
+  float rf;                 // feature cutoff (nm), at most rc
+  float* features;          // [n_atoms][32]
+  float* tail;              // [n_atoms]
+  float* dtail;             // [n_atoms][32] d tail / d features
+  long long* short_sum;     // [n_atoms] switched short-range HCT integral, 2^-40
+  float* params;            // [kRadiiMlpParams]
+  float* moments;           // [2][kRadiiMlpTrainable]
+  int* adam_t;
+  float* snap_features;     // [n_atoms][32] judge snapshot
+  float* snap_target;       // [n_atoms] exact minus short-range integral
+  float* loss;              // [train_steps]
+  int n_segments;           // independent systems (segments of the batch)
+  const int* seg_first;     // [n_segments] first particle
+  const int* seg_count;     // [n_segments] particles
+  float* seg_offset;        // [n_segments] tail offset fixed at the last judge
+  int train_steps, batch, judge_interval;
+  float learning_rate, tolerance;
+  unsigned long long seed;
+  LearnedState* state;
+  const unsigned long long* step;  // MD step counter
+  int* status;                     // engine status word (tensor-core wait timeouts)
+};
+// Decides this evaluation's mode (judge every judge_interval MD steps when allowed).
+void launch_learned_control(const LearnedGbArgs& a, bool judge_allowed, int step_offset,
+                            cudaStream_t s);
+// Block boxes, short-range block lists, features + I_short, network tail and gradient.
+void launch_learned_front(const LearnedGbArgs& a, const GbArgs& g, int sm_count, cudaStream_t s);
+// Short-range and network forces (learned evaluations); judge, normalisation and training
+// (judge evaluations).
 template <class Real>
-void launch_gbsa(const GbArgs& a, bool energy, cudaStream_t s);
+void launch_learned_back(const LearnedGbArgs& a, const GbArgs& g, int sm_count, cudaStream_t s);
+
+template <class Real>
+void launch_gbsa(const GbArgs& a, bool energy, cudaStream_t s,
+                 const LearnedGbArgs* learned = nullptr, int sm_count = 148);
 
 // ---- exceptions and bonded terms (exceptions always in f64) ------------------------------
 struct ExceptionArgs {
@@ -255,10 +316,14 @@ void launch_constrain_velocities(const IntegrateArgs& a, cudaStream_t s);
 // then feature mean[32], feature 1/std[32], target mean, target scale.
 constexpr int kRadiiMlpParams = 6403;
 constexpr int kRadiiMlpTrainable = 6337;
+constexpr int kRadiiMlpOffMean = 6337, kRadiiMlpOffInvStd = 6369, kRadiiMlpOffTMean = 6401,
+              kRadiiMlpOffTScale = 6402;
 constexpr int kRadiiFeatures = 32;
 // tail[n] = network output in integral units; dtail[n][32] = d tail / d features (may be null).
+// `gate` (may be null): the kernel does nothing while *gate == 0.
 void launch_mlp_infer(int n, const float* features, const float* params, float* tail,
-                      float* dtail, int* status, int sm_count, cudaStream_t s);
+                      float* dtail, int* status, int sm_count, cudaStream_t s,
+                      const int* gate = nullptr);
 // `steps` Adam steps on batches of `batch` (multiple of 128) particles drawn from the n
 // snapshot rows (all of them in order when batch == n).  adam_m / adam_v hold the moments of
 // the trainable block, *adam_t the step count; grad_out (may be null) receives the gradient of
@@ -266,6 +331,6 @@ void launch_mlp_infer(int n, const float* features, const float* params, float* 
 void launch_mlp_train(int n, const float* features, const float* targets, float* params,
                       float* adam_m, float* adam_v, int* adam_t, int steps, int batch, float lr,
                       unsigned long long seed, float* grad_out, float* loss_out, int* status,
-                      cudaStream_t s);
+                      cudaStream_t s, const int* gate = nullptr);
 
 }  // namespace ommb200

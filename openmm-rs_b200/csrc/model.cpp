@@ -175,7 +175,11 @@ std::unique_ptr<SystemDef> merge_systems(std::vector<std::unique_ptr<SystemDef>>
                       src->solvent_dielectric == gb->solvent_dielectric &&
                       src->solute_dielectric == gb->solute_dielectric &&
                       src->surface_area_energy == gb->surface_area_energy &&
-                      src->force_group == gb->force_group,
+                      src->force_group == gb->force_group &&
+                      src->learned.enabled == gb->learned.enabled &&
+                      src->learned.judge_interval == gb->learned.judge_interval &&
+                      src->learned.radius_tolerance == gb->learned.radius_tolerance &&
+                      src->learned.train_steps == gb->learned.train_steps,
                   "the GBSAOBCForces of a batch must share their global settings");
           gb->charge.insert(gb->charge.end(), src->charge.begin(), src->charge.end());
           gb->radius.insert(gb->radius.end(), src->radius.begin(), src->radius.end());

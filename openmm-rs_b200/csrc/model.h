@@ -68,6 +68,18 @@ struct NonbondedDef : ForceDef {
   void effective_pme_parameters(const double box[9], double* alpha, int dims[3]) const;
 };
 
+// Learned Born radii (no reference counterpart): a network predicts the long-range tail of the
+// HCT integral; the exact pass judges it every `judge_interval` MD steps.
+struct LearnedRadiiDef {
+  bool enabled = false;
+  int judge_interval = 50;
+  double radius_tolerance = 0.01;  // largest per-particle radius relative error allowed
+  int train_steps = 10;            // Adam steps after each judge
+  int batch = 4096;                // particles per Adam step
+  double learning_rate = 1e-3;
+  int seed = 1;
+};
+
 struct GbsaObcDef : ForceDef {
   GbsaObcDef() : ForceDef(kGbsaObc) { name = "GBSAOBCForce"; }
   std::vector<double> charge, radius, scale;
@@ -76,6 +88,7 @@ struct GbsaObcDef : ForceDef {
   double solvent_dielectric = 78.3;
   double solute_dielectric = 1.0;
   double surface_area_energy = 2.25936;
+  LearnedRadiiDef learned;
 };
 
 struct BondDef {

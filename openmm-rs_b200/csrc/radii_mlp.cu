@@ -30,8 +30,8 @@ constexpr uint32_t kWaitLimit = 1u << 22;
 
 // parameter block (floats)
 constexpr int kOffW1 = 0, kOffB1 = 2048, kOffW2 = 2112, kOffB2 = 6208, kOffW3 = 6272,
-              kOffB3 = 6336, kOffMean = 6337, kOffInvStd = 6369, kOffTMean = 6401,
-              kOffTScale = 6402;
+              kOffB3 = 6336, kOffMean = kRadiiMlpOffMean, kOffInvStd = kRadiiMlpOffInvStd,
+              kOffTMean = kRadiiMlpOffTMean, kOffTScale = kRadiiMlpOffTScale;
 static_assert(kOffTScale + 1 == kRadiiMlpParams, "parameter block layout");
 
 // per-CTA constants next to the operands: b1, b2, w3, mean, inv_std, b3, t_mean, t_scale
@@ -122,7 +122,8 @@ __global__ void __launch_bounds__(128) mlp_infer_kernel(int n, const float* __re
                                                         const float* __restrict__ P,
                                                         float* __restrict__ tail,
                                                         float* __restrict__ dtail,
-                                                        int* status) {
+                                                        int* status, const int* gate) {
+  if (gate && *gate == 0) return;
   extern __shared__ __align__(1024) uint8_t sm[];
   using L = InferSmem;
   __shared__ int s_ok;
@@ -287,7 +288,8 @@ __global__ void __launch_bounds__(128) mlp_train_kernel(int n, const float* __re
                                                         int* adam_t, int steps, int batch,
                                                         float lr, unsigned long long seed,
                                                         float* grad_out, float* loss_out,
-                                                        int* status) {
+                                                        int* status, const int* gate) {
+  if (gate && *gate == 0) return;
   extern __shared__ __align__(1024) uint8_t sm[];
   using L = TrainSmem;
   __shared__ int s_ok;
@@ -481,25 +483,26 @@ __global__ void __launch_bounds__(128) mlp_train_kernel(int n, const float* __re
 }  // namespace
 
 void launch_mlp_infer(int n, const float* features, const float* params, float* tail,
-                      float* dtail, int* status, int sm_count, cudaStream_t s) {
+                      float* dtail, int* status, int sm_count, cudaStream_t s, const int* gate) {
   if (n <= 0) return;
   cudaFuncSetAttribute(mlp_infer_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        kInferSmemLaunch);
   const int tiles = (n + 127) / 128;
   const int grid = std::max(1, std::min(tiles, 2 * sm_count));
-  mlp_infer_kernel<<<grid, 128, kInferSmemLaunch, s>>>(n, features, params, tail, dtail, status);
+  mlp_infer_kernel<<<grid, 128, kInferSmemLaunch, s>>>(n, features, params, tail, dtail, status,
+                                                       gate);
 }
 
 void launch_mlp_train(int n, const float* features, const float* targets, float* params,
                       float* adam_m, float* adam_v, int* adam_t, int steps, int batch, float lr,
                       unsigned long long seed, float* grad_out, float* loss_out, int* status,
-                      cudaStream_t s) {
+                      cudaStream_t s, const int* gate) {
   if (n <= 0 || steps <= 0) return;
   cudaFuncSetAttribute(mlp_train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        TrainSmem::bytes);
   mlp_train_kernel<<<1, 128, TrainSmem::bytes, s>>>(n, features, targets, params, adam_m, adam_v,
                                                     adam_t, steps, batch, lr, seed, grad_out,
-                                                    loss_out, status);
+                                                    loss_out, status, gate);
 }
 
 }  // namespace ommb200

@@ -55,6 +55,11 @@ class Options(C.Structure):
                 ("neighbor_skin", C.c_double), ("steps_per_graph", C.c_int)]
 
 
+class LearnedRadiiStats(C.Structure):
+    _fields_ = [("judges", C.c_int64), ("learned_steps", C.c_int64), ("exact_steps", C.c_int64),
+                ("active", C.c_int), ("last_radius_error", C.c_double), ("last_loss", C.c_double)]
+
+
 class StateInfo(C.Structure):
     _fields_ = [("time", C.c_double), ("step_count", C.c_int64),
                 ("potential_energy", C.c_double), ("kinetic_energy", C.c_double),
@@ -127,6 +132,10 @@ def library() -> C.CDLL:
             "ommb200_context_kernel_times": [P, I, C.c_char_p, I, C.POINTER(D), C.POINTER(I),
                                              C.POINTER(I)],
             "ommb200_radii_mlp_forward": [I, P, P, P, P, P],
+            "ommb200_gbsa_obc_set_learned_radii": [P, I, I, D, I],
+            "ommb200_context_get_learned_radii_stats": [P, C.POINTER(LearnedRadiiStats)],
+            "ommb200_context_get_radii_mlp_params": [P, C.POINTER(C.c_float)],
+            "ommb200_context_set_radii_mlp_params": [P, C.POINTER(C.c_float)],
             "ommb200_radii_mlp_train": [I, P, P, P, P, P, I, I, D, C.c_uint64, P, P, P],
         }
         for name, args in sig.items():
@@ -331,6 +340,15 @@ class GBSAOBCForce(_Force):
 
     def set_nonbonded_method(self, method: int) -> None:
         _check(library().ommb200_gbsa_obc_set_method(self._h, int(method)))
+
+    def set_learned_radii(self, enabled: bool = True, judge_interval: int = 50,
+                          radius_tolerance: float = 0.01, train_steps: int = 10) -> None:
+        """Replace the O(N^2) descreening passes by a short-range integral plus a network
+        tail, judged (and trained) against the exact pass every `judge_interval` steps."""
+        _check(library().ommb200_gbsa_obc_set_learned_radii(self._h, int(enabled),
+                                                            int(judge_interval),
+                                                            float(radius_tolerance),
+                                                            int(train_steps)))
 
     def set_cutoff_distance(self, value) -> None:
         _check(library().ommb200_gbsa_obc_set_cutoff_distance(self._h, value))
@@ -543,6 +561,25 @@ class Context:
         _check(library().ommb200_context_debug_pair_list(
             self._h, cap, out.ctypes.data_as(C.POINTER(C.c_int32)), C.byref(count)))
         return out[:min(cap, count.value)]
+
+    def learned_radii_stats(self) -> dict:
+        st = LearnedRadiiStats()
+        _check(library().ommb200_context_get_learned_radii_stats(self._h, C.byref(st)))
+        return {"judges": st.judges, "learned_steps": st.learned_steps,
+                "exact_steps": st.exact_steps, "active": bool(st.active),
+                "last_radius_error": st.last_radius_error, "last_loss": st.last_loss}
+
+    def get_radii_mlp_params(self) -> np.ndarray:
+        p = np.zeros(RADII_MLP_PARAMS, dtype=np.float32)
+        _check(library().ommb200_context_get_radii_mlp_params(
+            self._h, p.ctypes.data_as(C.POINTER(C.c_float))))
+        return p
+
+    def set_radii_mlp_params(self, params) -> None:
+        """Install network parameters (normalisation included); trusted until the next judge."""
+        p = np.ascontiguousarray(np.asarray(params, dtype=np.float32).reshape(RADII_MLP_PARAMS))
+        _check(library().ommb200_context_set_radii_mlp_params(
+            self._h, p.ctypes.data_as(C.POINTER(C.c_float))))
 
     def count_pairs(self) -> int:
         """Number of interacting nonbonded pairs at the current positions (pair kernel)."""

@@ -43,10 +43,12 @@ def langevin(temperature=300.0, friction=1.0, step_size=0.002, seed=1234):
 
 
 def chain_system(chain, coulomb14=1.0, lj14=1.0, gbsa=True, solvent_dielectric=78.5,
-                 solute_dielectric=1.0, surface_area_energy=2.25936, cutoff=None) -> System:
+                 solute_dielectric=1.0, surface_area_energy=2.25936, cutoff=None,
+                 learned_radii=None, gb_force_group=0) -> System:
     """One implicit-solvent chain: NonbondedForce with 1-2/1-3 exclusions and 1-4 exceptions,
     harmonic bonds and angles, and (by default) a GBSAOBCForce; NoCutoff, or
-    CutoffNonPeriodic for both forces when `cutoff` (nm) is given."""
+    CutoffNonPeriodic for both forces when `cutoff` (nm) is given.  `learned_radii`: keyword
+    arguments of GBSAOBCForce.set_learned_radii (None = exact OBC)."""
     system = System()
     for _ in range(chain.n_atoms):
         system.add_particle(chain.mass)
@@ -79,6 +81,9 @@ def chain_system(chain, coulomb14=1.0, lj14=1.0, gbsa=True, solvent_dielectric=7
         gb.set_surface_area_energy(surface_area_energy)
         for q, r in zip(chain.charges, chain.radii):
             gb.add_particle(float(q), float(r), chain.gb_scale)
+        if learned_radii is not None:
+            gb.set_learned_radii(**learned_radii)
+        gb.set_force_group(gb_force_group)
         system.add_force(gb)
     return system
 

@@ -953,7 +953,7 @@ extern "C" int orc_gbsa_obc(int n, const double* pos, const double* charge, cons
 //   I_short_i = sum_j H(r_ij; rho_i, s_j) S(r_ij), S the quintic switch from rs to rc;
 //   tail_i    = the network's prediction from radial symmetry functions (Behler & Parrinello,
 //               Phys. Rev. Lett. 98, 146401 (2007)) G_if = sum_j exp(-eta (r_ij - mu_f)^2)
-//               fc(r_ij), fc(r) = (cos(pi r / rc) + 1) / 2, mu_f = mu0 + f dmu.
+//               fc(r_ij) over r_ij < rf, fc(r) = (cos(pi r / rf) + 1) / 2, mu_f = mu0 + f dmu.
 // Forces follow from dE/dI_i and dI_i/dr_ij = Phi'_ij(r) with
 //   Phi_ij(r) = H(r; i, j) S(r) + sum_f (d tail_i / d G_if) g_f(r).
 // ---------------------------------------------------------------------------------------
@@ -1012,11 +1012,11 @@ extern "C" int orc_radial_features(int n, const double* pos, int nf, double mu0,
 extern "C" int orc_learned_gbsa(int n, const double* pos, const double* charge,
                                 const double* radius, const double* scale,
                                 double solvent_dielectric, double solute_dielectric,
-                                double surface_area_energy, double rs, double rc, int nf,
-                                double mu0, double dmu, double eta, const double* tail,
+                                double surface_area_energy, double rs, double rc, double rf,
+                                int nf, double mu0, double dmu, double eta, const double* tail,
                                 const double* dtail_dg, double* forces, double* energy_out,
                                 double* born_out, double* short_out, double* full_out) {
-  if (nf <= 0 || nf > 64 || !(rs < rc)) return -1;
+  if (nf <= 0 || nf > 64 || !(rs < rc) || !(rf > 0.0)) return -1;
   std::vector<GbParticle> p(n);
   for (int i = 0; i < n; ++i) p[i] = {charge[i], radius[i], scale[i]};
   std::vector<double> integral(n, 0.0), full(n, 0.0), born(n), dedi(n, 0.0);
@@ -1098,7 +1098,7 @@ extern "C" int orc_learned_gbsa(int n, const double* pos, const double* charge,
                       descreening(p[i], p[j], r) * ds;
       double phi_ji = -2.0 * r * descreening_gradient(p[j], p[i], r) * sw +
                       descreening(p[j], p[i], r) * ds;
-      radial_functions(r, nf, mu0, dmu, eta, rc, g.data(), dg.data());
+      radial_functions(r, nf, mu0, dmu, eta, rf, g.data(), dg.data());
       for (int f = 0; f < nf; ++f) {
         phi_ij += dtail_dg[(size_t)i * nf + f] * dg[f];
         phi_ji += dtail_dg[(size_t)j * nf + f] * dg[f];

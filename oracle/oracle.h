@@ -88,13 +88,15 @@ int orc_gbsa_obc(int n, const double* pos, const double* charge, const double* r
 
 /* Learned Born radii (no reference counterpart): radial symmetry functions G [n][nf] over all
  * other particles within rc; and GB energy/forces (NoCutoff, gbsa_obc.rs:184-309) with the
- * HCT integral replaced by I_short (switched from rs to rc) + tail, tail and d tail/dG given
+ * HCT integral replaced by I_short (switched from rs to rc) + tail, features within rf, tail
+ * and d tail/dG given
  * per particle.  short_out / full_out (may be NULL) receive I_short and the exact integral. */
 int orc_radial_features(int n, const double* pos, int nf, double mu0, double dmu, double eta,
                         double rc, double* features);
 int orc_learned_gbsa(int n, const double* pos, const double* charge, const double* radius,
                      const double* scale, double solvent_dielectric, double solute_dielectric,
-                     double surface_area_energy, double rs, double rc, int nf, double mu0,
+                     double surface_area_energy, double rs, double rc, double rf, int nf,
+                     double mu0,
                      double dmu, double eta, const double* tail, const double* dtail_dg,
                      double* forces, double* energy, double* born, double* short_out,
                      double* full_out);

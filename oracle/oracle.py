@@ -326,7 +326,8 @@ def max_threads():
 LR_NF = 32                       # radial symmetry functions per particle
 LR_MU0, LR_DMU = 0.1, 1.1 / 31   # Gaussian centres 0.1 .. 1.2 nm
 LR_ETA = 1.0 / (2.0 * 0.07 ** 2)  # Gaussian width 0.07 nm
-LR_RC, LR_RS = 1.2, 1.0          # feature / short-range cutoff and switch start (nm)
+LR_RF = 1.2                      # feature cutoff (nm)
+LR_RC, LR_RS = 3.0, 2.7          # short-range integral cutoff and switch start (nm)
 LR_HIDDEN = 64
 # flat float32 parameter block: W1[32][64], b1[64], W2[64][64], b2[64], w3[64], b3, then the
 # fixed normalisation: feature mean[32], feature 1/std[32], target mean, target scale
@@ -336,7 +337,7 @@ LR_N_PARAMS = 6403
 LR_N_TRAIN = 6337
 
 
-def radial_features(pos, nf=LR_NF, mu0=LR_MU0, dmu=LR_DMU, eta=LR_ETA, rc=LR_RC):
+def radial_features(pos, nf=LR_NF, mu0=LR_MU0, dmu=LR_DMU, eta=LR_ETA, rc=LR_RF):
     """Radial symmetry functions (Behler & Parrinello 2007) G [n][nf] in f64."""
     pos = _f64(pos, (-1, 3))
     n = pos.shape[0]
@@ -350,7 +351,7 @@ def radial_features(pos, nf=LR_NF, mu0=LR_MU0, dmu=LR_DMU, eta=LR_ETA, rc=LR_RC)
 
 def learned_gbsa(pos, charge, radius, scale, tail, dtail_dg, solvent_dielectric=78.5,
                  solute_dielectric=1.0, surface_area_energy=2.25936, rs=LR_RS, rc=LR_RC,
-                 nf=LR_NF, mu0=LR_MU0, dmu=LR_DMU, eta=LR_ETA):
+                 rf=LR_RF, nf=LR_NF, mu0=LR_MU0, dmu=LR_DMU, eta=LR_ETA):
     """GB energy/forces with I = I_short + tail -> (forces, energy, born, I_short, I_full)."""
     pos = _f64(pos, (-1, 3))
     n = pos.shape[0]
@@ -360,7 +361,8 @@ def learned_gbsa(pos, charge, radius, scale, tail, dtail_dg, solvent_dielectric=
     rcode = lib().orc_learned_gbsa(
         n, _d(pos), _d(_f64(charge)), _d(_f64(radius)), _d(_f64(scale)),
         C.c_double(solvent_dielectric), C.c_double(solute_dielectric),
-        C.c_double(surface_area_energy), C.c_double(rs), C.c_double(rc), nf, C.c_double(mu0),
+        C.c_double(surface_area_energy), C.c_double(rs), C.c_double(rc), C.c_double(rf), nf,
+        C.c_double(mu0),
         C.c_double(dmu), C.c_double(eta), _d(_f64(tail)), _d(_f64(dtail_dg, (-1,))), _d(f),
         C.byref(en), _d(born), _d(short), _d(full))
     if rcode != 0:
