@@ -47,10 +47,12 @@ def parse():
                    help="skip the FP64-form, roofline and CPU-baseline legs")
     p.add_argument("--no-equilibrate", action="store_true",
                    help="start from the lattice (short runs for profiler captures)")
-    p.add_argument("--workload", choices=["water-23958", "water-1065000", "chains-256"],
+    p.add_argument("--workload", choices=["water-23958", "water-1065000", "chains-256",
+                                          "chains-learned"],
                    default="water-23958",
                    help="water-1065000: the 22 nm box of 355,000 waters; chains-256: 256 uneven "
-                        "implicit-solvent chains batched in one Context")
+                        "implicit-solvent chains batched in one Context; chains-learned: 16 "
+                        "chains of 5,000 atoms with learned Born radii vs exact OBC")
     return p.parse_args()
 
 
@@ -312,6 +314,9 @@ def main():
         TUNE = False
     if args.workload == "chains-256":
         main_chains(args)
+        return
+    if args.workload == "chains-learned":
+        main_learned(args)
         return
     if args.impl == "reference":
         run_reference(args)
@@ -656,6 +661,134 @@ def main_chains(args):
 
         dist.barrier()
         dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def main_learned(args):
+    """16 chains of 5,000 atoms in one BatchContext: MD steps/s with learned Born radii (judge
+    and training included) against the same batch with exact OBC radii, and the GB energy and
+    force error of the learned radii against the f64 oracle's exact OBC."""
+    import numpy as np
+    import torch
+
+    import ommb200
+    from ommb200 import synth, systems
+
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        if rank == 0:
+            sys.path.insert(0, str(ROOT / "oracle"))
+            import oracle as O
+
+            chs = [synth.chain(5000, seed=70 + k) for k in range(16)]
+            threads = O.max_threads()
+            sec, done, spent = chains_cpu(chs, threads, budget=10.0)
+            print(json.dumps({
+                "impl": "reference", "metric": "MD steps/s, 16 x 5,000-atom chains (exact OBC)",
+                "value": 1.0 / sec, "unit": "batch steps/s", "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * sec,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic", "config": {"workload": "chains-learned", "threads": threads},
+                "cpu_baseline": {"value": 1.0 / sec, "unit": "batch steps/s", "cores": threads,
+                                 "kind": "port", "sample": f"{done} chains, extrapolated"},
+                "e2e": {"value": 1.0 / sec, "unit": "batch steps/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}), flush=True)
+        return
+    torch.cuda.set_device(local)
+    chs = [synth.chain(5000, seed=70 + k) for k in range(16)]
+    n_atoms = sum(c.n_atoms for c in chs)
+    x0 = np.concatenate([c.positions for c in chs])
+    seed = 1000 + rank
+    learned = {"judge_interval": 50, "radius_tolerance": 0.01, "train_steps": 10}
+
+    def make(lr):
+        ctx = ommb200.BatchContext(
+            [systems.chain_system(c, learned_radii=lr, gb_force_group=1) for c in chs],
+            systems.langevin(step_size=CHAIN_DT_PS, seed=seed), precision=args.precision,
+            device=local)
+        ctx.set_positions(x0)
+        ctx.set_velocities_to_temperature(300.0, seed=seed)
+        return ctx
+
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{local}")
+    seg = args.segment
+    exact = make(None)
+    exact.step(500)
+    time_segments(exact, torch, args.warmup, seg, flush)
+    ms_exact = time_segments(exact, torch, args.steps, seg, flush)
+    exact.close()
+    ctx = make(learned)
+    ctx.step(1000)  # untimed: the first judges fix the normalisation and train the network
+    time_segments(ctx, torch, args.warmup, seg, flush)
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        pass
+    stats0 = ctx.learned_radii_stats()
+    sampler = ClockSampler(uuid)
+    ms = time_segments(ctx, torch, args.steps, seg, flush)
+    clocks = sampler.stop()
+    stats1 = ctx.learned_radii_stats()
+    e2e_ms, h2d, d2h = time_e2e(ctx, torch, n_atoms, args.steps, seg, flush)
+    md_steps = args.steps * seg
+    value = md_steps / (ms / 1000.0)
+    extras = {}
+    cpu = None
+    if rank == 0 and not args.skip_extras:
+        times = kernel_profile(ctx, 50)
+        extras["kernel_ms_per_md_step"] = {k: round(v[0] / 50, 5) for k, v in times.items()}
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import oracle as O
+
+        st = ctx.get_state(positions=True, forces=True)
+        gb_f = ctx.get_state(forces=True, groups=1 << 1).forces
+        pot, _ = ctx.system_energies(groups=1 << 1)
+        errs_e, f_num, f_den = [], 0.0, 0.0
+        t0 = time.perf_counter()
+        for k, (c, pos, f) in enumerate(zip(chs, ctx.split(st.positions), ctx.split(gb_f))):
+            n = c.n_atoms
+            f_ref, e_ref, _ = O.gbsa_obc(pos, c.charges, c.radii, np.full(n, c.gb_scale),
+                                         solvent_dielectric=78.5)
+            errs_e.append(abs(pot[k] - e_ref) / (n / 1000.0))
+            f_num += float(((f - f_ref) ** 2).sum())
+            f_den += float((f_ref ** 2).sum())
+        oracle_s = time.perf_counter() - t0
+        extras["learned_accuracy_vs_f64_exact_obc"] = {
+            "gb_energy_err_kj_mol_per_1000_atoms": {"mean": float(np.mean(errs_e)),
+                                                    "max": float(np.max(errs_e))},
+            "gb_force_rms_rel_err": (f_num / f_den) ** 0.5,
+            "oracle_seconds": oracle_s}
+        threads = os.cpu_count() or 1
+        sec, done, spent = chains_cpu(chs, threads, budget=10.0)
+        cpu = {"value": 1.0 / sec, "unit": "batch steps/s", "cores": threads, "kind": "port",
+               "sample": f"{done} chains, one f64 oracle MD step each (exact OBC) in "
+                         f"{spent:.1f} s, extrapolated to the batch by sum of n^2"}
+    d = {k: stats1[k] - stats0[k] for k in ("judges", "learned_steps", "exact_steps")}
+    out = {
+        "metric": "MD steps/s, 16 x 5,000-atom chains, learned Born radii",
+        "value": value, "unit": "batch steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "ms_per_md_step": ms / md_steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp32+bf16" if args.precision == "mixed" else "fp64+bf16", "data": "synthetic",
+        "exact_obc": {"value": md_steps / (ms_exact / 1000.0), "unit": "batch steps/s",
+                      "ms_per_md_step": ms_exact / md_steps},
+        "learned_over_exact": ms_exact / ms,
+        "learned_radii_timed": {**d, "last_radius_error": stats1["last_radius_error"],
+                                "active": stats1["active"]},
+        "config": {"workload": "chains-learned", "n_systems": len(chs), "n_atoms": n_atoms,
+                   "method": "NoCutoff NonbondedForce + GBSAOBCForce (78.5 / 1), bonds, angles",
+                   "learned_radii": learned, "integrator": "LangevinMiddle 300 K, 1/ps, 1 fs",
+                   "md_steps_per_bench_step": seg,
+                   "l2": "flushed (256 MiB write) between timed bench steps"},
+        "e2e": {"value": md_steps / (e2e_ms / 1000.0), "unit": "batch steps/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    }
+    out.update(extras)
+    ctx.close()
     if rank == 0:
         print(json.dumps(out), flush=True)
 

@@ -153,7 +153,7 @@ int ommb200_harmonic_angle_set_uses_pbc(ommb200_force* f, int use_pbc);
 
 /* ---- learned Born radii for GBSAOBCForce (no reference counterpart) ----
  * With learned radii enabled (NoCutoff GBSA only), the O(N^2) descreening passes are replaced
- * by a switched short-range integral (cutoff 3.0 nm, switch from 2.7 nm) plus a network tail
+ * by a switched short-range integral (cutoff 2.0 nm, switch from 1.8 nm) plus a network tail
  * predicted from 32 radial symmetry functions per particle (cutoff 1.2 nm).  Every judge_interval MD steps the
  * exact pass runs as judge: that step uses exact radii, the network is trained on the exact
  * radii (train_steps Adam steps, batches of 4,096 particles, lr 1e-3) and it is used for the

@@ -714,9 +714,9 @@ void Engine::setup_learned(const LearnedRadiiDef& def) {
   L.block_count = dcount;
   L.block_box = mem_.alloc<float4>(2 * (size_t)L.n_blocks);
   L.nbr = mem_.alloc<int>((size_t)L.n_blocks * L.max_nbr);
-  L.nbr_count = mem_.alloc<int>(L.n_blocks);
-  L.rc = 3.0f;
-  L.rs = 2.7f;
+  L.nbr_count = mem_.alloc<int>(2 * (size_t)L.n_blocks);
+  L.rc = 2.0f;
+  L.rs = 1.8f;
   L.rf = 1.2f;
   L.features = mem_.alloc<float>((size_t)n_ * kRadiiFeatures);
   L.tail = mem_.alloc<float>(n_);
@@ -1198,13 +1198,41 @@ void Engine::compute_forces(bool energy, uint32_t groups, bool in_step, int step
       enqueue_nonbonded<float>(energy, direct, recip, dump_mode_);
   }
   if (gb_def_ && ((groups >> gb_def_->force_group) & 1u)) {
-    prof_begin("gbsa");
-    if (learned_) launch_learned_control(lr_, in_step, step_offset, stream_);
-    if (dp_)
-      launch_gbsa<double>(gb_, energy, stream_, learned_ ? &lr_ : nullptr, sm_count_);
-    else
-      launch_gbsa<float>(gb_, energy, stream_, learned_ ? &lr_ : nullptr, sm_count_);
-    prof_end();
+    auto gb = [&](int phase, const char* name) {
+      prof_begin(name);
+      if (dp_)
+        launch_gbsa_phase<double>(gb_, phase, energy, sm_count_, stream_);
+      else
+        launch_gbsa_phase<float>(gb_, phase, energy, sm_count_, stream_);
+      prof_end();
+    };
+    auto lr = [&](int phase, const char* name) {
+      if (!learned_) return;
+      prof_begin(name);
+      if (dp_)
+        launch_learned_phase<double>(lr_, gb_, phase, sm_count_, stream_);
+      else
+        launch_learned_phase<float>(lr_, gb_, phase, sm_count_, stream_);
+      prof_end();
+    };
+    if (learned_) {
+      prof_begin("lr_control");
+      launch_learned_control(lr_, in_step, step_offset, stream_);
+      prof_end();
+    }
+    gb(kGbPack, "gb_pack");
+    lr(kLrLists, "lr_lists");
+    lr(kLrFeatures, "lr_features");
+    lr(kLrInfer, "lr_infer");
+    gb(kGbPass1, "gb_descreening");
+    gb(kGbRadii, "gb_radii");
+    gb(kGbPass2, "gb_pairs");
+    gb(kGbChain, "gb_chain");
+    gb(kGbPass3, "gb_descreening_forces");
+    lr(kLrForces, "lr_forces");
+    lr(kLrJudge, "lr_judge");
+    lr(kLrTrain, "lr_train");
+    lr(kLrOffsets, "lr_offsets");
   }
   for (auto& L : bonded_) {
     if (!((groups >> L.group) & 1u)) continue;

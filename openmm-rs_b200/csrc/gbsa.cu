@@ -79,15 +79,17 @@ __global__ void __launch_bounds__(128) gb_pass(const GbArgs a) {
         }
       } else if (kPass == 2) {
         if (use) {
+          // SFU forms (rcp, ex2, rsqrt) in the FP32 kernel, exact ones in FP64
           const Real product = ri_aux * rj_aux;
-          const Real d = r2 / (Real(4) * product);
-          const Real ex = exp_gb(-d);
+          const Real d = Real(0.25) * r2 * rcp_r(product);
+          const Real ex = exp2_r(Real(-1.4426950408889634) * d);
           const Real den2 = r2 + product * ex;
+          const Real inv = rsqrt_r(den2), inv2 = inv * inv;
           // prefactor q_i q_j, with q stored as q sqrt|prefactor|
           const Real coefficient = (Real)a.prefactor_sign * pi.w * pj.w;
-          const Real pe = coefficient / sqrt_r(den2);
-          fo = -pe * (Real(1) - Real(0.25) * ex) / den2;
-          const Real bd = Real(-0.5) * pe * ex * (Real(1) + d) / den2;
+          const Real pe = coefficient * inv;
+          fo = -pe * (Real(1) - Real(0.25) * ex) * inv2;
+          const Real bd = Real(-0.5) * pe * ex * (Real(1) + d) * inv2;
           acc_i += bd * rj_aux;
           if (!self) acc_j += bd * ri_aux;
           if (kEnergy) {
@@ -230,28 +232,39 @@ __global__ void gb_pack(const GbArgs a) {
 }  // namespace
 
 template <class Real>
-void launch_gbsa(const GbArgs& a, bool energy, cudaStream_t s, const LearnedGbArgs* learned,
-                 int sm_count) {
+void launch_gbsa_phase(const GbArgs& a, int phase, bool energy, int sm_count, cudaStream_t s) {
   const int tb = 256;
   const int gs = ceil_div(a.n_slots, tb);
   const int gt = (int)std::min<long long>((a.n_tiles + 3) / 4, (long long)sm_count * 16);
-  gb_pack<Real><<<gs, tb, 0, s>>>(a);
-  if (learned) launch_learned_front(*learned, a, sm_count, s);
-  gb_pass<Real, 1, false><<<gt, 128, 0, s>>>(a);
-  if (energy)
-    gb_radii<Real, true><<<gs, tb, 0, s>>>(a);
-  else
-    gb_radii<Real, false><<<gs, tb, 0, s>>>(a);
-  if (energy)
-    gb_pass<Real, 2, true><<<gt, 128, 0, s>>>(a);
-  else
-    gb_pass<Real, 2, false><<<gt, 128, 0, s>>>(a);
-  gb_chain<Real><<<gs, tb, 0, s>>>(a);
-  gb_pass<Real, 3, false><<<gt, 128, 0, s>>>(a);
-  if (learned) launch_learned_back<Real>(*learned, a, sm_count, s);
+  switch (phase) {
+    case kGbPack:
+      gb_pack<Real><<<gs, tb, 0, s>>>(a);
+      break;
+    case kGbPass1:
+      gb_pass<Real, 1, false><<<gt, 128, 0, s>>>(a);
+      break;
+    case kGbRadii:
+      if (energy)
+        gb_radii<Real, true><<<gs, tb, 0, s>>>(a);
+      else
+        gb_radii<Real, false><<<gs, tb, 0, s>>>(a);
+      break;
+    case kGbPass2:
+      if (energy)
+        gb_pass<Real, 2, true><<<gt, 128, 0, s>>>(a);
+      else
+        gb_pass<Real, 2, false><<<gt, 128, 0, s>>>(a);
+      break;
+    case kGbChain:
+      gb_chain<Real><<<gs, tb, 0, s>>>(a);
+      break;
+    case kGbPass3:
+      gb_pass<Real, 3, false><<<gt, 128, 0, s>>>(a);
+      break;
+  }
 }
 
-template void launch_gbsa<float>(const GbArgs&, bool, cudaStream_t, const LearnedGbArgs*, int);
-template void launch_gbsa<double>(const GbArgs&, bool, cudaStream_t, const LearnedGbArgs*, int);
+template void launch_gbsa_phase<float>(const GbArgs&, int, bool, int, cudaStream_t);
+template void launch_gbsa_phase<double>(const GbArgs&, int, bool, int, cudaStream_t);
 
 }  // namespace ommb200

@@ -196,8 +196,8 @@ struct LearnedGbArgs {
   const int* block_first;   // [n_blocks] first block of the block's segment
   const int* block_count;   // [n_blocks] blocks of that segment
   float4* block_box;        // [n_blocks][2] centre, half extents
-  int* nbr;                 // [n_blocks][max_nbr] blocks of the segment within rc
-  int* nbr_count;           // [n_blocks]
+  int* nbr;                 // [n_blocks][max_nbr] near blocks from the front, far from the back
+  int* nbr_count;           // [n_blocks][2] near (within rf) and far (rf..rc) block counts
   float rc, rs;             // short-range integral cutoff and switch start (nm)
   float rf;                 // feature cutoff (nm), at most rc
   float* features;          // [n_atoms][32]
@@ -224,16 +224,20 @@ struct LearnedGbArgs {
 // Decides this evaluation's mode (judge every judge_interval MD steps when allowed).
 void launch_learned_control(const LearnedGbArgs& a, bool judge_allowed, int step_offset,
                             cudaStream_t s);
-// Block boxes, short-range block lists, features + I_short, network tail and gradient.
-void launch_learned_front(const LearnedGbArgs& a, const GbArgs& g, int sm_count, cudaStream_t s);
-// Short-range and network forces (learned evaluations); judge, normalisation and training
-// (judge evaluations).
+// The learned-radii launches, in step order: lists (block boxes and short-range block lists),
+// features (+ I_short), infer (network tail and gradient) before the GB radii; forces (learned
+// evaluations), judge (+ normalisation), train and offsets (judge evaluations) after the chain
+// step.  Every kernel returns at once when its evaluation does not need it.
+enum LearnedPhase : int { kLrLists, kLrFeatures, kLrInfer, kLrForces, kLrJudge, kLrTrain,
+                          kLrOffsets };
 template <class Real>
-void launch_learned_back(const LearnedGbArgs& a, const GbArgs& g, int sm_count, cudaStream_t s);
+void launch_learned_phase(const LearnedGbArgs& a, const GbArgs& g, int phase, int sm_count,
+                          cudaStream_t s);
 
+// GBSAOBCForce launches, in step order.
+enum GbPhase : int { kGbPack, kGbPass1, kGbRadii, kGbPass2, kGbChain, kGbPass3 };
 template <class Real>
-void launch_gbsa(const GbArgs& a, bool energy, cudaStream_t s,
-                 const LearnedGbArgs* learned = nullptr, int sm_count = 148);
+void launch_gbsa_phase(const GbArgs& a, int phase, bool energy, int sm_count, cudaStream_t s);
 
 // ---- exceptions and bonded terms (exceptions always in f64) ------------------------------
 struct ExceptionArgs {

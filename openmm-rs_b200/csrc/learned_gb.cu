@@ -1,14 +1,14 @@
 // Learned Born radii for GBSAOBCForce (no reference counterpart; the OBC terms follow
 // forces/gbsa_obc.rs:184-309).  The HCT integral of particle i is split as
 //   I_i = I_short_i + tail_i,   I_short_i = sum_j H(r_ij; rho_i, s_j) S(r_ij)
-// with S the quintic switch from rs to rc (2.7 -> 3.0 nm), and tail_i predicted by the radii
+// with S the quintic switch from rs to rc (1.8 -> 2.0 nm), and tail_i predicted by the radii
 // network (radii_mlp.cu) from 32 radial symmetry functions (Behler & Parrinello, Phys. Rev.
 // Lett. 98, 146401 (2007)) G_if = sum_j exp(-eta (r_ij - mu_f)^2) fc(r_ij) over r_ij < rf =
 // 1.2 nm, fc(r) = (cos(pi r / rf) + 1) / 2.
 // Everything here is short-ranged: per 32-slot block a list of the blocks of its segment whose
-// boxes come within rc, then one warp per block gathers features and I_short (front), or the
+// boxes come within rc, then one CTA per block gathers features and I_short (front), or the
 // forces -dE/dx through I_short and the network (back), visiting each ordered pair from the
-// i side only, so each particle's sums are private to one lane and need no atomics.
+// i side only, so each particle's sums belong to one lane per warp and meet in a fixed order.
 //
 // The exact pass still runs every `judge_interval` MD steps as the judge: it supplies that
 // step's radii, the network is compared with it (largest per-particle radius relative error),
@@ -17,6 +17,7 @@
 // `tolerance`); otherwise the exact passes run.
 #include "gb_math.cuh"
 #include "kernels.h"
+#include "pair_math.cuh"
 
 namespace ommb200 {
 namespace {
@@ -39,6 +40,27 @@ __device__ __forceinline__ float switch_value(float r, float rs, float rc, float
   const float w = rc - rs, t = (r - rs) / w;
   *deriv = -30.f * t * t * (1.f - t) * (1.f - t) / w;
   return 1.f + t * t * t * (-10.f + t * (15.f - 6.f * t));
+}
+
+// gbsa_obc.rs:278-309 with SFU reciprocals and logarithm: the descreening integral H and the
+// derivative factor G (dH/dr = -2 r G) of one ordered pair.
+__device__ __forceinline__ void descreening_fast(float radius, float scaled, float r, float inv_r,
+                                                 float* h, float* grad) {
+  if (radius >= r + scaled) {
+    *h = 0.f;
+    *grad = 0.f;
+    return;
+  }
+  const float lo_den = fmaxf(radius, fabsf(r - scaled));
+  const float lower = rcp_r(lo_den), upper = rcp_r(r + scaled);
+  const float l2u2 = lower * lower - upper * upper;
+  const float lg = __logf(lo_den * upper);  // log(upper / lower)
+  float v = lower - upper - 0.25f * r * l2u2 + 0.5f * inv_r * lg +
+            0.25f * scaled * scaled * inv_r * l2u2;
+  if (radius < scaled - r) v += 2.f * (rcp_r(radius) - lower);
+  *h = v;
+  *grad = (0.125f * (1.f + scaled * scaled * inv_r * inv_r) * l2u2 + 0.25f * lg * inv_r * inv_r) *
+          inv_r;
 }
 
 __device__ __forceinline__ float3 position(const double* pos, int atom) {
@@ -92,8 +114,9 @@ __global__ void lr_boxes(LearnedGbArgs a, GbArgs g) {
   }
 }
 
-// One warp per block I: the blocks of I's segment whose boxes come within rc of I's box
-// (I itself included), in block order.
+// One warp per block I: the blocks of I's segment whose boxes come within rf of I's box ("near":
+// features and integral; stored from the front of I's row, I itself included) and those
+// within rc but not rf ("far": integral only; stored from the back), in block order.
 __global__ void lr_neighbors(LearnedGbArgs a) {
   if (!a.state->need) return;
   const int lane = threadIdx.x & 31;
@@ -101,37 +124,75 @@ __global__ void lr_neighbors(LearnedGbArgs a) {
   if (I >= a.n_blocks) return;
   const float4 ci = a.block_box[2 * I], hi = a.block_box[2 * I + 1];
   const int first = a.block_first[I], count = a.block_count[I];
-  const float rc2 = a.rc * a.rc;
-  int n = 0;
+  const float rc2 = a.rc * a.rc, rf2 = a.rf * a.rf;
+  int* row = a.nbr + (size_t)I * a.max_nbr;
+  int n_near = 0, n_far = 0;
   for (int base = 0; base < count; base += 32) {
     const int J = first + base + lane;
-    bool near = false;
+    float gap2 = INFINITY;
     if (base + lane < count) {
       const float4 cj = a.block_box[2 * J], hj = a.block_box[2 * J + 1];
       const float gx = fmaxf(fabsf(cj.x - ci.x) - hi.x - hj.x, 0.f);
       const float gy = fmaxf(fabsf(cj.y - ci.y) - hi.y - hj.y, 0.f);
       const float gz = fmaxf(fabsf(cj.z - ci.z) - hi.z - hj.z, 0.f);
-      near = gx * gx + gy * gy + gz * gz < rc2;
+      gap2 = gx * gx + gy * gy + gz * gz;
     }
-    const unsigned m = __ballot_sync(kFull, near);
-    if (near) {
-      const int k = n + __popc(m & ((1u << lane) - 1u));
-      if (k < a.max_nbr) a.nbr[I * a.max_nbr + k] = J;
-    }
-    n += __popc(m);
+    const bool near = gap2 < rf2, far = !near && gap2 < rc2;
+    const unsigned mn = __ballot_sync(kFull, near), mf = __ballot_sync(kFull, far);
+    const unsigned below = (1u << lane) - 1u;
+    // a segment has at most max_nbr blocks, so the two ends never meet
+    if (near) row[n_near + __popc(mn & below)] = J;
+    if (far) row[a.max_nbr - 1 - (n_far + __popc(mf & below))] = J;
+    n_near += __popc(mn);
+    n_far += __popc(mf);
   }
-  if (lane == 0) a.nbr_count[I] = min(n, a.max_nbr);
+  if (lane == 0) {
+    a.nbr_count[2 * I] = n_near;
+    a.nbr_count[2 * I + 1] = n_far;
+  }
 }
 
-// One warp per block I, lane = particle i: radial features and the switched short-range
-// integral over every particle j != i of I's neighbour blocks within rc.
+// Block J and whether it is near, for entry q of I's lists (near entries first).
+__device__ __forceinline__ int list_block(const LearnedGbArgs& a, int I, int q, int n_near,
+                                          bool* near) {
+  *near = q < n_near;
+  const int* row = a.nbr + (size_t)I * a.max_nbr;
+  return *near ? row[q] : row[a.max_nbr - 1 - (q - n_near)];
+}
+
+// e_f = exp(-eta (r - mu_f)^2) for all f from three exponentials: the centre f = 15 and the
+// first ratios of neighbouring Gaussians, which then change by q = exp(-2 eta dmu^2) per step.
+// Every e_f is at most 1 and, for r < 1.2 nm, e_15 stays far above the FP32 range limit.
+__device__ __forceinline__ void gaussians(float r, float q, float* e) {
+  constexpr int c = 15;
+  const float x = r - (kMu0 + c * kDmu);
+  const float a = 2.f * kEta * kDmu * x, b = kEta * kDmu * kDmu;
+  e[c] = __expf(-kEta * x * x);
+  float up = __expf(a - b), down = __expf(-a - b);
+#pragma unroll
+  for (int f = c + 1; f < kNF; ++f) {
+    e[f] = e[f - 1] * up;
+    up *= q;
+  }
+#pragma unroll
+  for (int f = c - 1; f >= 0; --f) {
+    e[f] = e[f + 1] * down;
+    down *= q;
+  }
+}
+
+// One CTA per block I, lane = particle i; the CTA's warps share I's near / far list and their
+// partial sums meet in shared memory in a fixed order.  Radial features (near blocks, r < rf)
+// and the switched short-range integral (r < rc) over every particle j != i.
 __global__ void __launch_bounds__(32 * kWarps) lr_features(LearnedGbArgs a, GbArgs g) {
   if (!a.state->need) return;
   __shared__ float4 s_pos[kWarps][32];  // xyz, 1 for a particle / 0 for padding
   __shared__ float s_scaled[kWarps][32];
+  __shared__ float s_red[kWarps][32][kNF + 1];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const float rc2 = a.rc * a.rc;
-  for (int I = blockIdx.x * kWarps + w; I < a.n_blocks; I += gridDim.x * kWarps) {
+  const float rc2 = a.rc * a.rc, rf2 = a.rf * a.rf;
+  const float q = __expf(-2.f * kEta * kDmu * kDmu);
+  for (int I = blockIdx.x; I < a.n_blocks; I += gridDim.x) {
     const int ai = g.slot_atom[32 * I + lane];
     float3 pi = make_float3(0.f, 0.f, 0.f);
     float off_i = 1.f;
@@ -143,9 +204,10 @@ __global__ void __launch_bounds__(32 * kWarps) lr_features(LearnedGbArgs a, GbAr
 #pragma unroll
     for (int f = 0; f < kNF; ++f) G[f] = 0.f;
     float ishort = 0.f;
-    const int nn = a.nbr_count[I];
-    for (int q = 0; q < nn; ++q) {
-      const int J = a.nbr[I * a.max_nbr + q];
+    const int n_near = a.nbr_count[2 * I], nn = n_near + a.nbr_count[2 * I + 1];
+    for (int it = w; it < nn; it += kWarps) {
+      bool near;
+      const int J = list_block(a, I, it, n_near, &near);
       const int aj = g.slot_atom[32 * J + lane];
       if (aj >= 0) {
         const float3 p = position(g.pos, aj);
@@ -164,45 +226,59 @@ __global__ void __launch_bounds__(32 * kWarps) lr_features(LearnedGbArgs a, GbAr
           const float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
           const float r2 = dx * dx + dy * dy + dz * dz;
           if (r2 >= rc2) continue;
-          const float r = sqrtf(r2);
-          float ds;
+          const float inv_r = rsqrt_r(r2), r = r2 * inv_r;
+          float ds, h, gr;
           const float sw = switch_value(r, a.rs, a.rc, &ds);
-          ishort += descreening<float>(off_i, s_scaled[w][jl], r) * sw;
-          if (r >= a.rf) continue;
+          descreening_fast(off_i, s_scaled[w][jl], r, inv_r, &h, &gr);
+          ishort = fmaf(h, sw, ishort);
+          if (!near || r2 >= rf2) continue;
           const float fc = 0.5f * (cosf(kPiF * r / a.rf) + 1.f);
+          float e[kNF];
+          gaussians(r, q, e);
 #pragma unroll
-          for (int f = 0; f < kNF; ++f) {
-            const float x = r - (kMu0 + f * kDmu);
-            G[f] = fmaf(__expf(-kEta * x * x), fc, G[f]);
-          }
+          for (int f = 0; f < kNF; ++f) G[f] = fmaf(e[f], fc, G[f]);
         }
       }
       __syncwarp();
     }
-    if (ai >= 0) {
+#pragma unroll
+    for (int f = 0; f < kNF; ++f) s_red[w][lane][f] = G[f];
+    s_red[w][lane][kNF] = ishort;
+    __syncthreads();
+    if (w == 0 && ai >= 0) {
       float4* out = reinterpret_cast<float4*>(a.features + (size_t)ai * kNF);
+      float v[kNF + 1];
+#pragma unroll
+      for (int f = 0; f <= kNF; ++f) {
+        float t = s_red[0][lane][f];
+        for (int u = 1; u < kWarps; ++u) t += s_red[u][lane][f];
+        v[f] = t;
+      }
 #pragma unroll
       for (int f = 0; f < kNF / 4; ++f)
-        out[f] = make_float4(G[4 * f], G[4 * f + 1], G[4 * f + 2], G[4 * f + 3]);
-      a.short_sum[ai] = to_fixed((double)ishort, kBornScale);
+        out[f] = make_float4(v[4 * f], v[4 * f + 1], v[4 * f + 2], v[4 * f + 3]);
+      a.short_sum[ai] = to_fixed((double)v[kNF], kBornScale);
     }
+    __syncthreads();
   }
 }
 
-// One warp per block I, lane = particle i: F_i = sum_j (D_i Phi'_ij + D_j Phi'_ji) / r d_ij,
+// One CTA per block I as above: F_i = sum_j (D_i Phi'_ij + D_j Phi'_ji) / r d_ij,
 // Phi_ij = H(r; i, j) S(r) + sum_f (d tail_i / d G_if) g_f(r), D = dE/dI (half the chain
 // value the GB chain kernel leaves per slot).
 template <class Real>
 __global__ void __launch_bounds__(32 * kWarps) lr_forces(LearnedGbArgs a, GbArgs g) {
   if (!a.state->use_learned) return;
   __shared__ float4 s_pos[kWarps][32];
-  __shared__ float4 s_par[kWarps][32];      // offset radius, scaled radius, D, valid
+  __shared__ float4 s_par[kWarps][32];        // offset radius, scaled radius, D, valid
   __shared__ float s_w[kWarps][32][kNF + 1];  // D_j d tail_j / d G_j (padded rows)
+  __shared__ float s_red[kWarps][32][3];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const float rc2 = a.rc * a.rc;
+  const float rc2 = a.rc * a.rc, rf2 = a.rf * a.rf;
   const Real* chain = reinterpret_cast<const Real*>(g.dedr_slot);
   const float fc_k = kPiF / a.rf;
-  for (int I = blockIdx.x * kWarps + w; I < a.n_blocks; I += gridDim.x * kWarps) {
+  const float q = __expf(-2.f * kEta * kDmu * kDmu);
+  for (int I = blockIdx.x; I < a.n_blocks; I += gridDim.x) {
     const int si = 32 * I + lane;
     const int ai = g.slot_atom[si];
     float3 pi = make_float3(0.f, 0.f, 0.f);
@@ -217,18 +293,19 @@ __global__ void __launch_bounds__(32 * kWarps) lr_forces(LearnedGbArgs a, GbArgs
       d_i = 0.5f * (float)chain[si];
       const float4* dt = reinterpret_cast<const float4*>(a.dtail + (size_t)ai * kNF);
 #pragma unroll
-      for (int q = 0; q < kNF / 4; ++q) {
-        const float4 v = dt[q];
-        wi[4 * q] = d_i * v.x;
-        wi[4 * q + 1] = d_i * v.y;
-        wi[4 * q + 2] = d_i * v.z;
-        wi[4 * q + 3] = d_i * v.w;
+      for (int qq = 0; qq < kNF / 4; ++qq) {
+        const float4 v = dt[qq];
+        wi[4 * qq] = d_i * v.x;
+        wi[4 * qq + 1] = d_i * v.y;
+        wi[4 * qq + 2] = d_i * v.z;
+        wi[4 * qq + 3] = d_i * v.w;
       }
     }
     float fx = 0.f, fy = 0.f, fz = 0.f;
-    const int nn = a.nbr_count[I];
-    for (int q = 0; q < nn; ++q) {
-      const int J = a.nbr[I * a.max_nbr + q];
+    const int n_near = a.nbr_count[2 * I], nn = n_near + a.nbr_count[2 * I + 1];
+    for (int it = w; it < nn; it += kWarps) {
+      bool near;
+      const int J = list_block(a, I, it, n_near, &near);
       const int sj = 32 * J + lane;
       const int aj = g.slot_atom[sj];
       if (aj >= 0) {
@@ -238,14 +315,16 @@ __global__ void __launch_bounds__(32 * kWarps) lr_forces(LearnedGbArgs a, GbArgs
         s_pos[w][lane] = make_float4(p.x, p.y, p.z, 1.f);
         s_par[w][lane] = make_float4(off, (float)((g.radius[aj] - kDielectricOffset) * g.scale[aj]),
                                      dj, 1.f);
-        const float4* dt = reinterpret_cast<const float4*>(a.dtail + (size_t)aj * kNF);
+        if (near) {
+          const float4* dt = reinterpret_cast<const float4*>(a.dtail + (size_t)aj * kNF);
 #pragma unroll
-        for (int qq = 0; qq < kNF / 4; ++qq) {
-          const float4 v = dt[qq];
-          s_w[w][lane][4 * qq] = dj * v.x;
-          s_w[w][lane][4 * qq + 1] = dj * v.y;
-          s_w[w][lane][4 * qq + 2] = dj * v.z;
-          s_w[w][lane][4 * qq + 3] = dj * v.w;
+          for (int qq = 0; qq < kNF / 4; ++qq) {
+            const float4 v = dt[qq];
+            s_w[w][lane][4 * qq] = dj * v.x;
+            s_w[w][lane][4 * qq + 1] = dj * v.y;
+            s_w[w][lane][4 * qq + 2] = dj * v.z;
+            s_w[w][lane][4 * qq + 3] = dj * v.w;
+          }
         }
       } else {
         s_pos[w][lane] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -260,28 +339,31 @@ __global__ void __launch_bounds__(32 * kWarps) lr_forces(LearnedGbArgs a, GbArgs
           const float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
           const float r2 = dx * dx + dy * dy + dz * dz;
           if (r2 >= rc2) continue;
-          const float r = sqrtf(r2);
+          const float inv_r = rsqrt_r(r2), r = r2 * inv_r;
           const float4 pr = s_par[w][jl];
-          float ds;
+          float ds, hij, hji, gij, gji;
           const float sw = switch_value(r, a.rs, a.rc, &ds);
           // dH/dr = -2 r descreening_gradient (gbsa_obc.rs:297-309)
-          const float hij = descreening<float>(off_i, pr.y, r);
-          const float hji = descreening<float>(pr.x, sc_i, r);
-          const float gij = descreening_gradient<float>(off_i, pr.y, r);
-          const float gji = descreening_gradient<float>(pr.x, sc_i, r);
+          descreening_fast(off_i, pr.y, r, inv_r, &hij, &gij);
+          descreening_fast(pr.x, sc_i, r, inv_r, &hji, &gji);
           float phi = d_i * (-2.f * r * gij * sw + hij * ds) + pr.z * (-2.f * r * gji * sw + hji * ds);
-          if (r < a.rf) {
+          if (near && r2 < rf2) {
             float sn, cs;
             sincosf(fc_k * r, &sn, &cs);
             const float fc = 0.5f * (cs + 1.f), dfc = -0.5f * fc_k * sn;
+            float e[kNF];
+            gaussians(r, q, e);
+            // sum_f W_f g_f'(r),  g_f' = e_f (-2 eta (r - mu_f) fc + dfc)
+            float s0 = 0.f, s1 = 0.f;
 #pragma unroll
             for (int f = 0; f < kNF; ++f) {
-              const float x = r - (kMu0 + f * kDmu);
-              const float e = __expf(-kEta * x * x);
-              phi = fmaf(wi[f] + s_w[w][jl][f], e * fmaf(-2.f * kEta * x, fc, dfc), phi);
+              const float we = (wi[f] + s_w[w][jl][f]) * e[f];
+              s0 += we;
+              s1 = fmaf(we, r - (kMu0 + f * kDmu), s1);
             }
+            phi += dfc * s0 - 2.f * kEta * fc * s1;
           }
-          const float radial = phi / r;
+          const float radial = phi * inv_r;
           fx = fmaf(radial, dx, fx);
           fy = fmaf(radial, dy, fy);
           fz = fmaf(radial, dz, fz);
@@ -289,11 +371,22 @@ __global__ void __launch_bounds__(32 * kWarps) lr_forces(LearnedGbArgs a, GbArgs
       }
       __syncwarp();
     }
-    if (ai >= 0) {
-      add_fixed(g.force + ai, to_fixed(fx, (float)kForceScale));
-      add_fixed(g.force + g.n_atoms + ai, to_fixed(fy, (float)kForceScale));
-      add_fixed(g.force + 2 * g.n_atoms + ai, to_fixed(fz, (float)kForceScale));
+    s_red[w][lane][0] = fx;
+    s_red[w][lane][1] = fy;
+    s_red[w][lane][2] = fz;
+    __syncthreads();
+    if (w == 0 && ai >= 0) {
+      float f3[3];
+      for (int c = 0; c < 3; ++c) {
+        float t = s_red[0][lane][c];
+        for (int u = 1; u < kWarps; ++u) t += s_red[u][lane][c];
+        f3[c] = t;
+      }
+      add_fixed(g.force + ai, to_fixed(f3[0], (float)kForceScale));
+      add_fixed(g.force + g.n_atoms + ai, to_fixed(f3[1], (float)kForceScale));
+      add_fixed(g.force + 2 * g.n_atoms + ai, to_fixed(f3[2], (float)kForceScale));
     }
+    __syncthreads();
   }
 }
 
@@ -417,33 +510,48 @@ void launch_learned_control(const LearnedGbArgs& a, bool judge_allowed, int step
   lr_control<<<1, 1, 0, s>>>(a, judge_allowed ? 1 : 0, step_offset);
 }
 
-void launch_learned_front(const LearnedGbArgs& a, const GbArgs& g, int sm_count, cudaStream_t s) {
-  const int wb = ceil_div(a.n_blocks * 32, 128);
-  lr_boxes<<<wb, 128, 0, s>>>(a, g);
-  lr_neighbors<<<wb, 128, 0, s>>>(a);
-  lr_features<<<std::max(1, std::min(ceil_div(a.n_blocks, kWarps), sm_count * 8)), 32 * kWarps,
-                0, s>>>(a, g);
-  launch_mlp_infer(a.n_atoms, a.features, a.params, a.tail, a.dtail, a.status, sm_count, s,
-                   &a.state->need);
-}
-
 template <class Real>
-void launch_learned_back(const LearnedGbArgs& a, const GbArgs& g, int sm_count, cudaStream_t s) {
-  lr_forces<Real><<<std::max(1, std::min(ceil_div(a.n_blocks, kWarps), sm_count * 8)),
-                    32 * kWarps, 0, s>>>(a, g);
-  lr_judge<<<ceil_div(a.n_atoms, 256), 256, 0, s>>>(a, g);
-  lr_judge_finish<<<1, 1, 0, s>>>(a);
-  lr_normalize<<<1, 256, 0, s>>>(a);
-  launch_mlp_train(a.n_atoms, a.snap_features, a.snap_target, a.params, a.moments,
-                   a.moments + kRadiiMlpTrainable, a.adam_t, a.train_steps, a.batch,
-                   a.learning_rate, a.seed, nullptr, a.loss, a.status, s, &a.state->judge);
-  // the retrained network on the main configuration, then the per-system offsets
-  launch_mlp_infer(a.n_atoms, a.snap_features, a.params, a.tail, nullptr, a.status, sm_count, s,
-                   &a.state->judge);
-  lr_offsets<<<a.n_segments, 256, 0, s>>>(a, g);
+void launch_learned_phase(const LearnedGbArgs& a, const GbArgs& g, int phase, int sm_count,
+                          cudaStream_t s) {
+  const int wb = ceil_div(a.n_blocks * 32, 128);
+  const int ctas = std::max(1, std::min(a.n_blocks, sm_count * 8));
+  switch (phase) {
+    case kLrLists:
+      lr_boxes<<<wb, 128, 0, s>>>(a, g);
+      lr_neighbors<<<wb, 128, 0, s>>>(a);
+      break;
+    case kLrFeatures:
+      lr_features<<<ctas, 32 * kWarps, 0, s>>>(a, g);
+      break;
+    case kLrInfer:
+      launch_mlp_infer(a.n_atoms, a.features, a.params, a.tail, a.dtail, a.status, sm_count, s,
+                       &a.state->need);
+      break;
+    case kLrForces:
+      lr_forces<Real><<<ctas, 32 * kWarps, 0, s>>>(a, g);
+      break;
+    case kLrJudge:
+      lr_judge<<<ceil_div(a.n_atoms, 256), 256, 0, s>>>(a, g);
+      lr_judge_finish<<<1, 1, 0, s>>>(a);
+      lr_normalize<<<1, 256, 0, s>>>(a);
+      break;
+    case kLrTrain:
+      launch_mlp_train(a.n_atoms, a.snap_features, a.snap_target, a.params, a.moments,
+                       a.moments + kRadiiMlpTrainable, a.adam_t, a.train_steps, a.batch,
+                       a.learning_rate, a.seed, nullptr, a.loss, a.status, s, &a.state->judge);
+      break;
+    case kLrOffsets:
+      // the retrained network on the main configuration, then the per-system offsets
+      launch_mlp_infer(a.n_atoms, a.snap_features, a.params, a.tail, nullptr, a.status, sm_count,
+                       s, &a.state->judge);
+      lr_offsets<<<a.n_segments, 256, 0, s>>>(a, g);
+      break;
+  }
 }
 
-template void launch_learned_back<float>(const LearnedGbArgs&, const GbArgs&, int, cudaStream_t);
-template void launch_learned_back<double>(const LearnedGbArgs&, const GbArgs&, int, cudaStream_t);
+template void launch_learned_phase<float>(const LearnedGbArgs&, const GbArgs&, int, int,
+                                          cudaStream_t);
+template void launch_learned_phase<double>(const LearnedGbArgs&, const GbArgs&, int, int,
+                                           cudaStream_t);
 
 }  // namespace ommb200

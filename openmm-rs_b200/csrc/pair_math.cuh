@@ -33,11 +33,13 @@ __device__ __forceinline__ float rcp_r(float x) {
   asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
   return y;
 }
+__device__ __forceinline__ double rcp_r(double x) { return 1.0 / x; }
 __device__ __forceinline__ float exp2_r(float x) {
   float y;
   asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
   return y;
 }
+__device__ __forceinline__ double exp2_r(double x) { return exp2(x); }
 
 // erfc(x) = exp(-x^2) P(1 / (1 + 0.46 x)), own least-squares fit (csrc/fit_erfc.py).
 __device__ __forceinline__ float erfc_poly(float x) {

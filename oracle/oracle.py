@@ -327,7 +327,7 @@ LR_NF = 32                       # radial symmetry functions per particle
 LR_MU0, LR_DMU = 0.1, 1.1 / 31   # Gaussian centres 0.1 .. 1.2 nm
 LR_ETA = 1.0 / (2.0 * 0.07 ** 2)  # Gaussian width 0.07 nm
 LR_RF = 1.2                      # feature cutoff (nm)
-LR_RC, LR_RS = 3.0, 2.7          # short-range integral cutoff and switch start (nm)
+LR_RC, LR_RS = 2.0, 1.8          # short-range integral cutoff and switch start (nm)
 LR_HIDDEN = 64
 # flat float32 parameter block: W1[32][64], b1[64], W2[64][64], b2[64], w3[64], b3, then the
 # fixed normalisation: feature mean[32], feature 1/std[32], target mean, target scale
