@@ -61,6 +61,48 @@ def dist_env():
             int(os.environ.get("LOCAL_RANK", 0)))
 
 
+def init_replicas(world, local, backend="nccl"):
+    """One process per GPU, each an independent replica: the process group carries only the
+    barriers around the timed region and the max-over-ranks timing reduction (a short timeout,
+    so ranks that lose each other fail instead of waiting)."""
+    if world <= 1:
+        return
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    kw = {"device_id": torch.device("cuda", local)} if backend == "nccl" else {}
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120), **kw)
+
+
+def replica_barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(values, world, device):
+    """Element-wise maximum of per-rank timings (the job takes as long as its slowest rank)."""
+    if world <= 1:
+        return [float(v) for v in values]
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t]
+
+
+def close_replicas(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def ns_per_day(md_steps, seconds):
     return md_steps * DT_PS / 1000.0 / seconds * 86400.0
 
@@ -254,6 +296,49 @@ def cpu_baseline(w, x0, threads, gpu_forces):
                       f"evaluation {first:.2f} s", "energy": e}, err
 
 
+def nve_drift(w, x, v, device, ps=50.0, sample_ps=1.0):
+    """Total-energy drift of the mixed-precision engine without a thermostat (LangevinMiddle at
+    zero friction) over `ps` picoseconds from an equilibrated state: least-squares slope of
+    E_pot + E_kin sampled every `sample_ps`."""
+    import numpy as np
+
+    import ommb200
+    from ommb200 import systems
+
+    ctx = ommb200.Context(systems.water_system(w), systems.langevin(friction=0.0, seed=1),
+                          precision="mixed", device=device)
+    ctx.set_positions(x)
+    ctx.set_velocities(v)
+    every = int(round(sample_ps / DT_PS))
+    t, e = [], []
+    for k in range(int(round(ps / sample_ps)) + 1):
+        st = ctx.get_state(energy=True)
+        t.append(k * sample_ps)
+        e.append(st.potential_energy + st.kinetic_energy)
+        if k * sample_ps < ps:
+            ctx.step(every)
+    ctx.close()
+    slope = float(np.polyfit(t, e, 1)[0]) * 1000.0  # kJ/mol/ns
+    dof = 3 * w.n_atoms - 3 * w.n_waters  # rigid waters: 6 degrees of freedom each
+    return {"ps": ps, "kj_mol_per_ns": slope, "kj_mol_per_ns_per_dof": slope / dof,
+            "energy_rms_fluctuation_kj_mol": float(np.std(e)), "dof": dof,
+            "samples": len(e)}
+
+
+def cpu_one_core(w, x0):
+    """The oracle's PME force evaluation on one host thread (the reference is single-threaded),
+    as ns/day if every MD step cost one such evaluation."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+
+    t0 = time.perf_counter()
+    O.nonbonded(x0, w.charges(), w.sigmas(), w.epsilons(), w.exceptions(), method="PME",
+                cutoff=0.9, ewald_tolerance=5e-4, box=w.box, threads=1)
+    sec = time.perf_counter() - t0
+    return {"value": ns_per_day(1, sec), "unit": "ns/day", "cores": 1, "kind": "port",
+            "sample": f"one f64 PME force evaluation in {sec:.2f} s"}
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -328,13 +413,7 @@ def main():
 
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+    init_replicas(world, local)
     seed = 1000 + rank
     w, ctx = build_context(args.precision, seed, local)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{local}")
@@ -343,10 +422,7 @@ def main():
     time_segments(ctx, torch, args.warmup, args.segment, flush)
 
     def barrier():
-        if world > 1:
-            import torch.distributed as dist
-
-            dist.barrier()
+        replica_barrier(world)
         torch.cuda.synchronize()
 
     uuid = None
@@ -363,12 +439,7 @@ def main():
     barrier()
     e2e_ms, h2d, d2h = time_e2e(ctx, torch, w.n_atoms, args.steps, args.segment, flush)
     barrier()
-    if world > 1:
-        import torch.distributed as dist
-
-        t = torch.tensor([ms, e2e_ms], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, e2e_ms = float(t[0]), float(t[1])
+    ms, e2e_ms = max_over_ranks([ms, e2e_ms], world, f"cuda:{local}")
     md_steps = args.steps * args.segment
     value = world * ns_per_day(md_steps, ms / 1000.0)
     e2e_value = world * ns_per_day(md_steps, e2e_ms / 1000.0)
@@ -404,10 +475,11 @@ def main():
                                             "note": "of measured; latency-bound at this size"}
         per_step = {k: (v[0] / v[1], v[1] / prof_steps) for k, v in times.items()}
         extras["kernel_ms_per_md_step"] = {k: round(v[0] * v[1], 5) for k, v in per_step.items()}
-        # our kernels per MD step: rebuild 9, pack 2, pair 1, PME spread/convert/convolve/
-        # gather 4, exceptions 1, integrate 1; plus one counter kernel per graph launch
-        per_md = 9 + 2 + 1 + 4 + 1 + 1
-        launches = md_steps * per_md + args.steps * (args.segment // 20)
+        # our kernels per MD step: rebuild condition 1, pack 1, pair 1, PME spread/convert/
+        # convolve/gather 4, exceptions 1, integrate 1; the 9 rebuild kernels only on rebuild
+        # steps; one counter kernel per graph launch of 20 steps
+        per_md = 1 + 1 + 1 + 4 + 1 + 1
+        launches = md_steps * per_md + 9 * rebuilds_timed + args.steps * (args.segment // 20)
         extras["pairs_in_cutoff"] = pairs
         nl = ctx.nlist_stats()
         nl["pair_efficiency"] = pairs / max(1, nl["tiles"] * 1024)
@@ -427,6 +499,9 @@ def main():
             extras["force_rms_rel_err_vs_fp64_oracle"] = err
             extras["energy_rel_err_vs_fp64_oracle"] = abs(e_gpu - cpu.pop("energy")) / abs(e_gpu)
             extras["host_cpu"] = {"nproc": os.cpu_count(), "model": _cpu_model()}
+            extras["cpu_baseline_1_core"] = cpu_one_core(w, x0)
+        st_eq = ctx.get_state(positions=True, velocities=True)
+        extras["nve_drift"] = nve_drift(w, st_eq.positions, st_eq.velocities, local)
     out = {
         "metric": METRIC, "value": value, "unit": "ns/day", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
@@ -453,11 +528,7 @@ def main():
     }
     out.update(extras)
     ctx.close()
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.barrier()
-        dist.destroy_process_group()
+    close_replicas(world)
     if rank == 0:
         print(json.dumps(out), flush=True)
 
@@ -548,13 +619,7 @@ def main_chains(args):
                     "d2h_bytes_per_step": 0}}), flush=True)
         return
     torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+    init_replicas(world, local)
     chs = synth.chain_batch(256, 200, 2000, seed=7)
     sizes = np.array([c.n_atoms for c in chs])
     seed = 1000 + rank
@@ -568,10 +633,7 @@ def main_chains(args):
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{local}")
     seg = args.segment
     time_segments(ctx, torch, args.warmup, seg, flush)
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.barrier()
+    replica_barrier(world)
     torch.cuda.synchronize()
     uuid = None
     try:
@@ -582,12 +644,8 @@ def main_chains(args):
     ms = time_segments(ctx, torch, args.steps, seg, flush)
     clocks = sampler.stop()
     e2e_ms, h2d, d2h = time_e2e(ctx, torch, int(sizes.sum()), args.steps, seg, flush)
-    if world > 1:
-        import torch.distributed as dist
-
-        t = torch.tensor([ms, e2e_ms], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, e2e_ms = float(t[0]), float(t[1])
+    replica_barrier(world)
+    ms, e2e_ms = max_over_ranks([ms, e2e_ms], world, f"cuda:{local}")
     md_steps = args.steps * seg
     value = world * md_steps / (ms / 1000.0)
     extras = {}
@@ -656,11 +714,7 @@ def main_chains(args):
     }
     out.update(extras)
     ctx.close()
-    if world > 1:
-        import torch.distributed as dist
-
-        dist.barrier()
-        dist.destroy_process_group()
+    close_replicas(world)
     if rank == 0:
         print(json.dumps(out), flush=True)
 
@@ -696,6 +750,7 @@ def main_learned(args):
                         "d2h_bytes_per_step": 0}}), flush=True)
         return
     torch.cuda.set_device(local)
+    init_replicas(world, local)
     chs = [synth.chain(5000, seed=70 + k) for k in range(16)]
     n_atoms = sum(c.n_atoms for c in chs)
     x0 = np.concatenate([c.positions for c in chs])
@@ -727,13 +782,17 @@ def main_learned(args):
     except Exception:
         pass
     stats0 = ctx.learned_radii_stats()
+    replica_barrier(world)
+    torch.cuda.synchronize()
     sampler = ClockSampler(uuid)
     ms = time_segments(ctx, torch, args.steps, seg, flush)
     clocks = sampler.stop()
     stats1 = ctx.learned_radii_stats()
     e2e_ms, h2d, d2h = time_e2e(ctx, torch, n_atoms, args.steps, seg, flush)
+    replica_barrier(world)
+    ms, e2e_ms, ms_exact = max_over_ranks([ms, e2e_ms, ms_exact], world, f"cuda:{local}")
     md_steps = args.steps * seg
-    value = md_steps / (ms / 1000.0)
+    value = world * md_steps / (ms / 1000.0)
     extras = {}
     cpu = None
     if rank == 0 and not args.skip_extras:
@@ -768,11 +827,12 @@ def main_learned(args):
     d = {k: stats1[k] - stats0[k] for k in ("judges", "learned_steps", "exact_steps")}
     out = {
         "metric": "MD steps/s, 16 x 5,000-atom chains, learned Born radii",
-        "value": value, "unit": "batch steps/s", "n_gpus": world, "steps": args.steps,
+        "value": value, "unit": "batch steps/s (summed over replicas)", "n_gpus": world,
+        "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "ms_per_md_step": ms / md_steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "fp32+bf16" if args.precision == "mixed" else "fp64+bf16", "data": "synthetic",
-        "exact_obc": {"value": md_steps / (ms_exact / 1000.0), "unit": "batch steps/s",
+        "exact_obc": {"value": world * md_steps / (ms_exact / 1000.0), "unit": "batch steps/s",
                       "ms_per_md_step": ms_exact / md_steps},
         "learned_over_exact": ms_exact / ms,
         "learned_radii_timed": {**d, "last_radius_error": stats1["last_radius_error"],
@@ -782,13 +842,14 @@ def main_learned(args):
                    "learned_radii": learned, "integrator": "LangevinMiddle 300 K, 1/ps, 1 fs",
                    "md_steps_per_bench_step": seg,
                    "l2": "flushed (256 MiB write) between timed bench steps"},
-        "e2e": {"value": md_steps / (e2e_ms / 1000.0), "unit": "batch steps/s",
+        "e2e": {"value": world * md_steps / (e2e_ms / 1000.0), "unit": "batch steps/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "clocks": clocks,
         "cpu_baseline": cpu,
     }
     out.update(extras)
     ctx.close()
+    close_replicas(world)
     if rank == 0:
         print(json.dumps(out), flush=True)
 

@@ -200,6 +200,7 @@ Engine::Engine(std::unique_ptr<SystemDef> system, std::unique_ptr<IntegratorDef>
   OMMB200_CK(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, opt_.device));
   OMMB200_CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
   OMMB200_CK(cudaStreamCreateWithFlags(&pme_stream_, cudaStreamNonBlocking));
+  OMMB200_CK(cudaStreamCreateWithFlags(&aux_stream_, cudaStreamNonBlocking));
   OMMB200_CK(cudaEventCreateWithFlags(&fork_ev_, cudaEventDisableTiming));
   OMMB200_CK(cudaEventCreateWithFlags(&join_ev_, cudaEventDisableTiming));
   if (integ_->random_seed != 0) {
@@ -264,6 +265,7 @@ Engine::~Engine() {
   if (fork_ev_) cudaEventDestroy(fork_ev_);
   if (join_ev_) cudaEventDestroy(join_ev_);
   if (pme_stream_) cudaStreamDestroy(pme_stream_);
+  if (aux_stream_) cudaStreamDestroy(aux_stream_);
   if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -1039,12 +1041,45 @@ void Engine::set_profiling(bool enabled) {
   kernel_times_.clear();
 }
 
+// In a captured step the neighbour-list rebuild is the body of an IF node whose condition a
+// one-thread kernel copies from the rebuild flag, so steps without a rebuild skip its nine
+// launches instead of running them as early-exit kernels.
+void Engine::enqueue_conditional_rebuild() {
+  cudaStreamCaptureStatus st;
+  cudaGraph_t cap = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
+  OMMB200_CK(cudaStreamGetCaptureInfo(stream_, &st, nullptr, &cap, &deps, &nd));
+  cudaGraphConditionalHandle handle;
+  OMMB200_CK(cudaGraphConditionalHandleCreate(&handle, cap, 0, cudaGraphCondAssignDefault));
+  launch_nlist_condition(nl_, handle, stream_);
+  OMMB200_CK(cudaStreamGetCaptureInfo(stream_, &st, nullptr, &cap, &deps, &nd));
+  cudaGraphNodeParams params{};
+  params.type = cudaGraphNodeTypeConditional;
+  params.conditional.handle = handle;
+  params.conditional.type = cudaGraphCondTypeIf;
+  params.conditional.size = 1;
+  cudaGraphNode_t node;
+  OMMB200_CK(cudaGraphAddNode(&node, cap, deps, nd, &params));
+  OMMB200_CK(cudaStreamUpdateCaptureDependencies(stream_, &node, 1,
+                                                 cudaStreamSetCaptureDependencies));
+  cudaGraph_t body = params.conditional.phGraph_out[0];
+  OMMB200_CK(cudaStreamBeginCaptureToGraph(aux_stream_, body, nullptr, nullptr, 0,
+                                           cudaStreamCaptureModeThreadLocal));
+  launch_nlist_rebuild(nl_, dp_, aux_stream_);
+  cudaGraph_t done = nullptr;
+  OMMB200_CK(cudaStreamEndCapture(aux_stream_, &done));
+}
+
 template <class Real>
 void Engine::enqueue_nonbonded(bool energy, bool direct, bool reciprocal, bool dump) {
   const NonbondedDef& nb = *nb_;
   if (nb_periodic_) {
     prof_begin("nlist_rebuild");
-    launch_nlist_rebuild(nl_, dp_, stream_);
+    if (capturing_)
+      enqueue_conditional_rebuild();
+    else
+      launch_nlist_rebuild(nl_, dp_, stream_);
     prof_end();
   }
   // fork: PME on its own stream (serialised on the main stream while profiling, so that
@@ -1286,15 +1321,18 @@ void Engine::run_graph_steps(int launches) {
   const int k = graph_steps_;
   if (!graph_exec_) {
     OMMB200_CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+    capturing_ = true;
     try {
       for (int s = 0; s < k; ++s) enqueue_step(s);
       launch_advance_counter(rng_step_, k, stream_);
     } catch (...) {
+      capturing_ = false;
       cudaGraph_t g = nullptr;
       cudaStreamEndCapture(stream_, &g);
       if (g) cudaGraphDestroy(g);
       throw;
     }
+    capturing_ = false;
     OMMB200_CK(cudaStreamEndCapture(stream_, &graph_));
     OMMB200_CK(cudaGraphInstantiate(&graph_exec_, graph_, 0));
   }

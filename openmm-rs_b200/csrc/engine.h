@@ -101,6 +101,7 @@ class Engine {
   void setup_integrator();
   void update_box_dependents();
   void build_static_tiles();
+  void enqueue_conditional_rebuild();
   // `in_step`: an MD step's evaluation (the learned radii may judge and train there);
   // `step_offset`: its position inside the captured group of steps.
   void compute_forces(bool energy, uint32_t groups, bool in_step = false, int step_offset = 0);
@@ -133,6 +134,8 @@ class Engine {
   // the integrator, so it overlaps the real-space pair kernel (also inside the CUDA graph).
   cudaStream_t pme_stream_ = nullptr;
   cudaEvent_t fork_ev_ = nullptr, join_ev_ = nullptr;
+  cudaStream_t aux_stream_ = nullptr;  // captures conditional-node bodies
+  bool capturing_ = false;             // a step group is being captured into the graph
   DeviceArena mem_;
 
   // state

@@ -62,6 +62,9 @@ struct NlistArgs {
 };
 
 void launch_nlist_rebuild(const NlistArgs& a, bool double_entries, cudaStream_t s);
+// Sets `handle` (a conditional graph node's condition) to whether a rebuild is pending.
+void launch_nlist_condition(const NlistArgs& a, cudaGraphConditionalHandle handle,
+                            cudaStream_t s);
 
 // ---- nonbonded pair kernel -------------------------------------------------------------
 enum ElecKind : int { kElecEwald = 0, kElecReactionField = 1, kElecCoulomb = 2 };

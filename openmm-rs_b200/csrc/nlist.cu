@@ -426,6 +426,12 @@ __global__ void nl_finish(NlistArgs a) {
   }
 }
 
+// Inside a captured step: the rebuild kernels sit in the body of a conditional graph node
+// that runs only when the integrator raised the flag.
+__global__ void nl_set_condition(const int* rebuild, cudaGraphConditionalHandle handle) {
+  cudaGraphSetConditional(handle, *rebuild != 0 ? 1u : 0u);
+}
+
 __global__ void nl_clear_flag(NlistArgs a) {
   if (*a.rebuild == 0) return;
   *a.rebuild = 0;
@@ -433,6 +439,11 @@ __global__ void nl_clear_flag(NlistArgs a) {
 }
 
 }  // namespace
+
+void launch_nlist_condition(const NlistArgs& a, cudaGraphConditionalHandle handle,
+                            cudaStream_t s) {
+  nl_set_condition<<<1, 1, 0, s>>>(a.rebuild, handle);
+}
 
 void launch_nlist_rebuild(const NlistArgs& a, bool double_entries, cudaStream_t s) {
   const int tb = 256;
