@@ -53,6 +53,13 @@ def parse():
                    help="water-1065000: the 22 nm box of 355,000 waters; chains-256: 256 uneven "
                         "implicit-solvent chains batched in one Context; chains-learned: 16 "
                         "chains of 5,000 atoms with learned Born radii vs exact OBC")
+    p.add_argument("--no-graph", action="store_true",
+                   help="launch kernels one by one instead of from CUDA graphs (profiler "
+                        "captures: kernels inside graphs with conditional nodes cannot be "
+                        "profiled individually)")
+    p.add_argument("--systems", type=int, default=16,
+                   help="chains-learned: number of chains (small cases for profiler captures)")
+    p.add_argument("--atoms", type=int, default=5000, help="chains-learned: atoms per chain")
     return p.parse_args()
 
 
@@ -192,7 +199,7 @@ def build_context(precision, seed, device):
 
     w, x, v = equilibrate(seed, device)
     ctx = ommb200.Context(systems.water_system(w), systems.langevin(seed=seed),
-                          precision=precision, device=device)
+                          precision=precision, device=device, use_cuda_graph=USE_GRAPH)
     ctx.set_positions(x)
     ctx.set_velocities(v)
     TUNED[precision] = ctx.autotune(200) if TUNE else None
@@ -201,6 +208,7 @@ def build_context(precision, seed, device):
 
 TUNE = True
 TUNED = {}
+USE_GRAPH = True
 
 
 def time_segments(ctx, torch, segments, md_steps, flush):
@@ -391,7 +399,8 @@ def run_reference(args):
 
 def main():
     args = parse()
-    global EQUILIBRATION_STEPS, TUNE, WORKLOAD
+    global EQUILIBRATION_STEPS, TUNE, WORKLOAD, USE_GRAPH
+    USE_GRAPH = not args.no_graph
     if args.workload.startswith("water"):
         WORKLOAD = args.workload
     if args.no_equilibrate:
@@ -625,7 +634,8 @@ def main_chains(args):
     seed = 1000 + rank
     ctx = ommb200.BatchContext([systems.chain_system(c) for c in chs],
                                systems.langevin(step_size=CHAIN_DT_PS, seed=seed),
-                               precision=args.precision, device=local)
+                               precision=args.precision, device=local,
+                               use_cuda_graph=not args.no_graph)
     ctx.set_positions(np.concatenate([c.positions for c in chs]))
     ctx.set_velocities_to_temperature(300.0, seed=seed)
     ctx.step(500)  # untimed: relax the random-walk start
@@ -735,11 +745,12 @@ def main_learned(args):
             sys.path.insert(0, str(ROOT / "oracle"))
             import oracle as O
 
-            chs = [synth.chain(5000, seed=70 + k) for k in range(16)]
+            chs = [synth.chain(args.atoms, seed=70 + k) for k in range(args.systems)]
             threads = O.max_threads()
             sec, done, spent = chains_cpu(chs, threads, budget=10.0)
             print(json.dumps({
-                "impl": "reference", "metric": "MD steps/s, 16 x 5,000-atom chains (exact OBC)",
+                "impl": "reference",
+                "metric": f"MD steps/s, {args.systems} x {args.atoms:,}-atom chains (exact OBC)",
                 "value": 1.0 / sec, "unit": "batch steps/s", "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * sec,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -751,7 +762,7 @@ def main_learned(args):
         return
     torch.cuda.set_device(local)
     init_replicas(world, local)
-    chs = [synth.chain(5000, seed=70 + k) for k in range(16)]
+    chs = [synth.chain(args.atoms, seed=70 + k) for k in range(args.systems)]
     n_atoms = sum(c.n_atoms for c in chs)
     x0 = np.concatenate([c.positions for c in chs])
     seed = 1000 + rank
@@ -761,7 +772,7 @@ def main_learned(args):
         ctx = ommb200.BatchContext(
             [systems.chain_system(c, learned_radii=lr, gb_force_group=1) for c in chs],
             systems.langevin(step_size=CHAIN_DT_PS, seed=seed), precision=args.precision,
-            device=local)
+            device=local, use_cuda_graph=not args.no_graph)
         ctx.set_positions(x0)
         ctx.set_velocities_to_temperature(300.0, seed=seed)
         return ctx
@@ -826,7 +837,7 @@ def main_learned(args):
                          f"{spent:.1f} s, extrapolated to the batch by sum of n^2"}
     d = {k: stats1[k] - stats0[k] for k in ("judges", "learned_steps", "exact_steps")}
     out = {
-        "metric": "MD steps/s, 16 x 5,000-atom chains, learned Born radii",
+        "metric": f"MD steps/s, {args.systems} x {args.atoms:,}-atom chains, learned Born radii",
         "value": value, "unit": "batch steps/s (summed over replicas)", "n_gpus": world,
         "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "ms_per_md_step": ms / md_steps,

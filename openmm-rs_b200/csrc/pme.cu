@@ -95,6 +95,113 @@ __global__ void spread_kernel(const PmeArgs<Real> a) {
   }
 }
 
+// Staged spreading: a CTA takes 64 consecutive sorted slots (spatially compact: part of one
+// x-y column, z-sorted), two threads per atom, and adds the atoms' 125-point stencils into a
+// shared-memory copy of the grid box they touch, then adds that box to the global grid, so
+// each grid point receives one global atomic per CTA instead of one per stencil.  Shared
+// accumulation uses native 32-bit atomics on a split of each 64-bit fixed-point value,
+// v = hi 2^20 + lo with 0 <= lo < 2^20: at most 64 contributions per cell keep both partial
+// sums inside 32 bits (for |q| < 16 e), and hi_sum 2^20 + lo_sum recovers the exact 64-bit
+// total, so the integer grid is identical to direct spreading.  A CTA whose box exceeds
+// kSpreadCells (it straddles a periodic edge of the column order) or that holds a larger
+// charge spreads directly.
+constexpr int kSpreadAtoms = 64;
+constexpr int kSpreadCells = 4096;
+
+template <class Real>
+__global__ void __launch_bounds__(2 * kSpreadAtoms) spread_staged_kernel(const PmeArgs<Real> a) {
+  __shared__ int c_hi[kSpreadCells];
+  __shared__ unsigned int c_lo[kSpreadCells];
+  __shared__ int s_lo[3], s_hi[3], s_big;
+  const int tid = threadIdx.x, half = tid / kSpreadAtoms;  // half 0: ix 0..2, half 1: ix 3..4
+  const int s = blockIdx.x * kSpreadAtoms + (tid % kSpreadAtoms);
+  int atom = -1;
+  if (s < a.n_order) atom = a.order ? a.order[s] : s;
+  const double qd = atom >= 0 ? a.charge[atom] : 0.0;
+  int base[3] = {0, 0, 0};
+  Real frac[3] = {Real(0), Real(0), Real(0)};
+  const bool ok = atom >= 0 && qd != 0.0 && stencil(a, atom, base, frac);
+  if (tid < 3) {
+    s_lo[tid] = 0x7fffffff;
+    s_hi[tid] = -1;
+  }
+  if (tid == 0) s_big = 0;
+  __syncthreads();
+  if (ok && half == 0) {
+    for (int d = 0; d < 3; ++d) {
+      atomicMin(&s_lo[d], base[d]);
+      atomicMax(&s_hi[d], base[d]);
+    }
+    if (fabs(qd) >= 16.0) s_big = 1;  // the 32-bit partial sums need |q| < 16 e
+  }
+  __syncthreads();
+  if (s_hi[0] < 0) return;  // no charged atom in this CTA (uniform)
+  const int lo0 = s_lo[0], lo1 = s_lo[1], lo2 = s_lo[2];
+  const int ex = s_hi[0] - lo0 + 5, ey = s_hi[1] - lo1 + 5, ez = s_hi[2] - lo2 + 5;
+  const long long n_cells = s_big ? (long long)kSpreadCells + 1 : (long long)ex * ey * ez;
+  Real w[3][5], dw[3][5];
+  if (ok) {
+#pragma unroll
+    for (int d = 0; d < 3; ++d) spline5(frac[d], w[d], dw[d]);
+  }
+  const Real q = (Real)qd;
+  const Real gscale = Real(kGridScale);
+  const int ix0 = half == 0 ? 0 : 3, ix1 = half == 0 ? 3 : 5;
+  if (n_cells > kSpreadCells) {  // direct spreading (uniform branch)
+    if (!ok) return;
+    for (int ix = ix0; ix < ix1; ++ix) {
+      int gx = base[0] + ix;
+      gx -= gx >= a.nx ? a.nx : 0;
+      const Real qx = q * w[0][ix];
+      for (int iy = 0; iy < 5; ++iy) {
+        int gy = base[1] + iy;
+        gy -= gy >= a.ny ? a.ny : 0;
+        const Real qxy = qx * w[1][iy];
+        long long* row = a.grid_fixed + ((long long)gx * a.ny + gy) * a.nz;
+#pragma unroll
+        for (int iz = 0; iz < 5; ++iz) {
+          int gz = base[2] + iz;
+          gz -= gz >= a.nz ? a.nz : 0;
+          add_fixed(row + gz, to_fixed(qxy * w[2][iz], gscale));
+        }
+      }
+    }
+    return;
+  }
+  const int nc = (int)n_cells;
+  for (int c = tid; c < nc; c += 2 * kSpreadAtoms) {
+    c_hi[c] = 0;
+    c_lo[c] = 0u;
+  }
+  __syncthreads();
+  if (ok) {
+    for (int ix = ix0; ix < ix1; ++ix) {
+      const Real qx = q * w[0][ix];
+      for (int iy = 0; iy < 5; ++iy) {
+        const Real qxy = qx * w[1][iy];
+        const int row = ((base[0] - lo0 + ix) * ey + (base[1] - lo1 + iy)) * ez + (base[2] - lo2);
+#pragma unroll
+        for (int iz = 0; iz < 5; ++iz) {
+          const long long v = to_fixed(qxy * w[2][iz], gscale);
+          atomicAdd(&c_hi[row + iz], (int)(v >> 20));
+          atomicAdd(&c_lo[row + iz], (unsigned int)(v & 0xFFFFF));
+        }
+      }
+    }
+  }
+  __syncthreads();
+  for (int c = tid; c < nc; c += 2 * kSpreadAtoms) {
+    const long long v = (long long)c_hi[c] * (1ll << 20) + (long long)c_lo[c];
+    if (v == 0) continue;
+    const int cz = c % ez, cy = (c / ez) % ey, cx = c / (ez * ey);
+    int gx = lo0 + cx, gy = lo1 + cy, gz = lo2 + cz;
+    gx -= gx >= a.nx ? a.nx : 0;
+    gy -= gy >= a.ny ? a.ny : 0;
+    gz -= gz >= a.nz ? a.nz : 0;
+    add_fixed(a.grid_fixed + ((long long)gx * a.ny + gy) * a.nz + gz, v);
+  }
+}
+
 template <class Real>
 __global__ void convert_kernel(const PmeArgs<Real> a) {
   const long long total = (long long)a.nx * a.ny * a.nz;
@@ -221,7 +328,11 @@ __global__ void gather_kernel(const PmeArgs<Real> a) {
 
 template <class Real>
 void launch_pme_spread(const PmeArgs<Real>& a, cudaStream_t s) {
-  spread_kernel<Real><<<ceil_div(a.n_order, 128), 128, 0, s>>>(a);
+  if (a.order) {  // sorted slots: spatially compact CTAs
+    spread_staged_kernel<Real><<<ceil_div(a.n_order, kSpreadAtoms), 2 * kSpreadAtoms, 0, s>>>(a);
+  } else {
+    spread_kernel<Real><<<ceil_div(a.n_order, 128), 128, 0, s>>>(a);
+  }
 }
 template <class Real>
 void launch_pme_convert(const PmeArgs<Real>& a, cudaStream_t s) {
