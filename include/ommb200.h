@@ -197,6 +197,22 @@ int ommb200_context_step(ommb200_context* ctx, int steps);
 int ommb200_context_get_state(ommb200_context* ctx, int flags, uint32_t groups,
                               double* positions, double* velocities, double* forces,
                               ommb200_state_info* info);
+/* context.rs:689-705 update_nonbonded_force_parameters (nonbonded.rs:721-767): copy the
+ * particle and exception parameters of `source` (a NonbondedForce handle the caller keeps)
+ * into the Context's NonbondedForce.  Same particle and exception counts, same exception
+ * pairs, and no excluded pair may become an interacting one (OMMB200_ERR_INVALID_ARG). */
+int ommb200_context_update_nonbonded_parameters(ommb200_context* ctx, const ommb200_force* source);
+/* context.rs:680-687 update_gbsa_obc_force_parameters (gbsa_obc.rs:134-141): charges, radii
+ * and scale factors of `source` (same particle count). */
+int ommb200_context_update_gbsa_obc_parameters(ommb200_context* ctx, const ommb200_force* source);
+/* Checkpoints (the reference's set_state, context.rs:274-293, restores positions, velocities,
+ * box and time but not the random stream): the complete dynamic state as opaque bytes --
+ * positions, velocities, box, time, step count, random-stream counter and seed, neighbour-list
+ * reference positions and learned-radii network / optimiser.  Loading it into a Context built
+ * from the same System and options continues the trajectory bit for bit. */
+int ommb200_context_checkpoint_size(const ommb200_context* ctx, int64_t* bytes);
+int ommb200_context_create_checkpoint(ommb200_context* ctx, void* buffer, int64_t bytes);
+int ommb200_context_load_checkpoint(ommb200_context* ctx, const void* buffer, int64_t bytes);
 /* Autotuner (no reference counterpart): times trial_steps MD steps from the current state
  * for each candidate Verlet skin (which sets the neighbour-list rebuild interval) and
  * pair-kernel grid, keeps the fastest and restores positions, velocities and the random

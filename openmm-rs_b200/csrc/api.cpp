@@ -640,6 +640,38 @@ int ommb200_radii_mlp_train(int n, const float* features, const float* targets, 
   });
 }
 
+int ommb200_context_update_nonbonded_parameters(ommb200_context* ctx, const ommb200_force* source) {
+  return guarded([&] {
+    OMMB200_CTX;
+    E.update_nonbonded(*nbf(source));
+  });
+}
+int ommb200_context_update_gbsa_obc_parameters(ommb200_context* ctx, const ommb200_force* source) {
+  return guarded([&] {
+    OMMB200_CTX;
+    E.update_gbsa(*force_of<GbsaObcDef, kGbsaObc>(source));
+  });
+}
+int ommb200_context_checkpoint_size(const ommb200_context* ctx, int64_t* bytes) {
+  return guarded([&] {
+    require(ctx && ctx->engine && bytes, "null argument");
+    *bytes = (int64_t)ctx->engine->checkpoint_bytes();
+  });
+}
+int ommb200_context_create_checkpoint(ommb200_context* ctx, void* buffer, int64_t bytes) {
+  return guarded([&] {
+    OMMB200_CTX;
+    require(buffer != nullptr && bytes >= 0, "invalid buffer");
+    E.save_checkpoint(static_cast<uint8_t*>(buffer), (size_t)bytes);
+  });
+}
+int ommb200_context_load_checkpoint(ommb200_context* ctx, const void* buffer, int64_t bytes) {
+  return guarded([&] {
+    OMMB200_CTX;
+    require(buffer != nullptr && bytes >= 0, "invalid buffer");
+    E.load_checkpoint(static_cast<const uint8_t*>(buffer), (size_t)bytes);
+  });
+}
 int ommb200_context_get_learned_radii_stats(ommb200_context* ctx,
                                             ommb200_learned_radii_stats* out) {
   return guarded([&] {

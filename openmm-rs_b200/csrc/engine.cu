@@ -298,40 +298,24 @@ void Engine::setup_nonbonded(const NonbondedDef& nb) {
     for (int a = 0; a < 3; ++a) require(grid_[a] >= 5, "PME grid dimensions must be at least five");
   }
 
-  // per-particle parameters
-  const double sk = std::sqrt(kOne4PiEps0);
-  std::vector<double> qs(n_), hs(n_), se(n_);
-  for (int i = 0; i < n_; ++i) {
-    qs[i] = nb.charge[i] * sk;
-    hs[i] = 0.5 * nb.sigma[i];
-    se[i] = 2.0 * std::sqrt(nb.epsilon[i]);  // pair product = 4 sqrt(eps_i eps_j)
-  }
+  // per-particle parameters and exceptions (uploaded by upload_nonbonded_parameters)
   qscaled_ = mem_.alloc<double>(n_);
   charge_ = mem_.alloc<double>(n_);
   half_sigma_ = mem_.alloc<double>(n_);
   sqrt_eps_ = mem_.alloc<double>(n_);
-  OMMB200_CK(cudaMemcpy(qscaled_, qs.data(), 8 * n_, cudaMemcpyHostToDevice));
-  OMMB200_CK(cudaMemcpy(charge_, nb.charge.data(), 8 * n_, cudaMemcpyHostToDevice));
-  OMMB200_CK(cudaMemcpy(half_sigma_, hs.data(), 8 * n_, cudaMemcpyHostToDevice));
-  OMMB200_CK(cudaMemcpy(sqrt_eps_, se.data(), 8 * n_, cudaMemcpyHostToDevice));
-
   // exceptions: excluded from the pair kernel, evaluated in f64 (nonbonded.rs:995-1036)
   n_exceptions_ = (int)nb.exceptions.size();
   std::vector<int2> ep(std::max(n_exceptions_, 1));
-  std::vector<double4> epar(std::max(n_exceptions_, 1));
   std::vector<std::vector<int>> partners(n_);
   for (int k = 0; k < n_exceptions_; ++k) {
     const auto& e = nb.exceptions[k];
     ep[k] = make_int2(e.p1, e.p2);
-    epar[k] = make_double4(e.charge_prod * kOne4PiEps0, e.sigma, e.epsilon,
-                           nb.charge[e.p1] * nb.charge[e.p2] * kOne4PiEps0);
     partners[e.p1].push_back(e.p2);
     partners[e.p2].push_back(e.p1);
   }
   exc_pairs_ = mem_.alloc<int2>(ep.size());
-  exc_params_ = mem_.alloc<double4>(epar.size());
+  exc_params_ = mem_.alloc<double4>(ep.size());
   OMMB200_CK(cudaMemcpy(exc_pairs_, ep.data(), sizeof(int2) * ep.size(), cudaMemcpyHostToDevice));
-  OMMB200_CK(cudaMemcpy(exc_params_, epar.data(), sizeof(double4) * epar.size(), cudaMemcpyHostToDevice));
   std::vector<int> xs(n_ + 1, 0), xl;
   for (int i = 0; i < n_; ++i) {
     xs[i] = (int)xl.size();
@@ -456,10 +440,86 @@ void Engine::setup_nonbonded(const NonbondedDef& nb) {
     }
     OMMB200_CK(cudaMemcpy(moduli_, mod.data(), 8 * mod.size(), cudaMemcpyHostToDevice));
   }
-  if (nb_periodic_ && nb.use_dispersion_correction) dispersion_coeff_ = dispersion_coefficient(nb);
+  upload_nonbonded_parameters(nb);
+}
+
+// Per-particle parameters, exception parameters and the parameter-dependent constants (self
+// energy, dispersion coefficient); the pair set and the tile masks do not depend on them.
+void Engine::upload_nonbonded_parameters(const NonbondedDef& nb) {
+  const double sk = std::sqrt(kOne4PiEps0);
+  std::vector<double> qs(n_), hs(n_), se(n_);
+  for (int i = 0; i < n_; ++i) {
+    qs[i] = nb.charge[i] * sk;
+    hs[i] = 0.5 * nb.sigma[i];
+    se[i] = 2.0 * std::sqrt(nb.epsilon[i]);  // pair product = 4 sqrt(eps_i eps_j)
+  }
+  OMMB200_CK(cudaMemcpy(qscaled_, qs.data(), 8 * n_, cudaMemcpyHostToDevice));
+  OMMB200_CK(cudaMemcpy(charge_, nb.charge.data(), 8 * n_, cudaMemcpyHostToDevice));
+  OMMB200_CK(cudaMemcpy(half_sigma_, hs.data(), 8 * n_, cudaMemcpyHostToDevice));
+  OMMB200_CK(cudaMemcpy(sqrt_eps_, se.data(), 8 * n_, cudaMemcpyHostToDevice));
+  std::vector<double4> epar(std::max(n_exceptions_, 1));
+  for (int k = 0; k < n_exceptions_; ++k) {
+    const auto& e = nb.exceptions[k];
+    epar[k] = make_double4(e.charge_prod * kOne4PiEps0, e.sigma, e.epsilon,
+                           nb.charge[e.p1] * nb.charge[e.p2] * kOne4PiEps0);
+  }
+  OMMB200_CK(cudaMemcpy(exc_params_, epar.data(), sizeof(double4) * epar.size(), cudaMemcpyHostToDevice));
+  dispersion_coeff_ =
+      (nb_periodic_ && nb.use_dispersion_correction) ? dispersion_coefficient(nb) : 0.0;
   double q2 = 0.0;
   for (double q : nb.charge) q2 += q * q;
   self_energy_ = nb_pme_ ? -kOne4PiEps0 * alpha_ / std::sqrt(kPiD) * q2 : 0.0;
+  if (nb_pme_ && volume_ > 0.0) {  // after Context creation: the neutralising term
+    double qt = 0.0;
+    for (double q : nb.charge) qt += q;
+    plasma_energy_ = kOne4PiEps0 * kPiD * qt * qt / (2.0 * alpha_ * alpha_ * volume_);
+  }
+}
+
+// context.rs:689-705 / nonbonded.rs:721-767: new particle and exception parameters, same
+// particles, same exception pairs, and no excluded pair may become an interacting one.
+void Engine::update_nonbonded(const NonbondedDef& src) {
+  require(nb_ != nullptr, "the System has no NonbondedForce");
+  NonbondedDef& nb = *const_cast<NonbondedDef*>(nb_);
+  require(src.charge.size() == nb.charge.size(), "particle count must match");
+  require(src.exceptions.size() == nb.exceptions.size(), "exception count must match");
+  for (size_t k = 0; k < nb.exceptions.size(); ++k) {
+    const ExceptionDef &o = nb.exceptions[k], &e = src.exceptions[k];
+    require(o.p1 == e.p1 && o.p2 == e.p2, "exception particle indices must not change");
+    require(o.charge_prod != 0.0 || o.epsilon != 0.0 || (e.charge_prod == 0.0 && e.epsilon == 0.0),
+            "excluded exceptions cannot become non-excluded without reinitialization");
+  }
+  for (size_t i = 0; i < src.charge.size(); ++i)
+    require(std::isfinite(src.charge[i]) && std::isfinite(src.sigma[i]) &&
+                std::isfinite(src.epsilon[i]) && src.sigma[i] >= 0.0 && src.epsilon[i] >= 0.0,
+            "nonbonded parameters must be finite with nonnegative sigma and epsilon");
+  sync();
+  nb.charge = src.charge;
+  nb.sigma = src.sigma;
+  nb.epsilon = src.epsilon;
+  nb.exceptions = src.exceptions;
+  upload_nonbonded_parameters(nb);
+}
+
+// context.rs:680-687 / gbsa_obc.rs:134-141: new charges, radii and scale factors.
+void Engine::update_gbsa(const GbsaObcDef& src) {
+  require(gb_def_ != nullptr, "the System has no GBSAOBCForce");
+  GbsaObcDef& g = *const_cast<GbsaObcDef*>(gb_def_);
+  require(src.charge.size() == g.charge.size(), "particle count must match");
+  for (size_t i = 0; i < src.charge.size(); ++i) {
+    require(std::isfinite(src.charge[i]), "GBSA charges must be finite");
+    require(std::isfinite(src.radius[i]) && src.radius[i] > 0.0,
+            "GBSA radii must be positive and finite");
+    require(std::isfinite(src.scale[i]) && src.scale[i] > 0.0,
+            "GBSA scaling factors must be positive and finite");
+  }
+  sync();
+  g.charge = src.charge;
+  g.radius = src.radius;
+  g.scale = src.scale;
+  OMMB200_CK(cudaMemcpy(const_cast<double*>(gb_.charge), g.charge.data(), 8 * n_, cudaMemcpyHostToDevice));
+  OMMB200_CK(cudaMemcpy(const_cast<double*>(gb_.radius), g.radius.data(), 8 * n_, cudaMemcpyHostToDevice));
+  OMMB200_CK(cudaMemcpy(const_cast<double*>(gb_.scale), g.scale.data(), 8 * n_, cudaMemcpyHostToDevice));
 }
 
 // Segment-padded slot order and every block pair within one segment as a tile:
@@ -1699,6 +1759,127 @@ int64_t Engine::debug_pair_list(int64_t max_pairs, int32_t* pairs) {
   harvest_profile();
   check_status();
   return (int64_t)count;
+}
+
+}  // namespace ommb200
+
+namespace ommb200 {
+
+namespace {
+struct CheckpointHeader {
+  char magic[8];
+  uint32_t version;
+  int32_t n_atoms, n_segments, precision, learned, dynamic_list, rebuild_flag, pair_grid;
+  double time;
+  int64_t step_count;
+  double box[9];
+  uint64_t seed, velocity_draws, rng_step;
+  double skin;
+};
+constexpr char kCheckpointMagic[8] = {'O', 'M', 'B', '2', 'C', 'K', 'P', 'T'};
+constexpr uint32_t kCheckpointVersion = 1;
+}  // namespace
+
+size_t Engine::checkpoint_bytes() const {
+  size_t b = sizeof(CheckpointHeader) + 2 * 24 * (size_t)n_;
+  if (nb_periodic_) b += 24 * (size_t)n_;
+  if (learned_)
+    b += 4 * (size_t)(kRadiiMlpParams + 2 * kRadiiMlpTrainable + 1 + segments_.size()) +
+         sizeof(LearnedState);
+  return b;
+}
+
+void Engine::save_checkpoint(uint8_t* out, size_t bytes) {
+  require(bytes >= checkpoint_bytes(), "checkpoint buffer too small");
+  CheckpointHeader h{};
+  std::memcpy(h.magic, kCheckpointMagic, 8);
+  h.version = kCheckpointVersion;
+  h.n_atoms = n_;
+  h.n_segments = (int32_t)segments_.size();
+  h.precision = opt_.precision;
+  h.learned = learned_ ? 1 : 0;
+  h.dynamic_list = nb_periodic_ ? 1 : 0;
+  h.pair_grid = pair_grid_;
+  h.time = time_;
+  h.step_count = step_count_;
+  std::copy(box_, box_ + 9, h.box);
+  h.seed = seed_;
+  h.velocity_draws = velocity_draws_;
+  h.skin = skin_;
+  int flag = 0;
+  OMMB200_CK(cudaMemcpyAsync(&h.rng_step, rng_step_, 8, cudaMemcpyDeviceToHost, stream_));
+  OMMB200_CK(cudaMemcpyAsync(&flag, rebuild_, 4, cudaMemcpyDeviceToHost, stream_));
+  uint8_t* p = out + sizeof(CheckpointHeader);
+  auto take = [&](const void* dev, size_t n) {
+    OMMB200_CK(cudaMemcpyAsync(p, dev, n, cudaMemcpyDeviceToHost, stream_));
+    p += n;
+  };
+  take(pos_, 24 * (size_t)n_);
+  take(vel_, 24 * (size_t)n_);
+  if (nb_periodic_) take(nl_.pos_ref, 24 * (size_t)n_);
+  if (learned_) {
+    take(lr_.params, 4 * kRadiiMlpParams);
+    take(lr_.moments, 8 * kRadiiMlpTrainable);
+    take(lr_.adam_t, 4);
+    take(lr_.seg_offset, 4 * segments_.size());
+    take(lr_.state, sizeof(LearnedState));
+  }
+  sync();
+  h.rebuild_flag = flag;
+  std::memcpy(out, &h, sizeof(h));
+}
+
+void Engine::load_checkpoint(const uint8_t* in, size_t bytes) {
+  require(bytes >= sizeof(CheckpointHeader), "checkpoint too short");
+  CheckpointHeader h;
+  std::memcpy(&h, in, sizeof(h));
+  require(std::memcmp(h.magic, kCheckpointMagic, 8) == 0 && h.version == kCheckpointVersion,
+          "not a checkpoint of this engine version");
+  require(h.n_atoms == n_ && h.n_segments == (int32_t)segments_.size() &&
+              h.precision == opt_.precision && h.learned == (learned_ ? 1 : 0) &&
+              h.dynamic_list == (nb_periodic_ ? 1 : 0),
+          "checkpoint was written by a Context of a different System or configuration");
+  require(bytes >= checkpoint_bytes(), "checkpoint too short");
+  for (double x : h.box) require(std::isfinite(x), "checkpoint box is not finite");
+  destroy_graph();
+  sync();
+  const uint8_t* p = in + sizeof(CheckpointHeader);
+  auto put = [&](void* dev, size_t n) {
+    OMMB200_CK(cudaMemcpy(dev, p, n, cudaMemcpyHostToDevice));
+    p += n;
+  };
+  put(pos_, 24 * (size_t)n_);
+  put(vel_, 24 * (size_t)n_);
+  std::copy(h.box, h.box + 9, box_);
+  update_box_dependents();
+  time_ = h.time;
+  step_count_ = h.step_count;
+  seed_ = h.seed;
+  velocity_draws_ = h.velocity_draws;
+  OMMB200_CK(cudaMemcpy(rng_step_, &h.rng_step, 8, cudaMemcpyHostToDevice));
+  if (nb_periodic_) {
+    skin_ = h.skin;
+    nl_.skin = h.skin;
+    pair_grid_ = h.pair_grid;
+    put(nl_.pos_ref, 24 * (size_t)n_);
+    // rebuild the neighbour list from the saved reference positions: the same input as the
+    // original run's last rebuild, so the tiles (and every force sum) are the same
+    NlistArgs from_ref = nl_;
+    from_ref.pos = nl_.pos_ref;
+    const int one = 1;
+    OMMB200_CK(cudaMemcpy(rebuild_, &one, 4, cudaMemcpyHostToDevice));
+    launch_nlist_rebuild(from_ref, dp_, stream_);
+    sync();
+    OMMB200_CK(cudaMemcpy(rebuild_, &h.rebuild_flag, 4, cudaMemcpyHostToDevice));
+  }
+  if (learned_) {
+    put(lr_.params, 4 * kRadiiMlpParams);
+    put(lr_.moments, 8 * kRadiiMlpTrainable);
+    put(lr_.adam_t, 4);
+    put(lr_.seg_offset, 4 * segments_.size());
+    put(lr_.state, sizeof(LearnedState));
+  }
+  check_status();
 }
 
 }  // namespace ommb200

@@ -88,6 +88,15 @@ class Engine {
   };
   std::vector<KernelTime> kernel_times() const { return kernel_times_; }
   cudaStream_t stream() const { return stream_; }
+  // context.rs:680-705: live parameter updates of the Context's NonbondedForce / GBSAOBCForce
+  void update_nonbonded(const NonbondedDef& src);
+  void update_gbsa(const GbsaObcDef& src);
+  // Complete dynamic state (positions, velocities, box, time, step count, random-stream
+  // counter, neighbour-list reference, learned-radii network and optimiser) as bytes;
+  // loading it into a Context of the same System continues the trajectory bit for bit.
+  size_t checkpoint_bytes() const;
+  void save_checkpoint(uint8_t* out, size_t bytes);
+  void load_checkpoint(const uint8_t* in, size_t bytes);
   // learned Born radii: counters of the device control block, last judge error and loss
   void learned_stats(ommb200_learned_radii_stats* out);
   void learned_params(float* out);
@@ -106,6 +115,7 @@ class Engine {
   // `step_offset`: its position inside the captured group of steps.
   void compute_forces(bool energy, uint32_t groups, bool in_step = false, int step_offset = 0);
   void setup_learned(const LearnedRadiiDef& def);
+  void upload_nonbonded_parameters(const NonbondedDef& nb);
   std::vector<long long> evaluate(bool energy, uint32_t groups, double* forces);
   void enqueue_step(int step_offset);
   void run_graph_steps(int graph_launches);

@@ -282,30 +282,39 @@ __global__ void convolve_kernel(const PmeArgs<Real> a, const double* moduli) {
   }
 }
 
+// pme.rs:377-425.  Eight lanes per atom: lane k < 5 sums the 25 grid points of stencil plane
+// ix = k, then the group reduces by a fixed shuffle tree and lane 0 commits the force.
 template <class Real>
 __global__ void gather_kernel(const PmeArgs<Real> a) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= a.n_order) return;
-  const int atom = a.order ? a.order[s] : s;
-  if (atom < 0) return;
-  const double qd = a.charge[atom];
-  if (qd == 0.0) return;
-  int base[3];
-  Real frac[3], w[3][5], dw[3][5];
-  if (!stencil(a, atom, base, frac)) return;
-#pragma unroll
-  for (int d = 0; d < 3; ++d) spline5(frac[d], w[d], dw[d]);
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = t >> 3, k = t & 7;
+  int atom = -1;
+  if (s < a.n_order) atom = a.order ? a.order[s] : s;
+  const double qd = atom >= 0 ? a.charge[atom] : 0.0;
+  int base[3] = {0, 0, 0};
+  Real frac[3] = {Real(0), Real(0), Real(0)};
+  const bool ok = atom >= 0 && qd != 0.0 && stencil(a, atom, base, frac);
   Real g0 = 0, g1 = 0, g2 = 0;
-  for (int ix = 0; ix < 5; ++ix) {
-    int gx = base[0] + ix;
+  if (ok && k < 5) {
+    Real w[3][5], dw[3][5];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) spline5(frac[d], w[d], dw[d]);
+    int gx = base[0] + k;
     gx -= gx >= a.nx ? a.nx : 0;
+    Real wx = w[0][0], dwx = dw[0][0];
+#pragma unroll
+    for (int i = 1; i < 5; ++i)
+      if (k == i) {
+        wx = w[0][i];
+        dwx = dw[0][i];
+      }
     for (int iy = 0; iy < 5; ++iy) {
       int gy = base[1] + iy;
       gy -= gy >= a.ny ? a.ny : 0;
       const Real* row = a.grid_real + ((long long)gx * a.ny + gy) * a.nz;
-      const Real wxy = w[0][ix] * w[1][iy];
-      const Real dxy = dw[0][ix] * w[1][iy];
-      const Real xdy = w[0][ix] * dw[1][iy];
+      const Real wxy = wx * w[1][iy];
+      const Real dxy = dwx * w[1][iy];
+      const Real xdy = wx * dw[1][iy];
 #pragma unroll
       for (int iz = 0; iz < 5; ++iz) {
         int gz = base[2] + iz;
@@ -317,6 +326,13 @@ __global__ void gather_kernel(const PmeArgs<Real> a) {
       }
     }
   }
+#pragma unroll
+  for (int o = 4; o > 0; o >>= 1) {
+    g0 += __shfl_xor_sync(0xffffffffu, g0, o, 8);
+    g1 += __shfl_xor_sync(0xffffffffu, g1, o, 8);
+    g2 += __shfl_xor_sync(0xffffffffu, g2, o, 8);
+  }
+  if (!ok || k != 0) return;
   const double gd[3] = {(double)g0 * a.nx, (double)g1 * a.ny, (double)g2 * a.nz};
   for (int c = 0; c < 3; ++c) {
     const double f = -qd * (gd[0] * a.recip[0][c] + gd[1] * a.recip[1][c] + gd[2] * a.recip[2][c]);
@@ -350,7 +366,7 @@ void launch_pme_convolve(const PmeArgs<Real>& a, bool energy, cudaStream_t s) {
 }
 template <class Real>
 void launch_pme_gather(const PmeArgs<Real>& a, cudaStream_t s) {
-  gather_kernel<Real><<<ceil_div(a.n_order, 128), 128, 0, s>>>(a);
+  gather_kernel<Real><<<ceil_div((long long)a.n_order * 8, 128), 128, 0, s>>>(a);
 }
 
 template void launch_pme_spread<float>(const PmeArgs<float>&, cudaStream_t);

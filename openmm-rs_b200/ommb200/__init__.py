@@ -133,6 +133,11 @@ def library() -> C.CDLL:
                                              C.POINTER(I)],
             "ommb200_radii_mlp_forward": [I, P, P, P, P, P],
             "ommb200_gbsa_obc_set_learned_radii": [P, I, I, D, I],
+            "ommb200_context_update_nonbonded_parameters": [P, P],
+            "ommb200_context_update_gbsa_obc_parameters": [P, P],
+            "ommb200_context_checkpoint_size": [P, C.POINTER(C.c_int64)],
+            "ommb200_context_create_checkpoint": [P, P, C.c_int64],
+            "ommb200_context_load_checkpoint": [P, P, C.c_int64],
             "ommb200_context_get_learned_radii_stats": [P, C.POINTER(LearnedRadiiStats)],
             "ommb200_context_get_radii_mlp_params": [P, C.POINTER(C.c_float)],
             "ommb200_context_set_radii_mlp_params": [P, C.POINTER(C.c_float)],
@@ -561,6 +566,27 @@ class Context:
         _check(library().ommb200_context_debug_pair_list(
             self._h, cap, out.ctypes.data_as(C.POINTER(C.c_int32)), C.byref(count)))
         return out[:min(cap, count.value)]
+
+    def update_nonbonded_parameters(self, force: "NonbondedForce") -> None:
+        """context.rs:689-705: take the particle and exception parameters of `force` (which
+        the caller keeps)."""
+        _check(library().ommb200_context_update_nonbonded_parameters(self._h, force._h))
+
+    def update_gbsa_obc_parameters(self, force: "GBSAOBCForce") -> None:
+        """context.rs:680-687: take the charges, radii and scale factors of `force`."""
+        _check(library().ommb200_context_update_gbsa_obc_parameters(self._h, force._h))
+
+    def create_checkpoint(self) -> bytes:
+        """The complete dynamic state (random stream included) as bytes."""
+        n = C.c_int64()
+        _check(library().ommb200_context_checkpoint_size(self._h, C.byref(n)))
+        buf = C.create_string_buffer(n.value)
+        _check(library().ommb200_context_create_checkpoint(self._h, buf, n.value))
+        return buf.raw
+
+    def load_checkpoint(self, data: bytes) -> None:
+        buf = C.create_string_buffer(bytes(data), len(data))
+        _check(library().ommb200_context_load_checkpoint(self._h, buf, len(data)))
 
     def learned_radii_stats(self) -> dict:
         st = LearnedRadiiStats()
