@@ -397,6 +397,7 @@ void Engine::setup_nonbonded(const NonbondedDef& nb) {
   a.sorted_atom = mem_.alloc<int>(n_slots_);
   a.atom_slot = mem_.alloc<int>(n_);
   a.image = mem_.alloc<int>(3 * (size_t)n_);
+  a.slot_wpos = mem_.alloc<double4>(n_slots_);
   a.block_center = mem_.alloc<double>(3 * (size_t)n_blocks_);
   a.block_half = mem_.alloc<double>(3 * (size_t)n_blocks_);
   if (nb_periodic_) {  // replaced by the first rebuild
@@ -988,6 +989,18 @@ void Engine::setup_integrator() {
 void Engine::update_box_dependents() {
   reciprocal_box(box_, recip_, &volume_);
   nl_.box = make_box(box_);
+  nl_.max_cand = 0;
+  if (nb_periodic_ && box_[3] == 0.0 && box_[6] == 0.0 && box_[7] == 0.0) {
+    // candidate blocks of one block in the column-neighbourhood kernel, for the largest skin
+    // the autotuner may pick: every column in reach times the most blocks a column can hold
+    const double reach = nb_->cutoff + std::max(skin_, kMaxTunedSkin);
+    const int nx = nl_.n_col[0], ny = nl_.n_col[1];
+    const int kx = (int)std::floor(reach * nx / box_[0] + 1e-6) + 1;
+    const int ky = (int)std::floor(reach * ny / box_[4] + 1e-6) + 1;
+    const long long cols = (long long)std::min(nx, 2 * kx + 1) * std::min(ny, 2 * ky + 1);
+    const long long cand = cols * (nl_.col_max / 32 + 1);
+    if (cand * 40 <= 200 * 1024) nl_.max_cand = (int)cand;
+  }
   for (auto& L : bonded_) L.args.box = make_box(box_);
   gb_.boxd = make_box(box_);
   gb_.boxf = cast_box<float>(gb_.boxd);

@@ -37,6 +37,7 @@ struct NlistArgs {
   int* n_blocks;      // device: blocks in use after the last rebuild
   int* sorted_atom;   // [slot_capacity] particle in each slot, -1 for padding
   int* atom_slot;     // [N] inverse of sorted_atom
+  double4* slot_wpos;    // [slot_capacity] wrapped rebuild position of each slot (w = 0)
   double* block_center;  // [3 * slot_capacity / 32]
   double* block_half;    // [3 * slot_capacity / 32] half extents of the bounding box
   int4* tiles;           // [tile_capacity] (I, flags, mask_slot, 0)
@@ -59,6 +60,7 @@ struct NlistArgs {
   int n_col[2];       // x-y column grid of the sort
   int n_cols;
   int col_max;        // largest column the per-column sort accepts
+  int max_cand;       // candidate blocks one block can have (rectangular boxes), 0 = unknown
 };
 
 void launch_nlist_rebuild(const NlistArgs& a, bool double_entries, cudaStream_t s);

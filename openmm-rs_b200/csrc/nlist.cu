@@ -172,6 +172,7 @@ __global__ void nl_bounds(NlistArgs a) {
                          a.pos_ref[3 * atom + 1] - (n1 * b.by + n2 * b.cy),
                          a.pos_ref[3 * atom + 2] - n2 * b.cz};
     for (int d = 0; d < 3; ++d) lo[d] = hi[d] = w[d];
+    a.slot_wpos[32 * blk + lane] = make_double4(w[0], w[1], w[2], 0.0);
   }
   for (int off = 16; off > 0; off >>= 1)
     for (int d = 0; d < 3; ++d) {
@@ -196,17 +197,51 @@ __device__ __forceinline__ double box_gap2(const double d[3], const double* hi, 
   return s;
 }
 
+// Exclusion partners of a lane's particle as slots, loaded once per block I: up to
+// kCachedPartners in registers; a particle with more keeps reading its CSR row.
+constexpr int kCachedPartners = 8;
+struct Partners {
+  int slot[kCachedPartners];
+  int n;  // cached count, or -1 when the particle has more partners than fit
+};
+
+__device__ __forceinline__ Partners load_partners(const NlistArgs& a, int ai) {
+  Partners p;
+  p.n = 0;
+#pragma unroll
+  for (int k = 0; k < kCachedPartners; ++k) p.slot[k] = -2;
+  if (ai < 0) return p;
+  const int e0 = a.excl_start[ai], e1 = a.excl_start[ai + 1];
+  if (e1 - e0 > kCachedPartners) {
+    p.n = -1;
+    return p;
+  }
+#pragma unroll
+  for (int k = 0; k < kCachedPartners; ++k)
+    if (e0 + k < e1) p.slot[k] = a.atom_slot[a.excl_list[e0 + k]];
+  p.n = e1 - e0;
+  return p;
+}
+
 // Mask of lane l over 32 entry slots: bit k set when entry k is padding or an exclusion
 // partner of the lane's particle; all bits when the lane itself is padding.
-__device__ __forceinline__ uint32_t entry_mask(const NlistArgs& a, int ai, const int* slots) {
+__device__ __forceinline__ uint32_t entry_mask(const NlistArgs& a, int ai, const Partners& pt,
+                                               const int* slots) {
   if (ai < 0) return kFull;
   uint32_t m = 0;
-  for (int k = 0; k < 32; ++k)
-    if (slots[k] < 0) m |= 1u << k;
-  for (int e = a.excl_start[ai]; e < a.excl_start[ai + 1]; ++e) {
-    const int sp = a.atom_slot[a.excl_list[e]];
-    for (int k = 0; k < 32; ++k)
-      if (slots[k] == sp) m |= 1u << k;
+  for (int k = 0; k < 32; ++k) {
+    const int sk = slots[k];
+    bool hit = sk < 0;
+#pragma unroll
+    for (int q = 0; q < kCachedPartners; ++q) hit = hit || sk == pt.slot[q];
+    if (hit) m |= 1u << k;
+  }
+  if (pt.n < 0) {
+    for (int e = a.excl_start[ai]; e < a.excl_start[ai + 1]; ++e) {
+      const int sp = a.atom_slot[a.excl_list[e]];
+      for (int k = 0; k < 32; ++k)
+        if (slots[k] == sp) m |= 1u << k;
+    }
   }
   return m;
 }
@@ -267,11 +302,12 @@ __global__ void __launch_bounds__(32 * kListWarps) nl_lists(NlistArgs a) {
     const double hi[3] = {a.block_half[3 * I], a.block_half[3 * I + 1], a.block_half[3 * I + 2]};
     const double ri = sqrt(hi[0] * hi[0] + hi[1] * hi[1] + hi[2] * hi[2]);
     const int ai = a.sorted_atom[32 * I + lane];
+    const Partners partners = load_partners(a, ai);
     // self tile
     {
       s_slot[w][lane] = ai < 0 ? -1 : 32 * I + lane;
       __syncwarp();
-      uint32_t m = entry_mask(a, ai, s_slot[w]);
+      uint32_t m = entry_mask(a, ai, partners, s_slot[w]);
       const bool image = a.periodic && a.min_width < reach + 2.0 * ri;
       commit_tile(a, I, kTileSelf | (image ? kTilePairImage : 0), m, lane);
       __syncwarp();
@@ -282,7 +318,7 @@ __global__ void __launch_bounds__(32 * kListWarps) nl_lists(NlistArgs a) {
       const int f = __reduce_or_sync(kFull, lane < count ? s_flag[w][lane] : 0);
       if (lane >= count) s_slot[w][lane] = -1;
       __syncwarp();
-      const uint32_t m = entry_mask(a, ai, s_slot[w]);
+      const uint32_t m = entry_mask(a, ai, partners, s_slot[w]);
       const int t = commit_tile(a, I, f, m, lane);
       double sh[3] = {0.0, 0.0, 0.0};
       if (lane < count)
@@ -325,22 +361,38 @@ __global__ void __launch_bounds__(32 * kListWarps) nl_lists(NlistArgs a) {
           cand = gap2 < reach2;
         }
         unsigned cm = __ballot_sync(kFull, cand);
-        while (cm) {
-          const int src = __ffs(cm) - 1;
+        // the candidate blocks' particles, one block ahead of the one being tested
+        auto fetch = [&](int src, int* aj, double4* wp) {
+          const int slot = 32 * (base + src) + lane;
+          *aj = a.sorted_atom[slot];
+          *wp = a.slot_wpos[slot];
+        };
+        int src = -1, aj_next = -1;
+        double4 wp_next = make_double4(0.0, 0.0, 0.0, 0.0);
+        if (cm) {
+          src = __ffs(cm) - 1;
           cm &= cm - 1;
+          fetch(src, &aj_next, &wp_next);
+        }
+        while (src >= 0) {
           const int Jc = base + src;
-          const double s0 = __shfl_sync(kFull, d[0], src), s1 = __shfl_sync(kFull, d[1], src),
-                       s2 = __shfl_sync(kFull, d[2], src);
-          const bool un = __shfl_sync(kFull, unsafe, src);
-          const int aj = a.sorted_atom[32 * Jc + lane];
+          const int aj = aj_next;
+          const double4 wp = wp_next;
+          const int cur = src;
+          src = -1;
+          if (cm) {
+            src = __ffs(cm) - 1;
+            cm &= cm - 1;
+            fetch(src, &aj_next, &wp_next);
+          }
+          const double s0 = __shfl_sync(kFull, d[0], cur), s1 = __shfl_sync(kFull, d[1], cur),
+                       s2 = __shfl_sync(kFull, d[2], cur);
+          const bool un = __shfl_sync(kFull, unsafe, cur);
           bool in = false;
           if (aj >= 0) {
             const Box<double>& b = a.box;
-            const double n0 = a.image[3 * aj], n1 = a.image[3 * aj + 1], n2 = a.image[3 * aj + 2];
             const double* cj = a.block_center + 3 * Jc;
-            double rel[3] = {a.pos_ref[3 * aj] - (n0 * b.ax + n1 * b.bx + n2 * b.cx) - cj[0] + s0,
-                             a.pos_ref[3 * aj + 1] - (n1 * b.by + n2 * b.cy) - cj[1] + s1,
-                             a.pos_ref[3 * aj + 2] - n2 * b.cz - cj[2] + s2};
+            double rel[3] = {wp.x - cj[0] + s0, wp.y - cj[1] + s1, wp.z - cj[2] + s2};
             if (un) {
               // conservative: the nearest image of the particle to I's centre, against a
               // sphere that contains I's box
@@ -417,6 +469,225 @@ __global__ void __launch_bounds__(32 * kListWarps) nl_lists(NlistArgs a) {
   }
 }
 
+// Rectangular boxes: one CTA of kCtaWarps warps per block I, in four phases.
+//   A  candidate blocks J > I of I's column neighbourhood whose boxes come within reach (the
+//      warps split the columns; two passes place every warp's candidates at fixed offsets)
+//   B  per candidate, the 32-bit mask of its particles within reach of I's box (one warp per
+//      candidate; the conservative sphere test for blocks near a periodic image of I)
+//   C  a prefix sum of the masks' populations packs the selected particles 32 to a tile
+//   D  each warp fills whole tiles: entries, flags, and exclusion masks
+// Candidates, masks and prefix sums live in shared memory; I's tiles are reserved with one
+// atomic, so they are contiguous.  The selected particles and their order are a function of
+// the rebuild positions alone, so the tile contents are deterministic.
+constexpr int kCtaWarps = 8;
+
+template <bool kDouble>
+__global__ void __launch_bounds__(32 * kCtaWarps) nl_lists_cta(NlistArgs a) {
+  if (*a.rebuild == 0) return;
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int cap = a.max_cand;
+  double* c_d = reinterpret_cast<double*>(smem);                    // [3][cap]
+  int* c_J = reinterpret_cast<int*>(c_d + 3 * (size_t)cap);          // [cap]
+  int* c_un = c_J + cap;                                             // [cap]
+  uint32_t* c_mask = reinterpret_cast<uint32_t*>(c_un + cap);        // [cap]
+  int* c_pre = reinterpret_cast<int*>(c_mask + cap);                 // [cap + 1]
+  __shared__ int s_wcount[kCtaWarps], s_wbase[kCtaWarps + 1];
+  __shared__ int s_tile0, s_ntiles;
+  __shared__ int s_slots[kCtaWarps][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int nb = *a.n_blocks;
+  const int I = blockIdx.x;
+  if (I >= nb) return;
+  const double reach = a.cutoff + a.skin;
+  const double reach2 = reach * reach;
+  const double ci[3] = {a.block_center[3 * I], a.block_center[3 * I + 1], a.block_center[3 * I + 2]};
+  const double hi[3] = {a.block_half[3 * I], a.block_half[3 * I + 1], a.block_half[3 * I + 2]};
+  const double ri = sqrt(hi[0] * hi[0] + hi[1] * hi[1] + hi[2] * hi[2]);
+  const Box<double>& bx = a.box;
+  const int first = a.sorted_atom[32 * I];
+  const int col = first >= 0 ? a.column[first] : 0;
+  const int nx = a.n_col[0], ny = a.n_col[1];
+  const int kx = (int)floor(reach * nx / bx.ax + 1e-6) + 1;
+  const int ky = (int)floor(reach * ny / bx.by + 1e-6) + 1;
+  const bool all_x = 2 * kx + 1 >= nx, all_y = 2 * ky + 1 >= ny;
+  const int x0 = col % nx, y0 = col / nx;
+  const int ny_iter = all_y ? ny : 2 * ky + 1, nx_iter = all_x ? nx : 2 * kx + 1;
+  const int n_colq = nx_iter * ny_iter;
+  // candidate test of block J (same arithmetic as the warp-per-block kernel)
+  auto test = [&](int J, double d[3], bool* unsafe) {
+    const double* cj = a.block_center + 3 * J;
+    const double* hj = a.block_half + 3 * J;
+    d[0] = cj[0] - ci[0];
+    d[1] = cj[1] - ci[1];
+    d[2] = cj[2] - ci[2];
+    min_image_fast(d[0], d[1], d[2], bx);
+    const double rj = sqrt(hj[0] * hj[0] + hj[1] * hj[1] + hj[2] * hj[2]);
+    const double dist = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    *unsafe = a.min_width - dist < reach + ri + rj;
+    double gap2 = box_gap2(d, hi, hj);
+    if (*unsafe) {
+      for (int m0 = -1; m0 <= 1; ++m0)
+        for (int m1 = -1; m1 <= 1; ++m1)
+          for (int m2 = -1; m2 <= 1; ++m2) {
+            const double e[3] = {d[0] + m0 * bx.ax + m1 * bx.bx + m2 * bx.cx,
+                                 d[1] + m1 * bx.by + m2 * bx.cy, d[2] + m2 * bx.cz};
+            gap2 = fmin(gap2, box_gap2(e, hi, hj));
+          }
+    }
+    return gap2 < reach2;
+  };
+  // phase A: two passes over this warp's columns
+  for (int pass = 0; pass < 2; ++pass) {
+    int n = 0;
+    for (int q = w; q < n_colq; q += kCtaWarps) {
+      const int oy = q / nx_iter, ox = q % nx_iter;
+      const int cy = all_y ? oy : (y0 + oy - ky + ny) % ny;
+      const int cx = all_x ? ox : (x0 + ox - kx + nx) % nx;
+      const int c = cy * nx + cx;
+      const int j0 = max(a.col_start[c] / 32, I + 1), j1 = min(a.col_start[c + 1] / 32, nb);
+      for (int base = j0; base < j1; base += 32) {
+        const int J = base + lane;
+        double d[3] = {0.0, 0.0, 0.0};
+        bool unsafe = false, cand = false;
+        if (J < j1) cand = test(J, d, &unsafe);
+        const unsigned m = __ballot_sync(kFull, cand);
+        if (pass == 1 && cand) {
+          const int k = s_wbase[w] + n + __popc(m & ((1u << lane) - 1u));
+          if (k < cap) {
+            c_J[k] = J;
+            c_un[k] = unsafe ? 1 : 0;
+            c_d[k] = d[0];
+            c_d[cap + k] = d[1];
+            c_d[2 * cap + k] = d[2];
+          }
+        }
+        n += __popc(m);
+      }
+    }
+    if (pass == 0) {
+      if (lane == 0) s_wcount[w] = n;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        int t = 0;
+        for (int u = 0; u < kCtaWarps; ++u) {
+          s_wbase[u] = t;
+          t += s_wcount[u];
+        }
+        s_wbase[kCtaWarps] = t;
+      }
+      __syncthreads();
+    }
+  }
+  __syncthreads();
+  int n_cand = s_wbase[kCtaWarps];
+  if (n_cand > cap) {  // cannot happen with the host-computed capacity
+    if (threadIdx.x == 0) report_status(a.status, kStatusTileOverflow);
+    n_cand = cap;
+  }
+  // phase B: one warp per candidate
+  for (int c = w; c < n_cand; c += kCtaWarps) {
+    const int J = c_J[c];
+    const bool un = c_un[c] != 0;
+    const int slot = 32 * J + lane;
+    const int aj = a.sorted_atom[slot];
+    bool in = false;
+    if (aj >= 0) {
+      const double4 wp = a.slot_wpos[slot];
+      const double* cj = a.block_center + 3 * J;
+      double rel[3] = {wp.x - cj[0] + c_d[c], wp.y - cj[1] + c_d[cap + c], wp.z - cj[2] + c_d[2 * cap + c]};
+      if (un) {
+        min_image_fast(rel[0], rel[1], rel[2], bx);
+        const double r = sqrt(rel[0] * rel[0] + rel[1] * rel[1] + rel[2] * rel[2]);
+        in = r < reach + ri + 1e-6;
+      } else {
+        in = box_gap2(rel, hi, nullptr) < reach2;
+      }
+    }
+    const unsigned m = __ballot_sync(kFull, in);
+    if (lane == 0) c_mask[c] = m;
+  }
+  __syncthreads();
+  // phase C: prefix sum of the masks' populations (warp 0), then reserve I's tiles
+  if (w == 0) {
+    int carry = 0;
+    for (int base = 0; base < n_cand; base += 32) {
+      const int c = base + lane;
+      const int v = c < n_cand ? __popc(c_mask[c]) : 0;
+      int incl = v;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += y;
+      }
+      if (c < n_cand) c_pre[c] = carry + incl - v;
+      carry += __shfl_sync(kFull, incl, 31);
+    }
+    if (lane == 0) {
+      c_pre[n_cand] = carry;
+      const int nt = 1 + (carry + 31) / 32;
+      int t0 = atomicAdd(a.n_tiles, nt);
+      if (t0 + nt > a.tile_capacity) {
+        report_status(a.status, kStatusTileOverflow);
+        t0 = -1;
+      }
+      s_tile0 = t0;
+      s_ntiles = nt;
+    }
+  }
+  __syncthreads();
+  if (s_tile0 < 0) return;
+  const int total = c_pre[n_cand];
+  const int ai = a.sorted_atom[32 * I + lane];
+  const Partners partners = load_partners(a, ai);
+  // phase D: whole tiles per warp; tile 0 is I's self tile
+  for (int k = w; k < s_ntiles; k += kCtaWarps) {
+    int slot = -1, flag = 0;
+    double sh[3] = {0.0, 0.0, 0.0};
+    if (k == 0) {
+      slot = ai < 0 ? -1 : 32 * I + lane;
+      flag = kTileSelf | ((a.min_width < reach + 2.0 * ri) ? kTilePairImage : 0);
+    } else {
+      const int e = 32 * (k - 1) + lane;
+      if (e < total) {
+        int lo = 0, hi_c = n_cand - 1;  // last candidate with c_pre <= e
+        while (lo < hi_c) {
+          const int mid = (lo + hi_c + 1) >> 1;
+          if (c_pre[mid] <= e) lo = mid;
+          else hi_c = mid - 1;
+        }
+        uint32_t mm = c_mask[lo];  // drop the e - c_pre[lo] lowest set bits
+        for (int r = e - c_pre[lo]; r > 0; --r) mm &= mm - 1u;
+        const int bit = __ffs(mm) - 1;
+        slot = 32 * c_J[lo] + bit;
+        flag = c_un[lo] ? kTilePairImage : 0;
+        sh[0] = c_d[lo];
+        sh[1] = c_d[cap + lo];
+        sh[2] = c_d[2 * cap + lo];
+      }
+      flag = __reduce_or_sync(kFull, flag);
+    }
+    s_slots[w][lane] = slot;
+    __syncwarp();
+    const uint32_t m = entry_mask(a, ai, partners, s_slots[w]);
+    const int t = s_tile0 + k;
+    int mslot = -1;
+    int flags = flag;
+    if (__any_sync(kFull, m != 0)) {
+      if (lane == 0) mslot = atomicAdd(a.n_masks, 1);
+      mslot = __shfl_sync(kFull, mslot, 0);
+      if (mslot < a.mask_capacity) {
+        a.masks[32 * mslot + lane] = m;
+        flags |= kTileHasMask;
+      } else {
+        if (lane == 0) report_status(a.status, kStatusTileOverflow);
+        mslot = -1;
+      }
+    }
+    if (lane == 0) a.tiles[t] = make_int4(I, flags, mslot, 0);
+    if (k > 0) write_entry<kDouble>(a, t, lane, slot, sh);
+    __syncwarp();
+  }
+}
+
 __global__ void nl_finish(NlistArgs a) {
   if (*a.rebuild == 0) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -456,11 +727,23 @@ void launch_nlist_rebuild(const NlistArgs& a, bool double_entries, cudaStream_t 
   while (m < a.col_max) m <<= 1;
   nl_col_sort<<<a.n_cols, 256, sizeof(unsigned long long) * m, s>>>(a);
   nl_bounds<<<ceil_div((long long)block_cap * 32, tb), tb, 0, s>>>(a);
-  const int gl = ceil_div(block_cap, kListWarps);
-  if (double_entries)
-    nl_lists<true><<<gl, 32 * kListWarps, 0, s>>>(a);
-  else
-    nl_lists<false><<<gl, 32 * kListWarps, 0, s>>>(a);
+  const bool rectangular = a.periodic && a.box.bx == 0.0 && a.box.cx == 0.0 && a.box.cy == 0.0;
+  if (rectangular && a.max_cand > 0) {
+    const size_t bytes = (size_t)a.max_cand * (3 * 8 + 4 + 4 + 4 + 4) + 4;
+    if (double_entries) {
+      cudaFuncSetAttribute(nl_lists_cta<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+      nl_lists_cta<true><<<block_cap, 32 * kCtaWarps, bytes, s>>>(a);
+    } else {
+      cudaFuncSetAttribute(nl_lists_cta<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+      nl_lists_cta<false><<<block_cap, 32 * kCtaWarps, bytes, s>>>(a);
+    }
+  } else {
+    const int gl = ceil_div(block_cap, kListWarps);
+    if (double_entries)
+      nl_lists<true><<<gl, 32 * kListWarps, 0, s>>>(a);
+    else
+      nl_lists<false><<<gl, 32 * kListWarps, 0, s>>>(a);
+  }
   nl_finish<<<std::max(1, std::min(ceil_div(a.n_cols, tb), 148 * 4)), tb, 0, s>>>(a);
   nl_clear_flag<<<1, 1, 0, s>>>(a);
 }
