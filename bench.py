@@ -491,7 +491,9 @@ def main():
         launches = md_steps * per_md + 9 * rebuilds_timed + args.steps * (args.segment // 20)
         extras["pairs_in_cutoff"] = pairs
         nl = ctx.nlist_stats()
-        nl["pair_efficiency"] = pairs / max(1, nl["tiles"] * 1024)
+        # self tiles are 32 x 32 pair slots, neighbour tiles 2 x 16 x 16 (halves of block I)
+        slots = nl["blocks"] * 1024 + (nl["tiles"] - nl["blocks"]) * 512
+        nl["pair_efficiency"] = pairs / max(1, slots)
         nl["md_steps_per_rebuild"] = md_steps / max(1, rebuilds_timed)  # timed region only
         extras["nlist"] = nl
         # FP64-on-GPU form of the same kernels

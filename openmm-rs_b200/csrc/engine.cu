@@ -375,13 +375,19 @@ void Engine::setup_nonbonded(const NonbondedDef& nb) {
     const double wx = box_[0] / a.n_col[0], wy = box_[4] / a.n_col[1];
     const double hz = 32.0 / (density * wx * wy);
     const double gathered = density * (wx + 2 * reach) * (wy + 2 * reach) * (hz + 2 * reach) / 2.0;
-    const long long per_block = (long long)(1.5 * gathered / 32.0) + 8;
+    // rectangular boxes pack 16 entries per half of a block and tile, triclinic ones 32
+    const bool halves = box_[3] == 0.0 && box_[6] == 0.0 && box_[7] == 0.0;
+    const double per_tile = halves ? 16.0 : 32.0;
+    const long long per_block = (long long)(1.5 * gathered / per_tile) + 8;
     const bool small_box = a.min_width < 2.0 * (reach + 2.0);
-    const long long all_pairs = blocks * (blocks + 1) / 2 + blocks;
+    const long long all_pairs = (blocks * (blocks + 1) / 2 + blocks) * (halves ? 2 : 1);
     a.tile_capacity = (int)std::min<long long>(all_pairs, small_box ? all_pairs : blocks * per_block);
     // a masked tile holds an exclusion or a padding slot: at most one per exception plus two
-    // per block (self tile, last partial neighbour tile), so this pool cannot overflow
-    a.mask_capacity = (int)std::min<long long>(a.tile_capacity, (long long)n_exceptions_ + 2 * blocks + 64);
+    // per block (self tile, last partial neighbour tile) with 32-entry tiles; with halves a
+    // block's longer half can leave several tiles half padded, so every tile gets a slot
+    a.mask_capacity = halves ? a.tile_capacity
+                             : (int)std::min<long long>(a.tile_capacity,
+                                                        (long long)n_exceptions_ + 2 * blocks + 64);
   } else {
     a.slot_capacity = static_slots_;
     long long tiles = 0;
@@ -999,7 +1005,7 @@ void Engine::update_box_dependents() {
     const int ky = (int)std::floor(reach * ny / box_[4] + 1e-6) + 1;
     const long long cols = (long long)std::min(nx, 2 * kx + 1) * std::min(ny, 2 * ky + 1);
     const long long cand = cols * (nl_.col_max / 32 + 1);
-    if (cand * 40 <= 200 * 1024) nl_.max_cand = (int)cand;
+    if (cand * 48 <= 200 * 1024) nl_.max_cand = (int)cand;
   }
   for (auto& L : bonded_) L.args.box = make_box(box_);
   gb_.boxd = make_box(box_);

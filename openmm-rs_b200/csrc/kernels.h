@@ -19,6 +19,7 @@ enum TileFlags : int {
   kTileHasMask = 1,    // exclusion/padding mask stored at masks[32 * mask_slot]
   kTilePairImage = 2,  // apply the minimum image per pair (small boxes)
   kTileSelf = 4,       // entries are block I itself; each pair is seen twice
+  kTileHalves = 8,     // entries 0-15 pair with slots 0-15 of I only, entries 16-31 with 16-31
 };
 
 struct NlistArgs {

@@ -472,9 +472,11 @@ __global__ void __launch_bounds__(32 * kListWarps) nl_lists(NlistArgs a) {
 // Rectangular boxes: one CTA of kCtaWarps warps per block I, in four phases.
 //   A  candidate blocks J > I of I's column neighbourhood whose boxes come within reach (the
 //      warps split the columns; two passes place every warp's candidates at fixed offsets)
-//   B  per candidate, the 32-bit mask of its particles within reach of I's box (one warp per
-//      candidate; the conservative sphere test for blocks near a periodic image of I)
-//   C  a prefix sum of the masks' populations packs the selected particles 32 to a tile
+//   B  per candidate, the 32-bit masks of its particles within reach of each half of I (slots
+//      0-15 and 16-31; one warp per candidate; the conservative sphere test for blocks near a
+//      periodic image of I)
+//   C  prefix sums of the masks' populations pack each half's particles 16 to a half tile;
+//      tile k carries the k-th 16 entries of both halves
 //   D  each warp fills whole tiles: entries, flags, and exclusion masks
 // Candidates, masks and prefix sums live in shared memory; I's tiles are reserved with one
 // atomic, so they are contiguous.  The selected particles and their order are a function of
@@ -489,8 +491,8 @@ __global__ void __launch_bounds__(32 * kCtaWarps) nl_lists_cta(NlistArgs a) {
   double* c_d = reinterpret_cast<double*>(smem);                    // [3][cap]
   int* c_J = reinterpret_cast<int*>(c_d + 3 * (size_t)cap);          // [cap]
   int* c_un = c_J + cap;                                             // [cap]
-  uint32_t* c_mask = reinterpret_cast<uint32_t*>(c_un + cap);        // [cap]
-  int* c_pre = reinterpret_cast<int*>(c_mask + cap);                 // [cap + 1]
+  uint32_t* c_mask = reinterpret_cast<uint32_t*>(c_un + cap);        // [2][cap] per half of I
+  int* c_pre = reinterpret_cast<int*>(c_mask + 2 * (size_t)cap);     // [2][cap + 1]
   __shared__ int s_wcount[kCtaWarps], s_wbase[kCtaWarps + 1];
   __shared__ int s_tile0, s_ntiles;
   __shared__ int s_slots[kCtaWarps][32];
@@ -504,6 +506,32 @@ __global__ void __launch_bounds__(32 * kCtaWarps) nl_lists_cta(NlistArgs a) {
   const double hi[3] = {a.block_half[3 * I], a.block_half[3 * I + 1], a.block_half[3 * I + 2]};
   const double ri = sqrt(hi[0] * hi[0] + hi[1] * hi[1] + hi[2] * hi[2]);
   const Box<double>& bx = a.box;
+  // boxes of the two halves of I (slots 0-15 and 16-31), relative to I's centre
+  double hc[3], hh[3];
+  {
+    const int ai0 = a.sorted_atom[32 * I + lane];
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, up[3] = {-INFINITY, -INFINITY, -INFINITY};
+    if (ai0 >= 0) {
+      const double4 wp = a.slot_wpos[32 * I + lane];
+      lo[0] = up[0] = wp.x - ci[0];
+      lo[1] = up[1] = wp.y - ci[1];
+      lo[2] = up[2] = wp.z - ci[2];
+    }
+    for (int o = 8; o > 0; o >>= 1)
+      for (int d = 0; d < 3; ++d) {
+        lo[d] = fmin(lo[d], __shfl_xor_sync(kFull, lo[d], o));
+        up[d] = fmax(up[d], __shfl_xor_sync(kFull, up[d], o));
+      }
+    for (int d = 0; d < 3; ++d) {
+      const bool empty = lo[d] > up[d];
+      hc[d] = empty ? 0.0 : 0.5 * (lo[d] + up[d]);
+      hh[d] = empty ? -1.0 : 0.5 * (up[d] - lo[d]);  // negative: the half holds no particle
+    }
+  }
+  const double hcA[3] = {__shfl_sync(kFull, hc[0], 0), __shfl_sync(kFull, hc[1], 0), __shfl_sync(kFull, hc[2], 0)};
+  const double hhA[3] = {__shfl_sync(kFull, hh[0], 0), __shfl_sync(kFull, hh[1], 0), __shfl_sync(kFull, hh[2], 0)};
+  const double hcB[3] = {__shfl_sync(kFull, hc[0], 16), __shfl_sync(kFull, hc[1], 16), __shfl_sync(kFull, hc[2], 16)};
+  const double hhB[3] = {__shfl_sync(kFull, hh[0], 16), __shfl_sync(kFull, hh[1], 16), __shfl_sync(kFull, hh[2], 16)};
   const int first = a.sorted_atom[32 * I];
   const int col = first >= 0 ? a.column[first] : 0;
   const int nx = a.n_col[0], ny = a.n_col[1];
@@ -584,46 +612,63 @@ __global__ void __launch_bounds__(32 * kCtaWarps) nl_lists_cta(NlistArgs a) {
     if (threadIdx.x == 0) report_status(a.status, kStatusTileOverflow);
     n_cand = cap;
   }
-  // phase B: one warp per candidate
+  // phase B: one warp per candidate; a particle is kept for a half of I when it lies within
+  // reach of that half's box (the conservative sphere around it near a periodic image)
   for (int c = w; c < n_cand; c += kCtaWarps) {
     const int J = c_J[c];
     const bool un = c_un[c] != 0;
     const int slot = 32 * J + lane;
     const int aj = a.sorted_atom[slot];
-    bool in = false;
+    bool in_a = false, in_b = false;
     if (aj >= 0) {
       const double4 wp = a.slot_wpos[slot];
       const double* cj = a.block_center + 3 * J;
-      double rel[3] = {wp.x - cj[0] + c_d[c], wp.y - cj[1] + c_d[cap + c], wp.z - cj[2] + c_d[2 * cap + c]};
-      if (un) {
-        min_image_fast(rel[0], rel[1], rel[2], bx);
-        const double r = sqrt(rel[0] * rel[0] + rel[1] * rel[1] + rel[2] * rel[2]);
-        in = r < reach + ri + 1e-6;
-      } else {
-        in = box_gap2(rel, hi, nullptr) < reach2;
-      }
+      const double rel[3] = {wp.x - cj[0] + c_d[c], wp.y - cj[1] + c_d[cap + c],
+                             wp.z - cj[2] + c_d[2 * cap + c]};
+      auto near_half = [&](const double* hcen, const double* hext) {
+        if (hext[0] < 0.0) return false;
+        double rh[3] = {rel[0] - hcen[0], rel[1] - hcen[1], rel[2] - hcen[2]};
+        if (un) {
+          min_image_fast(rh[0], rh[1], rh[2], bx);
+          const double rad = sqrt(hext[0] * hext[0] + hext[1] * hext[1] + hext[2] * hext[2]);
+          return sqrt(rh[0] * rh[0] + rh[1] * rh[1] + rh[2] * rh[2]) < reach + rad + 1e-6;
+        }
+        return box_gap2(rh, hext, nullptr) < reach2;
+      };
+      in_a = near_half(hcA, hhA);
+      in_b = near_half(hcB, hhB);
     }
-    const unsigned m = __ballot_sync(kFull, in);
-    if (lane == 0) c_mask[c] = m;
+    const unsigned ma = __ballot_sync(kFull, in_a), mb = __ballot_sync(kFull, in_b);
+    if (lane == 0) {
+      c_mask[c] = ma;
+      c_mask[cap + c] = mb;
+    }
   }
   __syncthreads();
-  // phase C: prefix sum of the masks' populations (warp 0), then reserve I's tiles
-  if (w == 0) {
+  // phase C: prefix sums of the masks' populations per half (warps 0 and 1), then reserve
+  // I's tiles: the self tile and one tile per 16 entries of the longer half
+  if (w < 2) {
+    const uint32_t* mk = c_mask + (size_t)w * cap;
+    int* pre = c_pre + (size_t)w * (cap + 1);
     int carry = 0;
     for (int base = 0; base < n_cand; base += 32) {
       const int c = base + lane;
-      const int v = c < n_cand ? __popc(c_mask[c]) : 0;
+      const int v = c < n_cand ? __popc(mk[c]) : 0;
       int incl = v;
       for (int o = 1; o < 32; o <<= 1) {
         const int y = __shfl_up_sync(kFull, incl, o);
         if (lane >= o) incl += y;
       }
-      if (c < n_cand) c_pre[c] = carry + incl - v;
+      if (c < n_cand) pre[c] = carry + incl - v;
       carry += __shfl_sync(kFull, incl, 31);
     }
+    if (lane == 0) pre[n_cand] = carry;
+  }
+  __syncthreads();
+  if (w == 0) {
     if (lane == 0) {
-      c_pre[n_cand] = carry;
-      const int nt = 1 + (carry + 31) / 32;
+      const int tot_a = c_pre[n_cand], tot_b = c_pre[(cap + 1) + n_cand];
+      const int nt = 1 + (max(tot_a, tot_b) + 15) / 16;
       int t0 = atomicAdd(a.n_tiles, nt);
       if (t0 + nt > a.tile_capacity) {
         report_status(a.status, kStatusTileOverflow);
@@ -635,7 +680,10 @@ __global__ void __launch_bounds__(32 * kCtaWarps) nl_lists_cta(NlistArgs a) {
   }
   __syncthreads();
   if (s_tile0 < 0) return;
-  const int total = c_pre[n_cand];
+  const int half = lane >> 4;
+  const uint32_t* my_mask = c_mask + (size_t)half * cap;
+  const int* my_pre = c_pre + (size_t)half * (cap + 1);
+  const int total = my_pre[n_cand];
   const int ai = a.sorted_atom[32 * I + lane];
   const Partners partners = load_partners(a, ai);
   // phase D: whole tiles per warp; tile 0 is I's self tile
@@ -646,16 +694,16 @@ __global__ void __launch_bounds__(32 * kCtaWarps) nl_lists_cta(NlistArgs a) {
       slot = ai < 0 ? -1 : 32 * I + lane;
       flag = kTileSelf | ((a.min_width < reach + 2.0 * ri) ? kTilePairImage : 0);
     } else {
-      const int e = 32 * (k - 1) + lane;
+      const int e = 16 * (k - 1) + (lane & 15);  // this half's entry
       if (e < total) {
-        int lo = 0, hi_c = n_cand - 1;  // last candidate with c_pre <= e
+        int lo = 0, hi_c = n_cand - 1;  // last candidate with pre <= e
         while (lo < hi_c) {
           const int mid = (lo + hi_c + 1) >> 1;
-          if (c_pre[mid] <= e) lo = mid;
+          if (my_pre[mid] <= e) lo = mid;
           else hi_c = mid - 1;
         }
-        uint32_t mm = c_mask[lo];  // drop the e - c_pre[lo] lowest set bits
-        for (int r = e - c_pre[lo]; r > 0; --r) mm &= mm - 1u;
+        uint32_t mm = my_mask[lo];  // drop the e - pre[lo] lowest set bits
+        for (int r = e - my_pre[lo]; r > 0; --r) mm &= mm - 1u;
         const int bit = __ffs(mm) - 1;
         slot = 32 * c_J[lo] + bit;
         flag = c_un[lo] ? kTilePairImage : 0;
@@ -663,7 +711,7 @@ __global__ void __launch_bounds__(32 * kCtaWarps) nl_lists_cta(NlistArgs a) {
         sh[1] = c_d[cap + lo];
         sh[2] = c_d[2 * cap + lo];
       }
-      flag = __reduce_or_sync(kFull, flag);
+      flag = __reduce_or_sync(kFull, flag) | kTileHalves;
     }
     s_slots[w][lane] = slot;
     __syncwarp();
@@ -729,7 +777,7 @@ void launch_nlist_rebuild(const NlistArgs& a, bool double_entries, cudaStream_t 
   nl_bounds<<<ceil_div((long long)block_cap * 32, tb), tb, 0, s>>>(a);
   const bool rectangular = a.periodic && a.box.bx == 0.0 && a.box.cx == 0.0 && a.box.cy == 0.0;
   if (rectangular && a.max_cand > 0) {
-    const size_t bytes = (size_t)a.max_cand * (3 * 8 + 4 + 4 + 4 + 4) + 4;
+    const size_t bytes = (size_t)a.max_cand * (3 * 8 + 4 + 4 + 2 * 4 + 2 * 4) + 8;
     if (double_entries) {
       cudaFuncSetAttribute(nl_lists_cta<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
       nl_lists_cta<true><<<block_cap, 32 * kCtaWarps, bytes, s>>>(a);

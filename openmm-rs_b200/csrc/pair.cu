@@ -7,7 +7,9 @@
 // (i, j) pair is seen once in 32 steps with conflict-free shared-memory reads.  The force on
 // each j-entry travels with the entry: it is rotated one lane per step by a warp shuffle and
 // is back in lane j after 32 steps.  Self tiles (entries = block I) visit each pair from both
-// sides and keep only i-forces, at half energy.  Forces are summed in `Real` within a tile and
+// sides and keep only i-forces, at half energy.  "Halves" tiles hold 16 entries for each half
+// of block I (gathered against that half's smaller box): each half-warp rotates its own 16
+// entries in 16 steps.  Forces are summed in `Real` within a tile and
 // committed as 64-bit fixed point, so the total does not depend on tile order.
 //
 // Pair membership reproduces the reference exactly: pairs whose squared distance falls
@@ -44,6 +46,7 @@ __global__ void __launch_bounds__(32 * kPairWarps) pair_kernel(const PairArgs<Re
     const int I = tile.x;
     const bool self = (tile.y & kTileSelf) != 0;
     const bool pair_image = (tile.y & kTilePairImage) != 0;
+    const bool halves = (tile.y & kTileHalves) != 0;
     const int si = 32 * I + lane;
     const T4 pi = posq[si];
     const T2 li = ljp[si];
@@ -80,9 +83,15 @@ __global__ void __launch_bounds__(32 * kPairWarps) pair_kernel(const PairArgs<Re
     Real fix = 0, fiy = 0, fiz = 0, fjx = 0, fjy = 0, fjz = 0;
     double e_tile = 0.0;
     double w_tile[6] = {0, 0, 0, 0, 0, 0};
+    // halves tiles: lanes 0-15 (first half of block I) meet entries 0-15 in 16 steps, lanes
+    // 16-31 entries 16-31; otherwise every lane meets all 32 entries.  j-forces travel one
+    // lane per step within their group and are back at their entry's lane at the end.
+    const int hb = halves ? (lane & 16) : 0, kmask = halves ? 15 : 31;
+    const int nsteps = halves ? 16 : 32;
+    const int src = hb | ((lane + 1) & kmask);
 #pragma unroll 4
-    for (int k = self ? 1 : 0; k < 32; ++k) {
-      const int jl = (lane + k) & 31;
+    for (int k = self ? 1 : 0; k < nsteps; ++k) {
+      const int jl = hb | ((lane + k) & kmask);
       const T4 pj = s_pos[w][jl];
       const T2 lj = s_lj[w][jl];
       Real dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
@@ -129,7 +138,6 @@ __global__ void __launch_bounds__(32 * kPairWarps) pair_kernel(const PairArgs<Re
         fjx = fma(-fo, dx, fjx);
         fjy = fma(-fo, dy, fjy);
         fjz = fma(-fo, dz, fjz);
-        const int src = (lane + 1) & 31;
         fjx = __shfl_sync(FULL, fjx, src);
         fjy = __shfl_sync(FULL, fjy, src);
         fjz = __shfl_sync(FULL, fjz, src);
