@@ -484,7 +484,7 @@ __global__ void __launch_bounds__(32 * kListWarps) nl_lists(NlistArgs a) {
 constexpr int kCtaWarps = 8;
 
 template <bool kDouble>
-__global__ void __launch_bounds__(32 * kCtaWarps) nl_lists_cta(NlistArgs a) {
+__global__ void __launch_bounds__(32 * kCtaWarps, 4) nl_lists_cta(NlistArgs a) {
   if (*a.rebuild == 0) return;
   extern __shared__ __align__(16) unsigned char smem[];
   const int cap = a.max_cand;
@@ -614,14 +614,25 @@ __global__ void __launch_bounds__(32 * kCtaWarps) nl_lists_cta(NlistArgs a) {
   }
   // phase B: one warp per candidate; a particle is kept for a half of I when it lies within
   // reach of that half's box (the conservative sphere around it near a periodic image)
+  int aj_n = -1;
+  double4 wp_n = make_double4(0.0, 0.0, 0.0, 0.0);
+  if (w < n_cand) {  // this warp's first candidate, fetched ahead
+    const int slot = 32 * c_J[w] + lane;
+    aj_n = a.sorted_atom[slot];
+    wp_n = a.slot_wpos[slot];
+  }
   for (int c = w; c < n_cand; c += kCtaWarps) {
     const int J = c_J[c];
     const bool un = c_un[c] != 0;
-    const int slot = 32 * J + lane;
-    const int aj = a.sorted_atom[slot];
+    const int aj = aj_n;
+    const double4 wp = wp_n;
+    if (c + kCtaWarps < n_cand) {  // the next candidate's particles, in flight meanwhile
+      const int slot = 32 * c_J[c + kCtaWarps] + lane;
+      aj_n = a.sorted_atom[slot];
+      wp_n = a.slot_wpos[slot];
+    }
     bool in_a = false, in_b = false;
     if (aj >= 0) {
-      const double4 wp = a.slot_wpos[slot];
       const double* cj = a.block_center + 3 * J;
       const double rel[3] = {wp.x - cj[0] + c_d[c], wp.y - cj[1] + c_d[cap + c],
                              wp.z - cj[2] + c_d[2 * cap + c]};
