@@ -182,7 +182,7 @@ def equilibrate(seed, device, steps=None):
     if seed not in _EQUILIBRATED:
         w = synth.water_preset(WORKLOAD)
         ctx = ommb200.Context(systems.water_system(w), systems.langevin(friction=20.0, seed=seed),
-                              precision="mixed", device=device)
+                              precision="mixed", device=device, use_cuda_graph=USE_GRAPH)
         ctx.set_positions(w.positions)
         ctx.set_velocities_to_temperature(300.0, seed=seed)
         if steps:
@@ -347,6 +347,25 @@ def cpu_one_core(w, x0):
             "sample": f"one f64 PME force evaluation in {sec:.2f} s"}
 
 
+def profiled_traffic(name, tiles_now):
+    """DRAM bytes per launch of a kernel from the committed ncu summary `profiles/<name>.md`
+    (lines `traffic_bytes_per_launch: B` and `tiles_at_capture: T`), scaled to the current
+    launch by its tile count (the traffic is the tile entries and the particles they name)."""
+    try:
+        text = (ROOT / "profiles" / f"{name}.md").read_text()
+    except OSError:
+        return None
+    vals = {}
+    for key in ("traffic_bytes_per_launch", "tiles_at_capture"):
+        for line in text.splitlines():
+            if line.strip("`").startswith(key + ":"):
+                vals[key] = float(line.strip("`").split(":")[1])
+    if "traffic_bytes_per_launch" not in vals:
+        return None
+    scale = tiles_now / vals["tiles_at_capture"] if vals.get("tiles_at_capture") else 1.0
+    return vals["traffic_bytes_per_launch"] * scale
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -451,6 +470,7 @@ def main():
     ms, e2e_ms = max_over_ranks([ms, e2e_ms], world, f"cuda:{local}")
     md_steps = args.steps * args.segment
     value = world * ns_per_day(md_steps, ms / 1000.0)
+    tiles_timed = ctx.nlist_stats()["tiles"]
     e2e_value = world * ns_per_day(md_steps, e2e_ms / 1000.0)
 
     extras = {}
@@ -473,7 +493,8 @@ def main():
                                    "FP32 figure",
                     "algorithmic": f"{pairs} in-cutoff pairs x {FLOPS_PER_PAIR} flops per launch",
                     "avg_launch_ms": 1000.0 * t_pair,
-                    "traffic": None}
+                    "traffic": None, "traffic_source": "profiles/pair_kernel_water-23958.md "
+                                                      "(one ncu capture, scaled by tiles)"}
         peaks = measured_peaks()
         hbm = peaks.get("hbm_gbs")
         integ_ms, integ_n = times.get("integrate", (0.0, 1))
@@ -491,6 +512,7 @@ def main():
         launches = md_steps * per_md + 9 * rebuilds_timed + args.steps * (args.segment // 20)
         extras["pairs_in_cutoff"] = pairs
         nl = ctx.nlist_stats()
+        roofline["traffic"] = profiled_traffic(f"pair_kernel_{WORKLOAD}", nl["tiles"])
         # self tiles are 32 x 32 pair slots, neighbour tiles 2 x 16 x 16 (halves of block I)
         slots = nl["blocks"] * 1024 + (nl["tiles"] - nl["blocks"]) * 512
         nl["pair_efficiency"] = pairs / max(1, slots)
@@ -529,7 +551,7 @@ def main():
                    "l2": "flushed (256 MiB write) between timed bench steps; MD steps inside a "
                          "bench step run back to back",
                    "parallelism": f"replicas x{world}",
-                   "autotuned": TUNED.get(args.precision)},
+                   "autotuned": TUNED.get(args.precision), "tiles": tiles_timed},
         "e2e": {"value": e2e_value, "unit": "ns/day", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
