@@ -199,7 +199,13 @@ Engine::Engine(std::unique_ptr<SystemDef> system, std::unique_ptr<IntegratorDef>
   OMMB200_CK(cudaSetDevice(opt_.device));
   OMMB200_CK(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, opt_.device));
   OMMB200_CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
-  OMMB200_CK(cudaStreamCreateWithFlags(&pme_stream_, cudaStreamNonBlocking));
+  {
+    // the reciprocal-space chain (spread, transform, gather) is a sequence of small kernels that
+    // runs beside the pair kernel: its CTAs go ahead of queued pair CTAs
+    int lowest = 0, greatest = 0;
+    OMMB200_CK(cudaDeviceGetStreamPriorityRange(&lowest, &greatest));
+    OMMB200_CK(cudaStreamCreateWithPriority(&pme_stream_, cudaStreamNonBlocking, greatest));
+  }
   OMMB200_CK(cudaStreamCreateWithFlags(&aux_stream_, cudaStreamNonBlocking));
   OMMB200_CK(cudaEventCreateWithFlags(&fork_ev_, cudaEventDisableTiming));
   OMMB200_CK(cudaEventCreateWithFlags(&join_ev_, cudaEventDisableTiming));
@@ -435,11 +441,74 @@ void Engine::setup_nonbonded(const NonbondedDef& nb) {
     pme_k_ = mem_.alloc_bytes(2 * rs * gk);
     influence_ = mem_.alloc_bytes(rs * gk);
     moduli_ = mem_.alloc<double>(grid_[0] + grid_[1] + grid_[2]);
-    OMMB200_CKFFT(cufftPlan3d(&fft_fwd_, grid_[0], grid_[1], grid_[2], dp_ ? CUFFT_D2Z : CUFFT_R2C));
-    OMMB200_CKFFT(cufftPlan3d(&fft_inv_, grid_[0], grid_[1], grid_[2], dp_ ? CUFFT_Z2D : CUFFT_C2R));
-    fft_ready_ = true;
-    OMMB200_CKFFT(cufftSetStream(fft_fwd_, stream_));
-    OMMB200_CKFFT(cufftSetStream(fft_inv_, stream_));
+    // own transform while every axis factors into radices 2, 3, 4, 5, 7, 8 and the
+    // plane kernels' buffers fit in shared memory; cuFFT otherwise
+    own_fft_ = true;
+    for (int d = 0; d < 3; ++d) {
+      int m = grid_[d], k = 0;
+      for (int r : {8, 4, 2, 3, 5, 7})
+        while (m % r == 0 && k < 16) {
+          fft_.rad[d][k++] = r;
+          m /= r;
+        }
+      fft_.nrad[d] = k;
+      if (m != 1) own_fft_ = false;
+    }
+    if (own_fft_) {
+      fft_.pencils_x = 8;
+      const int ny = grid_[1], nz = grid_[2], nzh = nz / 2 + 1, nyp = (ny + 1) / 2;
+      auto items = [&](int d, int pencils) {  // most butterflies of one stage of axis d
+        int most = 0;
+        for (int k = 0; k < fft_.nrad[d]; ++k) most = std::max(most, pencils * grid_[d] / fft_.rad[d][k]);
+        return most;
+      };
+      auto block = [](int want, int lo, int hi) { return std::min(hi, std::max(lo, (want + 31) / 32 * 32)); };
+      // plane kernels: a third of a plane's elements per thread pass (copies), at least one
+      // butterfly per thread in every stage; x pass: at least the butterflies of a stage
+      fft_.threads[0] = fft_.threads[2] =
+          block(std::max(std::max(items(2, nyp), items(1, nzh)), nzh * ny / 3), 128, 512);
+      fft_.threads[1] = block(std::max(items(0, fft_.pencils_x), fft_.pencils_x * grid_[0] / 4), 64, 256);
+      PmeArgs<float> pf{};
+      PmeArgs<double> pd{};
+      pf.nx = pd.nx = grid_[0];
+      pf.ny = pd.ny = grid_[1];
+      pf.nz = pd.nz = grid_[2];
+      const size_t need = dp_ ? std::max(pme_transform_smem(pd, fft_, 0), pme_transform_smem(pd, fft_, 1))
+                              : std::max(pme_transform_smem(pf, fft_, 0), pme_transform_smem(pf, fft_, 1));
+      own_fft_ = need <= 200 * 1024;
+      if (own_fft_) {
+        if (dp_)
+          prepare_pme_transform(pd, fft_);
+        else
+          prepare_pme_transform(pf, fft_);
+        OMMB200_CK(cudaGetLastError());
+      }
+    }
+    if (own_fft_) {
+      for (int d = 0; d < 3; ++d) {
+        const int n = grid_[d];
+        std::vector<double> tw(2 * (size_t)n);
+        for (int m = 0; m < n; ++m) {
+          const double ang = 2.0 * kPiD * (double)m / (double)n;
+          tw[2 * m] = std::cos(ang);
+          tw[2 * m + 1] = -std::sin(ang);
+        }
+        void* dtw = mem_.alloc_bytes((dp_ ? 16 : 8) * (size_t)n);
+        if (dp_) {
+          OMMB200_CK(cudaMemcpy(dtw, tw.data(), 16 * (size_t)n, cudaMemcpyHostToDevice));
+        } else {
+          std::vector<float> f(tw.begin(), tw.end());
+          OMMB200_CK(cudaMemcpy(dtw, f.data(), 8 * (size_t)n, cudaMemcpyHostToDevice));
+        }
+        fft_.tw[d] = dtw;
+      }
+    } else {
+      OMMB200_CKFFT(cufftPlan3d(&fft_fwd_, grid_[0], grid_[1], grid_[2], dp_ ? CUFFT_D2Z : CUFFT_R2C));
+      OMMB200_CKFFT(cufftPlan3d(&fft_inv_, grid_[0], grid_[1], grid_[2], dp_ ? CUFFT_Z2D : CUFFT_C2R));
+      fft_ready_ = true;
+      OMMB200_CKFFT(cufftSetStream(fft_fwd_, stream_));
+      OMMB200_CKFFT(cufftSetStream(fft_inv_, stream_));
+    }
     std::vector<double> mod;
     for (int d = 0; d < 3; ++d) {
       auto m = bspline_moduli(grid_[d]);
@@ -1249,6 +1318,11 @@ void Engine::enqueue_nonbonded(bool energy, bool direct, bool reciprocal, bool d
     prof_begin("pme_spread");
     launch_pme_spread<Real>(m, ps);
     prof_end();
+    if (own_fft_) {
+      prof_begin("pme_transform");
+      launch_pme_transform<Real>(m, fft_, energy, ps);
+      prof_end();
+    } else {
     prof_begin("pme_convert");
     launch_pme_convert<Real>(m, ps);
     prof_end();
@@ -1269,6 +1343,7 @@ void Engine::enqueue_nonbonded(bool energy, bool direct, bool reciprocal, bool d
     else
       OMMB200_CKFFT(cufftExecC2R(fft_inv_, (cufftComplex*)pme_k_, (cufftReal*)pme_real_));
     prof_end();
+    }
     prof_begin("pme_gather");
     launch_pme_gather<Real>(m, ps);
     prof_end();
@@ -1413,7 +1488,7 @@ void Engine::run_graph_steps(int launches) {
     }
     capturing_ = false;
     OMMB200_CK(cudaStreamEndCapture(stream_, &graph_));
-    OMMB200_CK(cudaGraphInstantiate(&graph_exec_, graph_, 0));
+    OMMB200_CK(cudaGraphInstantiate(&graph_exec_, graph_, cudaGraphInstantiateFlagUseNodePriority));
   }
   for (int i = 0; i < launches; ++i) OMMB200_CK(cudaGraphLaunch(graph_exec_, stream_));
 }

@@ -186,6 +186,8 @@ class Engine {
   double* moduli_ = nullptr;
   cufftHandle fft_fwd_ = 0, fft_inv_ = 0;
   bool fft_ready_ = false;
+  bool own_fft_ = false;  // the engine's pencil transform instead of cuFFT
+  PmeFft fft_{};
   int n_exceptions_ = 0;
   int2* exc_pairs_ = nullptr;
   double4* exc_params_ = nullptr;

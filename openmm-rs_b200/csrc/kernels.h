@@ -137,6 +137,24 @@ struct PmeArgs {
 
 template <class Real>
 void launch_pme_spread(const PmeArgs<Real>& a, cudaStream_t s);
+// Own transform of the grid (replaces convert, the cuFFT pair and convolve): per axis the
+// split n = n1 n2 and the twiddle table W_n^m = exp(-2 pi i m / n) (float2 or double2).
+// Plan of the engine's own grid transform: per axis the radices of the Stockham stages and
+// the twiddle table W_n^m = exp(-2 pi i m / n), m < n (Real2 elements); block sizes of the
+// forward-plane, x-pass and inverse-plane kernels; kz pencils per x-pass CTA.
+struct PmeFft {
+  int nrad[3];
+  int rad[3][16];
+  int threads[3];
+  int pencils_x;
+  const void* tw[3];
+};
+template <class Real>
+size_t pme_transform_smem(const PmeArgs<Real>& a, const PmeFft& f, int kernel);
+template <class Real>
+void prepare_pme_transform(const PmeArgs<Real>& a, const PmeFft& f);
+template <class Real>
+void launch_pme_transform(const PmeArgs<Real>& a, const PmeFft& f, bool energy, cudaStream_t s);
 template <class Real>
 void launch_pme_convert(const PmeArgs<Real>& a, cudaStream_t s);
 template <class Real>

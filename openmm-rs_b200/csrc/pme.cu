@@ -340,7 +340,419 @@ __global__ void gather_kernel(const PmeArgs<Real> a) {
   }
 }
 
+// ---- own 3-D transform of the PME grid -------------------------------------------------
+// Replaces the fixed-point conversion, the real-to-complex / complex-to-real cuFFT pair and
+// the convolution by three kernels over the half spectrum [x][y][kz <= nz/2]:
+//   planes_forward  one CTA per x plane: fixed-point grid -> real (grid zeroed), z transform
+//                   of two real rows at once as one complex row, y transform
+//   x_convolve      one CTA per (y, run of kz): x transform, influence function (+ energy
+//                   and virial), inverse x transform
+//   planes_inverse  one CTA per x plane: inverse y transform, inverse z transform of two
+//                   Hermitian rows at once, real rows -> potential grid for the gather
+// Every 1-D transform is a mixed-radix Stockham FFT in shared memory (radices 2, 3, 4, 5, 7,
+// 8; one radix-R butterfly per thread and stage), forward sign exp(-2 pi i jk/n) and
+// unnormalised like cuFFT; the inverse is conj(F(conj(x))).  Sizes with other prime factors
+// use cuFFT.
+template <class C2>
+__device__ __forceinline__ C2 cmul(C2 a, C2 w) {
+  C2 r;
+  r.x = a.x * w.x - a.y * w.y;
+  r.y = a.x * w.y + a.y * w.x;
+  return r;
+}
+template <class C2>
+__device__ __forceinline__ C2 conjg(C2 a) {
+  a.y = -a.y;
+  return a;
+}
+template <class C2>
+__device__ __forceinline__ void bfly2(C2& a, C2& b) {
+  const C2 t = a;
+  a.x = t.x + b.x;
+  a.y = t.y + b.y;
+  b.x = t.x - b.x;
+  b.y = t.y - b.y;
+}
+// multiplication by -i
+template <class C2>
+__device__ __forceinline__ C2 mul_mi(C2 a) {
+  C2 r;
+  r.x = a.y;
+  r.y = -a.x;
+  return r;
+}
+template <class C2>
+__device__ __forceinline__ void dft4(C2& a0, C2& a1, C2& a2, C2& a3) {
+  bfly2(a0, a2);  // a0 = x0 + x2, a2 = x0 - x2
+  bfly2(a1, a3);  // a1 = x1 + x3, a3 = x1 - x3
+  a3 = mul_mi(a3);
+  bfly2(a0, a1);  // y0, y2
+  bfly2(a2, a3);  // y1, y3
+  const C2 y1 = a2, y2 = a1;
+  a1 = y1;
+  a2 = y2;
+}
+
+// Forward DFT of R values in registers.  Radices 2, 4, 8 use butterflies; the odd primes use
+// the direct sum with W_R^q = tw[q n / R] from the length-n twiddle table.
+template <int R, class C2>
+__device__ __forceinline__ void dft_reg(C2 (&v)[R], const C2* tw, int n) {
+  using S = decltype(v[0].x);
+  if constexpr (R == 2) {
+    bfly2(v[0], v[1]);
+  } else if constexpr (R == 4) {
+    dft4(v[0], v[1], v[2], v[3]);
+  } else if constexpr (R == 8) {
+    dft4(v[0], v[2], v[4], v[6]);
+    dft4(v[1], v[3], v[5], v[7]);
+    const S h = (S)0.70710678118654752440;  // 1/sqrt(2)
+    C2 o1, o2, o3;
+    o1.x = h * (v[3].x + v[3].y);  // W_8 = (1 - i)/sqrt(2)
+    o1.y = h * (v[3].y - v[3].x);
+    o2 = mul_mi(v[5]);              // W_8^2 = -i
+    o3.x = h * (v[7].y - v[7].x);  // W_8^3 = -(1 + i)/sqrt(2)
+    o3.y = -h * (v[7].x + v[7].y);
+    C2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6], d0 = v[1];
+    bfly2(e0, d0);
+    bfly2(e1, o1);
+    bfly2(e2, o2);
+    bfly2(e3, o3);
+    v[0] = e0; v[4] = d0;
+    v[1] = e1; v[5] = o1;
+    v[2] = e2; v[6] = o2;
+    v[3] = e3; v[7] = o3;
+  } else {
+    const int st = n / R;
+    C2 out[R];
+#pragma unroll
+    for (int s = 0; s < R; ++s) {
+      C2 acc = v[0];
+#pragma unroll
+      for (int q = 1; q < R; ++q) {
+        const C2 w = tw[((q * s) % R) * st];
+        acc.x += v[q].x * w.x - v[q].y * w.y;
+        acc.y += v[q].x * w.y + v[q].y * w.x;
+      }
+      out[s] = acc;
+    }
+#pragma unroll
+    for (int s = 0; s < R; ++s) v[s] = out[s];
+  }
+}
+
+// One Stockham stage over P pencils of length n (pencil p at in + p n): butterfly j of a
+// pencil reads in[j + r n/R], applies the twiddles W_n^(r k n/(ns R)) of its position
+// k = j mod ns in the current sub-transforms of length ns, and writes out[(j/ns) ns R + k + r ns].
+// Not inlined: every transform of a kernel shares one copy of each radix's code, which keeps
+// the instruction footprint of a CTA (one CTA per SM, every stage a new code path) small.
+template <int R, class C2>
+__device__ __noinline__ void stockham_stage(const C2* in, C2* out, const C2* tw, int n, int ns, int P) {
+  const int nr = n / R, items = P * nr, span = n / (ns * R);
+  for (int t = threadIdx.x; t < items; t += blockDim.x) {
+    const int p = t / nr, j = t - p * nr, q = j / ns, k = j - q * ns;
+    const C2* src = in + p * n + j;
+    C2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = src[r * nr];
+    if (ns > 1) {
+      const int step = k * span;
+#pragma unroll
+      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], tw[r * step]);
+    }
+    dft_reg<R>(v, tw, n);
+    C2* dst = out + p * n + q * ns * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) dst[r * ns] = v[r];
+  }
+}
+
+// Forward transform of P pencils held in a (b: scratch of the same size); returns the buffer
+// that holds the result.  The callers synchronise before and after.
+template <class C2>
+__device__ C2* stockham(C2* a, C2* b, const C2* tw, const PmeFft& f, int axis, int n, int P) {
+  int ns = 1;
+  for (int s = 0; s < f.nrad[axis]; ++s) {
+    const int R = f.rad[axis][s];
+    switch (R) {
+      case 2: stockham_stage<2>(a, b, tw, n, ns, P); break;
+      case 3: stockham_stage<3>(a, b, tw, n, ns, P); break;
+      case 4: stockham_stage<4>(a, b, tw, n, ns, P); break;
+      case 5: stockham_stage<5>(a, b, tw, n, ns, P); break;
+      case 7: stockham_stage<7>(a, b, tw, n, ns, P); break;
+      default: stockham_stage<8>(a, b, tw, n, ns, P); break;
+    }
+    __syncthreads();
+    C2* t = a;
+    a = b;
+    b = t;
+    ns *= R;
+  }
+  return a;
+}
+
+template <class C2>
+__device__ __forceinline__ void load_twiddles(C2* dst, const void* src, int n) {
+  const C2* t = reinterpret_cast<const C2*>(src);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = t[i];
+}
+
+// Reciprocal-space energy and virial of half-spectrum element (x, y, z) with |S|^2 = s2 and
+// influence value infl (pme.rs:307-372): the element and its conjugate partner each carry
+// half of the virial, elements with 0 < z < nz/2 count twice.
+template <class Real>
+__device__ __forceinline__ void mode_energy(const PmeArgs<Real>& a, int x, int y, int z, double s2,
+                                            double infl, double& e, double (&w)[6]) {
+  const double wz = (z == 0 || (a.nz % 2 == 0 && z == a.nz / 2)) ? 1.0 : 2.0;
+  e += wz * 0.5 * infl * s2;
+  const int idx[2][3] = {{x, y, z}, {(a.nx - x) % a.nx, (a.ny - y) % a.ny, (a.nz - z) % a.nz}};
+  for (int p = 0; p < 2; ++p) {
+    const double m[3] = {freq(idx[p][0], a.nx), freq(idx[p][1], a.ny), freq(idx[p][2], a.nz)};
+    double k[3];
+    for (int c = 0; c < 3; ++c) k[c] = m[0] * a.recip[0][c] + m[1] * a.recip[1][c] + m[2] * a.recip[2][c];
+    const double k2 = k[0] * k[0] + k[1] * k[1] + k[2] * k[2];
+    const double bm = a.moduli[idx[p][0]] * a.moduli[a.nx + idx[p][1]] * a.moduli[a.nx + a.ny + idx[p][2]];
+    const double pa = kPiD * kPiD / (a.alpha * a.alpha);
+    const double g_m = kOne4PiEps0 * exp(-pa * k2) / (kPiD * a.volume * k2 * bm);
+    const double em = wz * 0.5 * 0.5 * g_m * s2;
+    const double c = 2.0 * (1.0 + pa * k2) / k2;
+    w[0] += em * (1.0 - c * k[0] * k[0]);
+    w[1] += em * (1.0 - c * k[1] * k[1]);
+    w[2] += em * (1.0 - c * k[2] * k[2]);
+    w[3] -= em * c * k[0] * k[1];
+    w[4] -= em * c * k[0] * k[2];
+    w[5] -= em * c * k[1] * k[2];
+  }
+}
+
+// Warp sums of the energy and virial in fixed point, one atomic per warp and term (every
+// thread of the block calls it).
+template <class Real>
+__device__ __forceinline__ void commit_energy(const PmeArgs<Real>& a, double e, const double (&w)[6]) {
+  long long ef = to_fixed(e, kEnergyScale);
+  long long wf[6];
+  for (int c = 0; c < 6; ++c) wf[c] = to_fixed(w[c], kEnergyScale);
+  for (int off = 16; off > 0; off >>= 1) {
+    ef += __shfl_xor_sync(0xffffffffu, ef, off);
+    for (int c = 0; c < 6; ++c) wf[c] += __shfl_xor_sync(0xffffffffu, wf[c], off);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    add_fixed(a.energy, ef);
+    for (int c = 0; c < 6; ++c) add_fixed(a.energy + 1 + c, wf[c]);
+  }
+}
+
+// Shared memory of a plane kernel: z and y twiddles, two buffers of `plane` elements.
+__host__ __device__ inline int fft_plane_elems(int ny, int nz) {
+  const int a = (ny + 1) / 2 * nz, b = (nz / 2 + 1) * ny;
+  return a > b ? a : b;
+}
+
+constexpr int kPlaneThreads = 512, kXPassThreads = 256;  // block size caps of the transform
+constexpr int kLoadBatch = 4;  // global loads each thread keeps in flight in the copy loops
+
+// for i in [0, total), strided over the block: v = load(i) for kLoadBatch items at a time,
+// then use(i, v) for each, so that the loads of a batch overlap.
+template <class T, class Load, class Use>
+__device__ __forceinline__ void batched(int total, Load load, Use use) {
+  for (int i0 = threadIdx.x; i0 < total; i0 += kLoadBatch * blockDim.x) {
+    T v[kLoadBatch];
+#pragma unroll
+    for (int u = 0; u < kLoadBatch; ++u) {
+      const int i = i0 + u * blockDim.x;
+      if (i < total) v[u] = load(i);
+    }
+#pragma unroll
+    for (int u = 0; u < kLoadBatch; ++u) {
+      const int i = i0 + u * blockDim.x;
+      if (i < total) use(i, v[u]);
+    }
+  }
+}
+
+template <class Real>
+__global__ void __launch_bounds__(kPlaneThreads) planes_forward(const PmeArgs<Real> a, const PmeFft f) {
+  using C2 = typename Cplx<Real>::T;
+  extern __shared__ __align__(16) unsigned char fsm[];
+  const int ny = a.ny, nz = a.nz, nzh = nz / 2 + 1, nyp = (ny + 1) / 2, x = blockIdx.x;
+  const int pe = fft_plane_elems(ny, nz);
+  C2* twz = reinterpret_cast<C2*>(fsm);
+  C2* twy = twz + nz;
+  C2* A = twy + ny;
+  C2* B = A + pe;
+  load_twiddles(twz, f.tw[2], nz);
+  load_twiddles(twy, f.tw[1], ny);
+  // rows y = 2 yp (real part) and 2 yp + 1 (imaginary part) as one complex row
+  long long* plane = a.grid_fixed + (long long)x * ny * nz;
+  batched<longlong2>(
+      nyp * nz,
+      [&](int i) {
+        const int yp = i / nz, z = i - yp * nz;
+        const long long* g0 = plane + (long long)(2 * yp) * nz + z;
+        longlong2 r;
+        r.x = __ldcg(g0);
+        r.y = 2 * yp + 1 < ny ? __ldcg(g0 + nz) : 0;
+        return r;
+      },
+      [&](int i, longlong2 r) {
+        C2 v;
+        v.x = (Real)((double)r.x * kGridScaleInv);
+        v.y = (Real)((double)r.y * kGridScaleInv);
+        A[i] = v;
+      });
+  __syncthreads();
+  for (int i = threadIdx.x; i < ny * nz; i += blockDim.x) plane[i] = 0;  // ready for the next spread
+  C2* r = stockham(A, B, twz, f, 2, nz, nyp);
+  C2* o = r == A ? B : A;
+  // split the two real rows' spectra: X_even = (Z_k + conj Z_-k)/2, X_odd = -i (Z_k - conj Z_-k)/2,
+  // into pencils along y: o[kz][y]
+  for (int i = threadIdx.x; i < nzh * ny; i += blockDim.x) {
+    const int kz = i / ny, y = i - kz * ny, yp = y >> 1;
+    const C2 zk = r[yp * nz + kz], zm = r[yp * nz + (kz == 0 ? 0 : nz - kz)];
+    C2 v;
+    if ((y & 1) == 0) {
+      v.x = (Real)0.5 * (zk.x + zm.x);
+      v.y = (Real)0.5 * (zk.y - zm.y);
+    } else {
+      v.x = (Real)0.5 * (zk.y + zm.y);
+      v.y = (Real)0.5 * (zm.x - zk.x);
+    }
+    o[i] = v;
+  }
+  __syncthreads();
+  C2* s = stockham(o, r, twy, f, 1, ny, nzh);
+  C2* out = reinterpret_cast<C2*>(a.grid_k) + (long long)x * ny * nzh;
+  for (int i = threadIdx.x; i < ny * nzh; i += blockDim.x) {
+    const int y = i / nzh, kz = i - y * nzh;
+    out[i] = s[kz * ny + y];
+  }
+}
+
+template <class Real, bool kEnergy>
+__global__ void __launch_bounds__(kXPassThreads) x_convolve(const PmeArgs<Real> a, const PmeFft f) {
+  using C2 = typename Cplx<Real>::T;
+  extern __shared__ __align__(16) unsigned char fsm[];
+  const int nx = a.nx, nzh = a.nz / 2 + 1, P0 = f.pencils_x;
+  const int nkb = (nzh + P0 - 1) / P0;
+  const int y = blockIdx.x / nkb, kz0 = (blockIdx.x - y * nkb) * P0, P = min(P0, nzh - kz0);
+  C2* tw = reinterpret_cast<C2*>(fsm);
+  C2* A = tw + nx;
+  C2* B = A + P0 * nx;
+  load_twiddles(tw, f.tw[0], nx);
+  C2* g = reinterpret_cast<C2*>(a.grid_k);
+  const long long sx = (long long)a.ny * nzh, base = (long long)y * nzh + kz0;
+  batched<C2>(
+      nx * P, [&](int i) { const int x = i / P, p = i - x * P; return __ldcg(g + base + x * sx + p); },
+      [&](int i, C2 v) { const int x = i / P, p = i - x * P; A[p * nx + x] = v; });
+  __syncthreads();
+  C2* r = stockham(A, B, tw, f, 0, nx, P);
+  C2* o = r == A ? B : A;
+  double e = 0.0, w[6] = {0, 0, 0, 0, 0, 0};
+  batched<Real>(
+      P * nx, [&](int i) { const int p = i / nx, x = i - p * nx; return __ldg(a.influence + base + x * sx + p); },
+      [&](int i, Real infl) {
+        const int p = i / nx, x = i - p * nx;
+        C2 v = r[i];
+        if (kEnergy && base + x * sx + p != 0)
+          mode_energy(a, x, y, kz0 + p, (double)v.x * v.x + (double)v.y * v.y, (double)infl, e, w);
+        v.x *= infl;
+        v.y *= -infl;  // conjugated for the inverse transform
+        r[i] = v;
+      });
+  if (kEnergy) commit_energy(a, e, w);
+  __syncthreads();
+  C2* s = stockham(r, o, tw, f, 0, nx, P);
+  for (int i = threadIdx.x; i < nx * P; i += blockDim.x) {
+    const int x = i / P, p = i - x * P;
+    g[base + x * sx + p] = conjg(s[p * nx + x]);
+  }
+}
+
+template <class Real>
+__global__ void __launch_bounds__(kPlaneThreads) planes_inverse(const PmeArgs<Real> a, const PmeFft f) {
+  using C2 = typename Cplx<Real>::T;
+  extern __shared__ __align__(16) unsigned char fsm[];
+  const int ny = a.ny, nz = a.nz, nzh = nz / 2 + 1, nyp = (ny + 1) / 2, x = blockIdx.x;
+  const int pe = fft_plane_elems(ny, nz);
+  C2* twz = reinterpret_cast<C2*>(fsm);
+  C2* twy = twz + nz;
+  C2* A = twy + ny;
+  C2* B = A + pe;
+  load_twiddles(twz, f.tw[2], nz);
+  load_twiddles(twy, f.tw[1], ny);
+  const C2* in = reinterpret_cast<const C2*>(a.grid_k) + (long long)x * ny * nzh;
+  batched<C2>(
+      ny * nzh, [&](int i) { return __ldcg(in + i); },
+      [&](int i, C2 v) { const int y = i / nzh, kz = i - y * nzh; A[kz * ny + y] = conjg(v); });
+  __syncthreads();
+  // r = F(conj H): the inverse y transform of H is conj(r)
+  C2* r = stockham(A, B, twy, f, 1, ny, nzh);
+  C2* o = r == A ? B : A;
+  // rows 2 yp and 2 yp + 1 of the inverse, Hermitian-completed along z, as one row
+  // Z = Ha + i Hb, stored conjugated: conj Z = conj Ha - i conj Hb
+  for (int i = threadIdx.x; i < nyp * nz; i += blockDim.x) {
+    const int yp = i / nz, k = i - yp * nz, y0 = 2 * yp;
+    const bool lo = k < nzh;
+    const int kk = lo ? k : nz - k;
+    C2 ca = r[kk * ny + y0];  // conj Ha[k] for k < nzh
+    if (!lo) ca = conjg(ca);
+    C2 cb;
+    cb.x = cb.y = 0;
+    if (y0 + 1 < ny) {
+      cb = r[kk * ny + y0 + 1];
+      if (!lo) cb = conjg(cb);
+    }
+    C2 v;
+    v.x = ca.x + cb.y;
+    v.y = ca.y - cb.x;
+    o[i] = v;
+  }
+  __syncthreads();
+  // s = F(conj Z); the inverse is conj(s): row 2 yp = Re s, row 2 yp + 1 = -Im s
+  C2* s = stockham(o, r, twz, f, 2, nz, nyp);
+  Real* out = a.grid_real + (long long)x * ny * nz;
+  for (int i = threadIdx.x; i < ny * nz; i += blockDim.x) {
+    const int y = i / nz, z = i - y * nz;
+    const C2 v = s[(y >> 1) * nz + z];
+    out[i] = (y & 1) ? -v.y : v.x;
+  }
+}
+
 }  // namespace
+
+template <class Real>
+size_t pme_transform_smem(const PmeArgs<Real>& a, const PmeFft& f, int kernel) {
+  using C2 = typename Cplx<Real>::T;
+  if (kernel == 1) return sizeof(C2) * (size_t)a.nx * (1 + 2 * f.pencils_x);
+  return sizeof(C2) * ((size_t)a.ny + a.nz + 2 * (size_t)fft_plane_elems(a.ny, a.nz));
+}
+
+template <class Real>
+void launch_pme_transform(const PmeArgs<Real>& a, const PmeFft& f, bool energy, cudaStream_t s) {
+  const size_t sp = pme_transform_smem(a, f, 0), sx = pme_transform_smem(a, f, 1);
+  const int nzh = a.nz / 2 + 1, nkb = ceil_div(nzh, f.pencils_x);
+  planes_forward<Real><<<a.nx, f.threads[0], sp, s>>>(a, f);
+  if (energy)
+    x_convolve<Real, true><<<a.ny * nkb, f.threads[1], sx, s>>>(a, f);
+  else
+    x_convolve<Real, false><<<a.ny * nkb, f.threads[1], sx, s>>>(a, f);
+  planes_inverse<Real><<<a.nx, f.threads[2], sp, s>>>(a, f);
+}
+
+template <class Real>
+void prepare_pme_transform(const PmeArgs<Real>& a, const PmeFft& f) {
+  const int sp = (int)pme_transform_smem(a, f, 0), sx = (int)pme_transform_smem(a, f, 1);
+  cudaFuncSetAttribute((const void*)planes_forward<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, sp);
+  cudaFuncSetAttribute((const void*)planes_inverse<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, sp);
+  cudaFuncSetAttribute((const void*)x_convolve<Real, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sx);
+  cudaFuncSetAttribute((const void*)x_convolve<Real, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sx);
+}
+
+template size_t pme_transform_smem<float>(const PmeArgs<float>&, const PmeFft&, int);
+template size_t pme_transform_smem<double>(const PmeArgs<double>&, const PmeFft&, int);
+template void launch_pme_transform<float>(const PmeArgs<float>&, const PmeFft&, bool, cudaStream_t);
+template void launch_pme_transform<double>(const PmeArgs<double>&, const PmeFft&, bool, cudaStream_t);
+template void prepare_pme_transform<float>(const PmeArgs<float>&, const PmeFft&);
+template void prepare_pme_transform<double>(const PmeArgs<double>&, const PmeFft&);
 
 template <class Real>
 void launch_pme_spread(const PmeArgs<Real>& a, cudaStream_t s) {

@@ -364,6 +364,38 @@ def test_force_groups_split_direct_and_reciprocal():
     assert rms_rel(r.forces, f_rec) < 1e-9
 
 
+# Grid shapes of the reciprocal part: odd and even axes, radices 2 to 8 in the engine's own
+# transform, and prime factors 11, 13, 17 that take the cuFFT path.
+@pytest.mark.parametrize("precision,bound", [("mixed", MIXED_FORCE_RMS), ("double", DOUBLE_FORCE_RMS)])
+@pytest.mark.parametrize("grid", [(25, 27, 30), (32, 21, 28), (45, 35, 49), (16, 24, 20),
+                                  (22, 26, 34), (5, 6, 7)])
+def test_pme_grid_shapes_match_oracle(grid, precision, bound):
+    w = synth.water_box(100, 2.0, (5, 5, 4), seed=4)
+    s = ommb200.System()
+    for m in w.masses():
+        s.add_particle(float(m))
+    s.set_default_periodic_box_vectors(*w.box)
+    nb = ommb200.NonbondedForce()
+    nb.set_nonbonded_method("PME")
+    nb.set_cutoff_distance(0.9)
+    nb.set_pme_parameters(3.2, *grid)
+    for q, sg, e in zip(w.charges(), w.sigmas(), w.epsilons()):
+        nb.add_particle(float(q), float(sg), float(e))
+    for ex in w.exceptions():
+        nb.add_exception(*ex)
+    nb.set_reciprocal_space_force_group(1)
+    s.add_force(nb)
+    ctx = ommb200.Context(s, systems.langevin(), precision=precision)
+    ctx.set_positions(w.positions)
+    r = ctx.get_state(forces=True, energy=True, groups=1 << 1)
+    f_rec, e_rec = O.nonbonded(w.positions, w.charges(), w.sigmas(), w.epsilons(), w.exceptions(),
+                               method="PME", cutoff=0.9, box=w.box, include_direct=False,
+                               pme=(3.2, grid))
+    e_tol = 2e-6 if precision == "mixed" else 1e-9
+    assert abs(r.potential_energy - e_rec) < e_tol * abs(e_rec)
+    assert rms_rel(r.forces, f_rec) < bound
+
+
 def test_nve_energy_is_conserved():
     # friction 0, temperature 0: LangevinMiddle reduces to velocity Verlet with SETTLE
     w, x, v = equilibrated_water()
