@@ -170,39 +170,59 @@ __device__ __forceinline__ void ou_update(const IntegrateArgs& a, int atom, doub
   }
 }
 
-__device__ void water_step(const IntegrateArgs& a, int w, uint64_t step, int n) {
+// One rigid water on four lanes: lane k < 3 loads, kicks, draws the noise for and stores atom
+// k (the Gaussian draws, the longest part of the chain, run side by side); the two SETTLE
+// solves (velocity projection after the kick, positions after the drift) run on all four
+// lanes from shuffled copies of the three atoms.
+__device__ __forceinline__ void share3(double (&o)[3][3], const double mine[3], unsigned gmask) {
+  for (int k = 0; k < 3; ++k)
+    for (int c = 0; c < 3; ++c) o[k][c] = __shfl_sync(gmask, mine[c], k, 4);
+}
+
+// o = m[k] without indexing the array by a run-time value (keeps m in registers)
+__device__ __forceinline__ void pick3(const double (&m)[3][3], int k, double o[3]) {
+#pragma unroll
+  for (int q = 0; q < 3; ++q)
+    if (q == k)
+      for (int c = 0; c < 3; ++c) o[c] = m[q][c];
+}
+
+__device__ void water_step_lanes(const IntegrateArgs& a, int w, int k, uint64_t step, int n,
+                                 unsigned gmask) {
   const int4 idx = a.water[w];
-  const int at[3] = {idx.x, idx.y, idx.z};
+  const int atom = k == 0 ? idx.x : k == 1 ? idx.y : idx.z;
   const double im[3] = {1.0 / a.geom.m_o, 1.0 / a.geom.m_h, 1.0 / a.geom.m_h};
-  double r[3][3], x[3][3], v[3][3];
-  for (int k = 0; k < 3; ++k) {
-    ld3(a.pos, at[k], r[k]);
-    ld3(a.vel, at[k], v[k]);
+  const double imk = k == 0 ? im[0] : im[1];
+  double rk[3] = {0, 0, 0}, vk[3] = {0, 0, 0};
+  if (k < 3) {
+    ld3(a.pos, atom, rk);
+    ld3(a.vel, atom, vk);
     double f[3];
-    force3(a.force, n, at[k], f);
-    for (int c = 0; c < 3; ++c) v[k][c] += f[c] * im[k] * a.dt;
+    force3(a.force, n, atom, f);
+    for (int c = 0; c < 3; ++c) vk[c] += f[c] * imk * a.dt;
   }
+  double r[3][3], v[3][3], x[3][3];
+  share3(r, rk, gmask);
+  share3(v, vk, gmask);
   bool ok = settle_velocities(r, im, v);
-  double prop[3][3];
-  for (int k = 0; k < 3; ++k) {
-    for (int c = 0; c < 3; ++c) x[k][c] = r[k][c];
-    ou_update(a, at[k], im[k], step, x[k], v[k]);
-    for (int c = 0; c < 3; ++c) prop[k][c] = x[k][c];
+  double xk[3] = {rk[0], rk[1], rk[2]};
+  double wk[3] = {0, 0, 0};
+  if (k < 3) {
+    pick3(v, k, wk);
+    ou_update(a, atom, imk, step, xk, wk);
   }
+  share3(x, xk, gmask);
   ok = ok && settle_positions(a.geom, r, x);
+  if (k == 3) return;
   const double inv_dt = 1.0 / a.dt;
-  bool fin = true;
-  for (int k = 0; k < 3; ++k) {
-    for (int c = 0; c < 3; ++c) v[k][c] += (x[k][c] - prop[k][c]) * inv_dt;
-    fin = fin && finite3(x[k]) && finite3(v[k]);
-  }
-  if (!ok) report_status(a.status, kStatusConstraint);
-  if (!fin) report_status(a.status, kStatusNonfinite);
-  for (int k = 0; k < 3; ++k) {
-    st3(a.pos, at[k], x[k]);
-    st3(a.vel, at[k], v[k]);
-    check_rebuild(a, at[k], x[k]);
-  }
+  double xo[3];
+  pick3(x, k, xo);
+  for (int c = 0; c < 3; ++c) wk[c] += (xo[c] - xk[c]) * inv_dt;
+  if (k == 0 && !ok) report_status(a.status, kStatusConstraint);
+  if (!(finite3(xo) && finite3(wk))) report_status(a.status, kStatusNonfinite);
+  st3(a.pos, atom, xo);
+  st3(a.vel, atom, wk);
+  check_rebuild(a, atom, xo);
 }
 
 __device__ void free_step(const IntegrateArgs& a, int atom, uint64_t step, int n) {
@@ -306,11 +326,12 @@ __device__ void cluster_step(const IntegrateArgs& a, int c, uint64_t step, int n
 __global__ void integrate_kernel(const IntegrateArgs a, int n) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   const uint64_t step = *a.rng_step + (uint64_t)a.step_offset;
-  if (t < a.n_water) {
-    water_step(a, t, step, n);
+  if (t < 4 * a.n_water) {
+    const int lane = threadIdx.x & 31;
+    water_step_lanes(a, t >> 2, t & 3, step, n, 0xFu << (lane & ~3));
     return;
   }
-  t -= a.n_water;
+  t -= 4 * a.n_water;
   if (t < a.n_free) {
     free_step(a, a.free_atoms[t], step, n);
     return;
@@ -371,7 +392,7 @@ int threads_needed(const IntegrateArgs& a) { return a.n_water + a.n_free + a.n_c
 }  // namespace
 
 void launch_integrate(const IntegrateArgs& a, cudaStream_t s) {
-  const int t = threads_needed(a);
+  const int t = threads_needed(a) + 3 * a.n_water;  // four lanes per water
   if (t == 0) return;
   integrate_kernel<<<ceil_div(t, 128), 128, 0, s>>>(a, a.n_atoms);
 }
