@@ -47,5 +47,52 @@ __device__ __forceinline__ Real descreening_gradient(Real radius, Real scaled, R
          inverse;
 }
 
+__device__ __forceinline__ float rcp_approx(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// FP32 form of the integral and its gradient together, with SFU reciprocals and logarithm;
+// inv_r = 1 / r.
+__device__ __forceinline__ void descreening_fast(float radius, float scaled, float r, float inv_r,
+                                                 float* h, float* grad) {
+  if (radius >= r + scaled) {
+    *h = 0.f;
+    *grad = 0.f;
+    return;
+  }
+  const float lo_den = fmaxf(radius, fabsf(r - scaled));
+  const float lower = rcp_approx(lo_den), upper = rcp_approx(r + scaled);
+  const float l2u2 = lower * lower - upper * upper;
+  const float lg = __logf(lo_den * upper);  // log(upper / lower)
+  float v = lower - upper - 0.25f * r * l2u2 + 0.5f * inv_r * lg +
+            0.25f * scaled * scaled * inv_r * l2u2;
+  if (radius < scaled - r) v += 2.f * (rcp_approx(radius) - lower);
+  *h = v;
+  *grad = (0.125f * (1.f + scaled * scaled * inv_r * inv_r) * l2u2 + 0.25f * lg * inv_r * inv_r) *
+          inv_r;
+}
+
+// The pair passes' forms: SFU arithmetic in FP32, the exact expressions in FP64.
+__device__ __forceinline__ float descreening_pair(float radius, float scaled, float r, float inv_r) {
+  float h, g;
+  descreening_fast(radius, scaled, r, inv_r, &h, &g);
+  return h;
+}
+__device__ __forceinline__ double descreening_pair(double radius, double scaled, double r, double) {
+  return descreening<double>(radius, scaled, r);
+}
+__device__ __forceinline__ float descreening_gradient_pair(float radius, float scaled, float r,
+                                                           float inv_r) {
+  float h, g;
+  descreening_fast(radius, scaled, r, inv_r, &h, &g);
+  return g;
+}
+__device__ __forceinline__ double descreening_gradient_pair(double radius, double scaled, double r,
+                                                            double) {
+  return descreening_gradient<double>(radius, scaled, r);
+}
+
 }  // namespace gb
 }  // namespace ommb200

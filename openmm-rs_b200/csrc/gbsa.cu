@@ -69,13 +69,20 @@ __global__ void __launch_bounds__(128) gb_pass(const GbArgs a) {
       }
       const Real r2 = dx * dx + dy * dy + dz * dz;
       bool use = ai >= 0 && bj >= 0;
-      const Real r = sqrt_r(use ? r2 : Real(1));
+      Real r, inv_r;
+      if constexpr (sizeof(Real) == 4) {  // SFU reciprocal square root in the FP32 kernel
+        inv_r = rsqrt_r(use ? r2 : Real(1));
+        r = (use ? r2 : Real(1)) * inv_r;
+      } else {
+        r = sqrt_r(use ? r2 : Real(1));
+        inv_r = Real(1) / r;
+      }
       if (a.use_cutoff) use = use && r <= (Real)a.cutoff;  // gbsa_obc.rs:169 (<=)
       Real fo = 0;
       if (kPass == 1) {
         if (use) {
-          acc_i += descreening<Real>(qi.x, qj.y, r);
-          if (!self) acc_j += descreening<Real>(qj.x, qi.y, r);
+          acc_i += descreening_pair(qi.x, qj.y, r, inv_r);
+          if (!self) acc_j += descreening_pair(qj.x, qi.y, r, inv_r);
         }
       } else if (kPass == 2) {
         if (use) {
@@ -99,8 +106,8 @@ __global__ void __launch_bounds__(128) gb_pass(const GbArgs a) {
         }
       } else {
         if (use)
-          fo = -(ri_aux * descreening_gradient<Real>(qi.x, qj.y, r) +
-                 rj_aux * descreening_gradient<Real>(qj.x, qi.y, r));
+          fo = -(ri_aux * descreening_gradient_pair(qi.x, qj.y, r, inv_r) +
+                 rj_aux * descreening_gradient_pair(qj.x, qi.y, r, inv_r));
       }
       if (kPass != 1) {
         // self tiles visit each pair from both sides; each visit moves only its own lane

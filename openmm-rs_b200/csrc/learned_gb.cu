@@ -44,25 +44,6 @@ __device__ __forceinline__ float switch_value(float r, float rs, float rc, float
 
 // gbsa_obc.rs:278-309 with SFU reciprocals and logarithm: the descreening integral H and the
 // derivative factor G (dH/dr = -2 r G) of one ordered pair.
-__device__ __forceinline__ void descreening_fast(float radius, float scaled, float r, float inv_r,
-                                                 float* h, float* grad) {
-  if (radius >= r + scaled) {
-    *h = 0.f;
-    *grad = 0.f;
-    return;
-  }
-  const float lo_den = fmaxf(radius, fabsf(r - scaled));
-  const float lower = rcp_r(lo_den), upper = rcp_r(r + scaled);
-  const float l2u2 = lower * lower - upper * upper;
-  const float lg = __logf(lo_den * upper);  // log(upper / lower)
-  float v = lower - upper - 0.25f * r * l2u2 + 0.5f * inv_r * lg +
-            0.25f * scaled * scaled * inv_r * l2u2;
-  if (radius < scaled - r) v += 2.f * (rcp_r(radius) - lower);
-  *h = v;
-  *grad = (0.125f * (1.f + scaled * scaled * inv_r * inv_r) * l2u2 + 0.25f * lg * inv_r * inv_r) *
-          inv_r;
-}
-
 __device__ __forceinline__ float3 position(const double* pos, int atom) {
   return make_float3((float)pos[3 * atom], (float)pos[3 * atom + 1], (float)pos[3 * atom + 2]);
 }
