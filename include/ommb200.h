@@ -261,8 +261,8 @@ int ommb200_context_get_system_energies(ommb200_context* ctx, uint32_t groups,
 
 /* ---- allocation-free force evaluation (no counterpart in the reference) ----
  * For callers that must not allocate device memory: code inside another framework's memory
- * pool, a plugin that may only use the buffers it is handed, or a stream being captured into a
- * CUDA graph.  Evaluates NonbondedForce forces and energy of a non-periodic system without
+ * pool, whose accounting a private allocation would bypass, or a plugin that may only use the
+ * buffers it is handed.  Evaluates NonbondedForce forces and energy of a non-periodic system without
  * exceptions (method OMMB200_NO_CUTOFF or OMMB200_CUTOFF_NON_PERIODIC) with the Context's
  * mixed-precision arithmetic.  All pointers are device pointers on the current device:
  * positions[3n], charges[n], sigmas[n], epsilons[n] in; forces[3n] and energy[1] out.  Work is

@@ -137,9 +137,8 @@ struct PmeArgs {
 
 template <class Real>
 void launch_pme_spread(const PmeArgs<Real>& a, cudaStream_t s);
-// Own transform of the grid (replaces convert, the cuFFT pair and convolve): per axis the
-// split n = n1 n2 and the twiddle table W_n^m = exp(-2 pi i m / n) (float2 or double2).
-// Plan of the engine's own grid transform: per axis the radices of the Stockham stages and
+// Plan of the engine's own grid transform (it replaces the conversion kernel, the cuFFT pair
+// and the convolution kernel): per axis the radices of the Stockham stages and
 // the twiddle table W_n^m = exp(-2 pi i m / n), m < n (Real2 elements); block sizes of the
 // forward-plane, x-pass and inverse-plane kernels; kz pencils per x-pass CTA.
 struct PmeFft {

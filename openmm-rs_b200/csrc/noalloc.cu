@@ -1,7 +1,7 @@
 // Allocation-free variant of the nonbonded pair kernel, for callers that cannot call
-// cudaMalloc: code running inside another framework's memory pool, a plugin that may only
-// use the buffers it is handed, or a stream that is being captured into a CUDA graph, where a
-// fresh allocation would break the capture.  The caller passes device inputs and outputs; the
+// cudaMalloc: code running inside another framework's memory pool, whose accounting a private
+// allocation would bypass, or a plugin that may only use the buffers it is handed.  The
+// caller passes device inputs and outputs; the
 // kernel's scratch (packed block coordinates and 64-bit fixed-point accumulators) lives in the
 // file-scope array below, which every GPU that loads the library holds until the process
 // exits.  It serves non-periodic systems of at most kNoAllocMaxAtoms particles without

@@ -1,8 +1,8 @@
 """The allocation-free entry point against the Context path, through the C ABI.
 
 ommb200_nonbonded_forces_noalloc serves callers that must not allocate device memory -- code
-inside another framework's memory pool, a plugin that may only use the buffers it is handed,
-or a stream being captured into a CUDA graph.  Its scratch is one static device array shared
+inside another framework's memory pool, or a plugin that may only use the buffers it is
+handed.  Its scratch is one static device array shared
 by every call, which keeps the previous call's contents, so the check runs two calls in a row
 and compares both with the Context's forces and energy (mixed precision, 5e-6 force RMS).
 """
