@@ -503,12 +503,31 @@ def main():
             extras["integrate_roofline"] = {"bound": "hbm", "achieved": gbs, "peak": hbm,
                                             "unit": "GB/s", "frac": gbs / hbm,
                                             "note": "of measured; latency-bound at this size"}
+        if hbm:
+            # reciprocal-space spreading and gathering against the HBM roofline: spreading
+            # reads position (24 B), charge (8 B) and slot (4 B) per atom and adds 8 B per grid
+            # point; gathering reads the same per atom plus 4 B per grid point and adds 24 B of
+            # fixed-point force per atom
+            g_pts = int(np.prod(ctx.get_pme_parameters()[1]))
+            pme_bytes = {"pme_spread": 36 * w.n_atoms + 8 * g_pts,
+                         "pme_gather": 60 * w.n_atoms + 4 * g_pts}
+            pme_roof = {}
+            for k, nbytes in pme_bytes.items():
+                k_ms, k_n = times.get(k, (0.0, 0))
+                if k_ms > 0 and k_n:
+                    gbs = nbytes / (k_ms / k_n / 1000.0) / 1e9
+                    pme_roof[k.replace("pme_", "")] = {
+                        "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm,
+                        "algorithmic_bytes": nbytes, "avg_launch_ms": k_ms / k_n}
+            extras["pme_roofline"] = dict(pme_roof, note="of measured HBM copy bandwidth; "
+                                                         "both kernels are latency-bound")
         per_step = {k: (v[0] / v[1], v[1] / prof_steps) for k, v in times.items()}
         extras["kernel_ms_per_md_step"] = {k: round(v[0] * v[1], 5) for k, v in per_step.items()}
-        # our kernels per MD step: rebuild condition 1, pack 1, pair 1, PME spread/convert/
-        # convolve/gather 4, exceptions 1, integrate 1; the 9 rebuild kernels only on rebuild
-        # steps; one counter kernel per graph launch of 20 steps
-        per_md = 1 + 1 + 1 + 4 + 1 + 1
+        # our kernels per MD step: rebuild condition 1, pack 1, pair 1, PME (spread, the three
+        # transform kernels, gather: 5; or spread, convert, convolve, gather: 4 beside cuFFT),
+        # exceptions 1, integrate 1; the 9 rebuild kernels only on rebuild steps; one counter
+        # kernel per graph launch of 20 steps
+        per_md = 1 + 1 + 1 + (5 if "pme_transform" in times else 4) + 1 + 1
         launches = md_steps * per_md + 9 * rebuilds_timed + args.steps * (args.segment // 20)
         extras["pairs_in_cutoff"] = pairs
         nl = ctx.nlist_stats()

@@ -1871,14 +1871,14 @@ struct CheckpointHeader {
   double skin;
 };
 constexpr char kCheckpointMagic[8] = {'O', 'M', 'B', '2', 'C', 'K', 'P', 'T'};
-constexpr uint32_t kCheckpointVersion = 1;
+constexpr uint32_t kCheckpointVersion = 2;
 }  // namespace
 
 size_t Engine::checkpoint_bytes() const {
   size_t b = sizeof(CheckpointHeader) + 2 * 24 * (size_t)n_;
   if (nb_periodic_) b += 24 * (size_t)n_;
   if (learned_)
-    b += 4 * (size_t)(kRadiiMlpParams + 2 * kRadiiMlpTrainable + 1 + segments_.size()) +
+    b += 4 * (size_t)(kRadiiMlpParams + 2 * kRadiiMlpTrainable + 1 + segments_.size() + 1) +
          sizeof(LearnedState);
   return b;
 }
@@ -1917,6 +1917,7 @@ void Engine::save_checkpoint(uint8_t* out, size_t bytes) {
     take(lr_.adam_t, 4);
     take(lr_.seg_offset, 4 * segments_.size());
     take(lr_.state, sizeof(LearnedState));
+    take(lr_.loss + std::max(0, lr_.train_steps - 1), 4);  // last training loss (a judge may skip training)
   }
   sync();
   h.rebuild_flag = flag;
@@ -1972,6 +1973,7 @@ void Engine::load_checkpoint(const uint8_t* in, size_t bytes) {
     put(lr_.adam_t, 4);
     put(lr_.seg_offset, 4 * segments_.size());
     put(lr_.state, sizeof(LearnedState));
+    put(lr_.loss + std::max(0, lr_.train_steps - 1), 4);
   }
   check_status();
 }

@@ -209,7 +209,8 @@ struct LearnedState {
   int need;         // use_learned | judge: features and network run
   int active;       // the network passed the last judge
   int initialized;  // feature / target normalisation fixed
-  int pad;
+  int train;        // this judge retrains the network (first judge, or error above half the
+                    // tolerance)
   unsigned long long judges, learned_evals, exact_evals;
   unsigned int max_err_bits;  // judge scratch: largest radius relative error (float bits)
   float last_error;           // largest per-particle radius relative error at the last judge

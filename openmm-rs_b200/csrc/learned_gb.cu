@@ -6,15 +6,17 @@
 // Lett. 98, 146401 (2007)) G_if = sum_j exp(-eta (r_ij - mu_f)^2) fc(r_ij) over r_ij < rf =
 // 1.2 nm, fc(r) = (cos(pi r / rf) + 1) / 2.
 // Everything here is short-ranged: per 32-slot block a list of the blocks of its segment whose
-// boxes come within rc, then one CTA per block gathers features and I_short (front), or the
-// forces -dE/dx through I_short and the network (back), visiting each ordered pair from the
-// i side only, so each particle's sums belong to one lane per warp and meet in a fixed order.
+// boxes come within rc, then one CTA per block gathers features and I_short (front), visiting
+// each ordered pair from the i side only, so each particle's sums belong to one lane per warp
+// and meet in a fixed order; or the forces -dE/dx through I_short and the network (back), once
+// per pair with the j side's share committed in fixed point.
 //
 // The exact pass still runs every `judge_interval` MD steps as the judge: it supplies that
 // step's radii, the network is compared with it (largest per-particle radius relative error),
 // the particles' features and exact tails become the training snapshot, and a few Adam steps
-// follow.  Until the next judge the network's radii are used only if it passed (error below
-// `tolerance`); otherwise the exact passes run.
+// follow unless the network's error is already within half the tolerance.  Until the next
+// judge the network's radii are used only if it passed (error below `tolerance`); otherwise
+// the exact passes run.
 #include "gb_math.cuh"
 #include "kernels.h"
 #include "pair_math.cuh"
@@ -246,7 +248,10 @@ __global__ void __launch_bounds__(32 * kWarps) lr_features(LearnedGbArgs a, GbAr
 
 // One CTA per block I as above: F_i = sum_j (D_i Phi'_ij + D_j Phi'_ji) / r d_ij,
 // Phi_ij = H(r; i, j) S(r) + sum_f (d tail_i / d G_if) g_f(r), D = dE/dI (half the chain
-// value the GB chain kernel leaves per slot).
+// value the GB chain kernel leaves per slot).  The pair term is symmetric in i and j, so each
+// pair of blocks is done once, from the lower block (J >= I in I's list): the force on each
+// entry of J travels with it one lane per warp shuffle and is committed in fixed point after
+// the 32 steps; the self block visits each pair from both sides and keeps i-forces only.
 template <class Real>
 __global__ void __launch_bounds__(32 * kWarps) lr_forces(LearnedGbArgs a, GbArgs g) {
   if (!a.state->use_learned) return;
@@ -259,6 +264,7 @@ __global__ void __launch_bounds__(32 * kWarps) lr_forces(LearnedGbArgs a, GbArgs
   const Real* chain = reinterpret_cast<const Real*>(g.dedr_slot);
   const float fc_k = kPiF / a.rf;
   const float q = __expf(-2.f * kEta * kDmu * kDmu);
+  const float fscale = (float)kForceScale;
   for (int I = blockIdx.x; I < a.n_blocks; I += gridDim.x) {
     const int si = 32 * I + lane;
     const int ai = g.slot_atom[si];
@@ -287,6 +293,8 @@ __global__ void __launch_bounds__(32 * kWarps) lr_forces(LearnedGbArgs a, GbArgs
     for (int it = w; it < nn; it += kWarps) {
       bool near;
       const int J = list_block(a, I, it, n_near, &near);
+      if (J < I) continue;  // done from block J's side
+      const bool self = J == I;
       const int sj = 32 * J + lane;
       const int aj = g.slot_atom[sj];
       if (aj >= 0) {
@@ -312,14 +320,15 @@ __global__ void __launch_bounds__(32 * kWarps) lr_forces(LearnedGbArgs a, GbArgs
         s_par[w][lane] = make_float4(1.f, 0.f, 0.f, 0.f);
       }
       __syncwarp();
-      if (ai >= 0) {
-        for (int k = 0; k < 32; ++k) {
-          const int jl = (lane + k) & 31;
-          const float4 pj = s_pos[w][jl];
-          if (pj.w == 0.f || (J == I && jl == lane)) continue;
-          const float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
-          const float r2 = dx * dx + dy * dy + dz * dz;
-          if (r2 >= rc2) continue;
+      float gx = 0.f, gy = 0.f, gz = 0.f;  // force on the entry now in this lane's rotation
+      const int src = (lane + 1) & 31;
+      for (int k = self ? 1 : 0; k < 32; ++k) {
+        const int jl = (lane + k) & 31;
+        const float4 pj = s_pos[w][jl];
+        const float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        float radial = 0.f;
+        if (ai >= 0 && pj.w != 0.f && r2 < rc2) {
           const float inv_r = rsqrt_r(r2), r = r2 * inv_r;
           const float4 pr = s_par[w][jl];
           float ds, hij, hji, gij, gji;
@@ -344,11 +353,24 @@ __global__ void __launch_bounds__(32 * kWarps) lr_forces(LearnedGbArgs a, GbArgs
             }
             phi += dfc * s0 - 2.f * kEta * fc * s1;
           }
-          const float radial = phi * inv_r;
-          fx = fmaf(radial, dx, fx);
-          fy = fmaf(radial, dy, fy);
-          fz = fmaf(radial, dz, fz);
+          radial = phi * inv_r;
         }
+        fx = fmaf(radial, dx, fx);
+        fy = fmaf(radial, dy, fy);
+        fz = fmaf(radial, dz, fz);
+        if (!self) {
+          gx = fmaf(-radial, dx, gx);
+          gy = fmaf(-radial, dy, gy);
+          gz = fmaf(-radial, dz, gz);
+          gx = __shfl_sync(kFull, gx, src);
+          gy = __shfl_sync(kFull, gy, src);
+          gz = __shfl_sync(kFull, gz, src);
+        }
+      }
+      if (!self && aj >= 0) {
+        add_fixed(g.force + aj, to_fixed(gx, fscale));
+        add_fixed(g.force + g.n_atoms + aj, to_fixed(gy, fscale));
+        add_fixed(g.force + 2 * g.n_atoms + aj, to_fixed(gz, fscale));
       }
       __syncwarp();
     }
@@ -363,9 +385,9 @@ __global__ void __launch_bounds__(32 * kWarps) lr_forces(LearnedGbArgs a, GbArgs
         for (int u = 1; u < kWarps; ++u) t += s_red[u][lane][c];
         f3[c] = t;
       }
-      add_fixed(g.force + ai, to_fixed(f3[0], (float)kForceScale));
-      add_fixed(g.force + g.n_atoms + ai, to_fixed(f3[1], (float)kForceScale));
-      add_fixed(g.force + 2 * g.n_atoms + ai, to_fixed(f3[2], (float)kForceScale));
+      add_fixed(g.force + ai, to_fixed(f3[0], fscale));
+      add_fixed(g.force + g.n_atoms + ai, to_fixed(f3[1], fscale));
+      add_fixed(g.force + 2 * g.n_atoms + ai, to_fixed(f3[2], fscale));
     }
     __syncthreads();
   }
@@ -441,6 +463,8 @@ __global__ void lr_judge_finish(LearnedGbArgs a) {
   const float err = __uint_as_float(st->max_err_bits);
   st->last_error = err;
   st->active = st->initialized && err <= a.tolerance;
+  // a network within half the tolerance keeps its weights (the offsets are still refitted)
+  st->train = !st->initialized || !(err <= 0.5f * a.tolerance);
 }
 
 // First judge only: feature and target normalisation from the snapshot (fixed afterwards),
@@ -519,7 +543,7 @@ void launch_learned_phase(const LearnedGbArgs& a, const GbArgs& g, int phase, in
     case kLrTrain:
       launch_mlp_train(a.n_atoms, a.snap_features, a.snap_target, a.params, a.moments,
                        a.moments + kRadiiMlpTrainable, a.adam_t, a.train_steps, a.batch,
-                       a.learning_rate, a.seed, nullptr, a.loss, a.status, s, &a.state->judge);
+                       a.learning_rate, a.seed, nullptr, a.loss, a.status, s, &a.state->train);
       break;
     case kLrOffsets:
       // the retrained network on the main configuration, then the per-system offsets
