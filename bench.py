@@ -588,6 +588,9 @@ def main():
 # FP32 work per pair of the Coulomb (NoCutoff) pair kernel: the Ewald count above with the
 # 28-flop screened term replaced by the 2-flop bare Coulomb term.
 FLOPS_PER_PAIR_COULOMB = FLOPS_PER_PAIR - 28 + 2
+# GB pair term of pass 2 on top of the shared distance and force work (FMA = 2, MUFU = 1):
+# 3 MUFU (rcp, ex2, rsqrt) + 13 multiplies/adds + 6 FMAs (two of them the dE/dR sums)
+FLOPS_PER_PAIR_GB2 = 3 + 13 + 2 * 6
 CHAIN_DT_PS = 0.001
 
 
@@ -709,16 +712,25 @@ def main_chains(args):
         extras["kernel_ms_per_md_step"] = {k: round(v[0] / prof, 5) for k, v in times.items()}
         n_excl = int((2 * sizes - 3).sum())
         pairs = int((sizes * (sizes - 1) // 2).sum()) - n_excl
-        pair_ms, pair_n = times.get("pair", (0.0, 1))
-        t_pair = pair_ms / max(pair_n, 1) / 1000.0
         fp32_peak = ommb200.measure_fp32_peak(local)
-        achieved = pairs * FLOPS_PER_PAIR_COULOMB / t_pair / 1e12 if t_pair > 0 else None
+        if "pair" in times:  # a separate nonbonded pair kernel
+            kname, flops = "pair_kernel<float, Coulomb>", pairs * FLOPS_PER_PAIR_COULOMB
+            algo = f"{pairs} pairs x {FLOPS_PER_PAIR_COULOMB} flops per launch"
+            pair_ms, pair_n = times["pair"]
+        else:  # the Coulomb/LJ terms run inside GB pass 2 over every pair of each chain
+            all_pairs = int((sizes * (sizes - 1) // 2).sum())
+            kname = "gb_pass<float, 2> with the NoCutoff nonbonded terms"
+            flops = pairs * FLOPS_PER_PAIR_COULOMB + all_pairs * FLOPS_PER_PAIR_GB2
+            algo = (f"{pairs} nonbonded pairs x {FLOPS_PER_PAIR_COULOMB} + {all_pairs} GB pairs "
+                    f"x {FLOPS_PER_PAIR_GB2} flops per launch")
+            pair_ms, pair_n = times.get("gb_pairs", (0.0, 1))
+        t_pair = pair_ms / max(pair_n, 1) / 1000.0
+        achieved = flops / t_pair / 1e12 if t_pair > 0 else None
         extras["roofline"] = {
-            "bound": "fp32", "kernel": "pair_kernel<float, Coulomb>", "achieved": achieved,
+            "bound": "fp32", "kernel": kname, "achieved": achieved,
             "peak": fp32_peak, "unit": "TFLOP/s",
             "frac": achieved / fp32_peak if achieved else None,
-            "algorithmic": f"{pairs} pairs x {FLOPS_PER_PAIR_COULOMB} flops per launch",
-            "avg_launch_ms": 1000.0 * t_pair, "traffic": None}
+            "algorithmic": algo, "avg_launch_ms": 1000.0 * t_pair, "traffic": None}
         # one Context per chain, stepped in turn: a sample of the first 32 chains
         sample = chs[:32]
         total = 0.0

@@ -653,6 +653,7 @@ void Engine::build_static_tiles() {
       }
     }
   const int nt = (int)tiles.size(), nm = (int)(masks.size() / 32);
+  static_tile_count_ = nt;
   const int nb = n_blocks_;
   OMMB200_CK(cudaMemcpy(a.tiles, tiles.data(), sizeof(int4) * nt, cudaMemcpyHostToDevice));
   if (dp_)
@@ -818,6 +819,18 @@ void Engine::setup_gbsa(const GbsaObcDef& g) {
   a.dedr_self = mem_.alloc<double>(n_);
   a.force = force_;
   a.energy = energy_;
+  // a NoCutoff NonbondedForce over the same segment-padded tiles joins GB pass 2 (one distance
+  // and one force rotation per pair instead of two kernels)
+  if (nb_ && nb_->method == kNoCutoff && !nb_periodic_ && g.method == 0 &&
+      static_tile_count_ == a.n_tiles) {
+    nb_gb_fusable_ = true;
+    a.nb_tiles = nl_.tiles;
+    a.nb_masks = nl_.masks;
+    a.nb_charge = qscaled_;
+    a.nb_half_sigma = half_sigma_;
+    a.nb_two_sqrt_eps = sqrt_eps_;
+    a.nb_params = mem_.alloc_bytes(4 * rs * a.n_slots);
+  }
   if (g.learned.enabled) setup_learned(g.learned);
 }
 
@@ -1220,7 +1233,7 @@ void Engine::enqueue_conditional_rebuild() {
 }
 
 template <class Real>
-void Engine::enqueue_nonbonded(bool energy, bool direct, bool reciprocal, bool dump) {
+void Engine::enqueue_nonbonded(bool energy, bool direct, bool reciprocal, bool dump, bool pairs) {
   const NonbondedDef& nb = *nb_;
   if (nb_periodic_) {
     prof_begin("nlist_rebuild");
@@ -1238,7 +1251,7 @@ void Engine::enqueue_nonbonded(bool energy, bool direct, bool reciprocal, bool d
     OMMB200_CK(cudaEventRecord(fork_ev_, stream_));
     OMMB200_CK(cudaStreamWaitEvent(ps, fork_ev_, 0));
   }
-  if (direct) {
+  if (direct && pairs) {
     prof_begin("pack");
     launch_pack<Real>(n_slots_, nl_.sorted_atom, pos_, nl_.image, nl_.block_center, qscaled_,
                       half_sigma_, sqrt_eps_, posq_, ljp_, nl_.box, stream_);
@@ -1376,15 +1389,20 @@ void Engine::compute_forces(bool energy, uint32_t groups, bool in_step, int step
   prof_begin("zero_forces");
   OMMB200_CK(cudaMemsetAsync(force_, 0, sizeof(long long) * 3 * (size_t)n_, stream_));
   prof_end();
+  gb_.fuse_nonbonded = 0;
   if (nb_) {
     const int g = nb_->force_group;
     const int rg = nb_->reciprocal_force_group < 0 ? g : nb_->reciprocal_force_group;
     const bool direct = nb_->include_direct_space && ((groups >> g) & 1u);
     const bool recip = nb_pme_ && ((groups >> rg) & 1u);
+    // the pair terms go to GB pass 2 when both forces are evaluated (not while dumping pairs)
+    const bool fuse = nb_gb_fusable_ && direct && !dump_mode_ &&
+                      ((groups >> gb_def_->force_group) & 1u);
+    gb_.fuse_nonbonded = fuse ? 1 : 0;
     if (dp_)
-      enqueue_nonbonded<double>(energy, direct, recip, dump_mode_);
+      enqueue_nonbonded<double>(energy, direct, recip, dump_mode_, !fuse);
     else
-      enqueue_nonbonded<float>(energy, direct, recip, dump_mode_);
+      enqueue_nonbonded<float>(energy, direct, recip, dump_mode_, !fuse);
   }
   if (gb_def_ && ((groups >> gb_def_->force_group) & 1u)) {
     auto gb = [&](int phase, const char* name) {

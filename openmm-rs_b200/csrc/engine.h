@@ -123,7 +123,7 @@ class Engine {
   void sync();
   void destroy_graph();
   template <class Real>
-  void enqueue_nonbonded(bool energy, bool direct, bool reciprocal, bool dump);
+  void enqueue_nonbonded(bool energy, bool direct, bool reciprocal, bool dump, bool pairs);
   void prof_begin(const char* name);
   void prof_end();
   void harvest_profile();
@@ -171,6 +171,8 @@ class Engine {
   double* charge_ = nullptr;
   double* half_sigma_ = nullptr;
   double* sqrt_eps_ = nullptr;  // 2 sqrt(epsilon)
+  int static_tile_count_ = 0;    // tiles of the non-periodic (segment-padded) pair list
+  bool nb_gb_fusable_ = false;   // NoCutoff pair terms can run inside GB pass 2
   void* posq_ = nullptr;
   void* ljp_ = nullptr;
   bool params_packed_ = false;

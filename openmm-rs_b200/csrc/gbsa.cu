@@ -24,7 +24,10 @@ namespace {
 
 using namespace gb;
 
-template <class Real, int kPass, bool kEnergy>
+// kNb (pass 2 only): the NoCutoff NonbondedForce pair terms (bare Coulomb + LJ 12-6 with the
+// tile's exclusion mask, energy and virial as the nonbonded pair kernel computes them) join the
+// GB pair term, sharing the distance and the force rotation.
+template <class Real, int kPass, bool kEnergy, bool kNb = false>
 __global__ void __launch_bounds__(128) gb_pass(const GbArgs a) {
   if (kPass != 2 && a.use_learned && *a.use_learned) return;  // the network replaces them
   using T4 = typename V4<Real>::T4;
@@ -33,6 +36,7 @@ __global__ void __launch_bounds__(128) gb_pass(const GbArgs a) {
   __shared__ T4 s_pos[4][32];
   __shared__ T2 s_par[4][32];
   __shared__ Real s_aux[4][32];
+  __shared__ T4 s_nb[kNb ? 4 : 1][32];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const T4* posq = reinterpret_cast<const T4*>(a.posq);
   const T2* par = reinterpret_cast<const T2*>(a.params);
@@ -52,10 +56,20 @@ __global__ void __launch_bounds__(128) gb_pass(const GbArgs a) {
     s_pos[w][lane] = posq[sj];
     s_par[w][lane] = par[sj];
     s_aux[w][lane] = kPass == 2 ? born[sj] : (kPass == 3 ? dedr[sj] : Real(0));
+    T4 nbi;
+    uint32_t excl = 0u;
+    if constexpr (kNb) {
+      const T4* nbp = reinterpret_cast<const T4*>(a.nb_params);
+      nbi = nbp[si];
+      s_nb[w][lane] = nbp[sj];
+      const int4 nt = a.nb_tiles[t];
+      if (nt.y & kTileHasMask) excl = a.nb_masks[32 * nt.z + lane];
+    }
     __syncwarp();
     Real acc_i = 0, acc_j = 0;  // pass 1: descreening sums; pass 2: dE/dR
     Real fix = 0, fiy = 0, fiz = 0, fjx = 0, fjy = 0, fjz = 0;
-    double e_tile = 0.0;
+    double e_tile = 0.0, e_nb = 0.0;
+    double w_nb[6] = {0, 0, 0, 0, 0, 0};
     for (int k = self ? 1 : 0; k < 32; ++k) {
       const int jl = (lane + k) & 31;
       const T4 pj = s_pos[w][jl];
@@ -102,6 +116,26 @@ __global__ void __launch_bounds__(128) gb_pass(const GbArgs a) {
           if (kEnergy) {
             const double e = a.use_cutoff ? (double)pe - (double)coefficient / a.cutoff : (double)pe;
             e_tile += (self ? 0.5 : 1.0) * e;
+          }
+        }
+        if constexpr (kNb) {
+          if (use && ((excl >> jl) & 1u) == 0u) {
+            const T4 nbj = s_nb[w][jl];
+            PairArgs<Real> none{};
+            Real f_nb, en_nb;
+            pair_terms<Real, kElecCoulomb, kEnergy, false>(none, r2, nbi.x * nbj.x, nbi.y + nbj.y,
+                                                           nbi.z * nbj.z, f_nb, en_nb);
+            fo += f_nb;
+            if (kEnergy) {
+              const double scale = self ? 0.5 : 1.0;
+              e_nb += scale * (double)en_nb;
+              w_nb[0] -= scale * (double)(f_nb * dx * dx);
+              w_nb[1] -= scale * (double)(f_nb * dy * dy);
+              w_nb[2] -= scale * (double)(f_nb * dz * dz);
+              w_nb[3] -= scale * (double)(f_nb * dx * dy);
+              w_nb[4] -= scale * (double)(f_nb * dx * dz);
+              w_nb[5] -= scale * (double)(f_nb * dy * dz);
+            }
           }
         }
       } else {
@@ -152,6 +186,17 @@ __global__ void __launch_bounds__(128) gb_pass(const GbArgs a) {
       for (int off = 16; off > 0; off >>= 1) e_tile += __shfl_xor_sync(FULL, e_tile, off);
       const long long ef = to_fixed(e_tile, kEnergyScale);
       if (lane == 0 && ef) add_fixed(a.energy + 8 * a.block_segment[I], ef);
+      if constexpr (kNb) {  // rounded per tile on its own, as the nonbonded pair kernel does
+        for (int off = 16; off > 0; off >>= 1) {
+          e_nb += __shfl_xor_sync(FULL, e_nb, off);
+          for (int c = 0; c < 6; ++c) w_nb[c] += __shfl_xor_sync(FULL, w_nb[c], off);
+        }
+        if (lane == 0) {
+          long long* dst = a.energy + 8 * a.block_segment[I];
+          add_fixed(dst, to_fixed(e_nb, kEnergyScale));
+          for (int c = 0; c < 6; ++c) add_fixed(dst + 1 + c, to_fixed(w_nb[c], kEnergyScale));
+        }
+      }
     }
     __syncwarp();
   }
@@ -234,6 +279,16 @@ __global__ void gb_pack(const GbArgs a) {
   }
   reinterpret_cast<typename V4<Real>::T4*>(a.posq)[s] = p;
   reinterpret_cast<typename V4<Real>::T2*>(a.params)[s] = q;
+  if (a.nb_params) {
+    typename V4<Real>::T4 nb;
+    nb.x = nb.y = nb.z = nb.w = Real(0);
+    if (atom >= 0) {
+      nb.x = (Real)a.nb_charge[atom];
+      nb.y = (Real)a.nb_half_sigma[atom];
+      nb.z = (Real)a.nb_two_sqrt_eps[atom];
+    }
+    reinterpret_cast<typename V4<Real>::T4*>(a.nb_params)[s] = nb;
+  }
 }
 
 }  // namespace
@@ -257,10 +312,16 @@ void launch_gbsa_phase(const GbArgs& a, int phase, bool energy, int sm_count, cu
         gb_radii<Real, false><<<gs, tb, 0, s>>>(a);
       break;
     case kGbPass2:
-      if (energy)
+      if (a.fuse_nonbonded) {
+        if (energy)
+          gb_pass<Real, 2, true, true><<<gt, 128, 0, s>>>(a);
+        else
+          gb_pass<Real, 2, false, true><<<gt, 128, 0, s>>>(a);
+      } else if (energy) {
         gb_pass<Real, 2, true><<<gt, 128, 0, s>>>(a);
-      else
+      } else {
         gb_pass<Real, 2, false><<<gt, 128, 0, s>>>(a);
+      }
       break;
     case kGbChain:
       gb_chain<Real><<<gs, tb, 0, s>>>(a);

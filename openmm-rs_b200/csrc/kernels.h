@@ -199,6 +199,15 @@ struct GbArgs {
   const long long* short_sum;  // [n_atoms] switched short-range integral, 2^-40
   const float* tail;           // [n_atoms] network tail
   const float* seg_offset;     // [segments] tail offset per system
+  // NonbondedForce (NoCutoff) fused into pass 2 while fuse_nonbonded is set: its tiles are the
+  // GB tiles in the same order (every block pair of a segment), with their exclusion masks
+  int fuse_nonbonded;
+  const int4* nb_tiles;           // [n_tiles] (I, flags, mask slot, 0)
+  const uint32_t* nb_masks;       // 32 per masked tile
+  const double* nb_charge;        // [n_atoms] q sqrt(ke)
+  const double* nb_half_sigma;    // [n_atoms] sigma / 2
+  const double* nb_two_sqrt_eps;  // [n_atoms] 2 sqrt(epsilon)
+  void* nb_params;                // [n_slots] Real4: q sqrt(ke), sigma / 2, 2 sqrt(eps), 0
 };
 
 // ---- learned Born radii (learned_gb.cu) -----------------------------------------------------
