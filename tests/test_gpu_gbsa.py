@@ -104,3 +104,25 @@ def test_chain_dynamics_is_stable_and_deterministic():
         assert np.isfinite(st.positions).all() and np.isfinite(st.potential_energy)
         out.append(st.positions)
     assert np.array_equal(out[0], out[1])
+
+
+@pytest.mark.parametrize("precision,tol", [("mixed", 1e-6), ("double", 1e-10)])
+def test_fused_nonbonded_gb_pass_matches_the_separate_kernels(precision, tol):
+    # With the NonbondedForce and the GBSAOBCForce in different force groups, evaluating one
+    # group at a time runs the nonbonded pair kernel and GB pass 2 separately; evaluating both
+    # runs the nonbonded pair terms inside GB pass 2.  Both must give the same forces and the
+    # same per-system energies (a batch of two chains routes energies by segment).
+    chs = [synth.chain(500, seed=31), synth.chain(300, seed=32)]
+    ctx = ommb200.BatchContext([systems.chain_system(c, gb_force_group=1) for c in chs],
+                               systems.langevin(step_size=0.001), precision=precision)
+    ctx.set_positions(np.concatenate([c.positions for c in chs]))
+    both = ctx.get_state(forces=True, energy=True)
+    g0 = ctx.get_state(forces=True, energy=True, groups=1 << 0)
+    g1 = ctx.get_state(forces=True, energy=True, groups=1 << 1)
+    split = g0.forces + g1.forces
+    assert np.abs(both.forces - split).max() < tol * np.abs(split).max()
+    assert abs(both.potential_energy - g0.potential_energy - g1.potential_energy) < \
+        tol * abs(both.potential_energy) + 1e-6
+    e_both = np.asarray(ctx.system_energies()[0])
+    e_split = np.asarray(ctx.system_energies(1 << 0)[0]) + np.asarray(ctx.system_energies(1 << 1)[0])
+    assert np.abs(e_both - e_split).max() < tol * np.abs(e_both).max() + 1e-6
