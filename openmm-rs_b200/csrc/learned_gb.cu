@@ -519,7 +519,7 @@ template <class Real>
 void launch_learned_phase(const LearnedGbArgs& a, const GbArgs& g, int phase, int sm_count,
                           cudaStream_t s) {
   const int wb = ceil_div(a.n_blocks * 32, 128);
-  const int ctas = std::max(1, std::min(a.n_blocks, sm_count * 8));
+  const int ctas = std::max(1, a.n_blocks);  // one CTA per block: the scheduler balances uneven lists
   switch (phase) {
     case kLrLists:
       lr_boxes<<<wb, 128, 0, s>>>(a, g);
