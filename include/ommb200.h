@@ -151,6 +151,28 @@ int ommb200_harmonic_angle_add_angle(ommb200_force* f, int p1, int p2, int p3, d
                                      double k, int* index);
 int ommb200_harmonic_angle_set_uses_pbc(ommb200_force* f, int use_pbc);
 
+/* ---- MonteCarloBarostat (forces/barostat.rs) ----
+ * Isotropic Monte Carlo volume moves: every `frequency` steps (counted by the barostat itself,
+ * 76-86) the box and the positions (molecule centroids when molecules are scaled as rigid,
+ * else every particle) are scaled by (V'/V)^(1/3) with V' - V uniform in +-volume_scale,
+ * and the move is accepted by the Metropolis test on dE + P dV - N kT ln(V'/V) with E over
+ * the integrator's force groups (context/program.rs:5-47).  Needs a periodic System; not in
+ * batches.  The random stream is the engine's own counter-based one (Philox4x32-10 keyed by
+ * the seed), not the reference's ChaCha12 sequence. */
+int ommb200_monte_carlo_barostat_create(double pressure, double temperature, int frequency,
+                                        ommb200_force** out);                   /* new, 63-85 */
+int ommb200_monte_carlo_barostat_set_default_pressure(ommb200_force* f, double pressure); /* 90 */
+int ommb200_monte_carlo_barostat_get_default_pressure(const ommb200_force* f, double* out);
+int ommb200_monte_carlo_barostat_set_default_temperature(ommb200_force* f, double t);   /* 94 */
+int ommb200_monte_carlo_barostat_get_default_temperature(const ommb200_force* f, double* out);
+/* 98-101: a change reaches the Contexts that already hold this barostat */
+int ommb200_monte_carlo_barostat_set_frequency(ommb200_force* f, int frequency);
+int ommb200_monte_carlo_barostat_get_frequency(const ommb200_force* f, int* out);
+int ommb200_monte_carlo_barostat_set_scale_molecules_as_rigid(ommb200_force* f, int rigid); /* 106 */
+int ommb200_monte_carlo_barostat_get_scale_molecules_as_rigid(const ommb200_force* f, int* out);
+int ommb200_monte_carlo_barostat_set_random_number_seed(ommb200_force* f, int seed);   /* 112 */
+int ommb200_monte_carlo_barostat_get_random_number_seed(const ommb200_force* f, int* out);
+
 /* ---- learned Born radii for GBSAOBCForce (no reference counterpart) ----
  * With learned radii enabled (NoCutoff GBSA only), the O(N^2) descreening passes are replaced
  * by a switched short-range integral (cutoff 2.0 nm, switch from 1.8 nm) plus a network tail
@@ -193,6 +215,22 @@ int ommb200_context_apply_constraints(ommb200_context* ctx, double tolerance);  
 int ommb200_context_apply_velocity_constraints(ommb200_context* ctx, double tolerance);
 /* try_step (800-805): returns OMMB200_ERR_CONSTRAINT / _NONFINITE on failure. */
 int ommb200_context_step(ommb200_context* ctx, int steps);
+/* set_parameter / get_parameter (251-268): the global parameters of the System's forces
+ * ("MonteCarloPressure" in bar, "MonteCarloTemperature" in K); unknown names are
+ * OMMB200_ERR_INVALID_ARG. */
+int ommb200_context_set_parameter(ommb200_context* ctx, const char* name, double value);
+int ommb200_context_get_parameter(ommb200_context* ctx, const char* name, double* value);
+/* Barostat bookkeeping (no reference counterpart): attempted / accepted moves since the
+ * Context was created, the current volume step, and the last move: volumes before and after,
+ * energy change, Metropolis work and the uniform draw compared with exp(-work/kT) (-1 when
+ * the work was not positive). */
+typedef struct {
+  uint64_t attempted, accepted;
+  double volume_scale;
+  int last_accepted;
+  double last_old_volume, last_new_volume, last_energy_change, last_work, last_uniform;
+} ommb200_barostat_stats;
+int ommb200_context_get_barostat_stats(ommb200_context* ctx, ommb200_barostat_stats* out);
 /* try_get_state_options (1041-1105): any of the output arrays (3*N doubles) may be NULL. */
 int ommb200_context_get_state(ommb200_context* ctx, int flags, uint32_t groups,
                               double* positions, double* velocities, double* forces,

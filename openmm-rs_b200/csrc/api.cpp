@@ -75,6 +75,17 @@ IntegratorDef* integdef(ommb200_integrator* i) { return reinterpret_cast<Integra
 void set_out(int* out, int v) {
   if (out) *out = v;
 }
+void set_out(double* out, double v) {
+  if (out) *out = v;
+}
+void require_pressure(double p) { require(std::isfinite(p), "pressure must be finite"); }
+void require_temperature(double t) {
+  require(std::isfinite(t) && t >= 0.0, "temperature must be nonnegative and finite");
+}
+BarostatDef* barostat_of(ommb200_force* f) { return force_of<BarostatDef, kMonteCarloBarostat>(f); }
+const BarostatDef* barostat_of(const ommb200_force* f) {
+  return force_of<BarostatDef, kMonteCarloBarostat>(f);
+}
 
 void check_cuda(cudaError_t e) {
   if (e != cudaSuccess) throw Error(OMMB200_ERR_CUDA, cudaGetErrorString(e));
@@ -398,6 +409,62 @@ int ommb200_harmonic_angle_set_uses_pbc(ommb200_force* f, int use_pbc) {
   return guarded([&] { force_of<HarmonicAngleDef, kHarmonicAngle>(f)->use_pbc = use_pbc != 0; });
 }
 
+// ---- MonteCarloBarostat (forces/barostat.rs:63-119) -------------------------------------------
+
+int ommb200_monte_carlo_barostat_create(double pressure, double temperature, int frequency,
+                                        ommb200_force** out) {
+  return guarded([&] {
+    require(out != nullptr, "null output pointer");
+    require_pressure(pressure);
+    require_temperature(temperature);
+    require(frequency >= 0, "frequency must be nonnegative");
+    auto* d = new BarostatDef();
+    d->default_pressure = pressure;
+    d->default_temperature = temperature;
+    d->frequency = frequency;
+    *out = reinterpret_cast<ommb200_force*>(static_cast<ForceDef*>(d));
+  });
+}
+int ommb200_monte_carlo_barostat_set_default_pressure(ommb200_force* f, double pressure) {
+  return guarded([&] {
+    require_pressure(pressure);
+    barostat_of(f)->default_pressure = pressure;
+  });
+}
+int ommb200_monte_carlo_barostat_get_default_pressure(const ommb200_force* f, double* out) {
+  return guarded([&] { set_out(out, barostat_of(f)->default_pressure); });
+}
+int ommb200_monte_carlo_barostat_set_default_temperature(ommb200_force* f, double t) {
+  return guarded([&] {
+    require_temperature(t);
+    barostat_of(f)->default_temperature = t;
+  });
+}
+int ommb200_monte_carlo_barostat_get_default_temperature(const ommb200_force* f, double* out) {
+  return guarded([&] { set_out(out, barostat_of(f)->default_temperature); });
+}
+int ommb200_monte_carlo_barostat_set_frequency(ommb200_force* f, int frequency) {
+  return guarded([&] {
+    require(frequency >= 0, "frequency must be nonnegative");
+    barostat_of(f)->frequency = frequency;
+  });
+}
+int ommb200_monte_carlo_barostat_get_frequency(const ommb200_force* f, int* out) {
+  return guarded([&] { set_out(out, barostat_of(f)->frequency); });
+}
+int ommb200_monte_carlo_barostat_set_scale_molecules_as_rigid(ommb200_force* f, int rigid) {
+  return guarded([&] { barostat_of(f)->scale_molecules_as_rigid = rigid != 0; });
+}
+int ommb200_monte_carlo_barostat_get_scale_molecules_as_rigid(const ommb200_force* f, int* out) {
+  return guarded([&] { set_out(out, barostat_of(f)->scale_molecules_as_rigid ? 1 : 0); });
+}
+int ommb200_monte_carlo_barostat_set_random_number_seed(ommb200_force* f, int seed) {
+  return guarded([&] { barostat_of(f)->random_seed = seed; });
+}
+int ommb200_monte_carlo_barostat_get_random_number_seed(const ommb200_force* f, int* out) {
+  return guarded([&] { set_out(out, barostat_of(f)->random_seed); });
+}
+
 // ---- LangevinMiddleIntegrator -----------------------------------------------------------
 int ommb200_langevin_middle_create(double temperature, double friction, double step_size,
                                    ommb200_integrator** out) {
@@ -592,6 +659,27 @@ int ommb200_context_step(ommb200_context* ctx, int steps) {
     OMMB200_CTX;
     require(steps >= 0, "step count must be nonnegative");
     E.step(steps);
+  });
+}
+int ommb200_context_set_parameter(ommb200_context* ctx, const char* name, double value) {
+  return guarded([&] {
+    OMMB200_CTX;
+    require(name != nullptr, "null parameter name");
+    E.set_parameter(name, value);
+  });
+}
+int ommb200_context_get_parameter(ommb200_context* ctx, const char* name, double* value) {
+  return guarded([&] {
+    OMMB200_CTX;
+    require(name != nullptr && value != nullptr, "null argument");
+    *value = E.get_parameter(name);
+  });
+}
+int ommb200_context_get_barostat_stats(ommb200_context* ctx, ommb200_barostat_stats* out) {
+  return guarded([&] {
+    OMMB200_CTX;
+    require(out != nullptr, "null output pointer");
+    E.barostat_stats(out);
   });
 }
 int ommb200_context_get_state(ommb200_context* ctx, int flags, uint32_t groups, double* positions,

@@ -242,6 +242,11 @@ Engine::Engine(std::unique_ptr<SystemDef> system, std::unique_ptr<IntegratorDef>
                 OMMB200_ERR_UNSUPPORTED);
         gb_def_ = static_cast<const GbsaObcDef*>(f.get());
         break;
+      case kMonteCarloBarostat:
+        require(bar_def_ == nullptr, "only one MonteCarloBarostat per System is supported",
+                OMMB200_ERR_UNSUPPORTED);
+        bar_def_ = static_cast<BarostatDef*>(f.get());
+        break;
       default:
         break;
     }
@@ -253,6 +258,7 @@ Engine::Engine(std::unique_ptr<SystemDef> system, std::unique_ptr<IntegratorDef>
   setup_bonded();
   setup_integrator();
   update_box_dependents();
+  if (bar_def_) setup_barostat(*bar_def_);
   const int one = 1;
   OMMB200_CK(cudaMemcpy(rebuild_, &one, sizeof(int), cudaMemcpyHostToDevice));
 }
@@ -1077,6 +1083,7 @@ void Engine::setup_integrator() {
 void Engine::update_box_dependents() {
   reciprocal_box(box_, recip_, &volume_);
   nl_.box = make_box(box_);
+  nl_.min_width = std::min(box_[0], std::min(box_[4], box_[8]));
   nl_.max_cand = 0;
   if (nb_periodic_ && box_[3] == 0.0 && box_[6] == 0.0 && box_[7] == 0.0) {
     // candidate blocks of one block in the column-neighbourhood kernel, for the largest skin
@@ -1513,6 +1520,31 @@ void Engine::run_graph_steps(int launches) {
 
 void Engine::step(int steps) {
   if (steps <= 0) return;
+  if (!bar_def_) {
+    run_steps(steps);
+    return;
+  }
+  // the barostat counts every step and moves at the start of the step that brings its
+  // counter to the frequency, read live (barostat.rs:76-81, context.rs:904)
+  int done = 0;
+  while (done < steps) {
+    const uint64_t f = (uint64_t)std::max(0, bar_def_->frequency);
+    int chunk = steps - done;
+    if (f > 0) chunk = (int)std::min<uint64_t>(chunk, bar_counter_ + 1 >= f ? 0 : f - 1 - bar_counter_);
+    if (chunk > 0) {
+      run_steps(chunk);
+      bar_counter_ += (uint64_t)chunk;
+      done += chunk;
+      continue;
+    }
+    bar_counter_ = 0;
+    barostat_move();
+    run_steps(1);
+    done += 1;
+  }
+}
+
+void Engine::run_steps(int steps) {
   const int k = opt_.steps_per_graph > 0 ? opt_.steps_per_graph : 20;
   int remaining = steps;
   if (opt_.use_graph && !profiling_ && steps >= k) {
@@ -1688,10 +1720,17 @@ void Engine::get_state(int flags, uint32_t groups, double* pos, double* vel, dou
   for (int i = 0; i < n_; ++i)
     ke += host_masses_[i] * (vout[3 * i] * vout[3 * i] + vout[3 * i + 1] * vout[3 * i + 1] + vout[3 * i + 2] * vout[3 * i + 2]);
   info->kinetic_energy = 0.5 * ke;
-  double pe = (double)e[0] * kEnergyScaleInv;
   double w[6];
+  const double pe = assemble_energy(e, need_energy ? groups : 0u, w);
+  info->potential_energy = need_energy ? pe : 0.0;
+  const double vir[9] = {w[0], w[3], w[4], w[3], w[1], w[5], w[4], w[5], w[2]};
+  std::copy(vir, vir + 9, info->virial);
+}
+
+double Engine::assemble_energy(const long long e[8], uint32_t groups, double w[6]) const {
+  double pe = (double)e[0] * kEnergyScaleInv;
   for (int c = 0; c < 6; ++c) w[c] = (double)e[1 + c] * kEnergyScaleInv;
-  if (need_energy && nb_) {
+  if (groups && nb_) {
     const int g = nb_->force_group;
     const int rg = nb_->reciprocal_force_group < 0 ? g : nb_->reciprocal_force_group;
     const bool direct = nb_->include_direct_space && ((groups >> g) & 1u);
@@ -1706,9 +1745,206 @@ void Engine::get_state(int flags, uint32_t groups, double* pos, double* vel, dou
       for (int c = 0; c < 3; ++c) w[c] += ed;
     }
   }
-  info->potential_energy = need_energy ? pe : 0.0;
-  const double vir[9] = {w[0], w[3], w[4], w[3], w[1], w[5], w[4], w[5], w[2]};
-  std::copy(vir, vir + 9, info->virial);
+  return pe;
+}
+
+double Engine::potential_energy(uint32_t groups) {
+  long long e[8] = {0};
+  const std::vector<long long> terms = evaluate(true, groups, nullptr);
+  for (size_t k = 0; k < terms.size(); ++k) e[k % 8] += terms[k];
+  double w[6];
+  return assemble_energy(e, groups, w);
+}
+
+// ---- MonteCarloBarostat ---------------------------------------------------------------------
+// barostat.rs:198-213 (initialize) and context.rs:95-101; molecules as system.rs:100-141 finds
+// them: particles joined by constraints and by HarmonicBondForce bonds, each molecule's atoms
+// in increasing order, molecules ordered by their first atom.
+void Engine::setup_barostat(BarostatDef& def) {
+  bool periodic = nb_ && nb_periodic_;
+  if (gb_def_ && gb_def_->method == 2) periodic = true;
+  for (auto& f : sys_->forces) {
+    if (f->kind == kHarmonicBond && static_cast<const HarmonicBondDef*>(f.get())->use_pbc)
+      periodic = true;
+    if (f->kind == kHarmonicAngle && static_cast<const HarmonicAngleDef*>(f.get())->use_pbc)
+      periodic = true;
+  }
+  require(periodic, "a barostat cannot be used with a non-periodic system");
+  bar_def_ = &def;
+  bar_rigid_ = def.scale_molecules_as_rigid;
+  bar_pressure_ = def.default_pressure;
+  bar_temperature_ = def.default_temperature;
+  bar_volume_scale_ = 0.01 * box_[0] * box_[4] * box_[8];
+  bar_counter_ = bar_window_attempted_ = bar_window_accepted_ = 0;
+  bar_attempted_ = bar_accepted_ = bar_draws_ = 0;
+  if (def.random_seed == 0) {
+    std::random_device rd;
+    bar_seed_ = ((uint64_t)rd() << 32) | rd();
+  } else {
+    bar_seed_ = (uint64_t)(uint32_t)def.random_seed;
+  }
+  std::vector<int> parent(n_);
+  std::iota(parent.begin(), parent.end(), 0);
+  auto root = [&](int p) {
+    while (parent[p] != p) {
+      parent[p] = parent[parent[p]];
+      p = parent[p];
+    }
+    return p;
+  };
+  auto join = [&](int a, int b) {
+    a = root(a);
+    b = root(b);
+    parent[std::max(a, b)] = std::min(a, b);
+  };
+  for (auto& c : sys_->constraints) join(c.p1, c.p2);
+  for (auto& f : sys_->forces)
+    if (f->kind == kHarmonicBond)
+      for (auto& b : static_cast<const HarmonicBondDef*>(f.get())->bonds) join(b.p1, b.p2);
+  std::vector<std::vector<int>> groups(n_);
+  for (int i = 0; i < n_; ++i) groups[root(i)].push_back(i);
+  std::vector<int> start(1, 0), atoms;
+  for (auto& g : groups) {
+    if (g.empty()) continue;
+    atoms.insert(atoms.end(), g.begin(), g.end());
+    start.push_back((int)atoms.size());
+  }
+  n_molecules_ = (int)start.size() - 1;
+  bar_scaled_ = bar_rigid_ ? n_molecules_ : n_;
+  mol_start_ = mem_.alloc<int>(start.size());
+  mol_atoms_ = mem_.alloc<int>(std::max<size_t>(1, atoms.size()));
+  OMMB200_CK(cudaMemcpy(mol_start_, start.data(), 4 * start.size(), cudaMemcpyHostToDevice));
+  OMMB200_CK(cudaMemcpy(mol_atoms_, atoms.data(), 4 * atoms.size(), cudaMemcpyHostToDevice));
+  bar_saved_ = mem_.alloc<double>(3 * (size_t)n_);
+  bar_last_ = ommb200_barostat_stats{};
+  bar_last_.last_uniform = -1.0;
+}
+
+// The engine's own uniform stream for the barostat: Philox4x32-10 keyed by the seed, one
+// counter value per draw, 53 bits per uniform in [0, 1).
+double Engine::barostat_uniform() {
+  uint32_t c[4] = {(uint32_t)bar_draws_, (uint32_t)(bar_draws_ >> 32), 0x6d636261u, 0u};
+  philox4x32_10(c, (uint32_t)bar_seed_, (uint32_t)(bar_seed_ >> 32));
+  ++bar_draws_;
+  const uint64_t v = ((((uint64_t)c[0]) << 32) | c[1]) >> 11;
+  return (double)v * (1.0 / 9007199254740992.0);
+}
+
+// barostat.rs:172-189: every 10 attempts the volume step shrinks by 1.1 below a quarter
+// accepted and grows by 1.1 (at most 0.3 of the volume) above three quarters.
+void Engine::barostat_record(bool accepted, double previous_volume) {
+  ++bar_attempted_;
+  bar_accepted_ += accepted ? 1 : 0;
+  ++bar_window_attempted_;
+  bar_window_accepted_ += accepted ? 1 : 0;
+  bar_last_.last_accepted = accepted ? 1 : 0;
+  if (bar_window_attempted_ >= 10) {
+    const double fraction = (double)bar_window_accepted_ / (double)bar_window_attempted_;
+    if (fraction < 0.25) {
+      bar_volume_scale_ /= 1.1;
+    } else if (fraction > 0.75) {
+      bar_volume_scale_ = std::min(bar_volume_scale_ * 1.1, previous_volume * 0.3);
+    } else {
+      return;
+    }
+    bar_window_attempted_ = bar_window_accepted_ = 0;
+  }
+}
+
+// barostat.rs:121-169 and context/program.rs:5-47: propose a uniform scaling of the box and
+// the positions, compare the integrator's force groups' energy before and after, accept by
+// the Metropolis test; a rejected move restores positions and box.
+void Engine::barostat_move() {
+  constexpr double kBarNm3ToKjPerMol = 0.0602214076;  // barostat.rs:13
+  const uint32_t groups = integ_->integration_force_groups;
+  const double v_old = box_[0] * box_[4] * box_[8];
+  const double v_new = v_old + bar_volume_scale_ * 2.0 * (barostat_uniform() - 0.5);
+  bar_last_.last_old_volume = v_old;
+  bar_last_.last_new_volume = v_new;
+  bar_last_.last_energy_change = 0.0;
+  bar_last_.last_work = NAN;
+  bar_last_.last_uniform = -1.0;
+  if (!std::isfinite(v_new) || v_new <= 0.0) {
+    barostat_record(false, v_old);
+    return;
+  }
+  const double scale = std::cbrt(v_new / v_old);
+  double old_box[9], new_box[9];
+  std::copy(box_, box_ + 9, old_box);
+  for (int k = 0; k < 9; ++k) new_box[k] = box_[k] * scale;
+  // a box the cutoff no longer fits is not evaluated: the move is rejected
+  bool fits = true;
+  if (nb_ && nb_periodic_)
+    for (int a = 0; a < 3; ++a) fits = fits && nb_->cutoff <= 0.5 * new_box[4 * a];
+  if (gb_def_ && gb_def_->method == 2)
+    for (int a = 0; a < 3; ++a) fits = fits && 2.0 * gb_def_->cutoff <= new_box[4 * a];
+  if (!fits) {
+    barostat_record(false, v_old);
+    return;
+  }
+  const double e_old = potential_energy(groups);
+  const size_t bytes = 24 * (size_t)n_;
+  const int one = 1;
+  OMMB200_CK(cudaMemcpyAsync(bar_saved_, pos_, bytes, cudaMemcpyDeviceToDevice, stream_));
+  launch_scale_positions(pos_, n_, mol_start_, mol_atoms_, n_molecules_, scale, bar_rigid_, stream_);
+  std::copy(new_box, new_box + 9, box_);
+  update_box_dependents();
+  OMMB200_CK(cudaMemcpyAsync(rebuild_, &one, sizeof(int), cudaMemcpyHostToDevice, stream_));
+  const double e_new = potential_energy(groups);
+  const double kt = kBoltzmann * bar_temperature_;
+  const double work = (e_new - e_old) + bar_pressure_ * kBarNm3ToKjPerMol * (v_new - v_old) -
+                      (double)bar_scaled_ * kt * std::log(v_new / v_old);
+  bool accepted;
+  if (std::isnan(work)) {
+    accepted = false;
+  } else if (work <= 0.0) {
+    accepted = true;
+  } else {
+    const double u = barostat_uniform();
+    bar_last_.last_uniform = u;
+    accepted = kt > 0.0 && u <= std::exp(-work / kt);
+  }
+  bar_last_.last_energy_change = e_new - e_old;
+  bar_last_.last_work = work;
+  barostat_record(accepted, v_old);
+  if (accepted) {
+    destroy_graph();  // captured launches carry the old box
+  } else {
+    OMMB200_CK(cudaMemcpyAsync(pos_, bar_saved_, bytes, cudaMemcpyDeviceToDevice, stream_));
+    std::copy(old_box, old_box + 9, box_);
+    update_box_dependents();
+    OMMB200_CK(cudaMemcpyAsync(rebuild_, &one, sizeof(int), cudaMemcpyHostToDevice, stream_));
+  }
+  sync();
+  check_status();
+}
+
+void Engine::set_parameter(const std::string& name, double value) {
+  if (bar_def_ && name == "MonteCarloPressure") {  // barostat.rs:253-257
+    require(std::isfinite(value), "pressure must be finite");
+    bar_pressure_ = value;
+    return;
+  }
+  if (bar_def_ && name == "MonteCarloTemperature") {  // barostat.rs:258-264
+    require(std::isfinite(value) && value >= 0.0, "temperature must be nonnegative and finite");
+    bar_temperature_ = value;
+    return;
+  }
+  throw Error(OMMB200_ERR_INVALID_ARG, "unknown global parameter '" + name + "'");
+}
+
+double Engine::get_parameter(const std::string& name) const {
+  if (bar_def_ && name == "MonteCarloPressure") return bar_pressure_;
+  if (bar_def_ && name == "MonteCarloTemperature") return bar_temperature_;
+  throw Error(OMMB200_ERR_INVALID_ARG, "unknown global parameter '" + name + "'");
+}
+
+void Engine::barostat_stats(ommb200_barostat_stats* out) const {
+  require(bar_def_ != nullptr, "the System has no MonteCarloBarostat");
+  *out = bar_last_;
+  out->attempted = bar_attempted_;
+  out->accepted = bar_accepted_;
+  out->volume_scale = bar_volume_scale_;
 }
 
 void Engine::autotune(int trial_steps, double* skin_out, int* ctas_out, double* ms_out) {
@@ -1774,9 +2010,10 @@ void Engine::autotune(int trial_steps, double* skin_out, int* ctas_out, double* 
     pair_grid_ = sm_count_ * ctas;
     destroy_graph();
     restore();
-    step(std::min(trial_steps, 40));  // warm-up, builds the graph
+    // barostat moves stay out of the trials (run_steps does not count barostat steps)
+    run_steps(std::min(trial_steps, 40));  // warm-up, builds the graph
     OMMB200_CK(cudaEventRecord(t0, stream_));
-    step(trial_steps);
+    run_steps(trial_steps);
     OMMB200_CK(cudaEventRecord(t1, stream_));
     OMMB200_CK(cudaEventSynchronize(t1));
     float ms = 0.f;
@@ -1887,9 +2124,13 @@ struct CheckpointHeader {
   double box[9];
   uint64_t seed, velocity_draws, rng_step;
   double skin;
+  // barostat (zero without one): step counter, volume step and its window, totals, stream
+  uint64_t bar_counter, bar_window_attempted, bar_window_accepted, bar_attempted, bar_accepted;
+  uint64_t bar_seed, bar_draws;
+  double bar_volume_scale, bar_pressure, bar_temperature;
 };
 constexpr char kCheckpointMagic[8] = {'O', 'M', 'B', '2', 'C', 'K', 'P', 'T'};
-constexpr uint32_t kCheckpointVersion = 2;
+constexpr uint32_t kCheckpointVersion = 3;
 }  // namespace
 
 size_t Engine::checkpoint_bytes() const {
@@ -1918,6 +2159,16 @@ void Engine::save_checkpoint(uint8_t* out, size_t bytes) {
   h.seed = seed_;
   h.velocity_draws = velocity_draws_;
   h.skin = skin_;
+  h.bar_counter = bar_counter_;
+  h.bar_window_attempted = bar_window_attempted_;
+  h.bar_window_accepted = bar_window_accepted_;
+  h.bar_attempted = bar_attempted_;
+  h.bar_accepted = bar_accepted_;
+  h.bar_seed = bar_seed_;
+  h.bar_draws = bar_draws_;
+  h.bar_volume_scale = bar_volume_scale_;
+  h.bar_pressure = bar_pressure_;
+  h.bar_temperature = bar_temperature_;
   int flag = 0;
   OMMB200_CK(cudaMemcpyAsync(&h.rng_step, rng_step_, 8, cudaMemcpyDeviceToHost, stream_));
   OMMB200_CK(cudaMemcpyAsync(&flag, rebuild_, 4, cudaMemcpyDeviceToHost, stream_));
@@ -1967,6 +2218,18 @@ void Engine::load_checkpoint(const uint8_t* in, size_t bytes) {
   update_box_dependents();
   time_ = h.time;
   step_count_ = h.step_count;
+  if (bar_def_) {
+    bar_counter_ = h.bar_counter;
+    bar_window_attempted_ = h.bar_window_attempted;
+    bar_window_accepted_ = h.bar_window_accepted;
+    bar_attempted_ = h.bar_attempted;
+    bar_accepted_ = h.bar_accepted;
+    bar_seed_ = h.bar_seed;
+    bar_draws_ = h.bar_draws;
+    bar_volume_scale_ = h.bar_volume_scale;
+    bar_pressure_ = h.bar_pressure;
+    bar_temperature_ = h.bar_temperature;
+  }
   seed_ = h.seed;
   velocity_draws_ = h.velocity_draws;
   OMMB200_CK(cudaMemcpy(rng_step_, &h.rng_step, 8, cudaMemcpyHostToDevice));

@@ -97,6 +97,11 @@ class Engine {
   size_t checkpoint_bytes() const;
   void save_checkpoint(uint8_t* out, size_t bytes);
   void load_checkpoint(const uint8_t* in, size_t bytes);
+  // context.rs:251-268: global parameters of the System's forces (the barostat's pressure and
+  // temperature)
+  void set_parameter(const std::string& name, double value);
+  double get_parameter(const std::string& name) const;
+  void barostat_stats(ommb200_barostat_stats* out) const;
   // learned Born radii: counters of the device control block, last judge error and loss
   void learned_stats(ommb200_learned_radii_stats* out);
   void learned_params(float* out);
@@ -118,7 +123,17 @@ class Engine {
   void upload_nonbonded_parameters(const NonbondedDef& nb);
   std::vector<long long> evaluate(bool energy, uint32_t groups, double* forces);
   void enqueue_step(int step_offset);
+  void run_steps(int steps);
   void run_graph_steps(int graph_launches);
+  // MonteCarloBarostat (forces/barostat.rs, context/program.rs:5-47)
+  void setup_barostat(BarostatDef& def);
+  void barostat_move();
+  void barostat_record(bool accepted, double previous_volume);
+  double barostat_uniform();
+  // potential energy of `groups` (forces evaluated into the Context's buffers)
+  double potential_energy(uint32_t groups);
+  // long-range corrections added to the fixed-point sums e[8] (energy, virial) of `groups`
+  double assemble_energy(const long long e[8], uint32_t groups, double w[6]) const;
   void check_status();
   void sync();
   void destroy_graph();
@@ -135,6 +150,19 @@ class Engine {
   bool dp_ = false;
   int n_ = 0;
   double box_[9];
+  // barostat state: the live definition (frequency), Context values of pressure and
+  // temperature, step counter since the last move, volume step and its 10-attempt window,
+  // totals, random stream (seed, draws), last move; molecules as CSR lists of atoms
+  BarostatDef* bar_def_ = nullptr;
+  bool bar_rigid_ = true;  // captured at Context creation (barostat.rs:104-108)
+  double bar_pressure_ = 0.0, bar_temperature_ = 0.0, bar_volume_scale_ = 0.0;
+  uint64_t bar_counter_ = 0, bar_window_attempted_ = 0, bar_window_accepted_ = 0;
+  uint64_t bar_attempted_ = 0, bar_accepted_ = 0, bar_seed_ = 0, bar_draws_ = 0;
+  ommb200_barostat_stats bar_last_{};
+  int n_molecules_ = 0, bar_scaled_ = 0;
+  int* mol_start_ = nullptr;
+  int* mol_atoms_ = nullptr;
+  double* bar_saved_ = nullptr;
   double time_ = 0.0;
   int64_t step_count_ = 0;
   uint64_t seed_ = 0;

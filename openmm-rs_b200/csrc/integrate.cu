@@ -387,6 +387,30 @@ __global__ void constrain_velocities_kernel(const IntegrateArgs a) {
 
 __global__ void advance_kernel(unsigned long long* c, int by) { *c += (unsigned long long)by; }
 
+// Barostat volume move (context.rs:976-1028): every position coordinate times `scale`, or
+// (rigid) each molecule shifted by (scale - 1) times its centroid, the unweighted mean of its
+// particles summed in molecule order.
+__global__ void scale_positions_kernel(double* pos, int n_atoms, const int* mol_start,
+                                       const int* mol_atoms, int n_molecules, double scale,
+                                       int rigid) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (!rigid) {
+    if (t < 3 * n_atoms) pos[t] = scale * pos[t];
+    return;
+  }
+  if (t >= n_molecules) return;
+  const int a0 = mol_start[t], a1 = mol_start[t + 1];
+  double c[3] = {0.0, 0.0, 0.0};
+  for (int k = a0; k < a1; ++k)
+    for (int d = 0; d < 3; ++d) c[d] += pos[3 * mol_atoms[k] + d];
+  const double inv = 1.0 / (double)(a1 - a0);
+  const double f = scale - 1.0;
+  double off[3];
+  for (int d = 0; d < 3; ++d) off[d] = f * (c[d] * inv);
+  for (int k = a0; k < a1; ++k)
+    for (int d = 0; d < 3; ++d) pos[3 * mol_atoms[k] + d] += off[d];
+}
+
 int threads_needed(const IntegrateArgs& a) { return a.n_water + a.n_free + a.n_clusters; }
 
 }  // namespace
@@ -395,6 +419,14 @@ void launch_integrate(const IntegrateArgs& a, cudaStream_t s) {
   const int t = threads_needed(a) + 3 * a.n_water;  // four lanes per water
   if (t == 0) return;
   integrate_kernel<<<ceil_div(t, 128), 128, 0, s>>>(a, a.n_atoms);
+}
+
+void launch_scale_positions(double* pos, int n_atoms, const int* mol_start, const int* mol_atoms,
+                            int n_molecules, double scale, bool rigid, cudaStream_t s) {
+  const int n = rigid ? n_molecules : 3 * n_atoms;
+  if (n <= 0) return;
+  scale_positions_kernel<<<ceil_div(n, 128), 128, 0, s>>>(pos, n_atoms, mol_start, mol_atoms,
+                                                         n_molecules, scale, rigid ? 1 : 0);
 }
 
 void launch_advance_counter(unsigned long long* counter, int by, cudaStream_t s) {

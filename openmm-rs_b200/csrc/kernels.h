@@ -341,6 +341,9 @@ struct IntegrateArgs {
   int* status;
 };
 void launch_integrate(const IntegrateArgs& a, cudaStream_t s);
+// Barostat volume move: positions scaled, per particle or per molecule (CSR lists of atoms)
+void launch_scale_positions(double* pos, int n_atoms, const int* mol_start, const int* mol_atoms,
+                            int n_molecules, double scale, bool rigid, cudaStream_t s);
 void launch_advance_counter(unsigned long long* counter, int by, cudaStream_t s);
 
 // Velocity / position constraint projections used outside the step (apply_constraints,

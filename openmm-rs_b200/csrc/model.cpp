@@ -200,6 +200,8 @@ std::unique_ptr<SystemDef> merge_systems(std::vector<std::unique_ptr<SystemDef>>
           for (auto b : src->bonds) hb->bonds.push_back({b.p1 + off, b.p2 + off, b.length, b.k});
           break;
         }
+        case kMonteCarloBarostat:
+          throw Error(OMMB200_ERR_UNSUPPORTED, "a batch cannot carry a MonteCarloBarostat");
         case kHarmonicAngle: {
           auto* src = static_cast<HarmonicAngleDef*>(f.get());
           if (!ha) {

@@ -20,7 +20,8 @@ struct Error : std::runtime_error {
   Error(int c, const std::string& msg) : std::runtime_error(msg), code(c) {}
 };
 
-enum ForceKind { kNonbonded = 1, kGbsaObc = 2, kHarmonicBond = 3, kHarmonicAngle = 4 };
+enum ForceKind { kNonbonded = 1, kGbsaObc = 2, kHarmonicBond = 3, kHarmonicAngle = 4,
+                 kMonteCarloBarostat = 5 };
 
 // NonbondedMethod (nonbonded.rs:19-33); Ewald and LJPME are not engine methods.
 enum NonbondedMethod { kNoCutoff = 0, kCutoffNonPeriodic = 1, kCutoffPeriodic = 2, kEwald = 3,
@@ -109,6 +110,19 @@ struct HarmonicAngleDef : ForceDef {
   HarmonicAngleDef() : ForceDef(kHarmonicAngle) { name = "HarmonicAngleForce"; }
   std::vector<AngleDef> angles;
   bool use_pbc = false;
+};
+
+// MonteCarloBarostat (forces/barostat.rs:44-110): isotropic Monte Carlo volume moves every
+// `frequency` steps at `pressure` (bar) and `temperature` (K).  The Context reads `frequency`
+// from this object at every step, so changing it later reaches existing Contexts (the
+// reference shares it through an atomic, barostat.rs:98-101).
+struct BarostatDef : ForceDef {
+  BarostatDef() : ForceDef(kMonteCarloBarostat) { name = "MonteCarloBarostat"; }
+  double default_pressure = 1.0;
+  double default_temperature = 300.0;
+  int frequency = 25;
+  bool scale_molecules_as_rigid = true;  // barostat.rs:78
+  int random_seed = 0;                   // 0: pick from OS entropy at Context creation
 };
 
 struct ConstraintDef {

@@ -60,6 +60,13 @@ class LearnedRadiiStats(C.Structure):
                 ("active", C.c_int), ("last_radius_error", C.c_double), ("last_loss", C.c_double)]
 
 
+class BarostatStats(C.Structure):
+    _fields_ = [("attempted", C.c_uint64), ("accepted", C.c_uint64), ("volume_scale", C.c_double),
+                ("last_accepted", C.c_int), ("last_old_volume", C.c_double),
+                ("last_new_volume", C.c_double), ("last_energy_change", C.c_double),
+                ("last_work", C.c_double), ("last_uniform", C.c_double)]
+
+
 class StateInfo(C.Structure):
     _fields_ = [("time", C.c_double), ("step_count", C.c_int64),
                 ("potential_energy", C.c_double), ("kinetic_energy", C.c_double),
@@ -123,6 +130,20 @@ def library() -> C.CDLL:
             "ommb200_context_apply_constraints": [P, D],
             "ommb200_context_apply_velocity_constraints": [P, D],
             "ommb200_context_step": [P, I],
+            "ommb200_monte_carlo_barostat_create": [D, D, I, C.POINTER(P)],
+            "ommb200_monte_carlo_barostat_set_default_pressure": [P, D],
+            "ommb200_monte_carlo_barostat_get_default_pressure": [P, C.POINTER(D)],
+            "ommb200_monte_carlo_barostat_set_default_temperature": [P, D],
+            "ommb200_monte_carlo_barostat_get_default_temperature": [P, C.POINTER(D)],
+            "ommb200_monte_carlo_barostat_set_frequency": [P, I],
+            "ommb200_monte_carlo_barostat_get_frequency": [P, C.POINTER(I)],
+            "ommb200_monte_carlo_barostat_set_scale_molecules_as_rigid": [P, I],
+            "ommb200_monte_carlo_barostat_get_scale_molecules_as_rigid": [P, C.POINTER(I)],
+            "ommb200_monte_carlo_barostat_set_random_number_seed": [P, I],
+            "ommb200_monte_carlo_barostat_get_random_number_seed": [P, C.POINTER(I)],
+            "ommb200_context_set_parameter": [P, C.c_char_p, D],
+            "ommb200_context_get_parameter": [P, C.c_char_p, C.POINTER(D)],
+            "ommb200_context_get_barostat_stats": [P, C.POINTER(BarostatStats)],
             "ommb200_context_get_state": [P, I, C.c_uint32, C.POINTER(D), C.POINTER(D),
                                           C.POINTER(D), C.POINTER(StateInfo)],
             "ommb200_context_get_pme_parameters": [P, C.POINTER(D), C.POINTER(I), C.POINTER(I),
@@ -381,6 +402,60 @@ class HarmonicBondForce(_Force):
         _check(library().ommb200_harmonic_bond_set_uses_pbc(self._h, int(use_pbc)))
 
 
+class MonteCarloBarostat(_Force):
+    """forces/barostat.rs:44-119 (openmm-py barostat.rs): isotropic Monte Carlo volume moves
+    every `frequency` steps at `pressure` (bar) and `temperature` (K)."""
+
+    def __init__(self, pressure: float = 1.0, temperature: float = 300.0, frequency: int = 25):
+        h = C.c_void_p()
+        _check(library().ommb200_monte_carlo_barostat_create(float(pressure), float(temperature),
+                                                             int(frequency), C.byref(h)))
+        self._h = h
+        self._owned = False
+
+    PRESSURE = "MonteCarloPressure"
+    TEMPERATURE = "MonteCarloTemperature"
+
+    def _get(self, name, ctype):
+        v = ctype()
+        _check(getattr(library(), f"ommb200_monte_carlo_barostat_get_{name}")(self._h, C.byref(v)))
+        return v.value
+
+    def set_default_pressure(self, pressure: float) -> None:
+        _check(library().ommb200_monte_carlo_barostat_set_default_pressure(self._h, float(pressure)))
+
+    def get_default_pressure(self) -> float:
+        return self._get("default_pressure", C.c_double)
+
+    def set_default_temperature(self, temperature: float) -> None:
+        _check(library().ommb200_monte_carlo_barostat_set_default_temperature(self._h,
+                                                                              float(temperature)))
+
+    def get_default_temperature(self) -> float:
+        return self._get("default_temperature", C.c_double)
+
+    def set_frequency(self, frequency: int) -> None:
+        """Reaches the Contexts that already hold this barostat, as in the reference."""
+        _check(library().ommb200_monte_carlo_barostat_set_frequency(self._h, int(frequency)))
+
+    def get_frequency(self) -> int:
+        return self._get("frequency", C.c_int)
+
+    def set_scale_molecules_as_rigid(self, rigid: bool) -> None:
+        """Taken by a Context when it is created; later changes do not reach it."""
+        _check(library().ommb200_monte_carlo_barostat_set_scale_molecules_as_rigid(self._h,
+                                                                                   int(rigid)))
+
+    def get_scale_molecules_as_rigid(self) -> bool:
+        return bool(self._get("scale_molecules_as_rigid", C.c_int))
+
+    def set_random_number_seed(self, seed: int) -> None:
+        _check(library().ommb200_monte_carlo_barostat_set_random_number_seed(self._h, int(seed)))
+
+    def get_random_number_seed(self) -> int:
+        return self._get("random_number_seed", C.c_int)
+
+
 class HarmonicAngleForce(_Force):
     _create = "ommb200_harmonic_angle_create"
 
@@ -534,6 +609,21 @@ class Context:
 
     def step(self, steps: int) -> None:
         _check(library().ommb200_context_step(self._h, int(steps)))
+
+    def set_parameter(self, name: str, value: float) -> None:
+        """context.rs:251-261: a global parameter of the System's forces."""
+        _check(library().ommb200_context_set_parameter(self._h, name.encode(), float(value)))
+
+    def get_parameter(self, name: str) -> float:
+        v = C.c_double()
+        _check(library().ommb200_context_get_parameter(self._h, name.encode(), C.byref(v)))
+        return v.value
+
+    def barostat_stats(self) -> dict:
+        """Attempted / accepted volume moves, the current volume step and the last move."""
+        st = BarostatStats()
+        _check(library().ommb200_context_get_barostat_stats(self._h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in BarostatStats._fields_}
 
     def get_state(self, positions=False, velocities=False, forces=False, energy=False,
                   virial=False, groups=-1) -> State:

@@ -447,3 +447,83 @@ def adam_update(params, m, v, grad, t, lr, beta1=0.9, beta2=0.999, eps=1e-8):
     vh = v[:k] / (1 - beta2 ** t)
     params[:k] = params[:k] - lr * mh / (np.sqrt(vh) + eps)
     return params, m, v
+
+
+# ---- MonteCarloBarostat (forces/barostat.rs, system.rs, context.rs), pure Python ----------
+BOLTZMANN = 1.380649e-23 * 6.02214076e23 / 1000.0  # kJ/mol/K (integrators/langevin.rs)
+BAR_NM3_TO_KJ_PER_MOL = 0.0602214076                # barostat.rs:13
+
+
+def molecules(n, constraints=(), bonds=()):
+    """system.rs:100-141: particles joined by constraints and bonds (union-find whose root is
+    the smaller index), each molecule's particles in increasing order, molecules ordered by
+    their first particle."""
+    parent = list(range(n))
+
+    def root(p):
+        while parent[p] != p:
+            parent[p] = parent[parent[p]]
+            p = parent[p]
+        return p
+
+    for a, b in list(constraints) + list(bonds):
+        ra, rb = root(a), root(b)
+        parent[max(ra, rb)] = min(ra, rb)
+    groups = [[] for _ in range(n)]
+    for i in range(n):
+        groups[root(i)].append(i)
+    return [g for g in groups if g]
+
+
+def scale_positions(pos, mols, scale, rigid):
+    """context.rs:976-1028 with the diagonal transform of an isotropic move: every coordinate
+    times `scale`, or each molecule shifted by (scale - 1) times its unweighted centroid."""
+    out = np.array(pos, dtype=np.float64).reshape(-1, 3).copy()
+    if not rigid:
+        return scale * out
+    f = scale - 1.0
+    for m in mols:
+        c = np.zeros(3)
+        for a in m:
+            c = c + out[a]
+        c = c * (1.0 / len(m))
+        out[m] = out[m] + f * c
+    return out
+
+
+def barostat_work(energy_change, pressure, old_volume, new_volume, scaled, temperature):
+    """barostat.rs:144-148"""
+    kt = BOLTZMANN * temperature
+    return (energy_change + pressure * BAR_NM3_TO_KJ_PER_MOL * (new_volume - old_volume)
+            - scaled * kt * np.log(new_volume / old_volume))
+
+
+def barostat_accepts(work, temperature, uniform):
+    """barostat.rs:149-160: `uniform` is drawn only when the work is positive."""
+    kt = BOLTZMANN * temperature
+    if np.isnan(work):
+        return False
+    if work <= 0.0:
+        return True
+    return bool(kt > 0.0 and uniform <= np.exp(-work / kt))
+
+
+class VolumeStep:
+    """barostat.rs:172-189 and 202-204: the volume step starts at 1 % of the volume and adapts
+    every 10 attempts."""
+
+    def __init__(self, volume):
+        self.scale, self.attempted, self.accepted = 0.01 * volume, 0, 0
+
+    def record(self, accepted, previous_volume):
+        self.attempted += 1
+        self.accepted += int(accepted)
+        if self.attempted >= 10:
+            fraction = self.accepted / self.attempted
+            if fraction < 0.25:
+                self.scale /= 1.1
+            elif fraction > 0.75:
+                self.scale = min(self.scale * 1.1, previous_volume * 0.3)
+            else:
+                return
+            self.attempted = self.accepted = 0

@@ -285,3 +285,30 @@ def test_water_box_pme_parameters_follow_tolerance_rule():
         assert abs(alpha - 2.92029) < 1e-5 and dims == (grid,) * 3
     alpha, dims = O.pme_parameters(0.9, 5e-4, np.diag([22.0] * 3))
     assert dims == (196,) * 3
+
+
+def test_barostat_restatement():
+    # system.rs:100-141: union-find over constraints and bonds, smaller root
+    assert O.molecules(6, constraints=[(4, 5)], bonds=[(2, 0), (3, 4)]) == [[0, 2], [1], [3, 4, 5]]
+    # context.rs:976-1028: rigid moves shift molecules by their centroid, others scale points
+    pos = np.array([[0.2, 0.3, 0.4], [0.9, 0.3, 0.4], [1.4, 1.1, 0.8]])
+    r = O.scale_positions(pos, [[0, 1], [2]], 1.1, True)
+    assert np.allclose(r[1] - r[0], pos[1] - pos[0], atol=1e-15)
+    assert np.allclose(r[2], 1.1 * pos[2], atol=1e-15)
+    assert np.allclose(O.scale_positions(pos, [[0, 1], [2]], 1.1, False), 1.1 * pos)
+    # barostat.rs:144-160
+    kt = O.BOLTZMANN * 300.0
+    w = O.barostat_work(1.0, 1.0, 10.0, 10.1, 5, 300.0)
+    assert abs(w - (1.0 + O.BAR_NM3_TO_KJ_PER_MOL * 0.1 - 5 * kt * np.log(1.01))) < 1e-15
+    assert O.barostat_accepts(-1.0, 300.0, 0.99) and not O.barostat_accepts(np.nan, 300.0, 0.0)
+    assert O.barostat_accepts(kt, 300.0, np.exp(-1.0) - 1e-12)
+    assert not O.barostat_accepts(kt, 300.0, np.exp(-1.0) + 1e-12)
+    assert not O.barostat_accepts(1.0, 0.0, 0.0)
+    # barostat.rs:172-189: 10 rejections shrink the step by 1.1, 10 acceptances grow it
+    s = O.VolumeStep(100.0)
+    for _ in range(10):
+        s.record(False, 100.0)
+    assert abs(s.scale - 1.0 / 1.1) < 1e-15 and s.attempted == 0
+    for _ in range(10):
+        s.record(True, 100.0)
+    assert abs(s.scale - 1.0) < 1e-15
