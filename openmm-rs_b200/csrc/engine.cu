@@ -1101,34 +1101,16 @@ void Engine::update_box_dependents() {
   gb_.boxf = cast_box<float>(gb_.boxd);
   if (!nb_) return;
   if (nb_pme_) {
-    const int nx = grid_[0], ny = grid_[1], nz = grid_[2], nzh = nz / 2 + 1;
-    std::vector<double> mod[3] = {bspline_moduli(nx), bspline_moduli(ny), bspline_moduli(nz)};
-    auto freq = [](int k, int n) { return k < (n + 1) / 2 ? (double)k : (double)(k - n); };
-    const double pa = kPiD * kPiD / (alpha_ * alpha_);
-    auto G = [&](int x, int y, int z) {
-      const double m[3] = {freq(x, nx), freq(y, ny), freq(z, nz)};
-      double k2 = 0.0;
-      for (int c = 0; c < 3; ++c) {
-        const double kc = m[0] * recip_[0][c] + m[1] * recip_[1][c] + m[2] * recip_[2][c];
-        k2 += kc * kc;
-      }
-      return kOne4PiEps0 * std::exp(-pa * k2) / (kPiD * volume_ * k2 * mod[0][x] * mod[1][y] * mod[2][z]);
-    };
-    const size_t gk = (size_t)nx * ny * nzh;
-    std::vector<double> infl(gk, 0.0);
-    for (int x = 0; x < nx; ++x)
-      for (int y = 0; y < ny; ++y)
-        for (int z = 0; z < nzh; ++z) {
-          if (x == 0 && y == 0 && z == 0) continue;
-          infl[((size_t)x * ny + y) * nzh + z] =
-              0.5 * (G(x, y, z) + G((nx - x) % nx, (ny - y) % ny, (nz - z) % nz));
-        }
-    if (dp_) {
-      OMMB200_CK(cudaMemcpy(influence_, infl.data(), 8 * gk, cudaMemcpyHostToDevice));
-    } else {
-      std::vector<float> f(infl.begin(), infl.end());
-      OMMB200_CK(cudaMemcpy(influence_, f.data(), 4 * gk, cudaMemcpyHostToDevice));
-    }
+    PmeRecip r;
+    for (int a = 0; a < 3; ++a)
+      for (int c = 0; c < 3; ++c) r.m[a][c] = recip_[a][c];
+    if (dp_)
+      launch_pme_influence(static_cast<double*>(influence_), moduli_, grid_[0], grid_[1],
+                           grid_[2], r, alpha_, volume_, stream_);
+    else
+      launch_pme_influence(static_cast<float*>(influence_), moduli_, grid_[0], grid_[1],
+                           grid_[2], r, alpha_, volume_, stream_);
+    OMMB200_CK(cudaGetLastError());
     double qt = 0.0;
     for (double q : nb_->charge) qt += q;
     plasma_energy_ = kOne4PiEps0 * kPiD * qt * qt / (2.0 * alpha_ * alpha_ * volume_);

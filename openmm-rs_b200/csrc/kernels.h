@@ -137,6 +137,13 @@ struct PmeArgs {
 
 template <class Real>
 void launch_pme_spread(const PmeArgs<Real>& a, cudaStream_t s);
+// Influence table on the half spectrum for the current reciprocal box (device, f64 math).
+struct PmeRecip {
+  double m[3][3];
+};
+template <class Real>
+void launch_pme_influence(Real* out, const double* moduli, int nx, int ny, int nz,
+                          const PmeRecip& recip, double alpha, double volume, cudaStream_t s);
 // Plan of the engine's own grid transform (it replaces the conversion kernel, the cuFFT pair
 // and the convolution kernel): per axis the radices of the Stockham stages and
 // the twiddle table W_n^m = exp(-2 pi i m / n), m < n (Real2 elements); block sizes of the

@@ -754,6 +754,47 @@ template void launch_pme_transform<double>(const PmeArgs<double>&, const PmeFft&
 template void prepare_pme_transform<float>(const PmeArgs<float>&, const PmeFft&);
 template void prepare_pme_transform<double>(const PmeArgs<double>&, const PmeFft&);
 
+namespace {
+// pme.rs:332-350: the influence function on the half spectrum, averaged over each mode and its
+// conjugate partner, zero at k = 0 (one thread per half-grid point, f64).
+template <class Real>
+__global__ void influence_kernel(Real* out, const double* moduli, int nx, int ny, int nz,
+                                 PmeRecip r, double alpha, double volume) {
+  const int nzh = nz / 2 + 1;
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= (long long)nx * ny * nzh) return;
+  const int z = (int)(i % nzh), y = (int)((i / nzh) % ny), x = (int)(i / ((long long)nzh * ny));
+  if (i == 0) {
+    out[0] = Real(0);
+    return;
+  }
+  const double pa = kPiD * kPiD / (alpha * alpha);
+  auto g = [&](int gx, int gy, int gz) {
+    const double m[3] = {freq(gx, nx), freq(gy, ny), freq(gz, nz)};
+    double k2 = 0.0;
+    for (int c = 0; c < 3; ++c) {
+      const double kc = m[0] * r.m[0][c] + m[1] * r.m[1][c] + m[2] * r.m[2][c];
+      k2 += kc * kc;
+    }
+    return kOne4PiEps0 * exp(-pa * k2) /
+           (kPiD * volume * k2 * moduli[gx] * moduli[nx + gy] * moduli[nx + ny + gz]);
+  };
+  out[i] = (Real)(0.5 * (g(x, y, z) + g((nx - x) % nx, (ny - y) % ny, (nz - z) % nz)));
+}
+}  // namespace
+
+template <class Real>
+void launch_pme_influence(Real* out, const double* moduli, int nx, int ny, int nz,
+                          const PmeRecip& recip, double alpha, double volume, cudaStream_t s) {
+  const long long n = (long long)nx * ny * (nz / 2 + 1);
+  influence_kernel<Real><<<(int)((n + 255) / 256), 256, 0, s>>>(out, moduli, nx, ny, nz, recip,
+                                                                alpha, volume);
+}
+template void launch_pme_influence<float>(float*, const double*, int, int, int, const PmeRecip&,
+                                          double, double, cudaStream_t);
+template void launch_pme_influence<double>(double*, const double*, int, int, int, const PmeRecip&,
+                                           double, double, cudaStream_t);
+
 template <class Real>
 void launch_pme_spread(const PmeArgs<Real>& a, cudaStream_t s) {
   if (a.order) {  // sorted slots: spatially compact CTAs
