@@ -26,6 +26,11 @@ sys.path.insert(0, str(ROOT / "openmm-rs_b200"))
 WORKLOAD = "water-23958"
 DT_PS = 0.002
 METRIC = "ns/day @24k-atom PME water box (1 B200) + force RMS rel err vs FP64"
+METRIC_LARGE = "ns/day @1,065k-atom PME water box (1 B200) + force RMS rel err vs FP64"
+
+
+def water_metric():
+    return METRIC_LARGE if WORKLOAD == "water-1065000" else METRIC
 # Algorithmic FP32 work per in-cutoff pair of the mixed-precision PME pair kernel, FMA = 2,
 # MUFU (rsqrt, exp2, rcp) = 1: delta 3, r^2 5, rsqrt + 1/r^2 2, LJ 11, Ewald (r, exp2,
 # erfc fit with 7 FMAs, force) 28, f/r sum 1, i and j force accumulation 6 + 6 = 62.
@@ -399,7 +404,7 @@ def run_reference(args):
     secs = time.perf_counter() - t0
     value = ns_per_day(args.steps, secs)
     out = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": "ns/day",
+        "impl": "reference", "metric": water_metric(), "value": value, "unit": "ns/day",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000.0 * secs / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -533,7 +538,9 @@ def main():
         nl = ctx.nlist_stats()
         roofline["traffic"] = profiled_traffic(f"pair_kernel_{WORKLOAD}", nl["tiles"])
         # self tiles are 32 x 32 pair slots, neighbour tiles 2 x 16 x 16 (halves of block I)
-        slots = nl["blocks"] * 1024 + (nl["tiles"] - nl["blocks"]) * 512
+        # or 32 x 32 (whole blocks), as the autotuner chose
+        per_tile = 512 if ctx.tuning()["tile_entries"] == 16 else 1024
+        slots = nl["blocks"] * 1024 + (nl["tiles"] - nl["blocks"]) * per_tile
         nl["pair_efficiency"] = pairs / max(1, slots)
         nl["md_steps_per_rebuild"] = md_steps / max(1, rebuilds_timed)  # timed region only
         extras["nlist"] = nl
@@ -555,7 +562,7 @@ def main():
         st_eq = ctx.get_state(positions=True, velocities=True)
         extras["nve_drift"] = nve_drift(w, st_eq.positions, st_eq.velocities, local)
     out = {
-        "metric": METRIC, "value": value, "unit": "ns/day", "n_gpus": world,
+        "metric": water_metric(), "value": value, "unit": "ns/day", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms / args.steps, "ms_per_md_step": ms / md_steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,

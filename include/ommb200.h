@@ -252,11 +252,15 @@ int ommb200_context_checkpoint_size(const ommb200_context* ctx, int64_t* bytes);
 int ommb200_context_create_checkpoint(ommb200_context* ctx, void* buffer, int64_t bytes);
 int ommb200_context_load_checkpoint(ommb200_context* ctx, const void* buffer, int64_t bytes);
 /* Autotuner (no reference counterpart): times trial_steps MD steps from the current state
- * for each candidate Verlet skin (which sets the neighbour-list rebuild interval) and
- * pair-kernel grid, keeps the fastest and restores positions, velocities and the random
- * stream, so the trajectory is unchanged.  Outputs may be NULL. */
+ * for each candidate Verlet skin (which sets the neighbour-list rebuild interval), tile width
+ * (rectangular periodic boxes: 16 neighbour entries per half of a 32-particle block, or 32 per
+ * block) and pair-kernel grid, keeps the fastest and restores positions, velocities and the
+ * random stream, so the trajectory is unchanged.  Outputs may be NULL. */
 int ommb200_context_autotune(ommb200_context* ctx, int trial_steps, double* skin,
                              int* pair_ctas_per_sm, double* ms_per_step);
+/* The current tuning choices (no reference counterpart); outputs may be NULL. */
+int ommb200_context_get_tuning(ommb200_context* ctx, double* skin, int* pair_ctas_per_sm,
+                               int* tile_entries);
 /* PME parameters frozen at Context creation (nonbonded.rs:1078-1106). */
 int ommb200_context_get_pme_parameters(const ommb200_context* ctx, double* alpha, int* nx,
                                        int* ny, int* nz);

@@ -847,6 +847,13 @@ int ommb200_context_autotune(ommb200_context* ctx, int trial_steps, double* skin
     E.autotune(trial_steps, skin, pair_ctas_per_sm, ms_per_step);
   });
 }
+int ommb200_context_get_tuning(ommb200_context* ctx, double* skin, int* pair_ctas_per_sm,
+                               int* tile_entries) {
+  return guarded([&] {
+    OMMB200_CTX;
+    E.tuning(skin, pair_ctas_per_sm, tile_entries);
+  });
+}
 int ommb200_context_nlist_stats(ommb200_context* ctx, int* tiles, int* blocks, int* masked,
                                 int64_t* rebuilds) {
   return guarded([&] {

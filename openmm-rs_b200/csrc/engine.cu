@@ -359,6 +359,7 @@ void Engine::setup_nonbonded(const NonbondedDef& nb) {
   if (nb_periodic_) {
     skin_ = opt_.skin > 0.0 ? opt_.skin : 0.1;
     a.skin = skin_;
+    a.halves = 1;
     double recip[3][3], vol;
     reciprocal_box(box_, recip, &vol);
     const double density = n_ / vol;
@@ -2004,6 +2005,7 @@ void Engine::autotune(int trial_steps, double* skin_out, int* ctas_out, double* 
   };
   double best_skin = skin_, best_ms = 1e30;
   int best_ctas = pair_grid_ / std::max(1, sm_count_);
+  int best_halves = nl_.halves;
   try {
     if (nb_ && nb_periodic_) {
       for (double s : kTunedSkins) {
@@ -2013,6 +2015,18 @@ void Engine::autotune(int trial_steps, double* skin_out, int* ctas_out, double* 
           best_skin = s;
         }
       }
+    }
+    // tile width: 16 entries per half block against 32 per block (rectangular boxes)
+    if (nb_ && nb_periodic_ && nl_.max_cand > 0) {
+      for (int h : {1, 0}) {
+        nl_.halves = h;
+        const double ms = trial(best_skin, best_ctas);
+        if (ms < best_ms) {
+          best_ms = ms;
+          best_halves = h;
+        }
+      }
+      nl_.halves = best_halves;
     }
     if (nb_) {
       for (int c : kTunedPairCtasPerSm) {
@@ -2033,6 +2047,7 @@ void Engine::autotune(int trial_steps, double* skin_out, int* ctas_out, double* 
   cudaEventDestroy(t1);
   skin_ = best_skin;
   nl_.skin = best_skin;
+  nl_.halves = best_halves;
   pair_grid_ = sm_count_ * best_ctas;
   destroy_graph();
   restore();
@@ -2040,6 +2055,13 @@ void Engine::autotune(int trial_steps, double* skin_out, int* ctas_out, double* 
   if (skin_out) *skin_out = best_skin;
   if (ctas_out) *ctas_out = best_ctas;
   if (ms_out) *ms_out = best_ms;
+}
+
+void Engine::tuning(double* skin, int* pair_ctas_per_sm, int* tile_entries) const {
+  if (skin) *skin = skin_;
+  if (pair_ctas_per_sm) *pair_ctas_per_sm = pair_grid_ / std::max(1, sm_count_);
+  const bool rect = nb_ && nb_periodic_ && nl_.max_cand > 0;
+  if (tile_entries) *tile_entries = rect && nl_.halves ? 16 : 32;
 }
 
 void Engine::nlist_stats(int* tiles, int* blocks, int* masked, int64_t* rebuilds) {
@@ -2100,7 +2122,7 @@ namespace {
 struct CheckpointHeader {
   char magic[8];
   uint32_t version;
-  int32_t n_atoms, n_segments, precision, learned, dynamic_list, rebuild_flag, pair_grid;
+  int32_t n_atoms, n_segments, precision, learned, dynamic_list, rebuild_flag, pair_grid, halves;
   double time;
   int64_t step_count;
   double box[9];
@@ -2112,7 +2134,7 @@ struct CheckpointHeader {
   double bar_volume_scale, bar_pressure, bar_temperature;
 };
 constexpr char kCheckpointMagic[8] = {'O', 'M', 'B', '2', 'C', 'K', 'P', 'T'};
-constexpr uint32_t kCheckpointVersion = 3;
+constexpr uint32_t kCheckpointVersion = 4;
 }  // namespace
 
 size_t Engine::checkpoint_bytes() const {
@@ -2135,6 +2157,7 @@ void Engine::save_checkpoint(uint8_t* out, size_t bytes) {
   h.learned = learned_ ? 1 : 0;
   h.dynamic_list = nb_periodic_ ? 1 : 0;
   h.pair_grid = pair_grid_;
+  h.halves = nl_.halves;
   h.time = time_;
   h.step_count = step_count_;
   std::copy(box_, box_ + 9, h.box);
@@ -2219,6 +2242,7 @@ void Engine::load_checkpoint(const uint8_t* in, size_t bytes) {
     skin_ = h.skin;
     nl_.skin = h.skin;
     pair_grid_ = h.pair_grid;
+    nl_.halves = h.halves;
     put(nl_.pos_ref, 24 * (size_t)n_);
     // rebuild the neighbour list from the saved reference positions: the same input as the
     // original run's last rebuild, so the tiles (and every force sum) are the same

@@ -75,6 +75,9 @@ class Engine {
                  ommb200_state_info* info);
   void pme_parameters(double* alpha, int* nx, int* ny, int* nz) const;
   void nlist_stats(int* tiles, int* blocks, int* masked, int64_t* rebuilds);
+  // current skin, pair-kernel CTAs per SM and neighbour entries per i-group (16: halves of
+  // 32-particle blocks; 32: whole blocks)
+  void tuning(double* skin, int* pair_ctas_per_sm, int* tile_entries) const;
   // Times `trial_steps` MD steps for each candidate skin and pair-kernel grid from the
   // current state, keeps the fastest, and restores the state (positions, velocities, RNG
   // counter), so the trajectory is the same as without tuning.

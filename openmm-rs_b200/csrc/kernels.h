@@ -62,6 +62,7 @@ struct NlistArgs {
   int n_cols;
   int col_max;        // largest column the per-column sort accepts
   int max_cand;       // candidate blocks one block can have (rectangular boxes), 0 = unknown
+  int halves;         // rectangular boxes: 16 entries per half of a block (else 32 per block)
 };
 
 void launch_nlist_rebuild(const NlistArgs& a, bool double_entries, cudaStream_t s);

@@ -787,7 +787,7 @@ void launch_nlist_rebuild(const NlistArgs& a, bool double_entries, cudaStream_t 
   nl_col_sort<<<a.n_cols, 256, sizeof(unsigned long long) * m, s>>>(a);
   nl_bounds<<<ceil_div((long long)block_cap * 32, tb), tb, 0, s>>>(a);
   const bool rectangular = a.periodic && a.box.bx == 0.0 && a.box.cx == 0.0 && a.box.cy == 0.0;
-  if (rectangular && a.max_cand > 0) {
+  if (rectangular && a.max_cand > 0 && a.halves) {
     const size_t bytes = (size_t)a.max_cand * (3 * 8 + 4 + 4 + 2 * 4 + 2 * 4) + 8;
     if (double_entries) {
       cudaFuncSetAttribute(nl_lists_cta<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);

@@ -130,6 +130,7 @@ def library() -> C.CDLL:
             "ommb200_context_apply_constraints": [P, D],
             "ommb200_context_apply_velocity_constraints": [P, D],
             "ommb200_context_step": [P, I],
+            "ommb200_context_get_tuning": [P, C.POINTER(D), C.POINTER(I), C.POINTER(I)],
             "ommb200_monte_carlo_barostat_create": [D, D, I, C.POINTER(P)],
             "ommb200_monte_carlo_barostat_set_default_pressure": [P, D],
             "ommb200_monte_carlo_barostat_get_default_pressure": [P, C.POINTER(D)],
@@ -712,7 +713,17 @@ class Context:
         skin, ctas, ms = C.c_double(), C.c_int(), C.c_double()
         _check(library().ommb200_context_autotune(self._h, int(trial_steps), C.byref(skin),
                                                   C.byref(ctas), C.byref(ms)))
-        return {"skin_nm": skin.value, "pair_ctas_per_sm": ctas.value, "ms_per_step": ms.value}
+        out = {"skin_nm": skin.value, "pair_ctas_per_sm": ctas.value, "ms_per_step": ms.value}
+        out["tile_entries"] = self.tuning()["tile_entries"]
+        return out
+
+    def tuning(self) -> dict:
+        """Current skin, pair-kernel CTAs per SM and neighbour entries per i-group."""
+        skin, ctas, width = C.c_double(), C.c_int(), C.c_int()
+        _check(library().ommb200_context_get_tuning(self._h, C.byref(skin), C.byref(ctas),
+                                                    C.byref(width)))
+        return {"skin_nm": skin.value, "pair_ctas_per_sm": ctas.value,
+                "tile_entries": width.value}
 
     def nlist_stats(self) -> dict:
         """Neighbour-list state: tiles, blocks and masked tiles in use, rebuilds so far."""
