@@ -65,24 +65,25 @@ __global__ void __launch_bounds__(128) gb_pass(const GbArgs a) {
       const int4 nt = a.nb_tiles[t];
       if (nt.y & kTileHasMask) excl = a.nb_masks[32 * nt.z + lane];
     }
+    const unsigned valid_j = __ballot_sync(FULL, aj >= 0);  // entries holding a particle
     __syncwarp();
     Real acc_i = 0, acc_j = 0;  // pass 1: descreening sums; pass 2: dE/dR
     Real fix = 0, fiy = 0, fiz = 0, fjx = 0, fjy = 0, fjz = 0;
     double e_tile = 0.0, e_nb = 0.0;
     double w_nb[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll 4
     for (int k = self ? 1 : 0; k < 32; ++k) {
       const int jl = (lane + k) & 31;
       const T4 pj = s_pos[w][jl];
       const T2 qj = s_par[w][jl];
       const Real rj_aux = s_aux[w][jl];
-      const int bj = a.slot_atom[32 * J + jl];
       Real dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
       if (a.periodic) {
         if constexpr (sizeof(Real) == 4) min_image_fast(dx, dy, dz, a.boxf);
         else min_image_fast(dx, dy, dz, a.boxd);
       }
       const Real r2 = dx * dx + dy * dy + dz * dz;
-      bool use = ai >= 0 && bj >= 0;
+      bool use = ai >= 0 && ((valid_j >> jl) & 1u);
       Real r, inv_r;
       if constexpr (sizeof(Real) == 4) {  // SFU reciprocal square root in the FP32 kernel
         inv_r = rsqrt_r(use ? r2 : Real(1));
