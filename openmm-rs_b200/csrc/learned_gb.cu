@@ -39,8 +39,8 @@ __device__ __forceinline__ float switch_value(float r, float rs, float rc, float
     *deriv = 0.f;
     return 1.f;
   }
-  const float w = rc - rs, t = (r - rs) / w;
-  *deriv = -30.f * t * t * (1.f - t) * (1.f - t) / w;
+  const float inv_w = rcp_r(rc - rs), t = (r - rs) * inv_w;
+  *deriv = -30.f * t * t * (1.f - t) * (1.f - t) * inv_w;
   return 1.f + t * t * t * (-10.f + t * (15.f - 6.f * t));
 }
 
@@ -175,6 +175,7 @@ __global__ void __launch_bounds__(32 * kWarps) lr_features(LearnedGbArgs a, GbAr
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const float rc2 = a.rc * a.rc, rf2 = a.rf * a.rf;
   const float q = __expf(-2.f * kEta * kDmu * kDmu);
+  const float fc_k = kPiF / a.rf;
   for (int I = blockIdx.x; I < a.n_blocks; I += gridDim.x) {
     const int ai = g.slot_atom[32 * I + lane];
     float3 pi = make_float3(0.f, 0.f, 0.f);
@@ -215,7 +216,7 @@ __global__ void __launch_bounds__(32 * kWarps) lr_features(LearnedGbArgs a, GbAr
           descreening_fast(off_i, s_scaled[w][jl], r, inv_r, &h, &gr);
           ishort = fmaf(h, sw, ishort);
           if (!near || r2 >= rf2) continue;
-          const float fc = 0.5f * (cosf(kPiF * r / a.rf) + 1.f);
+          const float fc = 0.5f * (__cosf(fc_k * r) + 1.f);  // SFU cosine
           float e[kNF];
           gaussians(r, q, e);
 #pragma unroll
@@ -339,7 +340,7 @@ __global__ void __launch_bounds__(32 * kWarps) lr_forces(LearnedGbArgs a, GbArgs
           float phi = d_i * (-2.f * r * gij * sw + hij * ds) + pr.z * (-2.f * r * gji * sw + hji * ds);
           if (near && r2 < rf2) {
             float sn, cs;
-            sincosf(fc_k * r, &sn, &cs);
+            __sincosf(fc_k * r, &sn, &cs);  // SFU sine and cosine
             const float fc = 0.5f * (cs + 1.f), dfc = -0.5f * fc_k * sn;
             float e[kNF];
             gaussians(r, q, e);
