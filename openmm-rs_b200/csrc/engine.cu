@@ -46,7 +46,8 @@ void* DeviceArena::alloc_bytes(size_t bytes) {
 
 namespace {
 
-void require(bool ok, const std::string& msg, int code = OMMB200_ERR_INVALID_ARG) {
+// the message becomes a string only when the check fails (set_positions checks 3N values)
+void require(bool ok, const char* msg, int code = OMMB200_ERR_INVALID_ARG) {
   if (!ok) throw Error(code, msg);
 }
 
