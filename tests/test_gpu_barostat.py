@@ -202,3 +202,24 @@ def test_parameters_and_periodicity_are_validated():
     s.add_force(ommb200.MonteCarloBarostat(1.0, 300.0, 25))
     with pytest.raises(ommb200.InvalidArgument):
         ommb200.Context(s, ommb200.LangevinMiddleIntegrator(300.0, 1.0, 0.001))
+
+
+def test_graph_and_stream_paths_agree_with_volume_moves():
+    # moves every 30 steps: the graph path runs 20-step graphs between moves and drops the
+    # captured graph after every accepted move; it must follow the stream path bit for bit
+    w = synth.water_preset("water-1944")
+    out = []
+    for graph in (True, False):
+        s = systems.water_system(w)
+        bar = ommb200.MonteCarloBarostat(1.0, 300.0, 30)
+        bar.set_random_number_seed(21)
+        s.add_force(bar)
+        ctx = ommb200.Context(s, systems.langevin(seed=9), use_cuda_graph=graph)
+        ctx.set_positions(w.positions)
+        ctx.set_velocities_to_temperature(300.0, seed=6)
+        ctx.step(200)
+        out.append((box_and_positions(ctx), ctx.barostat_stats()))
+    (ba, pa), sa = out[0]
+    (bb, pb), sb = out[1]
+    assert sa["attempted"] == sb["attempted"] == 6
+    assert np.array_equal(ba, bb) and np.array_equal(pa, pb) and sa == sb
