@@ -246,6 +246,40 @@ __device__ __forceinline__ uint32_t entry_mask(const NlistArgs& a, int ai, const
   return m;
 }
 
+// entry_mask restricted to the 16 entries [kb, kb + 16) a lane meets in a halves tile (the
+// other bits stay clear: the pair kernel never reads them).  The entries are read once; each
+// cached partner is compared with all 16, and only as many partners as the particle has.
+__device__ __forceinline__ uint32_t entry_mask_half(const NlistArgs& a, int ai, const Partners& pt,
+                                                    const int* slots, int kb) {
+  if (ai < 0) return kFull;
+  int sk[16];
+  uint32_t m = 0;
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    sk[k] = slots[kb + k];
+    if (sk[k] < 0) m |= 1u << (kb + k);
+  }
+  if (pt.n < 0) {
+    for (int e = a.excl_start[ai]; e < a.excl_start[ai + 1]; ++e) {
+      const int sp = a.atom_slot[a.excl_list[e]];
+#pragma unroll
+      for (int k = 0; k < 16; ++k)
+        if (sk[k] == sp) m |= 1u << (kb + k);
+    }
+    return m;
+  }
+#pragma unroll
+  for (int q = 0; q < kCachedPartners; ++q) {
+    if (q < pt.n) {
+      const int sp = pt.slot[q];
+#pragma unroll
+      for (int k = 0; k < 16; ++k)
+        if (sk[k] == sp) m |= 1u << (kb + k);
+    }
+  }
+  return m;
+}
+
 // Reserve a tile (and a mask slot if any lane needs one) and write its header and masks.
 __device__ __forceinline__ int commit_tile(const NlistArgs& a, int I, int flags, uint32_t mask,
                                            int lane) {
@@ -726,7 +760,8 @@ __global__ void __launch_bounds__(32 * kCtaWarps, 4) nl_lists_cta(NlistArgs a) {
     }
     s_slots[w][lane] = slot;
     __syncwarp();
-    const uint32_t m = entry_mask(a, ai, partners, s_slots[w]);
+    const uint32_t m = k == 0 ? entry_mask(a, ai, partners, s_slots[w])
+                              : entry_mask_half(a, ai, partners, s_slots[w], lane & 16);
     const int t = s_tile0 + k;
     int mslot = -1;
     int flags = flag;
