@@ -6,8 +6,9 @@
 // Lett. 98, 146401 (2007)) G_if = sum_j exp(-eta (r_ij - mu_f)^2) fc(r_ij) over r_ij < rf =
 // 1.2 nm, fc(r) = (cos(pi r / rf) + 1) / 2.
 // Everything here is short-ranged: per 32-slot block a list of the blocks of its segment whose
-// boxes come within rc, then one CTA per block gathers features and I_short (front), visiting
-// each ordered pair from the i side only, so each particle's sums belong to one lane per warp
+// boxes come within rc; one CTA per block sorts those blocks' particles into lists per half of
+// the block (within rf or rc of the half's box) and gathers features and I_short (front),
+// visiting each ordered pair from the i side only, so each particle's sums belong to one lane per warp
 // and meet in a fixed order; or the forces -dE/dx through I_short and the network (back), once
 // per pair with the j side's share committed in fixed point.
 //
@@ -44,8 +45,6 @@ __device__ __forceinline__ float switch_value(float r, float rs, float rc, float
   return 1.f + t * t * t * (-10.f + t * (15.f - 6.f * t));
 }
 
-// gbsa_obc.rs:278-309 with SFU reciprocals and logarithm: the descreening integral H and the
-// derivative factor G (dH/dr = -2 r G) of one ordered pair.
 __device__ __forceinline__ float3 position(const double* pos, int atom) {
   return make_float3((float)pos[3 * atom], (float)pos[3 * atom + 1], (float)pos[3 * atom + 2]);
 }
@@ -143,87 +142,296 @@ __device__ __forceinline__ int list_block(const LearnedGbArgs& a, int I, int q, 
   return *near ? row[q] : row[a.max_nbr - 1 - (q - n_near)];
 }
 
-// e_f = exp(-eta (r - mu_f)^2) for all f from three exponentials: the centre f = 15 and the
-// first ratios of neighbouring Gaussians, which then change by q = exp(-2 eta dmu^2) per step.
-// Every e_f is at most 1 and, for r < 1.2 nm, e_15 stays far above the FP32 range limit.
-__device__ __forceinline__ void gaussians(float r, float q, float* e) {
-  constexpr int c = 15;
-  const float x = r - (kMu0 + c * kDmu);
-  const float a = 2.f * kEta * kDmu * x, b = kEta * kDmu * kDmu;
-  e[c] = __expf(-kEta * x * x);
-  float up = __expf(a - b), down = __expf(-a - b);
-#pragma unroll
-  for (int f = c + 1; f < kNF; ++f) {
-    e[f] = e[f - 1] * up;
-    up *= q;
+// e_f = exp(-eta (r - mu_f)^2) around the centre feature c = 15, x = r - mu_c:
+//   e_{c +- k} = e_c U_+-^k Q_k,  U_+- = exp(+-2 eta dmu x - eta dmu^2),  Q_k = exp(-eta dmu^2 k (k-1)),
+// so one running product per side (three exponentials per pair) and the constants Q_k give all
+// 32.  Every e_f is at most 1, and for r < 1.2 nm the running products stay far inside the FP32
+// range (e_c >= 1e-18, U^k <= 1e30).
+constexpr int kCentre = 15;
+constexpr float kMuC = kMu0 + kCentre * kDmu;
+
+// exp(x), x <= 0, as a constant expression: the Taylor series of exp(x / 2^20), squared 20 times
+// (relative error about 1e-10 for |x| < 50).
+constexpr double const_exp(double x) {
+  const double y = x / 1048576.0;
+  double term = 1.0, sum = 1.0;
+  for (int n = 1; n < 12; ++n) {
+    term *= y / n;
+    sum += term;
   }
+  for (int k = 0; k < 20; ++k) sum *= sum;
+  return sum;
+}
+constexpr float gauss_q(int k) {
+  return (float)const_exp(-(double)kEta * (double)kDmu * (double)kDmu * k * (k - 1));
+}
+// Q_{|f - c|} per feature f
+__constant__ float c_gauss_q[kNF] = {
+    gauss_q(15), gauss_q(14), gauss_q(13), gauss_q(12), gauss_q(11), gauss_q(10), gauss_q(9),
+    gauss_q(8),  gauss_q(7),  gauss_q(6),  gauss_q(5),  gauss_q(4),  gauss_q(3),  gauss_q(2),
+    gauss_q(1),  gauss_q(0),  gauss_q(1),  gauss_q(2),  gauss_q(3),  gauss_q(4),  gauss_q(5),
+    gauss_q(6),  gauss_q(7),  gauss_q(8),  gauss_q(9),  gauss_q(10), gauss_q(11), gauss_q(12),
+    gauss_q(13), gauss_q(14), gauss_q(15), gauss_q(16)};
+
+// e_c and the two ratios U_+ (up) and U_- (down) of a pair at distance r.
+__device__ __forceinline__ void gauss_seeds(float r, float* ec, float* up, float* down) {
+  const float x = r - kMuC;
+  const float a = 2.f * kEta * kDmu * x, b = kEta * kDmu * kDmu;
+  *ec = __expf(-kEta * x * x);
+  *up = __expf(a - b);
+  *down = __expf(-a - b);
+}
+
+// G_f += scale e_f for all f.
+__device__ __forceinline__ void add_gaussians(float r, float scale, float* G) {
+  float ec, up, down;
+  gauss_seeds(r, &ec, &up, &down);
+  const float v0 = ec * scale;
+  G[kCentre] += v0;
+  float v = v0;
 #pragma unroll
-  for (int f = c - 1; f >= 0; --f) {
-    e[f] = e[f + 1] * down;
-    down *= q;
+  for (int f = kCentre + 1; f < kNF; ++f) {
+    v *= up;
+    G[f] = fmaf(v, c_gauss_q[f], G[f]);
+  }
+  v = v0;
+#pragma unroll
+  for (int f = kCentre - 1; f >= 0; --f) {
+    v *= down;
+    G[f] = fmaf(v, c_gauss_q[f], G[f]);
   }
 }
 
-// One CTA per block I, lane = particle i; the CTA's warps share I's near / far list and their
-// partial sums meet in shared memory in a fixed order.  Radial features (near blocks, r < rf)
-// and the switched short-range integral (r < rc) over every particle j != i.
+// With W_f premultiplied by Q_{|f - c|}: s0 = sum_f W_f e_f and t = sum_f W_f e_f mu_f.
+__device__ __forceinline__ void weighted_gaussians(float r, const float* wq, const float* sq,
+                                                   float* s0, float* t) {
+  float ec, up, down;
+  gauss_seeds(r, &ec, &up, &down);
+  float a0 = (wq[kCentre] + sq[kCentre]) * ec;
+  float a1 = a0 * kMuC;
+  float v = ec;
+#pragma unroll
+  for (int f = kCentre + 1; f < kNF; ++f) {
+    v *= up;
+    const float we = (wq[f] + sq[f]) * v;
+    a0 += we;
+    a1 = fmaf(we, kMu0 + f * kDmu, a1);
+  }
+  v = ec;
+#pragma unroll
+  for (int f = kCentre - 1; f >= 0; --f) {
+    v *= down;
+    const float we = (wq[f] + sq[f]) * v;
+    a0 += we;
+    a1 = fmaf(we, kMu0 + f * kDmu, a1);
+  }
+  *s0 = a0;
+  *t = a1;
+}
+
+template <class Real>
+__device__ __forceinline__ float4 slot_pos(const void* posq, int s) {
+  const typename V4<Real>::T4 p = reinterpret_cast<const typename V4<Real>::T4*>(posq)[s];
+  return make_float4((float)p.x, (float)p.y, (float)p.z, 0.f);
+}
+template <class Real>
+__device__ __forceinline__ float2 slot_par(const void* params, int s) {
+  const typename V4<Real>::T2 p = reinterpret_cast<const typename V4<Real>::T2*>(params)[s];
+  return make_float2((float)p.x, (float)p.y);
+}
+
+// Particle-level entry lists of a block I, built a chunk of I's block list at a time in shared
+// memory: every particle j of the chunk's blocks goes to the list of each half of I (slots 0-15,
+// 16-31) whose bounding box it comes within rf of ("near": features and integral) or within rc
+// of ("far": integral only).  A tile then pairs 16 entries of each half's list with that half's
+// 16 particles, so a lane meets only particles near its own half of the block.  The lists are
+// filled in block order by a prefix over the chunk, so every run visits the same pairs in the
+// same order.
+constexpr int kChunk = 16;             // blocks of I's list per chunk
+constexpr int kListCap = 32 * kChunk;  // entries per list per chunk
+enum : int { kNearA, kNearB, kFarA, kFarB };
+constexpr float kListMargin = 1e-4f;   // nm added to both cutoffs for the box tests
+
+// Centre and half extents of the two halves of block I (negative half extent: empty half).
+struct HalfBoxes {
+  float3 c[2], h[2];
+};
+
+struct EntryLists {
+  HalfBoxes box;  // the two halves of I
+  int slot[4][kListCap];
+  unsigned bits[kChunk][4];
+  int pre[4][kChunk + 1];
+  int block[kChunk];
+};
+
+__device__ __forceinline__ HalfBoxes half_boxes(float3 p, bool valid) {
+  float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  if (valid) {
+    lo[0] = hi[0] = p.x;
+    lo[1] = hi[1] = p.y;
+    lo[2] = hi[2] = p.z;
+  }
+  for (int o = 8; o > 0; o >>= 1)
+    for (int d = 0; d < 3; ++d) {
+      lo[d] = fminf(lo[d], __shfl_xor_sync(kFull, lo[d], o));
+      hi[d] = fmaxf(hi[d], __shfl_xor_sync(kFull, hi[d], o));
+    }
+  HalfBoxes b;
+  for (int h = 0; h < 2; ++h) {
+    float l[3], u[3];
+    for (int d = 0; d < 3; ++d) {
+      l[d] = __shfl_sync(kFull, lo[d], 16 * h);
+      u[d] = __shfl_sync(kFull, hi[d], 16 * h);
+    }
+    const bool empty = l[0] > u[0];
+    b.c[h] = make_float3(0.5f * (l[0] + u[0]), 0.5f * (l[1] + u[1]), 0.5f * (l[2] + u[2]));
+    b.h[h] = empty ? make_float3(-1.f, -1.f, -1.f)
+                   : make_float3(0.5f * (u[0] - l[0]), 0.5f * (u[1] - l[1]), 0.5f * (u[2] - l[2]));
+  }
+  return b;
+}
+
+__device__ __forceinline__ float box_gap2(float3 p, float3 c, float3 h) {
+  const float gx = fmaxf(fabsf(p.x - c.x) - h.x, 0.f);
+  const float gy = fmaxf(fabsf(p.y - c.y) - h.y, 0.f);
+  const float gz = fmaxf(fabsf(p.z - c.z) - h.z, 0.f);
+  return gx * gx + gy * gy + gz * gz;
+}
+
+// Fills L with the entries of blocks q0 .. q0 + kChunk - 1 of I's list (blocks below I skipped
+// when `upper`) and returns the number of blocks taken.  Ends with the CTA synchronised.
+template <class Real>
+__device__ int build_entry_lists(const LearnedGbArgs& a, const GbArgs& g, int I, int q0, int nn,
+                                 int n_near, bool upper, EntryLists& L) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int nq = min(kChunk, nn - q0);
+  const float rc_m = a.rc + kListMargin, rf_m = a.rf + kListMargin;
+  const float rc2 = rc_m * rc_m, rf2 = rf_m * rf_m;
+  for (int qq = w; qq < nq; qq += kWarps) {
+    bool unused;
+    const int J = list_block(a, I, q0 + qq, n_near, &unused);
+    bool in[4] = {false, false, false, false};
+    if (!(upper && J < I)) {
+      const int aj = g.slot_atom[32 * J + lane];
+      const float4 p4 = slot_pos<Real>(g.posq, 32 * J + lane);
+      if (aj >= 0) {
+        const float3 p = make_float3(p4.x, p4.y, p4.z);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const float3 hh = L.box.h[h];
+          if (hh.x < 0.f) continue;
+          const float gap2 = box_gap2(p, L.box.c[h], hh);
+          in[kNearA + h] = gap2 < rf2;
+          in[kFarA + h] = gap2 >= rf2 && gap2 < rc2;
+        }
+      }
+    }
+    const unsigned b0 = __ballot_sync(kFull, in[0]), b1 = __ballot_sync(kFull, in[1]);
+    const unsigned b2 = __ballot_sync(kFull, in[2]), b3 = __ballot_sync(kFull, in[3]);
+    if (lane == 0) {
+      L.bits[qq][0] = b0;
+      L.bits[qq][1] = b1;
+      L.bits[qq][2] = b2;
+      L.bits[qq][3] = b3;
+      L.block[qq] = J;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    int s = 0;
+    for (int qq = 0; qq < nq; ++qq) {
+      L.pre[threadIdx.x][qq] = s;
+      s += __popc(L.bits[qq][threadIdx.x]);
+    }
+    L.pre[threadIdx.x][nq] = s;
+  }
+  __syncthreads();
+  const unsigned below = (1u << lane) - 1u;
+  for (int qq = w; qq < nq; qq += kWarps) {
+    const int slot = 32 * L.block[qq] + lane;
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+      const unsigned b = L.bits[qq][l];
+      if ((b >> lane) & 1u) L.slot[l][L.pre[l][qq] + __popc(b & below)] = slot;
+    }
+  }
+  __syncthreads();
+  return nq;
+}
+
+// One CTA per block I, lane = particle i; the CTA's warps share I's entry lists (one tile of 16
+// entries per half at a time) and their partial sums meet in shared memory in a fixed order.
+// Radial features (near entries, r < rf) and the switched short-range integral (r < rc) over
+// every particle j != i.
+template <class Real>
 __global__ void __launch_bounds__(32 * kWarps) lr_features(LearnedGbArgs a, GbArgs g) {
   if (!a.state->need) return;
-  __shared__ float4 s_pos[kWarps][32];  // xyz, 1 for a particle / 0 for padding
+  __shared__ EntryLists s_lists;
+  __shared__ float4 s_pos[kWarps][32];  // xyz, slot as int bits (-1: no entry)
   __shared__ float s_scaled[kWarps][32];
   __shared__ float s_red[kWarps][32][kNF + 1];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int hbase = lane & 16;
   const float rc2 = a.rc * a.rc, rf2 = a.rf * a.rf;
-  const float q = __expf(-2.f * kEta * kDmu * kDmu);
   const float fc_k = kPiF / a.rf;
   for (int I = blockIdx.x; I < a.n_blocks; I += gridDim.x) {
-    const int ai = g.slot_atom[32 * I + lane];
-    float3 pi = make_float3(0.f, 0.f, 0.f);
-    float off_i = 1.f;
-    if (ai >= 0) {
-      pi = position(g.pos, ai);
-      off_i = (float)(g.radius[ai] - kDielectricOffset);
+    const int si = 32 * I + lane;
+    const int ai = g.slot_atom[si];
+    const float4 p4 = slot_pos<Real>(g.posq, si);
+    const float3 pi = make_float3(p4.x, p4.y, p4.z);
+    const float off_i = ai >= 0 ? slot_par<Real>(g.params, si).x : 1.f;
+    {
+      const HalfBoxes boxes = half_boxes(pi, ai >= 0);
+      if (threadIdx.x == 0) s_lists.box = boxes;
     }
+    __syncthreads();
     float G[kNF];
 #pragma unroll
     for (int f = 0; f < kNF; ++f) G[f] = 0.f;
     float ishort = 0.f;
     const int n_near = a.nbr_count[2 * I], nn = n_near + a.nbr_count[2 * I + 1];
-    for (int it = w; it < nn; it += kWarps) {
-      bool near;
-      const int J = list_block(a, I, it, n_near, &near);
-      const int aj = g.slot_atom[32 * J + lane];
-      if (aj >= 0) {
-        const float3 p = position(g.pos, aj);
-        s_pos[w][lane] = make_float4(p.x, p.y, p.z, 1.f);
-        s_scaled[w][lane] = (float)((g.radius[aj] - kDielectricOffset) * g.scale[aj]);
-      } else {
-        s_pos[w][lane] = make_float4(0.f, 0.f, 0.f, 0.f);
-        s_scaled[w][lane] = 0.f;
-      }
-      __syncwarp();
-      if (ai >= 0) {
-        for (int k = 0; k < 32; ++k) {
-          const int jl = (lane + k) & 31;
-          const float4 pj = s_pos[w][jl];
-          if (pj.w == 0.f || (J == I && jl == lane)) continue;
-          const float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
-          const float r2 = dx * dx + dy * dy + dz * dz;
-          if (r2 >= rc2) continue;
-          const float inv_r = rsqrt_r(r2), r = r2 * inv_r;
-          float ds, h, gr;
-          const float sw = switch_value(r, a.rs, a.rc, &ds);
-          descreening_fast(off_i, s_scaled[w][jl], r, inv_r, &h, &gr);
-          ishort = fmaf(h, sw, ishort);
-          if (!near || r2 >= rf2) continue;
-          const float fc = 0.5f * (__cosf(fc_k * r) + 1.f);  // SFU cosine
-          float e[kNF];
-          gaussians(r, q, e);
-#pragma unroll
-          for (int f = 0; f < kNF; ++f) G[f] = fmaf(e[f], fc, G[f]);
+    for (int q0 = 0; q0 < nn; q0 += kChunk) {
+      const int nq = build_entry_lists<Real>(a, g, I, q0, nn, n_near, false, s_lists);
+      const int n_na = s_lists.pre[kNearA][nq], n_nb = s_lists.pre[kNearB][nq];
+      const int n_fa = s_lists.pre[kFarA][nq], n_fb = s_lists.pre[kFarB][nq];
+      const int t_near = (max(n_na, n_nb) + 15) >> 4, t_far = (max(n_fa, n_fb) + 15) >> 4;
+      for (int t = w; t < t_near + t_far; t += kWarps) {
+        const bool near = t < t_near;  // uniform over the warp
+        const int list = (near ? kNearA : kFarA) + (lane >> 4);
+        const int e = 16 * (near ? t : t - t_near) + (lane & 15);
+        const int slot = e < s_lists.pre[list][nq] ? s_lists.slot[list][e] : -1;
+        if (slot >= 0) {
+          const float4 p = slot_pos<Real>(g.posq, slot);
+          s_pos[w][lane] = make_float4(p.x, p.y, p.z, __int_as_float(slot));
+          s_scaled[w][lane] = slot_par<Real>(g.params, slot).y;
+        } else {
+          s_pos[w][lane] = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+          s_scaled[w][lane] = 0.f;
         }
+        __syncwarp();
+        if (ai >= 0) {
+          for (int k = 0; k < 16; ++k) {
+            const int jl = hbase | ((lane + k) & 15);
+            const float4 pj = s_pos[w][jl];
+            const int sj = __float_as_int(pj.w);
+            if (sj < 0 || sj == si) continue;
+            const float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
+            const float r2 = dx * dx + dy * dy + dz * dz;
+            if (r2 >= rc2) continue;
+            const float inv_r = rsqrt_r(r2), r = r2 * inv_r;
+            float ds, h, gr;
+            const float sw = switch_value(r, a.rs, a.rc, &ds);
+            descreening_fast(off_i, s_scaled[w][jl], r, inv_r, &h, &gr);
+            ishort = fmaf(h, sw, ishort);
+            if (!near || r2 >= rf2) continue;
+            const float fc = 0.5f * (__cosf(fc_k * r) + 1.f);  // SFU cosine
+            add_gaussians(r, fc, G);
+          }
+        }
+        __syncwarp();
       }
-      __syncwarp();
+      __syncthreads();  // the next chunk refills the lists
     }
 #pragma unroll
     for (int f = 0; f < kNF; ++f) s_red[w][lane][f] = G[f];
@@ -250,116 +458,122 @@ __global__ void __launch_bounds__(32 * kWarps) lr_features(LearnedGbArgs a, GbAr
 // One CTA per block I as above: F_i = sum_j (D_i Phi'_ij + D_j Phi'_ji) / r d_ij,
 // Phi_ij = H(r; i, j) S(r) + sum_f (d tail_i / d G_if) g_f(r), D = dE/dI (half the chain
 // value the GB chain kernel leaves per slot).  The pair term is symmetric in i and j, so each
-// pair of blocks is done once, from the lower block (J >= I in I's list): the force on each
-// entry of J travels with it one lane per warp shuffle and is committed in fixed point after
-// the 32 steps; the self block visits each pair from both sides and keeps i-forces only.
+// pair is done once, from the lower block (entries of blocks J >= I only): the force on each
+// entry travels with it one lane per warp shuffle within its half and is committed in fixed
+// point after the 16 steps; pairs inside block I are visited from both sides and keep their
+// i-forces only.
 template <class Real>
-__global__ void __launch_bounds__(32 * kWarps) lr_forces(LearnedGbArgs a, GbArgs g) {
+__global__ void __launch_bounds__(32 * kWarps, 5) lr_forces(LearnedGbArgs a, GbArgs g) {
   if (!a.state->use_learned) return;
-  __shared__ float4 s_pos[kWarps][32];
-  __shared__ float4 s_par[kWarps][32];        // offset radius, scaled radius, D, valid
-  __shared__ float s_w[kWarps][32][kNF + 1];  // D_j d tail_j / d G_j (padded rows)
+  __shared__ EntryLists s_lists;
+  __shared__ float4 s_pos[kWarps][32];        // xyz, slot as int bits (-1: no entry)
+  __shared__ float4 s_par[kWarps][32];        // offset radius, scaled radius, D
+  __shared__ float s_w[kWarps][32][kNF + 1];  // D_j d tail_j / d G_jf times Q_{|f - c|} (padded rows)
   __shared__ float s_red[kWarps][32][3];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int hbase = lane & 16;
   const float rc2 = a.rc * a.rc, rf2 = a.rf * a.rf;
   const Real* chain = reinterpret_cast<const Real*>(g.dedr_slot);
   const float fc_k = kPiF / a.rf;
-  const float q = __expf(-2.f * kEta * kDmu * kDmu);
   const float fscale = (float)kForceScale;
   for (int I = blockIdx.x; I < a.n_blocks; I += gridDim.x) {
     const int si = 32 * I + lane;
     const int ai = g.slot_atom[si];
-    float3 pi = make_float3(0.f, 0.f, 0.f);
+    const float4 p4 = slot_pos<Real>(g.posq, si);
+    const float3 pi = make_float3(p4.x, p4.y, p4.z);
     float off_i = 1.f, sc_i = 0.f, d_i = 0.f;
-    float wi[kNF];
+    float wi[kNF];  // D_i d tail_i / d G_if, times Q_{|f - c|}
 #pragma unroll
     for (int f = 0; f < kNF; ++f) wi[f] = 0.f;
     if (ai >= 0) {
-      pi = position(g.pos, ai);
-      off_i = (float)(g.radius[ai] - kDielectricOffset);
-      sc_i = (float)((g.radius[ai] - kDielectricOffset) * g.scale[ai]);
+      const float2 par = slot_par<Real>(g.params, si);
+      off_i = par.x;
+      sc_i = par.y;
       d_i = 0.5f * (float)chain[si];
       const float4* dt = reinterpret_cast<const float4*>(a.dtail + (size_t)ai * kNF);
 #pragma unroll
       for (int qq = 0; qq < kNF / 4; ++qq) {
         const float4 v = dt[qq];
-        wi[4 * qq] = d_i * v.x;
-        wi[4 * qq + 1] = d_i * v.y;
-        wi[4 * qq + 2] = d_i * v.z;
-        wi[4 * qq + 3] = d_i * v.w;
+        wi[4 * qq] = d_i * v.x * c_gauss_q[4 * qq];
+        wi[4 * qq + 1] = d_i * v.y * c_gauss_q[4 * qq + 1];
+        wi[4 * qq + 2] = d_i * v.z * c_gauss_q[4 * qq + 2];
+        wi[4 * qq + 3] = d_i * v.w * c_gauss_q[4 * qq + 3];
       }
     }
+    {
+      const HalfBoxes boxes = half_boxes(pi, ai >= 0);
+      if (threadIdx.x == 0) s_lists.box = boxes;
+    }
+    __syncthreads();
     float fx = 0.f, fy = 0.f, fz = 0.f;
     const int n_near = a.nbr_count[2 * I], nn = n_near + a.nbr_count[2 * I + 1];
-    for (int it = w; it < nn; it += kWarps) {
-      bool near;
-      const int J = list_block(a, I, it, n_near, &near);
-      if (J < I) continue;  // done from block J's side
-      const bool self = J == I;
-      const int sj = 32 * J + lane;
-      const int aj = g.slot_atom[sj];
-      if (aj >= 0) {
-        const float3 p = position(g.pos, aj);
-        const float off = (float)(g.radius[aj] - kDielectricOffset);
-        const float dj = 0.5f * (float)chain[sj];
-        s_pos[w][lane] = make_float4(p.x, p.y, p.z, 1.f);
-        s_par[w][lane] = make_float4(off, (float)((g.radius[aj] - kDielectricOffset) * g.scale[aj]),
-                                     dj, 1.f);
-        if (near) {
-          const float4* dt = reinterpret_cast<const float4*>(a.dtail + (size_t)aj * kNF);
+    for (int q0 = 0; q0 < nn; q0 += kChunk) {
+      const int nq = build_entry_lists<Real>(a, g, I, q0, nn, n_near, true, s_lists);
+      const int n_na = s_lists.pre[kNearA][nq], n_nb = s_lists.pre[kNearB][nq];
+      const int n_fa = s_lists.pre[kFarA][nq], n_fb = s_lists.pre[kFarB][nq];
+      const int t_near = (max(n_na, n_nb) + 15) >> 4, t_far = (max(n_fa, n_fb) + 15) >> 4;
+      for (int t = w; t < t_near + t_far; t += kWarps) {
+        const bool near = t < t_near;  // uniform over the warp
+        const int list = (near ? kNearA : kFarA) + (lane >> 4);
+        const int e = 16 * (near ? t : t - t_near) + (lane & 15);
+        const int slot = e < s_lists.pre[list][nq] ? s_lists.slot[list][e] : -1;
+        int aj = -1;
+        if (slot >= 0) {
+          aj = g.slot_atom[slot];
+          const float4 p = slot_pos<Real>(g.posq, slot);
+          const float2 par = slot_par<Real>(g.params, slot);
+          const float dj = 0.5f * (float)chain[slot];
+          s_pos[w][lane] = make_float4(p.x, p.y, p.z, __int_as_float(slot));
+          s_par[w][lane] = make_float4(par.x, par.y, dj, 0.f);
+          if (near) {
+            const float4* dt = reinterpret_cast<const float4*>(a.dtail + (size_t)aj * kNF);
 #pragma unroll
-          for (int qq = 0; qq < kNF / 4; ++qq) {
-            const float4 v = dt[qq];
-            s_w[w][lane][4 * qq] = dj * v.x;
-            s_w[w][lane][4 * qq + 1] = dj * v.y;
-            s_w[w][lane][4 * qq + 2] = dj * v.z;
-            s_w[w][lane][4 * qq + 3] = dj * v.w;
-          }
-        }
-      } else {
-        s_pos[w][lane] = make_float4(0.f, 0.f, 0.f, 0.f);
-        s_par[w][lane] = make_float4(1.f, 0.f, 0.f, 0.f);
-      }
-      __syncwarp();
-      float gx = 0.f, gy = 0.f, gz = 0.f;  // force on the entry now in this lane's rotation
-      const int src = (lane + 1) & 31;
-      for (int k = self ? 1 : 0; k < 32; ++k) {
-        const int jl = (lane + k) & 31;
-        const float4 pj = s_pos[w][jl];
-        const float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
-        const float r2 = dx * dx + dy * dy + dz * dz;
-        float radial = 0.f;
-        if (ai >= 0 && pj.w != 0.f && r2 < rc2) {
-          const float inv_r = rsqrt_r(r2), r = r2 * inv_r;
-          const float4 pr = s_par[w][jl];
-          float ds, hij, hji, gij, gji;
-          const float sw = switch_value(r, a.rs, a.rc, &ds);
-          // dH/dr = -2 r descreening_gradient (gbsa_obc.rs:297-309)
-          descreening_fast(off_i, pr.y, r, inv_r, &hij, &gij);
-          descreening_fast(pr.x, sc_i, r, inv_r, &hji, &gji);
-          float phi = d_i * (-2.f * r * gij * sw + hij * ds) + pr.z * (-2.f * r * gji * sw + hji * ds);
-          if (near && r2 < rf2) {
-            float sn, cs;
-            __sincosf(fc_k * r, &sn, &cs);  // SFU sine and cosine
-            const float fc = 0.5f * (cs + 1.f), dfc = -0.5f * fc_k * sn;
-            float e[kNF];
-            gaussians(r, q, e);
-            // sum_f W_f g_f'(r),  g_f' = e_f (-2 eta (r - mu_f) fc + dfc)
-            float s0 = 0.f, s1 = 0.f;
-#pragma unroll
-            for (int f = 0; f < kNF; ++f) {
-              const float we = (wi[f] + s_w[w][jl][f]) * e[f];
-              s0 += we;
-              s1 = fmaf(we, r - (kMu0 + f * kDmu), s1);
+            for (int qq = 0; qq < kNF / 4; ++qq) {
+              const float4 v = dt[qq];
+              s_w[w][lane][4 * qq] = dj * v.x * c_gauss_q[4 * qq];
+              s_w[w][lane][4 * qq + 1] = dj * v.y * c_gauss_q[4 * qq + 1];
+              s_w[w][lane][4 * qq + 2] = dj * v.z * c_gauss_q[4 * qq + 2];
+              s_w[w][lane][4 * qq + 3] = dj * v.w * c_gauss_q[4 * qq + 3];
             }
-            phi += dfc * s0 - 2.f * kEta * fc * s1;
           }
-          radial = phi * inv_r;
+        } else {
+          s_pos[w][lane] = make_float4(0.f, 0.f, 0.f, __int_as_float(-1));
+          s_par[w][lane] = make_float4(1.f, 0.f, 0.f, 0.f);
         }
-        fx = fmaf(radial, dx, fx);
-        fy = fmaf(radial, dy, fy);
-        fz = fmaf(radial, dz, fz);
-        if (!self) {
+        __syncwarp();
+        float gx = 0.f, gy = 0.f, gz = 0.f;  // force on the entry now in this lane's rotation
+        const int src = hbase | ((lane + 1) & 15);
+        for (int k = 0; k < 16; ++k) {
+          const int jl = hbase | ((lane + k) & 15);
+          const float4 pj = s_pos[w][jl];
+          const int sj = __float_as_int(pj.w);
+          const float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
+          const float r2 = dx * dx + dy * dy + dz * dz;
+          float radial = 0.f;
+          if (ai >= 0 && sj >= 0 && sj != si && r2 < rc2) {
+            const float inv_r = rsqrt_r(r2), r = r2 * inv_r;
+            const float4 pr = s_par[w][jl];
+            float ds, hij, hji, gij, gji;
+            const float sw = switch_value(r, a.rs, a.rc, &ds);
+            // dH/dr = -2 r descreening_gradient (gbsa_obc.rs:297-309)
+            descreening_fast(off_i, pr.y, r, inv_r, &hij, &gij);
+            descreening_fast(pr.x, sc_i, r, inv_r, &hji, &gji);
+            float phi = d_i * (-2.f * r * gij * sw + hij * ds) + pr.z * (-2.f * r * gji * sw + hji * ds);
+            if (near && r2 < rf2) {
+              float sn, cs;
+              __sincosf(fc_k * r, &sn, &cs);  // SFU sine and cosine
+              const float fc = 0.5f * (cs + 1.f), dfc = -0.5f * fc_k * sn;
+              // sum_f W_f g_f'(r),  g_f' = e_f (-2 eta (r - mu_f) fc + dfc),
+              // with sum_f W_f e_f (r - mu_f) = r s0 - t
+              float s0, t;
+              weighted_gaussians(r, wi, s_w[w][jl], &s0, &t);
+              phi += dfc * s0 - 2.f * kEta * fc * (r * s0 - t);
+            }
+            radial = phi * inv_r;
+          }
+          fx = fmaf(radial, dx, fx);
+          fy = fmaf(radial, dy, fy);
+          fz = fmaf(radial, dz, fz);
           gx = fmaf(-radial, dx, gx);
           gy = fmaf(-radial, dy, gy);
           gz = fmaf(-radial, dz, gz);
@@ -367,13 +581,14 @@ __global__ void __launch_bounds__(32 * kWarps) lr_forces(LearnedGbArgs a, GbArgs
           gy = __shfl_sync(kFull, gy, src);
           gz = __shfl_sync(kFull, gz, src);
         }
+        if (aj >= 0 && (slot >> 5) != I) {
+          add_fixed(g.force + aj, to_fixed(gx, fscale));
+          add_fixed(g.force + g.n_atoms + aj, to_fixed(gy, fscale));
+          add_fixed(g.force + 2 * g.n_atoms + aj, to_fixed(gz, fscale));
+        }
+        __syncwarp();
       }
-      if (!self && aj >= 0) {
-        add_fixed(g.force + aj, to_fixed(gx, fscale));
-        add_fixed(g.force + g.n_atoms + aj, to_fixed(gy, fscale));
-        add_fixed(g.force + 2 * g.n_atoms + aj, to_fixed(gz, fscale));
-      }
-      __syncwarp();
+      __syncthreads();  // the next chunk refills the lists
     }
     s_red[w][lane][0] = fx;
     s_red[w][lane][1] = fy;
@@ -527,7 +742,7 @@ void launch_learned_phase(const LearnedGbArgs& a, const GbArgs& g, int phase, in
       lr_neighbors<<<wb, 128, 0, s>>>(a);
       break;
     case kLrFeatures:
-      lr_features<<<ctas, 32 * kWarps, 0, s>>>(a, g);
+      lr_features<Real><<<ctas, 32 * kWarps, 0, s>>>(a, g);
       break;
     case kLrInfer:
       launch_mlp_infer(a.n_atoms, a.features, a.params, a.tail, a.dtail, a.status, sm_count, s,
