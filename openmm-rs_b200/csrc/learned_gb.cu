@@ -182,46 +182,65 @@ __device__ __forceinline__ void gauss_seeds(float r, float* ec, float* up, float
   *down = __expf(-a - b);
 }
 
-// G_f += scale e_f for all f.
+// G_f += scale e_f for all f.  Each side runs two products (odd and even steps, ratio U^2), which
+// halves the dependent chain.
 __device__ __forceinline__ void add_gaussians(float r, float scale, float* G) {
   float ec, up, down;
   gauss_seeds(r, &ec, &up, &down);
   const float v0 = ec * scale;
   G[kCentre] += v0;
-  float v = v0;
+  const float up2 = up * up, down2 = down * down;
+  float va = v0 * up, vb = v0 * up2;
 #pragma unroll
-  for (int f = kCentre + 1; f < kNF; ++f) {
-    v *= up;
-    G[f] = fmaf(v, c_gauss_q[f], G[f]);
+  for (int k = 1; kCentre + k < kNF; k += 2) {
+    G[kCentre + k] = fmaf(va, c_gauss_q[kCentre + k], G[kCentre + k]);
+    if (kCentre + k + 1 < kNF)
+      G[kCentre + k + 1] = fmaf(vb, c_gauss_q[kCentre + k + 1], G[kCentre + k + 1]);
+    va *= up2;
+    vb *= up2;
   }
-  v = v0;
+  va = v0 * down;
+  vb = v0 * down2;
 #pragma unroll
-  for (int f = kCentre - 1; f >= 0; --f) {
-    v *= down;
-    G[f] = fmaf(v, c_gauss_q[f], G[f]);
+  for (int k = 1; kCentre - k >= 0; k += 2) {
+    G[kCentre - k] = fmaf(va, c_gauss_q[kCentre - k], G[kCentre - k]);
+    if (kCentre - k - 1 >= 0)
+      G[kCentre - k - 1] = fmaf(vb, c_gauss_q[kCentre - k - 1], G[kCentre - k - 1]);
+    va *= down2;
+    vb *= down2;
   }
 }
 
-// With W_f premultiplied by Q_{|f - c|}: s0 = sum_f W_f e_f and t = sum_f W_f e_f mu_f.
-__device__ __forceinline__ void weighted_gaussians(float r, const float* wq, const float* sq,
+__device__ __forceinline__ float component(const float4& v, int c) {
+  return c == 0 ? v.x : (c == 1 ? v.y : (c == 2 ? v.z : v.w));
+}
+
+// With W_f premultiplied by Q_{|f - c|} (own weights wq in registers, the partner's sq as 16-byte
+// aligned shared rows): s0 = sum_f W_f e_f and t = sum_f W_f e_f mu_f.  Two products per side
+// as in add_gaussians.
+__device__ __forceinline__ void weighted_gaussians(float r, const float* wq, const float4* sq,
                                                    float* s0, float* t) {
   float ec, up, down;
   gauss_seeds(r, &ec, &up, &down);
-  float a0 = (wq[kCentre] + sq[kCentre]) * ec;
+  float a0 = (wq[kCentre] + component(sq[kCentre >> 2], kCentre & 3)) * ec;
   float a1 = a0 * kMuC;
-  float v = ec;
+  const float up2 = up * up, down2 = down * down;
+  float v[2] = {ec * up, ec * up2};
 #pragma unroll
   for (int f = kCentre + 1; f < kNF; ++f) {
-    v *= up;
-    const float we = (wq[f] + sq[f]) * v;
+    const int p = (f - kCentre - 1) & 1;
+    const float we = (wq[f] + component(sq[f >> 2], f & 3)) * v[p];
+    v[p] *= up2;
     a0 += we;
     a1 = fmaf(we, kMu0 + f * kDmu, a1);
   }
-  v = ec;
+  v[0] = ec * down;
+  v[1] = ec * down2;
 #pragma unroll
   for (int f = kCentre - 1; f >= 0; --f) {
-    v *= down;
-    const float we = (wq[f] + sq[f]) * v;
+    const int p = (kCentre - 1 - f) & 1;
+    const float we = (wq[f] + component(sq[f >> 2], f & 3)) * v[p];
+    v[p] *= down2;
     a0 += we;
     a1 = fmaf(we, kMu0 + f * kDmu, a1);
   }
@@ -338,13 +357,19 @@ __device__ int build_entry_lists(const LearnedGbArgs& a, const GbArgs& g, int I,
     }
   }
   __syncthreads();
-  if (threadIdx.x < 4) {
-    int s = 0;
-    for (int qq = 0; qq < nq; ++qq) {
-      L.pre[threadIdx.x][qq] = s;
-      s += __popc(L.bits[qq][threadIdx.x]);
+  if (w == 0) {  // exclusive prefix of the four lists' counts over the chunk's blocks (nq <= 32)
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+      const int c = lane < nq ? __popc(L.bits[lane][l]) : 0;
+      int incl = c;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += y;
+      }
+      if (lane < nq) L.pre[l][lane] = incl - c;
+      if (lane == nq - 1) L.pre[l][nq] = incl;
     }
-    L.pre[threadIdx.x][nq] = s;
   }
   __syncthreads();
   const unsigned below = (1u << lane) - 1u;
@@ -411,6 +436,7 @@ __global__ void __launch_bounds__(32 * kWarps) lr_features(LearnedGbArgs a, GbAr
         }
         __syncwarp();
         if (ai >= 0) {
+#pragma unroll 2
           for (int k = 0; k < 16; ++k) {
             const int jl = hbase | ((lane + k) & 15);
             const float4 pj = s_pos[w][jl];
@@ -468,7 +494,9 @@ __global__ void __launch_bounds__(32 * kWarps, 5) lr_forces(LearnedGbArgs a, GbA
   __shared__ EntryLists s_lists;
   __shared__ float4 s_pos[kWarps][32];        // xyz, slot as int bits (-1: no entry)
   __shared__ float4 s_par[kWarps][32];        // offset radius, scaled radius, D
-  __shared__ float s_w[kWarps][32][kNF + 1];  // D_j d tail_j / d G_jf times Q_{|f - c|} (padded rows)
+  // D_j d tail_j / d G_jf times Q_{|f - c|}; rows of kNF + 4 floats stay 16-byte aligned for
+  // vector access, and the rows of 8 consecutive entries fall in distinct banks
+  __shared__ __align__(16) float s_w[kWarps][32][kNF + 4];
   __shared__ float s_red[kWarps][32][3];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int hbase = lane & 16;
@@ -527,13 +555,12 @@ __global__ void __launch_bounds__(32 * kWarps, 5) lr_forces(LearnedGbArgs a, GbA
           s_par[w][lane] = make_float4(par.x, par.y, dj, 0.f);
           if (near) {
             const float4* dt = reinterpret_cast<const float4*>(a.dtail + (size_t)aj * kNF);
+            float4* row = reinterpret_cast<float4*>(s_w[w][lane]);
 #pragma unroll
             for (int qq = 0; qq < kNF / 4; ++qq) {
               const float4 v = dt[qq];
-              s_w[w][lane][4 * qq] = dj * v.x * c_gauss_q[4 * qq];
-              s_w[w][lane][4 * qq + 1] = dj * v.y * c_gauss_q[4 * qq + 1];
-              s_w[w][lane][4 * qq + 2] = dj * v.z * c_gauss_q[4 * qq + 2];
-              s_w[w][lane][4 * qq + 3] = dj * v.w * c_gauss_q[4 * qq + 3];
+              row[qq] = make_float4(dj * v.x * c_gauss_q[4 * qq], dj * v.y * c_gauss_q[4 * qq + 1],
+                                    dj * v.z * c_gauss_q[4 * qq + 2], dj * v.w * c_gauss_q[4 * qq + 3]);
             }
           }
         } else {
@@ -566,7 +593,7 @@ __global__ void __launch_bounds__(32 * kWarps, 5) lr_forces(LearnedGbArgs a, GbA
               // sum_f W_f g_f'(r),  g_f' = e_f (-2 eta (r - mu_f) fc + dfc),
               // with sum_f W_f e_f (r - mu_f) = r s0 - t
               float s0, t;
-              weighted_gaussians(r, wi, s_w[w][jl], &s0, &t);
+              weighted_gaussians(r, wi, reinterpret_cast<const float4*>(s_w[w][jl]), &s0, &t);
               phi += dfc * s0 - 2.f * kEta * fc * (r * s0 - t);
             }
             radial = phi * inv_r;
