@@ -215,37 +215,32 @@ __device__ __forceinline__ float component(const float4& v, int c) {
   return c == 0 ? v.x : (c == 1 ? v.y : (c == 2 ? v.z : v.w));
 }
 
-// With W_f premultiplied by Q_{|f - c|} (own weights wq in registers, the partner's sq as 16-byte
-// aligned shared rows): s0 = sum_f W_f e_f and t = sum_f W_f e_f mu_f.  Two products per side
-// as in add_gaussians.
+// s0 = sum_f W_f e_f and t = sum_f W_f e_f mu_f for the pair weights W_f = W_if + W_jf, given
+// premultiplied as A_f = W_f Q_{|f - c|} (own part wq in registers, the partner's sq as 16-byte
+// aligned shared rows).  With e_{c +- k} = e_c U_+-^k Q_k, U = U_+, D = U_-:
+//   s0 = e_c S,  S = A_c + U P_+(U) + D P_-(D),  P_+(U) = sum_{k>=1} A_{c+k} U^(k-1)  (likewise P_-),
+//   t  = e_c (mu_c S + dmu (U (P_+ + U P_+') - D (P_- + D P_-'))),
+// the polynomials and their derivatives by Horner's rule: three operations per feature.
 __device__ __forceinline__ void weighted_gaussians(float r, const float* wq, const float4* sq,
                                                    float* s0, float* t) {
   float ec, up, down;
   gauss_seeds(r, &ec, &up, &down);
-  float a0 = (wq[kCentre] + component(sq[kCentre >> 2], kCentre & 3)) * ec;
-  float a1 = a0 * kMuC;
-  const float up2 = up * up, down2 = down * down;
-  float v[2] = {ec * up, ec * up2};
+  float pu = wq[kNF - 1] + component(sq[(kNF - 1) >> 2], (kNF - 1) & 3), du = 0.f;
 #pragma unroll
-  for (int f = kCentre + 1; f < kNF; ++f) {
-    const int p = (f - kCentre - 1) & 1;
-    const float we = (wq[f] + component(sq[f >> 2], f & 3)) * v[p];
-    v[p] *= up2;
-    a0 += we;
-    a1 = fmaf(we, kMu0 + f * kDmu, a1);
+  for (int f = kNF - 2; f > kCentre; --f) {
+    du = fmaf(du, up, pu);
+    pu = fmaf(pu, up, wq[f] + component(sq[f >> 2], f & 3));
   }
-  v[0] = ec * down;
-  v[1] = ec * down2;
+  float pd = wq[0] + component(sq[0], 0), dd = 0.f;
 #pragma unroll
-  for (int f = kCentre - 1; f >= 0; --f) {
-    const int p = (kCentre - 1 - f) & 1;
-    const float we = (wq[f] + component(sq[f >> 2], f & 3)) * v[p];
-    v[p] *= down2;
-    a0 += we;
-    a1 = fmaf(we, kMu0 + f * kDmu, a1);
+  for (int f = 1; f < kCentre; ++f) {
+    dd = fmaf(dd, down, pd);
+    pd = fmaf(pd, down, wq[f] + component(sq[f >> 2], f & 3));
   }
-  *s0 = a0;
-  *t = a1;
+  const float sum = wq[kCentre] + component(sq[kCentre >> 2], kCentre & 3) + up * pu + down * pd;
+  const float moment = up * fmaf(up, du, pu) - down * fmaf(down, dd, pd);
+  *s0 = ec * sum;
+  *t = ec * fmaf(kMuC, sum, kDmu * moment);
 }
 
 template <class Real>
