@@ -280,6 +280,21 @@ __device__ __forceinline__ uint32_t entry_mask_half(const NlistArgs& a, int ai, 
   return m;
 }
 
+// Position of set bit r (0-based, r < popc(m)) of m: a binary search on the population of the
+// lower half of the remaining window, five steps without branches.
+__device__ __forceinline__ int nth_set_bit(uint32_t m, int r) {
+  int pos = 0;
+#pragma unroll
+  for (int w = 16; w > 0; w >>= 1) {
+    const int c = __popc(m & ((1u << w) - 1u));
+    const bool up = r >= c;
+    r -= up ? c : 0;
+    m = up ? m >> w : m;
+    pos += up ? w : 0;
+  }
+  return pos;
+}
+
 // Reserve a tile (and a mask slot if any lane needs one) and write its header and masks.
 __device__ __forceinline__ int commit_tile(const NlistArgs& a, int I, int flags, uint32_t mask,
                                            int lane) {
@@ -747,9 +762,7 @@ __global__ void __launch_bounds__(32 * kCtaWarps, 4) nl_lists_cta(NlistArgs a) {
           if (my_pre[mid] <= e) lo = mid;
           else hi_c = mid - 1;
         }
-        uint32_t mm = my_mask[lo];  // drop the e - pre[lo] lowest set bits
-        for (int r = e - my_pre[lo]; r > 0; --r) mm &= mm - 1u;
-        const int bit = __ffs(mm) - 1;
+        const int bit = nth_set_bit(my_mask[lo], e - my_pre[lo]);
         slot = 32 * c_J[lo] + bit;
         flag = c_un[lo] ? kTilePairImage : 0;
         sh[0] = c_d[lo];

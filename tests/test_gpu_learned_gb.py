@@ -92,6 +92,48 @@ def test_learned_forces_and_energy_match_oracle(precision):
         assert abs(pot[k] - e_ref) < 2e-5 * abs(e_ref)
 
 
+def compact_globule(n, seed, spacing=0.3):
+    """n particles on a jittered cubic lattice filling a ball: every 32-particle block lies
+    within the 2 nm integral cutoff of most others, so a block's neighbour list runs over
+    several of the kernels' 16-block chunks."""
+    rng = np.random.default_rng(seed)
+    m = int(np.ceil((6 * n / np.pi) ** (1 / 3))) + 2
+    g = (np.stack(np.meshgrid(*[np.arange(m)] * 3, indexing="ij"), -1).reshape(-1, 3)
+         - (m - 1) / 2) * spacing
+    g = g[np.argsort((g ** 2).sum(1), kind="stable")][:n]
+    pos = g + rng.uniform(-0.03, 0.03, g.shape)
+    q = rng.normal(0.0, 0.3, n)
+    return synth.Chain(positions=pos, charges=q - q.mean(), radii=rng.uniform(0.12, 0.2, n))
+
+
+@pytest.mark.parametrize("precision", ["mixed", "double"])
+def test_learned_matches_oracle_when_block_lists_span_chunks(precision):
+    chs = [compact_globule(1200, seed=5)]
+    nb = (1200 + 31) // 32
+    lo = np.array([chs[0].positions[32 * b:32 * b + 32].min(0) for b in range(nb)])
+    hi = np.array([chs[0].positions[32 * b:32 * b + 32].max(0) for b in range(nb)])
+    c, h = (lo + hi) / 2, (hi - lo) / 2
+    gap = np.maximum(np.abs(c[:, None] - c[None]) - h[:, None] - h[None], 0)
+    assert ((gap ** 2).sum(-1) < 4.0).sum(1).max() > 32  # more than two chunks of 16 blocks
+    rng = np.random.default_rng(2)
+    g = O.radial_features(chs[0].positions)
+    n = 1200
+    _, _, _, short, full = O.learned_gbsa(chs[0].positions, chs[0].charges, chs[0].radii,
+                                          np.full(n, chs[0].gb_scale), np.zeros(n),
+                                          np.zeros((n, 32)))
+    p = normalised_params(rng, g, full - short)
+    ctx = gb_only_context(chs, learned={"judge_interval": 1000}, precision=precision)
+    ctx.set_radii_mlp_params(p)
+    st = ctx.get_state(forces=True, energy=True)
+    pot, _ = ctx.system_energies()
+    assert ctx.learned_radii_stats()["active"]
+    f_ref, e_ref, *_ = oracle_learned(chs[0], p)
+    err = float(np.sqrt(((st.forces - f_ref) ** 2).sum() / (f_ref ** 2).sum()))
+    print(f"globule: force rms rel {err:.2e}, E {pot[0]:.6f} vs {e_ref:.6f}")
+    assert err < 2e-4
+    assert abs(pot[0] - e_ref) < 2e-5 * abs(e_ref)
+
+
 def test_judge_trains_and_the_network_gains_over_short_range_alone():
     chs = [synth.chain(1500, seed=11 + k) for k in range(4)]
     learned = {"judge_interval": 25, "radius_tolerance": 0.01, "train_steps": 40}
