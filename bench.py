@@ -845,6 +845,9 @@ def main_learned(args):
     exact.step(500)
     time_segments(exact, torch, args.warmup, seg, flush)
     ms_exact = time_segments(exact, torch, args.steps, seg, flush)
+    exact_kernels = None
+    if rank == 0 and not args.skip_extras:
+        exact_kernels = {k: round(v[0] / 50, 5) for k, v in kernel_profile(exact, 50).items()}
     exact.close()
     ctx = make(learned)
     ctx.step(1000)  # untimed: the first judges fix the normalisation and train the network
@@ -920,6 +923,17 @@ def main_learned(args):
         "clocks": clocks,
         "cpu_baseline": cpu,
     }
+    if exact_kernels is not None and "kernel_ms_per_md_step" in extras:
+        # the Born-radii work each mode does per MD step: the exact descreening passes, or the
+        # learned lists, features, network and forces plus the judges' exact passes and training
+        lk = extras["kernel_ms_per_md_step"]
+        radii = ("gb_descreening", "gb_descreening_forces")
+        exact_ms = sum(exact_kernels.get(k, 0.0) for k in radii)
+        learned_ms = sum(v for k, v in lk.items() if k.startswith("lr_") or k in radii)
+        out["exact_obc"]["kernel_ms_per_md_step"] = exact_kernels
+        out["born_radii_work"] = {"exact_ms_per_md_step": exact_ms,
+                                  "learned_ms_per_md_step": learned_ms,
+                                  "exact_over_learned": exact_ms / learned_ms if learned_ms else None}
     out.update(extras)
     ctx.close()
     close_replicas(world)
