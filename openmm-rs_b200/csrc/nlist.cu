@@ -27,6 +27,19 @@ namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
 
+// atomicAdd(counter, 1) for every calling lane, as one atomic per distinct key among the warp's
+// active lanes (a column's particles meet in few warps, so per-lane atomics on the same counter
+// would serialise); returns the lane's old-value offset like atomicAdd would.
+__device__ __forceinline__ int aggregated_add(int* counter, int key) {
+  const unsigned peers = __match_any_sync(__activemask(), key);
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(peers) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(counter, __popc(peers));
+  base = __shfl_sync(peers, base, leader);
+  return base + __popc(peers & ((1u << lane) - 1u));
+}
+
 __global__ void nl_columns(NlistArgs a) {
   if (*a.rebuild == 0) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -57,7 +70,7 @@ __global__ void nl_columns(NlistArgs a) {
   const int col = cy * a.n_col[0] + cx;
   a.column[i] = col;
   a.zkey[i] = fmaxf((float)z, 0.0f);
-  atomicAdd(&a.col_count[col], 1);
+  aggregated_add(&a.col_count[col], col);
 }
 
 // Single-CTA scan over the columns: padded slot starts, unpadded scatter starts, block count.
@@ -106,7 +119,7 @@ __global__ void nl_col_scatter(NlistArgs a) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= a.n_atoms) return;
   const int c = a.column[i];
-  a.scratch_atoms[a.col_scatter[c] + atomicAdd(&a.col_cursor[c], 1)] = i;
+  a.scratch_atoms[a.col_scatter[c] + aggregated_add(&a.col_cursor[c], c)] = i;
 }
 
 // One CTA per column: bitonic sort of (z, particle) keys in shared memory.
