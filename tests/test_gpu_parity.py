@@ -1,7 +1,7 @@
 """GPU parity of the engine against the f64 CPU oracle, through the C ABI (Python ctypes).
 
 Tolerances: FP64 form of the kernels agrees with the oracle to 1e-9 relative (force RMS)
-and 1e-9 relative (energy); the mixed FP32 / fixed-point form to the north-star bound of
+and 1e-9 relative (energy); the mixed FP32 / fixed-point form to the accuracy target of
 5e-6 force RMS relative error.  The interacting pair set must equal the reference's exactly.
 """
 import numpy as np
