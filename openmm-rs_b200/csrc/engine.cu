@@ -818,7 +818,7 @@ void Engine::setup_gbsa(const GbsaObcDef& g) {
   const size_t rs = dp_ ? 8 : 4;
   a.posq = mem_.alloc_bytes(4 * rs * a.n_slots);
   a.params = mem_.alloc_bytes(2 * rs * a.n_slots);
-  a.born_slot = mem_.alloc_bytes(rs * a.n_slots);
+  a.born_slot = mem_.alloc_bytes(2 * rs * a.n_slots);  // R, 1 / R
   a.dedr_slot = mem_.alloc_bytes(rs * a.n_slots);
   a.born_sum = mem_.alloc<long long>(n_);
   a.dedr_sum = mem_.alloc<long long>(n_);

@@ -26,8 +26,10 @@ using namespace gb;
 
 // kNb (pass 2 only): the NoCutoff NonbondedForce pair terms (bare Coulomb + LJ 12-6 with the
 // tile's exclusion mask, energy and virial as the nonbonded pair kernel computes them) join the
-// GB pair term, sharing the distance and the force rotation.
-template <class Real, int kPass, bool kEnergy, bool kNb = false>
+// GB pair term, sharing the distance, 1/r and the force rotation.  Pass 2 reads each slot's
+// Born radius with its reciprocal, so r^2 / (4 R_i R_j) needs no division, and needs r itself
+// only for the cutoff (kCutoff) and 1/r only for the nonbonded terms.
+template <class Real, int kPass, bool kEnergy, bool kCutoff, bool kNb = false>
 __global__ void __launch_bounds__(128) gb_pass(const GbArgs a) {
   if (kPass != 2 && a.use_learned && *a.use_learned) return;  // the network replaces them
   using T4 = typename V4<Real>::T4;
@@ -36,11 +38,12 @@ __global__ void __launch_bounds__(128) gb_pass(const GbArgs a) {
   __shared__ T4 s_pos[4][32];
   __shared__ T2 s_par[4][32];
   __shared__ Real s_aux[4][32];
+  __shared__ T2 s_born[kPass == 2 ? 4 : 1][32];  // pass 2: R, 1 / R
   __shared__ T4 s_nb[kNb ? 4 : 1][32];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const T4* posq = reinterpret_cast<const T4*>(a.posq);
   const T2* par = reinterpret_cast<const T2*>(a.params);
-  const Real* born = reinterpret_cast<const Real*>(a.born_slot);
+  const T2* born = reinterpret_cast<const T2*>(a.born_slot);
   const Real* dedr = reinterpret_cast<const Real*>(a.dedr_slot);
   for (int t = blockIdx.x * 4 + w; t < a.n_tiles; t += gridDim.x * 4) {
     const int2 tile = a.tiles[t];
@@ -51,11 +54,19 @@ __global__ void __launch_bounds__(128) gb_pass(const GbArgs a) {
     const T4 pi = posq[si];
     const T2 qi = par[si];  // (offset radius, scaled radius)
     Real ri_aux = Real(0);
-    if (kPass == 2) ri_aux = born[si];
-    if (kPass == 3) ri_aux = dedr[si];
+    T2 bi;
+    bi.x = bi.y = Real(1);
+    if (kPass == 2) {
+      bi = born[si];
+      s_born[w][lane] = born[sj];
+    } else {
+      s_par[w][lane] = par[sj];
+    }
+    if (kPass == 3) {
+      ri_aux = dedr[si];
+      s_aux[w][lane] = dedr[sj];
+    }
     s_pos[w][lane] = posq[sj];
-    s_par[w][lane] = par[sj];
-    s_aux[w][lane] = kPass == 2 ? born[sj] : (kPass == 3 ? dedr[sj] : Real(0));
     T4 nbi;
     uint32_t excl = 0u;
     if constexpr (kNb) {
@@ -66,6 +77,7 @@ __global__ void __launch_bounds__(128) gb_pass(const GbArgs a) {
       if (nt.y & kTileHasMask) excl = a.nb_masks[32 * nt.z + lane];
     }
     const unsigned valid_j = __ballot_sync(FULL, aj >= 0);  // entries holding a particle
+    const Real qsi = (Real)a.prefactor_sign * pi.w;
     __syncwarp();
     Real acc_i = 0, acc_j = 0;  // pass 1: descreening sums; pass 2: dE/dR
     Real fix = 0, fiy = 0, fiz = 0, fjx = 0, fjy = 0, fjz = 0;
@@ -75,8 +87,6 @@ __global__ void __launch_bounds__(128) gb_pass(const GbArgs a) {
     for (int k = self ? 1 : 0; k < 32; ++k) {
       const int jl = (lane + k) & 31;
       const T4 pj = s_pos[w][jl];
-      const T2 qj = s_par[w][jl];
-      const Real rj_aux = s_aux[w][jl];
       Real dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
       if (a.periodic) {
         if constexpr (sizeof(Real) == 4) min_image_fast(dx, dy, dz, a.boxf);
@@ -84,38 +94,42 @@ __global__ void __launch_bounds__(128) gb_pass(const GbArgs a) {
       }
       const Real r2 = dx * dx + dy * dy + dz * dz;
       bool use = ai >= 0 && ((valid_j >> jl) & 1u);
-      Real r, inv_r;
-      if constexpr (sizeof(Real) == 4) {  // SFU reciprocal square root in the FP32 kernel
-        inv_r = rsqrt_r(use ? r2 : Real(1));
-        r = (use ? r2 : Real(1)) * inv_r;
-      } else {
-        r = sqrt_r(use ? r2 : Real(1));
-        inv_r = Real(1) / r;
+      Real r = Real(1), inv_r = Real(1);
+      if (kPass != 2 || kCutoff || kNb) {
+        if constexpr (sizeof(Real) == 4) {  // SFU reciprocal square root in the FP32 kernel
+          inv_r = rsqrt_r(use ? r2 : Real(1));
+          r = (use ? r2 : Real(1)) * inv_r;
+        } else {
+          r = sqrt_r(use ? r2 : Real(1));
+          inv_r = Real(1) / r;
+        }
       }
-      if (a.use_cutoff) use = use && r <= (Real)a.cutoff;  // gbsa_obc.rs:169 (<=)
+      if (kCutoff) use = use && r <= (Real)a.cutoff;  // gbsa_obc.rs:169 (<=)
       Real fo = 0;
       if (kPass == 1) {
         if (use) {
+          const T2 qj = s_par[w][jl];
           acc_i += descreening_pair(qi.x, qj.y, r, inv_r);
           if (!self) acc_j += descreening_pair(qj.x, qi.y, r, inv_r);
         }
       } else if (kPass == 2) {
         if (use) {
-          // SFU forms (rcp, ex2, rsqrt) in the FP32 kernel, exact ones in FP64
-          const Real product = ri_aux * rj_aux;
-          const Real d = Real(0.25) * r2 * rcp_r(product);
+          // SFU forms (ex2, rsqrt) in the FP32 kernel, exact ones in FP64
+          const T2 bj = s_born[w][jl];
+          const Real product = bi.x * bj.x;
+          const Real d = Real(0.25) * r2 * (bi.y * bj.y);
           const Real ex = exp2_r(Real(-1.4426950408889634) * d);
           const Real den2 = r2 + product * ex;
           const Real inv = rsqrt_r(den2), inv2 = inv * inv;
           // prefactor q_i q_j, with q stored as q sqrt|prefactor|
-          const Real coefficient = (Real)a.prefactor_sign * pi.w * pj.w;
+          const Real coefficient = qsi * pj.w;
           const Real pe = coefficient * inv;
           fo = -pe * (Real(1) - Real(0.25) * ex) * inv2;
           const Real bd = Real(-0.5) * pe * ex * (Real(1) + d) * inv2;
-          acc_i += bd * rj_aux;
-          if (!self) acc_j += bd * ri_aux;
+          acc_i += bd * bj.x;
+          if (!self) acc_j += bd * bi.x;
           if (kEnergy) {
-            const double e = a.use_cutoff ? (double)pe - (double)coefficient / a.cutoff : (double)pe;
+            const double e = kCutoff ? (double)pe - (double)coefficient / a.cutoff : (double)pe;
             e_tile += (self ? 0.5 : 1.0) * e;
           }
         }
@@ -124,8 +138,9 @@ __global__ void __launch_bounds__(128) gb_pass(const GbArgs a) {
             const T4 nbj = s_nb[w][jl];
             PairArgs<Real> none{};
             Real f_nb, en_nb;
-            pair_terms<Real, kElecCoulomb, kEnergy, false>(none, r2, nbi.x * nbj.x, nbi.y + nbj.y,
-                                                           nbi.z * nbj.z, f_nb, en_nb);
+            pair_terms_r<Real, kElecCoulomb, kEnergy, false>(none, r2, inv_r, nbi.x * nbj.x,
+                                                             nbi.y + nbj.y, nbi.z * nbj.z, f_nb,
+                                                             en_nb);
             fo += f_nb;
             if (kEnergy) {
               const double scale = self ? 0.5 : 1.0;
@@ -140,9 +155,12 @@ __global__ void __launch_bounds__(128) gb_pass(const GbArgs a) {
           }
         }
       } else {
-        if (use)
+        if (use) {
+          const T2 qj = s_par[w][jl];
+          const Real rj_aux = s_aux[w][jl];
           fo = -(ri_aux * descreening_gradient_pair(qi.x, qj.y, r, inv_r) +
                  rj_aux * descreening_gradient_pair(qj.x, qi.y, r, inv_r));
+        }
       }
       if (kPass != 1) {
         // self tiles visit each pair from both sides; each visit moves only its own lane
@@ -209,9 +227,9 @@ __global__ void gb_radii(const GbArgs a) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= a.n_slots) return;
   const int atom = a.slot_atom[s];
-  Real* born = reinterpret_cast<Real*>(a.born_slot);
+  typename V4<Real>::T2* born = reinterpret_cast<typename V4<Real>::T2*>(a.born_slot);
   if (atom < 0) {
-    born[s] = Real(1);
+    born[s].x = born[s].y = Real(1);
     return;
   }
   const double rho = a.radius[atom];
@@ -225,7 +243,8 @@ __global__ void gb_radii(const GbArgs a) {
   const double R = 1.0 / (1.0 / offset - t / rho);
   a.chain[atom] = offset * (1.0 - 1.6 * psi + 14.55 * psi * psi) * (1.0 - t * t) / rho;
   a.born_radius[atom] = R;
-  born[s] = (Real)R;
+  born[s].x = (Real)R;
+  born[s].y = (Real)(1.0 / R);
   const double q = a.charge[atom];
   const double self_energy = 0.5 * a.prefactor * q * q / fabs(R);
   double dedr = -self_energy / R;
@@ -294,6 +313,14 @@ __global__ void gb_pack(const GbArgs a) {
 
 }  // namespace
 
+template <class Real, int kPass, bool kEnergy, bool kNb = false>
+void launch_gb_pass(const GbArgs& a, int grid, cudaStream_t s) {
+  if (a.use_cutoff)
+    gb_pass<Real, kPass, kEnergy, true, kNb><<<grid, 128, 0, s>>>(a);
+  else
+    gb_pass<Real, kPass, kEnergy, false, kNb><<<grid, 128, 0, s>>>(a);
+}
+
 template <class Real>
 void launch_gbsa_phase(const GbArgs& a, int phase, bool energy, int sm_count, cudaStream_t s) {
   const int tb = 256;
@@ -304,7 +331,7 @@ void launch_gbsa_phase(const GbArgs& a, int phase, bool energy, int sm_count, cu
       gb_pack<Real><<<gs, tb, 0, s>>>(a);
       break;
     case kGbPass1:
-      gb_pass<Real, 1, false><<<gt, 128, 0, s>>>(a);
+      launch_gb_pass<Real, 1, false>(a, gt, s);
       break;
     case kGbRadii:
       if (energy)
@@ -315,20 +342,20 @@ void launch_gbsa_phase(const GbArgs& a, int phase, bool energy, int sm_count, cu
     case kGbPass2:
       if (a.fuse_nonbonded) {
         if (energy)
-          gb_pass<Real, 2, true, true><<<gt, 128, 0, s>>>(a);
+          launch_gb_pass<Real, 2, true, true>(a, gt, s);
         else
-          gb_pass<Real, 2, false, true><<<gt, 128, 0, s>>>(a);
+          launch_gb_pass<Real, 2, false, true>(a, gt, s);
       } else if (energy) {
-        gb_pass<Real, 2, true><<<gt, 128, 0, s>>>(a);
+        launch_gb_pass<Real, 2, true>(a, gt, s);
       } else {
-        gb_pass<Real, 2, false><<<gt, 128, 0, s>>>(a);
+        launch_gb_pass<Real, 2, false>(a, gt, s);
       }
       break;
     case kGbChain:
       gb_chain<Real><<<gs, tb, 0, s>>>(a);
       break;
     case kGbPass3:
-      gb_pass<Real, 3, false><<<gt, 128, 0, s>>>(a);
+      launch_gb_pass<Real, 3, false>(a, gt, s);
       break;
   }
 }

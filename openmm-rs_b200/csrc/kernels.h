@@ -192,7 +192,7 @@ struct GbArgs {
   Box<float> boxf;
   void* posq;                 // [n_slots] Real4: x, y, z, q sqrt|prefactor|
   void* params;               // [n_slots] Real2: rho - 0.009, s (rho - 0.009)
-  void* born_slot;            // [n_slots] Real: Born radius
+  void* born_slot;            // [n_slots] Real2: Born radius and its reciprocal
   void* dedr_slot;            // [n_slots] Real: dE/dR R^2 chain
   long long* born_sum;        // [n_atoms] descreening sums, 2^-40
   long long* dedr_sum;        // [n_atoms] pair dE/dR sums, 2^-32

@@ -3,6 +3,7 @@
 // electrostatics (forces/nonbonded.rs:842-924 and 1186-1288).
 #pragma once
 
+#include "f32x2.cuh"
 #include "kernels.h"
 
 namespace ommb200 {
@@ -67,11 +68,11 @@ __device__ __forceinline__ bool exact_inside(const double* pos, int a, int b, in
   return r2 < rc2;
 }
 
-// dE/dr / r and E of one pair; `eps4` = 4 sqrt(eps_i eps_j), `sig` = (sigma_i + sigma_j) / 2.
+// dE/dr / r and E of one pair at squared distance r2 with inv_r = 1 / sqrt(r2);
+// `eps4` = 4 sqrt(eps_i eps_j), `sig` = (sigma_i + sigma_j) / 2.
 template <class Real, int kElec, bool kEnergy, bool kSwitch>
-__device__ __forceinline__ void pair_terms(const PairArgs<Real>& a, Real r2, Real qq, Real sig,
-                                           Real eps4, Real& f_over_r, Real& energy) {
-  const Real inv_r = rsqrt_r(r2);
+__device__ __forceinline__ void pair_terms_r(const PairArgs<Real>& a, Real r2, Real inv_r, Real qq,
+                                             Real sig, Real eps4, Real& f_over_r, Real& energy) {
   const Real inv_r2 = inv_r * inv_r;
   // LJ 12-6 (nonbonded.rs:1203-1214)
   const Real s2 = sig * sig * inv_r2;
@@ -119,6 +120,74 @@ __device__ __forceinline__ void pair_terms(const PairArgs<Real>& a, Real r2, Rea
   }
   f_over_r = f_lj + f_el;
   energy = e_lj + e_el;
+}
+
+template <class Real, int kElec, bool kEnergy, bool kSwitch>
+__device__ __forceinline__ void pair_terms(const PairArgs<Real>& a, Real r2, Real qq, Real sig,
+                                           Real eps4, Real& f_over_r, Real& energy) {
+  pair_terms_r<Real, kElec, kEnergy, kSwitch>(a, r2, rsqrt_r(r2), qq, sig, eps4, f_over_r, energy);
+}
+
+// pair_terms for two pairs at once in the lanes of packed FP32 values (same operations and
+// rounding as the scalar FP32 form, erfc by the same fit).
+template <int kElec, bool kEnergy, bool kSwitch>
+__device__ __forceinline__ void pair_terms_x2(const PairArgs<float>& a, float2 r2, float2 qq,
+                                              float2 sig, float2 eps4, float2& f_over_r,
+                                              float2& energy) {
+  const float2 inv_r = x2::rsqrt_approx(r2);
+  const float2 inv_r2 = x2::mul(inv_r, inv_r);
+  // LJ 12-6 (nonbonded.rs:1203-1214)
+  const float2 s2 = x2::mul(x2::mul(sig, sig), inv_r2);
+  const float2 s6 = x2::mul(x2::mul(s2, s2), s2);
+  const float2 e6 = x2::mul(eps4, s6);
+  float2 f_lj = x2::mul(x2::mul(e6, x2::fma(x2::bc(-12.f), s6, x2::bc(6.f))), inv_r2);
+  float2 e_lj = kEnergy ? x2::mul(e6, x2::add(s6, x2::bc(-1.f))) : x2::bc(0.f);
+  if (eps4.x == 0.f) f_lj.x = e_lj.x = 0.f;
+  if (eps4.y == 0.f) f_lj.y = e_lj.y = 0.f;
+  if (kSwitch) {  // nonbonded.rs:888-900, per lane (switching is the uncommon path)
+    const float2 r = x2::mul(r2, inv_r);
+    auto sw = [&](float rr, float e4, float s6v, float ir, float& f, float& e) {
+      if (rr > a.switch_r) {
+        const float e_full = e4 * s6v * (s6v - 1.f);
+        const float t = (rr - a.switch_r) * a.switch_inv_width;
+        const float s = 1.f + t * t * t * (-10.f + t * (15.f - 6.f * t));
+        const float ds = -30.f * t * t * (1.f - t) * (1.f - t) * a.switch_inv_width;
+        f = s * f + (e4 == 0.f ? 0.f : e_full) * ds * ir;
+        e = kEnergy ? e * s : 0.f;
+      }
+    };
+    sw(r.x, eps4.x, s6.x, inv_r.x, f_lj.x, e_lj.x);
+    sw(r.y, eps4.y, s6.y, inv_r.y, f_lj.y, e_lj.y);
+  }
+  float2 e_el = x2::bc(0.f);
+  if (kElec == kElecEwald) {
+    // screened_coulomb (nonbonded.rs:1263-1273): exp(-a^2 r^2) by exp2, erfc by the fit
+    const float2 r = x2::mul(r2, inv_r);
+    const float2 ex = x2::exp2_approx(x2::mul(x2::bc(a.exp_scale), r2));
+    const float2 t = x2::rcp_approx(x2::fma(x2::bc(0.46f), x2::mul(x2::bc(a.alpha), r), x2::bc(1.f)));
+    float2 p = x2::bc(0.10014041224442242f);
+    p = x2::fma(p, t, x2::bc(-0.504550213499043f));
+    p = x2::fma(p, t, x2::bc(0.8277608617691994f));
+    p = x2::fma(p, t, x2::bc(-0.35775472734883446f));
+    p = x2::fma(p, t, x2::bc(0.4707476000236329f));
+    p = x2::fma(p, t, x2::bc(0.1949991373822864f));
+    p = x2::fma(p, t, x2::bc(0.2692933367874065f));
+    p = x2::fma(p, t, x2::bc(-0.0006363939510855f));
+    const float2 ec = x2::mul(ex, p);
+    const float2 v = x2::fma(ec, inv_r, x2::mul(x2::bc(a.two_alpha_sqrtpi), ex));
+    f_over_r = x2::sub(f_lj, x2::mul(x2::mul(qq, v), inv_r2));
+    if (kEnergy) e_el = x2::mul(x2::mul(qq, ec), inv_r);
+  } else if (kElec == kElecReactionField) {
+    // reaction_field (nonbonded.rs:1222-1243)
+    f_over_r = x2::add(f_lj, x2::mul(qq, x2::sub(x2::bc(2.f * a.krf), x2::mul(inv_r, inv_r2))));
+    if (kEnergy)
+      e_el = x2::mul(qq, x2::sub(x2::fma(x2::bc(a.krf), r2, inv_r), x2::bc(a.crf)));
+  } else {
+    // coulomb_pair (nonbonded.rs:1186-1192)
+    f_over_r = x2::sub(f_lj, x2::mul(x2::mul(qq, inv_r), inv_r2));
+    if (kEnergy) e_el = x2::mul(qq, inv_r);
+  }
+  energy = x2::add(e_lj, e_el);
 }
 
 
