@@ -15,6 +15,8 @@
 //
 // Tiles pair blocks of the same segment (one segment per independent system in a batch), so
 // many systems of uneven size run in the same launches.
+#include <type_traits>
+
 #include "kernels.h"
 #include "gb_math.cuh"
 #include "pair_math.cuh"
@@ -221,6 +223,222 @@ __global__ void __launch_bounds__(128) gb_pass(const GbArgs a) {
   }
 }
 
+// Pass 2 in FP32 for non-periodic systems without a cutoff (the batched-chain workloads), with
+// two i-particles per lane and packed (f32x2) arithmetic: lane m of each 16-lane half of the
+// warp holds i-slots m and m + 16 of block I and meets the half's 16 entries of block J in 16
+// steps, so a warp evaluates 64 pairs per step; the entry's force and dE/dR rotate within the
+// half and are back at the entry's lane after the 16 steps, and the two halves' partial sums of
+// each i-slot are added at the end (lane ^ 16).  Tiles whose every pair is a valid particle pair
+// without exclusion take a loop without masks; self tiles (each pair seen from both sides, i
+// sums only, half energy), padded and excluded tiles apply bit masks kept in step order.
+template <bool kEnergy, bool kNb>
+__global__ void __launch_bounds__(128) gb_pairs_x2(const GbArgs a) {
+  constexpr unsigned FULL = 0xffffffffu;
+  __shared__ float4 s_pos[4][32];                // x, y, z, q sqrt|prefactor|
+  __shared__ float2 s_born[4][32];               // R, 1 / R
+  __shared__ float4 s_nb[kNb ? 4 : 1][32];       // q sqrt(ke), sigma / 2, 2 sqrt(eps), 0
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const float4* posq = reinterpret_cast<const float4*>(a.posq);
+  const float2* born = reinterpret_cast<const float2*>(a.born_slot);
+  const float4* nbp = reinterpret_cast<const float4*>(a.nb_params);
+  const int m = lane & 15, eb = lane & 16, i1 = m, i2 = m + 16;
+  const int src = eb | ((m + 1) & 15);
+  const float sign = (float)a.prefactor_sign;
+  for (int t = blockIdx.x * 4 + w; t < a.n_tiles; t += gridDim.x * 4) {
+    const int2 tile = a.tiles[t];
+    const int I = tile.x, J = tile.y;
+    const bool self = I == J;
+    const int ai = a.slot_atom[32 * I + lane], aj = a.slot_atom[32 * J + lane];
+    s_pos[w][lane] = posq[32 * J + lane];
+    s_born[w][lane] = born[32 * J + lane];
+    uint32_t excl = 0u;
+    if constexpr (kNb) {
+      s_nb[w][lane] = nbp[32 * J + lane];
+      const int4 nt = a.nb_tiles[t];
+      if (nt.y & kTileHasMask) excl = a.nb_masks[32 * nt.z + lane];
+    }
+    const unsigned valid_i = __ballot_sync(FULL, ai >= 0), valid_j = __ballot_sync(FULL, aj >= 0);
+    // step-ordered masks: bit k (i1) and 16 + k (i2) stand for entry eb + ((m + k) mod 16)
+    auto rot = [&](uint32_t bits) {
+      const uint32_t x = (bits >> eb) & 0xffffu;
+      return ((x >> m) | (x << (16 - m))) & 0xffffu;
+    };
+    uint32_t use_bits, ex_bits = 0u;
+    {
+      const uint32_t vj = rot(valid_j);
+      uint32_t u1 = ((valid_i >> i1) & 1u) ? vj : 0u, u2 = ((valid_i >> i2) & 1u) ? vj : 0u;
+      if (self) {  // the diagonal: entry eb + m at step 0 is i1 (eb = 0) or i2 (eb = 16)
+        u1 &= eb == 0 ? ~1u : ~0u;
+        u2 &= eb == 16 ? ~1u : ~0u;
+      }
+      use_bits = u1 | (u2 << 16);
+      if (kNb) ex_bits = rot(__shfl_sync(FULL, excl, i1)) | (rot(__shfl_sync(FULL, excl, i2)) << 16);
+    }
+    const bool plain = __all_sync(FULL, use_bits == 0xffffffffu && ex_bits == 0u);
+    const float4 p1 = posq[32 * I + i1], p2 = posq[32 * I + i2];
+    const float2 b1 = born[32 * I + i1], b2 = born[32 * I + i2];
+    float4 n1 = make_float4(0.f, 0.f, 0.f, 0.f), n2 = n1;
+    if (kNb) {
+      n1 = nbp[32 * I + i1];
+      n2 = nbp[32 * I + i2];
+    }
+    __syncwarp();
+    const float2 npx = make_float2(-p1.x, -p2.x), npy = make_float2(-p1.y, -p2.y),
+                 npz = make_float2(-p1.z, -p2.z);
+    const float2 qn = make_float2(-sign * p1.w, -sign * p2.w);  // minus the GB charge factor
+    const float2 Ri = make_float2(b1.x, b2.x), Rq = make_float2(0.25f * b1.y, 0.25f * b2.y);
+    const float2 nq = make_float2(n1.x, n2.x), ns = make_float2(n1.y, n2.y),
+                 ne = make_float2(n1.z, n2.z);
+    float2 fx = x2::bc(0.f), fy = x2::bc(0.f), fz = x2::bc(0.f), acc_i = x2::bc(0.f);
+    float fjx = 0.f, fjy = 0.f, fjz = 0.f, acc_j = 0.f;
+    double e_gb = 0.0, e_nb = 0.0;
+    double w_nb[6] = {0, 0, 0, 0, 0, 0};
+    auto steps = [&](auto masked_tag) {
+      constexpr bool kMasked = decltype(masked_tag)::value;
+      uint32_t ub = use_bits;
+      [[maybe_unused]] uint32_t xb = ex_bits;
+#pragma unroll 2
+      for (int k = 0; k < 16; ++k) {
+        const int jl = eb | ((m + k) & 15);
+        const float4 pj = s_pos[w][jl];
+        const float2 bj = s_born[w][jl];
+        const float2 dx = x2::add(x2::bc(pj.x), npx), dy = x2::add(x2::bc(pj.y), npy),
+                     dz = x2::add(x2::bc(pj.z), npz);
+        float2 r2 = x2::fma(dz, dz, x2::fma(dy, dy, x2::mul(dx, dx)));
+        bool u1 = true, u2 = true;
+        if (kMasked) {
+          u1 = (ub & 1u) != 0u;
+          u2 = (ub & 0x10000u) != 0u;
+          ub >>= 1;
+          r2 = x2::select(u1, u2, r2, 1.f);
+        }
+        // GB pair (gbsa_obc.rs:239-260): pe = -qn q_j / sqrt(r^2 + R_i R_j exp(-d)), d = r^2 / (4 R_i R_j)
+        const float2 product = x2::mul(Ri, x2::bc(bj.x));
+        const float2 d = x2::mul(r2, x2::mul(Rq, x2::bc(bj.y)));
+        const float2 ex = x2::exp2_approx(x2::mul(x2::bc(-1.4426950408889634f), d));
+        const float2 inv = x2::rsqrt_approx(x2::fma(product, ex, r2));
+        const float2 pen = x2::mul(x2::mul(qn, x2::bc(pj.w)), inv);  // -pe
+        const float2 pi2 = x2::mul(pen, x2::mul(inv, inv));          // -pe / den^2
+        float2 fo = x2::mul(pi2, x2::fma(x2::bc(-0.25f), ex, x2::bc(1.f)));
+        float2 bd = x2::mul(x2::mul(pi2, ex), x2::fma(d, x2::bc(0.5f), x2::bc(0.5f)));
+        if (kEnergy) {
+          const double sc = self ? 0.5 : 1.0;
+          if (u1) e_gb -= sc * (double)pen.x;
+          if (u2) e_gb -= sc * (double)pen.y;
+        }
+        if constexpr (kNb) {
+          bool x1 = true, x2v = true;  // not excluded
+          if (kMasked) {
+            x1 = (xb & 1u) == 0u;
+            x2v = (xb & 0x10000u) == 0u;
+            xb >>= 1;
+          }
+          const float4 nj = s_nb[w][jl];
+          const float2 inv_r = x2::rsqrt_approx(r2), inv_r2 = x2::mul(inv_r, inv_r);
+          const float2 sig = x2::add(ns, x2::bc(nj.y));
+          const float2 s2 = x2::mul(x2::mul(sig, sig), inv_r2);
+          const float2 s6 = x2::mul(x2::mul(s2, s2), s2);
+          const float2 eps4 = x2::mul(ne, x2::bc(nj.z));
+          const float2 e6 = x2::mul(eps4, s6);
+          float2 f_lj = x2::mul(x2::mul(e6, x2::fma(x2::bc(-12.f), s6, x2::bc(6.f))), inv_r2);
+          if (eps4.x == 0.f) f_lj.x = 0.f;
+          if (eps4.y == 0.f) f_lj.y = 0.f;
+          const float2 qq = x2::mul(nq, x2::bc(nj.x));
+          float2 f_nb = x2::sub(f_lj, x2::mul(x2::mul(qq, inv_r), inv_r2));
+          if (kMasked) f_nb = x2::select(u1 && x1, u2 && x2v, f_nb, 0.f);
+          if (kEnergy) {
+            const double sc = self ? 0.5 : 1.0;
+            const float2 e_lj = x2::mul(e6, x2::add(s6, x2::bc(-1.f)));
+            const float2 e_el = x2::mul(qq, inv_r);
+            const float2 fdx = x2::mul(f_nb, dx), fdy = x2::mul(f_nb, dy);
+            const float2 wxx = x2::mul(fdx, dx), wyy = x2::mul(fdy, dy),
+                         wzz = x2::mul(x2::mul(f_nb, dz), dz), wxy = x2::mul(fdx, dy),
+                         wxz = x2::mul(fdx, dz), wyz = x2::mul(fdy, dz);
+            for (int h = 0; h < 2; ++h) {
+              if (!(h ? (u2 && x2v) : (u1 && x1))) continue;
+              const float elj = h ? (eps4.y == 0.f ? 0.f : e_lj.y) : (eps4.x == 0.f ? 0.f : e_lj.x);
+              e_nb += sc * (double)(elj + (h ? e_el.y : e_el.x));
+              w_nb[0] -= sc * (double)(h ? wxx.y : wxx.x);
+              w_nb[1] -= sc * (double)(h ? wyy.y : wyy.x);
+              w_nb[2] -= sc * (double)(h ? wzz.y : wzz.x);
+              w_nb[3] -= sc * (double)(h ? wxy.y : wxy.x);
+              w_nb[4] -= sc * (double)(h ? wxz.y : wxz.x);
+              w_nb[5] -= sc * (double)(h ? wyz.y : wyz.x);
+            }
+          }
+          fo = x2::add(fo, f_nb);
+        }
+        if (kMasked) {
+          fo = x2::select(u1, u2, fo, 0.f);
+          bd = x2::select(u1, u2, bd, 0.f);
+        }
+        fx = x2::fma(fo, dx, fx);
+        fy = x2::fma(fo, dy, fy);
+        fz = x2::fma(fo, dz, fz);
+        acc_i = x2::fma(bd, x2::bc(bj.x), acc_i);
+        if (!self) {
+          fjx = fmaf(-fo.x, dx.x, fjx);
+          fjy = fmaf(-fo.x, dy.x, fjy);
+          fjz = fmaf(-fo.x, dz.x, fjz);
+          acc_j = fmaf(bd.x, Ri.x, acc_j);
+          fjx = fmaf(-fo.y, dx.y, fjx);
+          fjy = fmaf(-fo.y, dy.y, fjy);
+          fjz = fmaf(-fo.y, dz.y, fjz);
+          acc_j = fmaf(bd.y, Ri.y, acc_j);
+          fjx = __shfl_sync(FULL, fjx, src);
+          fjy = __shfl_sync(FULL, fjy, src);
+          fjz = __shfl_sync(FULL, fjz, src);
+          acc_j = __shfl_sync(FULL, acc_j, src);
+        }
+      }
+    };
+    if (plain && !self)
+      steps(std::false_type{});
+    else
+      steps(std::true_type{});
+    // the two halves' sums of this lane's i-slots; the lane commits i-slot `lane`
+    fx.x += __shfl_xor_sync(FULL, fx.x, 16);
+    fx.y += __shfl_xor_sync(FULL, fx.y, 16);
+    fy.x += __shfl_xor_sync(FULL, fy.x, 16);
+    fy.y += __shfl_xor_sync(FULL, fy.y, 16);
+    fz.x += __shfl_xor_sync(FULL, fz.x, 16);
+    fz.y += __shfl_xor_sync(FULL, fz.y, 16);
+    acc_i.x += __shfl_xor_sync(FULL, acc_i.x, 16);
+    acc_i.y += __shfl_xor_sync(FULL, acc_i.y, 16);
+    const bool second = eb != 0;
+    const float fs = float(kForceScale);
+    if (ai >= 0) {
+      add_fixed(a.force + ai, to_fixed(second ? fx.y : fx.x, fs));
+      add_fixed(a.force + a.n_atoms + ai, to_fixed(second ? fy.y : fy.x, fs));
+      add_fixed(a.force + 2 * a.n_atoms + ai, to_fixed(second ? fz.y : fz.x, fs));
+      add_fixed(a.dedr_sum + ai, to_fixed((double)(second ? acc_i.y : acc_i.x), kForceScale));
+    }
+    if (!self && aj >= 0) {
+      add_fixed(a.force + aj, to_fixed(fjx, fs));
+      add_fixed(a.force + a.n_atoms + aj, to_fixed(fjy, fs));
+      add_fixed(a.force + 2 * a.n_atoms + aj, to_fixed(fjz, fs));
+      add_fixed(a.dedr_sum + aj, to_fixed((double)acc_j, kForceScale));
+    }
+    if (kEnergy) {
+      for (int off = 16; off > 0; off >>= 1) e_gb += __shfl_xor_sync(FULL, e_gb, off);
+      const long long ef = to_fixed(e_gb, kEnergyScale);
+      if (lane == 0 && ef) add_fixed(a.energy + 8 * a.block_segment[I], ef);
+      if constexpr (kNb) {
+        for (int off = 16; off > 0; off >>= 1) {
+          e_nb += __shfl_xor_sync(FULL, e_nb, off);
+          for (int c = 0; c < 6; ++c) w_nb[c] += __shfl_xor_sync(FULL, w_nb[c], off);
+        }
+        if (lane == 0) {
+          long long* dst = a.energy + 8 * a.block_segment[I];
+          add_fixed(dst, to_fixed(e_nb, kEnergyScale));
+          for (int c = 0; c < 6; ++c) add_fixed(dst + 1 + c, to_fixed(w_nb[c], kEnergyScale));
+        }
+      }
+    }
+    __syncwarp();
+  }
+}
+
 // gbsa_obc.rs:214-237: radii, chain factor, self + ACE energies, dE/dR from them.
 template <class Real, bool kEnergy>
 __global__ void gb_radii(const GbArgs a) {
@@ -340,7 +558,18 @@ void launch_gbsa_phase(const GbArgs& a, int phase, bool energy, int sm_count, cu
         gb_radii<Real, false><<<gs, tb, 0, s>>>(a);
       break;
     case kGbPass2:
-      if (a.fuse_nonbonded) {
+      if (sizeof(Real) == 4 && !a.use_cutoff && !a.periodic) {
+        if (a.fuse_nonbonded) {
+          if (energy)
+            gb_pairs_x2<true, true><<<gt, 128, 0, s>>>(a);
+          else
+            gb_pairs_x2<false, true><<<gt, 128, 0, s>>>(a);
+        } else if (energy) {
+          gb_pairs_x2<true, false><<<gt, 128, 0, s>>>(a);
+        } else {
+          gb_pairs_x2<false, false><<<gt, 128, 0, s>>>(a);
+        }
+      } else if (a.fuse_nonbonded) {
         if (energy)
           launch_gb_pass<Real, 2, true, true>(a, gt, s);
         else
