@@ -306,12 +306,14 @@ int ommb200_context_get_system_energies(ommb200_context* ctx, uint32_t groups,
  * pool, whose accounting a private allocation would bypass, or a plugin that may only use the
  * buffers it is handed.  Evaluates NonbondedForce forces and energy of a non-periodic system without
  * exceptions (method OMMB200_NO_CUTOFF or OMMB200_CUTOFF_NON_PERIODIC) with the Context's
- * mixed-precision arithmetic.  All pointers are device pointers on the current device:
- * positions[3n], charges[n], sigmas[n], epsilons[n] in; forces[3n] and energy[1] out.  Work is
- * enqueued on `stream` (a cudaStream_t; NULL = legacy default stream) and not synchronised.
- * n is at most 8192: the scratch is a 384 KiB static device array that every GPU loading the
- * library keeps until exit.  The first call on a device looks up that array's address; make it
- * before any stream capture.  Calls share the array, so calls that overlap on the GPU race. */
+ * mixed-precision arithmetic; with a cutoff, LJ is cut plainly (no switching function) and the
+ * electrostatics are the reaction field.  All pointers are device pointers on the current
+ * device: positions[3n], charges[n], sigmas[n], epsilons[n] in; forces[3n] and energy[1] out.
+ * Work is enqueued on `stream` (a cudaStream_t; NULL = legacy default stream) and not
+ * synchronised.  n is at most 8192: the scratch is a 384 KiB static device array that every GPU
+ * loading the library keeps until exit.  The first call in each CUDA context looks up that
+ * array's address (the array is loaded per context); make it before any stream capture.  Calls
+ * share the array, so calls that overlap on the GPU race. */
 int ommb200_nonbonded_forces_noalloc(int n, const double* positions, const double* charges,
                                      const double* sigmas, const double* epsilons, int method,
                                      double cutoff, double reaction_field_dielectric,

@@ -1,4 +1,5 @@
-"""Derives the single-precision erfc used by the real-space pair kernel (erfc_fit.cuh).
+"""Derives the single-precision erfc used by the real-space pair kernel (the coefficients of
+`erfc_poly` and `pair_terms_x2` in pair_math.cuh).
 
 erfc(x) = exp(-x^2) * erfcx(x), and erfcx is smooth and bounded on [0, inf), so it is fitted
 as a degree-7 polynomial in t = 1 / (1 + p x), p = 0.46, over x in [0, 4.2] (alpha * cutoff

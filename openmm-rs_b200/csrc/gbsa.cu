@@ -357,7 +357,7 @@ __global__ void __launch_bounds__(128) gb_pairs_x2(const GbArgs a) {
             for (int h = 0; h < 2; ++h) {
               if (!(h ? (u2 && x2v) : (u1 && x1))) continue;
               const float elj = h ? (eps4.y == 0.f ? 0.f : e_lj.y) : (eps4.x == 0.f ? 0.f : e_lj.x);
-              e_nb += sc * (double)(elj + (h ? e_el.y : e_el.x));
+              e_nb += sc * ((double)elj + (double)(h ? e_el.y : e_el.x));
               w_nb[0] -= sc * (double)(h ? wxx.y : wxx.x);
               w_nb[1] -= sc * (double)(h ? wyy.y : wyy.x);
               w_nb[2] -= sc * (double)(h ? wzz.y : wzz.x);

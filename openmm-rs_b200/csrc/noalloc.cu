@@ -5,14 +5,17 @@
 // kernel's scratch (packed block coordinates and 64-bit fixed-point accumulators) lives in the
 // file-scope array below, which every GPU that loads the library holds until the process
 // exits.  It serves non-periodic systems of at most kNoAllocMaxAtoms particles without
-// exceptions (NoCutoff: bare Coulomb; CutoffNonPeriodic: reaction field), with the same
-// arithmetic as the Context's mixed-precision path.
+// exceptions (NoCutoff: bare Coulomb; CutoffNonPeriodic: reaction field, LJ cut plainly at the
+// cutoff with no switching function), with the same arithmetic as the Context's
+// mixed-precision path.
 //
 // Every call shares the one array and clears what must start at zero, so calls that overlap
 // on the GPU (different streams, or different host threads on the same device) race.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <map>
 #include <mutex>
 
 #include "../../include/ommb200.h"
@@ -51,23 +54,51 @@ ScratchView view(void* base) {
   return v;
 }
 
-// Device address of the array, looked up once per device with that device current.
-void* scratch_address() {
+// Device address of the array and the SM count, looked up once per CUDA context (the module,
+// and with it the array, is loaded per context) with that context current.  The context comes
+// from the driver's cuCtxGetCurrent, reached through the runtime's entry-point query so that
+// the library needs no link against the driver library.
+struct ScratchInfo {
+  void* addr;
+  int sm_count;
+};
+
+ScratchInfo scratch_info() {
+  using GetCurrent = CUresult (*)(CUcontext*);
   static std::mutex mu;
-  static void* addr[128] = {};
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) throw Error(OMMB200_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
-  if (dev < 0 || dev >= 128) throw Error(OMMB200_ERR_CUDA, "device ordinal out of range");
+  static GetCurrent get_current = nullptr;
+  static std::map<CUcontext, ScratchInfo> known;
   std::lock_guard<std::mutex> lock(mu);
-  if (!addr[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p)
-      throw Error(OMMB200_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-    addr[dev] = p;
+  auto fail = [](const char* what, cudaError_t e) {
+    throw Error(OMMB200_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+  };
+  if (!get_current) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    const cudaError_t e = cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q);
+    if (e != cudaSuccess || q != cudaDriverEntryPointSuccess || !fn)
+      fail("cudaGetDriverEntryPoint(cuCtxGetCurrent)", e);
+    get_current = reinterpret_cast<GetCurrent>(fn);
   }
-  return addr[dev];
+  CUcontext ctx = nullptr;
+  if (get_current(&ctx) == CUDA_SUCCESS && ctx) {
+    auto it = known.find(ctx);
+    if (it != known.end()) return it->second;
+  }
+  // first use in this context: the symbol lookup also initialises the runtime's context on
+  // this thread when none was current
+  ScratchInfo info{nullptr, 0};
+  cudaError_t e = cudaGetSymbolAddress(&info.addr, g_noalloc_scratch);
+  if (e != cudaSuccess || !info.addr) fail("cudaGetSymbolAddress", e);
+  if (get_current(&ctx) != CUDA_SUCCESS || !ctx)
+    throw Error(OMMB200_ERR_CUDA, "no current CUDA context");
+  int dev = 0;
+  e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) fail("cudaGetDevice", e);
+  e = cudaDeviceGetAttribute(&info.sm_count, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) fail("cudaDeviceGetAttribute", e);
+  known.emplace(ctx, info);
+  return info;
 }
 
 __global__ void na_prepare(int n, int slots, const double* pos, const double* q, const double* sigma,
@@ -188,7 +219,8 @@ void nonbonded_forces_noalloc(int n, const double* pos, const double* q, const d
   const bool cut = method == OMMB200_CUTOFF_NON_PERIODIC;
   if (cut && !(std::isfinite(cutoff) && cutoff > 0.0))
     throw Error(OMMB200_ERR_INVALID_ARG, "cutoff must be positive and finite");
-  const ScratchView s = view(scratch_address());
+  const ScratchInfo info = scratch_info();
+  const ScratchView s = view(info.addr);
   const int blocks = (n + 31) / 32, slots = 32 * blocks;
   PairArgs<float> a{};
   a.pos = pos;
@@ -207,7 +239,7 @@ void nonbonded_forces_noalloc(int n, const double* pos, const double* q, const d
   }
   na_prepare<<<(slots + 255) / 256, 256, 0, stream>>>(n, slots, pos, q, sigma, eps, s);
   const long long tiles = (long long)blocks * (blocks + 1) / 2;
-  const int grid = (int)std::min<long long>((tiles + 3) / 4, 148LL * 8);
+  const int grid = (int)std::min<long long>((tiles + 3) / 4, (long long)info.sm_count * 8);
   if (cut)
     na_pairs<kElecReactionField><<<grid, 128, 0, stream>>>(a, n, blocks, s);
   else

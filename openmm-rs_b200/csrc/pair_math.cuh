@@ -159,7 +159,9 @@ __device__ __forceinline__ void pair_terms_x2(const PairArgs<float>& a, float2 r
     sw(r.x, eps4.x, s6.x, inv_r.x, f_lj.x, e_lj.x);
     sw(r.y, eps4.y, s6.y, inv_r.y, f_lj.y, e_lj.y);
   }
-  float2 e_el = x2::bc(0.f);
+  // The energy adds the electrostatic term to the LJ one with one rounding (a fused multiply-add):
+  // rounding the product first would drop every LJ tail smaller than half its unit in the last
+  // place, a bias that grows with the number of distant pairs.
   if (kElec == kElecEwald) {
     // screened_coulomb (nonbonded.rs:1263-1273): exp(-a^2 r^2) by exp2, erfc by the fit
     const float2 r = x2::mul(r2, inv_r);
@@ -176,18 +178,18 @@ __device__ __forceinline__ void pair_terms_x2(const PairArgs<float>& a, float2 r
     const float2 ec = x2::mul(ex, p);
     const float2 v = x2::fma(ec, inv_r, x2::mul(x2::bc(a.two_alpha_sqrtpi), ex));
     f_over_r = x2::sub(f_lj, x2::mul(x2::mul(qq, v), inv_r2));
-    if (kEnergy) e_el = x2::mul(x2::mul(qq, ec), inv_r);
+    if (kEnergy) energy = x2::fma(x2::mul(qq, ec), inv_r, e_lj);
   } else if (kElec == kElecReactionField) {
     // reaction_field (nonbonded.rs:1222-1243)
     f_over_r = x2::add(f_lj, x2::mul(qq, x2::sub(x2::bc(2.f * a.krf), x2::mul(inv_r, inv_r2))));
     if (kEnergy)
-      e_el = x2::mul(qq, x2::sub(x2::fma(x2::bc(a.krf), r2, inv_r), x2::bc(a.crf)));
+      energy = x2::fma(qq, x2::sub(x2::fma(x2::bc(a.krf), r2, inv_r), x2::bc(a.crf)), e_lj);
   } else {
     // coulomb_pair (nonbonded.rs:1186-1192)
     f_over_r = x2::sub(f_lj, x2::mul(x2::mul(qq, inv_r), inv_r2));
-    if (kEnergy) e_el = x2::mul(qq, inv_r);
+    if (kEnergy) energy = x2::fma(qq, inv_r, e_lj);
   }
-  energy = x2::add(e_lj, e_el);
+  if (!kEnergy) energy = x2::bc(0.f);
 }
 
 

@@ -4,7 +4,8 @@ ommb200_nonbonded_forces_noalloc serves callers that must not allocate device me
 inside another framework's memory pool, or a plugin that may only use the buffers it is
 handed.  Its scratch is one static device array shared
 by every call, which keeps the previous call's contents, so the check runs two calls in a row
-and compares both with the Context's forces and energy (mixed precision, 5e-6 force RMS).
+and compares both with the Context's forces and energy (mixed precision, 5e-6 force RMS; energy
+within 1e-6 relative plus 5e-7 kJ/mol per particle of FP32 pair-sum noise).
 """
 import ctypes as C
 
@@ -46,12 +47,40 @@ def context_reference(pos, q, sigma, eps, method, cutoff):
     return st.forces, st.potential_energy
 
 
-@pytest.mark.parametrize("method", ["NoCutoff", "CutoffNonPeriodic"])
-def test_noalloc_matches_context_on_two_calls(method):
+def near_cutoff_pairs(cutoff, seed):
+    """32 isolated pairs (5 nm apart, beyond the cutoff of each other) at squared distances
+    within 5e-5 rc^2 of rc^2, half inside and half outside: the exact decision band."""
+    rng = np.random.default_rng(seed)
+    n_pairs = 32
+    delta = rng.uniform(1e-8, 5e-5, n_pairs) * np.where(np.arange(n_pairs) % 2 == 0, 1.0, -1.0)
+    r = cutoff * np.sqrt(1.0 + delta)
+    pos = np.zeros((2 * n_pairs, 3))
+    pos[0::2, 0] = 5.0 * np.arange(n_pairs)
+    pos[1::2, 0] = pos[0::2, 0] + r
+    pos[:, 1] = rng.uniform(-0.5, 0.5)
+    q = rng.normal(0.0, 0.5, 2 * n_pairs)
+    sigma = rng.uniform(0.25, 0.35, 2 * n_pairs)
+    eps = rng.uniform(0.1, 0.8, 2 * n_pairs)
+    return pos, q, sigma, eps
+
+
+CASES = [("NoCutoff", 1), ("NoCutoff", 33), ("NoCutoff", 1500), ("NoCutoff", 8192),
+         ("CutoffNonPeriodic", 1), ("CutoffNonPeriodic", 33), ("CutoffNonPeriodic", 1500),
+         ("CutoffNonPeriodic", 8192), ("CutoffNonPeriodic", "near")]
+
+
+@pytest.mark.parametrize("method,n", CASES)
+def test_noalloc_matches_context_on_two_calls(method, n):
+    """n = 1 (one padded block, no pair), 33 (a second, nearly empty block), 8,192 (the whole
+    static scratch) and pairs straddling the cutoff, against the Context, on two calls."""
     import torch
 
-    n, cutoff = 1500, 1.0
-    pos, q, sigma, eps = particles(n, seed=12)
+    cutoff = 1.0
+    if n == "near":
+        pos, q, sigma, eps = near_cutoff_pairs(cutoff, seed=5)
+        n = len(q)
+    else:
+        pos, q, sigma, eps = particles(n, seed=12)
     f_ref, e_ref = context_reference(pos, q, sigma, eps, method, cutoff)
     dev = torch.device("cuda", 0)
     t = {k: torch.tensor(np.ascontiguousarray(v), dtype=torch.float64, device=dev)
@@ -78,9 +107,15 @@ def test_noalloc_matches_context_on_two_calls(method):
         torch.cuda.synchronize(dev)
         f = out_f.cpu().numpy()
         e = float(out_e.item())
-        err = float(np.sqrt(((f - f_ref) ** 2).sum() / (f_ref ** 2).sum()))
+        norm = (f_ref ** 2).sum()
+        if norm == 0.0:  # a single particle: no pair at all
+            assert not f.any() and e == 0.0 and e_ref == 0.0, (call, e, e_ref)
+            continue
+        err = float(np.sqrt(((f - f_ref) ** 2).sum() / norm))
         assert err < FORCE_RMS, (call, err)
-        assert abs(e - e_ref) < 1e-6 * abs(e_ref) + 1e-6, (call, e, e_ref)
+        # FP32 rounding of every pair energy leaves noise that grows with the particle count;
+        # it shows where the net energy is a small difference of large terms (reaction field)
+        assert abs(e - e_ref) < 1e-6 * abs(e_ref) + 5e-7 * n, (call, e, e_ref)
 
 
 def test_noalloc_rejects_more_than_its_static_capacity():
