@@ -309,19 +309,29 @@ def cpu_baseline(w, x0, threads, gpu_forces):
                       f"evaluation {first:.2f} s", "energy": e}, err
 
 
-def nve_drift(w, x, v, device, ps=50.0, sample_ps=1.0):
-    """Total-energy drift of the mixed-precision engine without a thermostat (LangevinMiddle at
-    zero friction) over `ps` picoseconds from an equilibrated state: least-squares slope of
-    E_pot + E_kin sampled every `sample_ps`."""
+def nve_drift(w, x, v, device, precision, ps=100.0, sample_ps=0.5, settle_ps=10.0, blocks=10):
+    """Total-energy drift without a thermostat (LangevinMiddle at zero friction and temperature,
+    which is velocity Verlet with SETTLE) over `ps` picoseconds at 2 fs, after `settle_ps` more
+    picoseconds at 1/ps coupling from the given state: the least-squares slope of
+    E_pot + E_kin sampled every `sample_ps`, with its standard error from the slope of `blocks`
+    block means (neighbouring samples are correlated, block means much less)."""
     import numpy as np
 
     import ommb200
     from ommb200 import systems
 
-    ctx = ommb200.Context(systems.water_system(w), systems.langevin(friction=0.0, seed=1),
-                          precision="mixed", device=device)
-    ctx.set_positions(x)
-    ctx.set_velocities(v)
+    settle = ommb200.Context(systems.water_system(w), systems.langevin(friction=1.0, seed=7),
+                             precision=precision, device=device)
+    settle.set_positions(x)
+    settle.set_velocities(v)
+    settle.step(int(round(settle_ps / DT_PS)))
+    st = settle.get_state(positions=True, velocities=True)
+    settle.close()
+    ctx = ommb200.Context(systems.water_system(w),
+                          systems.langevin(temperature=0.0, friction=0.0, seed=1),
+                          precision=precision, device=device)
+    ctx.set_positions(st.positions)
+    ctx.set_velocities(st.velocities)
     every = int(round(sample_ps / DT_PS))
     t, e = [], []
     for k in range(int(round(ps / sample_ps)) + 1):
@@ -331,11 +341,20 @@ def nve_drift(w, x, v, device, ps=50.0, sample_ps=1.0):
         if k * sample_ps < ps:
             ctx.step(every)
     ctx.close()
+    t, e = np.array(t), np.array(e)
     slope = float(np.polyfit(t, e, 1)[0]) * 1000.0  # kJ/mol/ns
+    per = len(e) // blocks
+    tb = t[:per * blocks].reshape(blocks, per).mean(1)
+    eb = e[:per * blocks].reshape(blocks, per).mean(1)
+    fit = np.polyfit(tb, eb, 1)
+    resid = eb - np.polyval(fit, tb)
+    stderr = float(np.sqrt((resid ** 2).sum() / (blocks - 2) / ((tb - tb.mean()) ** 2).sum())) * 1000.0
     dof = 3 * w.n_atoms - 3 * w.n_waters  # rigid waters: 6 degrees of freedom each
-    return {"ps": ps, "kj_mol_per_ns": slope, "kj_mol_per_ns_per_dof": slope / dof,
-            "energy_rms_fluctuation_kj_mol": float(np.std(e)), "dof": dof,
-            "samples": len(e)}
+    return {"precision": precision, "ps": ps, "settle_ps": settle_ps, "samples": len(e),
+            "kj_mol_per_ns": slope, "slope_stderr_kj_mol_per_ns": stderr,
+            "kj_mol_per_ns_per_dof": slope / dof, "slope_stderr_per_dof": stderr / dof,
+            "energy_rms_fluctuation_kj_mol": float(np.std(e - np.polyval(np.polyfit(t, e, 1), t))),
+            "dof": dof}
 
 
 def cpu_one_core(w, x0):
@@ -465,10 +484,12 @@ def main():
         pass
     barrier()
     rebuilds0 = ctx.nlist_stats()["rebuilds"]
+    prunes0 = ctx.nlist_prune_stats()["prunes"]
     sampler = ClockSampler(uuid)
     ms = time_segments(ctx, torch, args.steps, args.segment, flush)
     clocks = sampler.stop()
     rebuilds_timed = ctx.nlist_stats()["rebuilds"] - rebuilds0
+    prunes_timed = ctx.nlist_prune_stats()["prunes"] - prunes0
     barrier()
     e2e_ms, h2d, d2h = time_e2e(ctx, torch, w.n_atoms, args.steps, args.segment, flush)
     barrier()
@@ -528,12 +549,15 @@ def main():
                                                          "both kernels are latency-bound")
         per_step = {k: (v[0] / v[1], v[1] / prof_steps) for k, v in times.items()}
         extras["kernel_ms_per_md_step"] = {k: round(v[0] * v[1], 5) for k, v in per_step.items()}
-        # our kernels per MD step: rebuild condition 1, pack 1, pair 1, PME (spread, the three
-        # transform kernels, gather: 5; or spread, convert, convolve, gather: 4 beside cuFFT),
-        # exceptions 1, integrate 1; the 9 rebuild kernels only on rebuild steps; one counter
-        # kernel per graph launch of 20 steps
-        per_md = 1 + 1 + 1 + (5 if "pme_transform" in times else 4) + 1 + 1
-        launches = md_steps * per_md + 9 * rebuilds_timed + args.steps * (args.segment // 20)
+        # our kernels per MD step: rebuild condition 1, pack 1, prune condition 1 (pruned list),
+        # pair 1, PME (spread, the three transform kernels, gather: 5; or spread, convert,
+        # convolve, gather: 4 beside cuFFT), exceptions 1, integrate 1; the 8 rebuild kernels
+        # only on rebuild steps and the 3 prune kernels only on prune steps; one counter kernel
+        # per graph launch of 20 steps
+        pruned = ctx.nlist_prune_stats()["margin_nm"] > 0
+        per_md = 1 + 1 + (1 if pruned else 0) + 1 + (5 if "pme_transform" in times else 4) + 1 + 1
+        launches = (md_steps * per_md + 8 * rebuilds_timed + 3 * prunes_timed
+                    + args.steps * (args.segment // 20))
         extras["pairs_in_cutoff"] = pairs
         nl = ctx.nlist_stats()
         roofline["traffic"] = profiled_traffic(f"pair_kernel_{WORKLOAD}", nl["tiles"])
@@ -543,6 +567,8 @@ def main():
         slots = nl["blocks"] * 1024 + (nl["tiles"] - nl["blocks"]) * per_tile
         nl["pair_efficiency"] = pairs / max(1, slots)
         nl["md_steps_per_rebuild"] = md_steps / max(1, rebuilds_timed)  # timed region only
+        nl.update(ctx.nlist_prune_stats())
+        nl["md_steps_per_prune"] = md_steps / max(1, prunes_timed) if pruned else None
         extras["nlist"] = nl
         # FP64-on-GPU form of the same kernels
         _, ctx64 = build_context("double", seed, local)
@@ -559,8 +585,11 @@ def main():
             extras["energy_rel_err_vs_fp64_oracle"] = abs(e_gpu - cpu.pop("energy")) / abs(e_gpu)
             extras["host_cpu"] = {"nproc": os.cpu_count(), "model": _cpu_model()}
             extras["cpu_baseline_1_core"] = cpu_one_core(w, x0)
-        st_eq = ctx.get_state(positions=True, velocities=True)
-        extras["nve_drift"] = nve_drift(w, st_eq.positions, st_eq.velocities, local)
+        if WORKLOAD == "water-23958":  # 2 x 110 ps of dynamics: the headline box only
+            st_eq = ctx.get_state(positions=True, velocities=True)
+            mixed = nve_drift(w, st_eq.positions, st_eq.velocities, local, "mixed")
+            fp64 = nve_drift(w, st_eq.positions, st_eq.velocities, local, "double")
+            extras["nve_drift"] = {"mixed": mixed, "fp64": fp64}
     out = {
         "metric": water_metric(), "value": value, "unit": "ns/day", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,

@@ -353,12 +353,29 @@ int ommb200_context_debug_pair_list(ommb200_context* ctx, int64_t max_pairs, int
 int ommb200_context_set_profiling(ommb200_context* ctx, int enabled);
 int ommb200_context_kernel_times(ommb200_context* ctx, int max_entries, char* names,
                                  int names_len, double* ms, int* launches, int* count);
-/* Neighbour-list state after the last force evaluation: tiles (32 x 32 pair blocks) in use,
- * 32-slot particle blocks in use, tiles carrying exclusion masks, and list rebuilds so far. */
+/* Neighbour-list state after the last force evaluation: tiles (32 x 32 pair blocks) the pair
+ * kernel evaluates, 32-slot particle blocks in use, tiles of the last rebuild carrying exclusion
+ * masks, and list rebuilds so far. */
 int ommb200_context_nlist_stats(ommb200_context* ctx, int* tiles, int* blocks, int* masked,
                                 int64_t* rebuilds);
+/* Neighbour-list capacities (no reference counterpart; the reference builds its cell lists on
+ * the host at every evaluation): tile slots, particles one x-y column may hold, and how many
+ * times an overflow made them grow (the steps or the evaluation then ran again). */
+int ommb200_context_nlist_capacity(ommb200_context* ctx, int* tile_capacity, int* column_capacity,
+                                   int* regrows);
+/* The pruned pair list of periodic rectangular boxes (no reference counterpart): tiles of the
+ * last rebuild (the pair kernel's tiles are in ommb200_context_nlist_stats), prunes so far, and
+ * the margin beyond the cutoff the pruned list keeps (0 when the pair kernel reads the rebuild's
+ * tiles directly). */
+int ommb200_context_nlist_prune_stats(ommb200_context* ctx, int* rebuild_tiles, int64_t* prunes,
+                                      double* margin);
 /* The cudaStream_t every kernel of this Context is launched on (for CUDA-event timing). */
 int ommb200_context_get_stream(ommb200_context* ctx, void** stream);
+/* Diagnostics (no reference counterpart): the number of polls after which the tensor-core
+ * kernels stop waiting for their MMAs, set their status to OMMB200_ERR_TIMEOUT and return, so
+ * that the time-out path can be exercised; polls < 0 restores the default (about a
+ * millisecond).  Kernels captured in a Context's CUDA graph keep the limit of their capture. */
+int ommb200_set_tensor_core_wait_limit(long long polls);
 /* Measured FP32 FMA throughput of the device (TFLOP/s, FMA = 2 flops): the roofline
  * denominator of the FP32 pair kernel. */
 int ommb200_measure_fp32_peak(int device, double* tflops);

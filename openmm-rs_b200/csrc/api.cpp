@@ -861,6 +861,23 @@ int ommb200_context_nlist_stats(ommb200_context* ctx, int* tiles, int* blocks, i
     E.nlist_stats(tiles, blocks, masked, rebuilds);
   });
 }
+int ommb200_set_tensor_core_wait_limit(long long polls) {
+  return guarded([&] { set_tensor_wait_limit(polls); });
+}
+int ommb200_context_nlist_capacity(ommb200_context* ctx, int* tile_capacity, int* column_capacity,
+                                   int* regrows) {
+  return guarded([&] {
+    OMMB200_CTX;
+    E.nlist_capacity(tile_capacity, column_capacity, regrows);
+  });
+}
+int ommb200_context_nlist_prune_stats(ommb200_context* ctx, int* rebuild_tiles, int64_t* prunes,
+                                      double* margin) {
+  return guarded([&] {
+    OMMB200_CTX;
+    E.nlist_prune_stats(rebuild_tiles, prunes, margin);
+  });
+}
 int ommb200_context_get_stream(ommb200_context* ctx, void** stream) {
   return guarded([&] {
     OMMB200_CTX;

@@ -432,6 +432,15 @@ void Engine::setup_nonbonded(const NonbondedDef& nb) {
   a.tiles = mem_.alloc<int4>(a.tile_capacity);
   a.entries = mem_.alloc_bytes((size_t)(dp_ ? 32 : 16) * 32 * (size_t)a.tile_capacity);
   a.masks = mem_.alloc<uint32_t>(32 * (size_t)a.mask_capacity);
+  if (nb_periodic_) {  // the pruned pair list (used while pruning() holds)
+    a.block_tiles = mem_.alloc<int>(2 * (size_t)(n_slots_ / 32));
+    prune_flag_ = mem_.alloc<int>(1);
+    pos_prune_ = mem_.alloc<double>(3 * (size_t)n_);
+    prune_count_ = mem_.alloc<unsigned long long>(1);
+    prune_n_tiles_ = mem_.alloc<int>(1);
+    a.prune = prune_flag_;
+    alloc_pruned_list();
+  }
   posq_ = mem_.alloc_bytes((dp_ ? 32 : 16) * (size_t)n_slots_);
   ljp_ = mem_.alloc_bytes((dp_ ? 16 : 8) * (size_t)n_slots_);
   if (!nb_periodic_) build_static_tiles();
@@ -1129,22 +1138,74 @@ void Engine::destroy_graph() {
 
 void Engine::sync() { OMMB200_CK(cudaStreamSynchronize(stream_)); }
 
-void Engine::check_status() {
+int Engine::take_status() {
   int st = 0;
   OMMB200_CK(cudaMemcpy(&st, status_, sizeof(int), cudaMemcpyDeviceToHost));
-  if (st == 0) return;
+  if (st == 0) return 0;
   const int zero = 0;
   OMMB200_CK(cudaMemcpy(status_, &zero, sizeof(int), cudaMemcpyHostToDevice));
+  return st;
+}
+
+void Engine::check_status() { raise_status(take_status()); }
+
+void Engine::raise_status(int st) {
   switch (st) {
+    case 0:
+      return;
+    case kStatusTimeout:
+      throw Error(OMMB200_ERR_TIMEOUT, "a tensor-core wait timed out");
     case kStatusConstraint:
       throw Error(OMMB200_ERR_CONSTRAINT, "constraint projection failed (no rigid solution or no convergence in 1000 iterations)");
     case kStatusNonfinite:
       throw Error(OMMB200_ERR_NONFINITE, "a position or velocity became nonfinite");
     case kStatusTileOverflow:
-      throw Error(OMMB200_ERR_NLIST_OVERFLOW, "neighbour tile list exceeded its capacity");
+      throw Error(OMMB200_ERR_NLIST_OVERFLOW,
+                  "neighbour tile list exceeded its capacity and cannot grow further");
     default:
       throw Error(OMMB200_ERR_CUDA, "device reported status " + std::to_string(st));
   }
+}
+
+bool Engine::grow_neighbor_capacity() {
+  if (!nb_periodic_) return false;
+  NlistArgs& a = nl_;
+  int demand_tiles = 0, demand_masks = 0;
+  OMMB200_CK(cudaMemcpy(&demand_tiles, a.n_tiles, sizeof(int), cudaMemcpyDeviceToHost));
+  OMMB200_CK(cudaMemcpy(&demand_masks, a.n_masks, sizeof(int), cudaMemcpyDeviceToHost));
+  bool grew = false;
+  // per-column sort: the keys of one column live in shared memory, at most 4096
+  if (a.col_max < 4096) {
+    a.col_max = std::min(4096, 2 * a.col_max);
+    grew = true;
+  }
+  // tiles and masks: half again as many as the failed build asked for (it counts its whole
+  // demand even past the capacity), and at least 1.5 times the current arrays
+  const long long blocks = a.slot_capacity / 32;
+  const long long all_pairs = (blocks * (blocks + 1) / 2 + blocks) * 2;
+  const long long want =
+      std::min<long long>(all_pairs, std::max<long long>(3LL * demand_tiles / 2, 3LL * a.tile_capacity / 2));
+  if (want > a.tile_capacity && want < (1LL << 31) / 32) {
+    a.tile_capacity = (int)want;
+    a.tiles = mem_.alloc<int4>(a.tile_capacity);
+    a.entries = mem_.alloc_bytes((size_t)(dp_ ? 32 : 16) * 32 * (size_t)a.tile_capacity);
+    grew = true;
+  }
+  const long long want_masks = std::min<long long>(
+      a.tile_capacity, std::max<long long>(3LL * demand_masks / 2, 3LL * a.mask_capacity / 2));
+  if (want_masks > a.mask_capacity) {
+    a.mask_capacity = (int)want_masks;
+    a.masks = mem_.alloc<uint32_t>(32 * (size_t)a.mask_capacity);
+    grew = true;
+  }
+  if (!grew) return false;
+  ++regrows_;
+  if (prune_tiles_) alloc_pruned_list();  // the pruned list holds at most the rebuild's tiles
+  update_box_dependents();  // the candidate capacity follows the column size
+  destroy_graph();          // the captured launches hold the old arrays
+  const int one = 1;
+  OMMB200_CK(cudaMemcpy(rebuild_, &one, sizeof(int), cudaMemcpyHostToDevice));
+  return true;
 }
 
 void Engine::prof_begin(const char* name) {
@@ -1199,12 +1260,21 @@ void Engine::set_profiling(bool enabled) {
 void Engine::enqueue_conditional_rebuild() {
   cudaStreamCaptureStatus st;
   cudaGraph_t cap = nullptr;
-  const cudaGraphNode_t* deps = nullptr;
-  size_t nd = 0;
-  OMMB200_CK(cudaStreamGetCaptureInfo(stream_, &st, nullptr, &cap, &deps, &nd));
+  OMMB200_CK(cudaStreamGetCaptureInfo(stream_, &st, nullptr, &cap, nullptr, nullptr));
   cudaGraphConditionalHandle handle;
   OMMB200_CK(cudaGraphConditionalHandleCreate(&handle, cap, 0, cudaGraphCondAssignDefault));
   launch_nlist_condition(nl_, handle, stream_);
+  enqueue_conditional_body(handle, [&](cudaStream_t s) { launch_nlist_rebuild(nl_, dp_, s); });
+}
+
+// An IF node at the current point of the captured stream; its body is `body`'s launches,
+// captured on the auxiliary stream, and runs when `handle` (set by a kernel just before) is set.
+void Engine::enqueue_conditional_body(cudaGraphConditionalHandle handle,
+                                      const std::function<void(cudaStream_t)>& body) {
+  cudaStreamCaptureStatus st;
+  cudaGraph_t cap = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t nd = 0;
   OMMB200_CK(cudaStreamGetCaptureInfo(stream_, &st, nullptr, &cap, &deps, &nd));
   cudaGraphNodeParams params{};
   params.type = cudaGraphNodeTypeConditional;
@@ -1215,12 +1285,42 @@ void Engine::enqueue_conditional_rebuild() {
   OMMB200_CK(cudaGraphAddNode(&node, cap, deps, nd, &params));
   OMMB200_CK(cudaStreamUpdateCaptureDependencies(stream_, &node, 1,
                                                  cudaStreamSetCaptureDependencies));
-  cudaGraph_t body = params.conditional.phGraph_out[0];
-  OMMB200_CK(cudaStreamBeginCaptureToGraph(aux_stream_, body, nullptr, nullptr, 0,
+  cudaGraph_t graph = params.conditional.phGraph_out[0];
+  OMMB200_CK(cudaStreamBeginCaptureToGraph(aux_stream_, graph, nullptr, nullptr, 0,
                                            cudaStreamCaptureModeThreadLocal));
-  launch_nlist_rebuild(nl_, dp_, aux_stream_);
+  body(aux_stream_);
   cudaGraph_t done = nullptr;
   OMMB200_CK(cudaStreamEndCapture(aux_stream_, &done));
+}
+
+bool Engine::pruning() const {
+  return nb_periodic_ && nl_.block_tiles && nl_.halves && nl_.max_cand > 0 && box_[3] == 0.0 &&
+         box_[6] == 0.0 && box_[7] == 0.0;
+}
+
+void Engine::alloc_pruned_list() {
+  prune_capacity_ = nl_.tile_capacity;
+  prune_tiles_ = mem_.alloc<int4>(prune_capacity_);
+  prune_entries_ = mem_.alloc_bytes((size_t)(dp_ ? 32 : 16) * 32 * (size_t)prune_capacity_);
+  prune_masks_ = mem_.alloc<uint32_t>(32 * (size_t)prune_capacity_);
+  prune_cols_ = mem_.alloc<uint32_t>(32 * (size_t)prune_capacity_);
+}
+
+PruneArgs Engine::prune_args() const {
+  PruneArgs p{};
+  p.tiles = prune_tiles_;
+  p.entries = prune_entries_;
+  p.masks = prune_masks_;
+  p.cols = prune_cols_;
+  p.n_tiles = prune_n_tiles_;
+  p.capacity = prune_capacity_;
+  p.prune = prune_flag_;
+  p.pos_prune = pos_prune_;
+  p.posq = posq_;
+  const double reach = nb_->cutoff + kPruneMargin + kPruneAllowance;
+  p.reach2 = reach * reach;
+  p.prune_count = prune_count_;
+  return p;
 }
 
 template <class Real>
@@ -1247,17 +1347,34 @@ void Engine::enqueue_nonbonded(bool energy, bool direct, bool reciprocal, bool d
     launch_pack<Real>(n_slots_, nl_.sorted_atom, pos_, nl_.image, nl_.block_center, qscaled_,
                       half_sigma_, sqrt_eps_, posq_, ljp_, nl_.box, stream_);
     prof_end();
+    const bool pruned = pruning();
+    if (pruned) {  // a pending prune (after a rebuild, or once a particle moved margin / 2)
+      const PruneArgs pa = prune_args();
+      prof_begin("nlist_prune");
+      if (capturing_) {
+        cudaStreamCaptureStatus st;
+        cudaGraph_t cap = nullptr;
+        OMMB200_CK(cudaStreamGetCaptureInfo(stream_, &st, nullptr, &cap, nullptr, nullptr));
+        cudaGraphConditionalHandle handle;
+        OMMB200_CK(cudaGraphConditionalHandleCreate(&handle, cap, 0, cudaGraphCondAssignDefault));
+        launch_prune_condition(pa, handle, stream_);
+        enqueue_conditional_body(handle, [&](cudaStream_t s) { launch_nlist_prune(nl_, pa, dp_, s); });
+      } else {
+        launch_nlist_prune(nl_, pa, dp_, stream_);
+      }
+      prof_end();
+    }
     PairArgs<Real> p{};
     p.n_atoms = n_;
     p.sorted_atom = nl_.sorted_atom;
     p.pos = pos_;
     p.posq = posq_;
     p.ljp = ljp_;
-    p.tiles = nl_.tiles;
-    p.entries = nl_.entries;
-    p.masks = nl_.masks;
-    p.n_tiles = nl_.n_tiles;
-    p.tile_capacity = nl_.tile_capacity;
+    p.tiles = pruned ? prune_tiles_ : nl_.tiles;
+    p.entries = pruned ? prune_entries_ : nl_.entries;
+    p.masks = pruned ? prune_masks_ : nl_.masks;
+    p.n_tiles = pruned ? prune_n_tiles_ : nl_.n_tiles;
+    p.tile_capacity = pruned ? prune_capacity_ : nl_.tile_capacity;
     p.force = force_;
     p.energy = energy_;
     p.block_segment = segments_.size() > 1 ? d_block_segment_ : nullptr;
@@ -1470,6 +1587,11 @@ IntegrateArgs Engine::integrate_args(int step_offset) const {
   a.half_skin2 = 0.25 * skin_ * skin_;
   a.rebuild = rebuild_;
   a.status = status_;
+  if (pruning() && a.pos_ref) {
+    a.pos_prune = pos_prune_;
+    a.half_margin2 = 0.25 * kPruneMargin * kPruneMargin;
+    a.prune = prune_flag_;
+  }
   return a;
 }
 
@@ -1528,25 +1650,39 @@ void Engine::step(int steps) {
   }
 }
 
+// A batch of steps that overflows the periodic neighbour list (a density fluctuation, a clumpy
+// start) is not lost: the list's capacities grow, the state saved at the start of the batch is
+// restored and the batch runs again.  Forces do not depend on the tile list (the pair set is
+// decided pair by pair, the sums are fixed point), so the re-run is the run that had enough room.
 void Engine::run_steps(int steps) {
   const int k = opt_.steps_per_graph > 0 ? opt_.steps_per_graph : 20;
-  int remaining = steps;
-  if (opt_.use_graph && !profiling_ && steps >= k) {
-    if (graph_steps_ != k) destroy_graph();
-    graph_steps_ = k;
-    run_graph_steps(steps / k);
-    remaining = steps % k;
+  for (int attempt = 0;; ++attempt) {
+    const bool guarded = nb_periodic_;
+    if (guarded) save_dynamic_state(step_snapshot_);
+    int remaining = steps;
+    if (opt_.use_graph && !profiling_ && steps >= k) {
+      if (graph_steps_ != k) destroy_graph();
+      graph_steps_ = k;
+      run_graph_steps(steps / k);
+      remaining = steps % k;
+    }
+    for (int s = 0; s < remaining; ++s) {
+      enqueue_step(0);
+      launch_advance_counter(rng_step_, 1, stream_);
+    }
+    OMMB200_CK(cudaGetLastError());
+    sync();
+    harvest_profile();
+    const int st = take_status();
+    if (st == kStatusTileOverflow && guarded && grow_neighbor_capacity()) {
+      restore_dynamic_state(step_snapshot_);
+      continue;
+    }
+    time_ += steps * integ_->step_size;
+    step_count_ += steps;
+    raise_status(st);
+    return;
   }
-  for (int s = 0; s < remaining; ++s) {
-    enqueue_step(0);
-    launch_advance_counter(rng_step_, 1, stream_);
-  }
-  OMMB200_CK(cudaGetLastError());
-  sync();
-  harvest_profile();
-  time_ += steps * integ_->step_size;
-  step_count_ += steps;
-  check_status();
 }
 
 void Engine::set_positions(const double* xyz) {
@@ -1583,11 +1719,10 @@ void Engine::set_velocities_to_temperature(double temperature, int seed) {
   }
   // LFMiddle velocity_time_offset = dt/2 (langevin.rs:204-206): v -= F/m * dt/2
   const double offset = 0.5 * integ_->step_size;
-  compute_forces(false, 0xffffffffu);
+  compute_forces_checked(false, 0xffffffffu);
   std::vector<long long> f(3 * (size_t)n_);
   OMMB200_CK(cudaMemcpyAsync(f.data(), force_, 8 * f.size(), cudaMemcpyDeviceToHost, stream_));
   sync();
-  check_status();
   for (int i = 0; i < n_; ++i) {
     if (host_masses_[i] == 0.0) continue;
     for (int c = 0; c < 3; ++c) v[3 * i + c] -= (double)f[(size_t)c * n_ + i] * kForceScaleInv / host_masses_[i] * offset;
@@ -1633,10 +1768,23 @@ void Engine::apply_velocity_constraints(double tolerance) {
 
 // Forces (into `forces`, may be null) and, with `energy`, the fixed-point energy/virial
 // terms of every segment: [8 * segment + (energy, virial xx yy zz xy xz yz)].
+// compute_forces with the energy sums zeroed first, synchronised, and run again after the
+// neighbour list grew when it overflowed; any other device error is raised.
+void Engine::compute_forces_checked(bool energy, uint32_t groups) {
+  for (;;) {
+    OMMB200_CK(cudaMemsetAsync(energy_, 0, 8 * segments_.size() * sizeof(long long), stream_));
+    compute_forces(energy, groups);
+    sync();
+    const int st = take_status();
+    if (st == kStatusTileOverflow && grow_neighbor_capacity()) continue;
+    raise_status(st);
+    return;
+  }
+}
+
 std::vector<long long> Engine::evaluate(bool energy, uint32_t groups, double* forces) {
   const size_t nterms = 8 * segments_.size();
-  OMMB200_CK(cudaMemsetAsync(energy_, 0, nterms * sizeof(long long), stream_));
-  compute_forces(energy, groups);
+  compute_forces_checked(energy, groups);
   if (forces) {
     std::vector<long long> f(3 * (size_t)n_);
     OMMB200_CK(cudaMemcpyAsync(f.data(), force_, 8 * f.size(), cudaMemcpyDeviceToHost, stream_));
@@ -1931,34 +2079,59 @@ void Engine::barostat_stats(ommb200_barostat_stats* out) const {
   out->volume_scale = bar_volume_scale_;
 }
 
-void Engine::autotune(int trial_steps, double* skin_out, int* ctas_out, double* ms_out) {
-  require(trial_steps > 0, "autotune needs a positive number of trial steps");
+// The dynamic state a re-run must start from: positions, velocities, the random-stream
+// counter and, with learned radii (they train during steps), the network, its optimiser and the
+// control block.  Host-side time and step counts are untouched.
+void Engine::save_dynamic_state(DynamicSnapshot& snap) {
   const size_t bytes = 24 * (size_t)n_;
-  double* save_x = mem_.alloc<double>(3 * (size_t)n_);
-  double* save_v = mem_.alloc<double>(3 * (size_t)n_);
-  unsigned long long rng = 0;
-  OMMB200_CK(cudaMemcpyAsync(save_x, pos_, bytes, cudaMemcpyDeviceToDevice, stream_));
-  OMMB200_CK(cudaMemcpyAsync(save_v, vel_, bytes, cudaMemcpyDeviceToDevice, stream_));
-  OMMB200_CK(cudaMemcpyAsync(&rng, rng_step_, 8, cudaMemcpyDeviceToHost, stream_));
-  // learned radii train during the trials: their network and counters are restored too
-  const size_t lr_bytes =
-      4 * (size_t)(kRadiiMlpParams + 2 * kRadiiMlpTrainable + 1 + segments_.size());
-  const size_t off_at = kRadiiMlpParams + 2 * kRadiiMlpTrainable + 1;
-  float* save_lr = learned_ ? mem_.alloc<float>(lr_bytes / 4) : nullptr;
-  LearnedState save_state{};
+  if (!snap.x) {
+    snap.x = mem_.alloc<double>(3 * (size_t)n_);
+    snap.v = mem_.alloc<double>(3 * (size_t)n_);
+    if (learned_) snap.lr = mem_.alloc<float>(kRadiiMlpParams + 2 * kRadiiMlpTrainable + 1 + segments_.size());
+  }
+  OMMB200_CK(cudaMemcpyAsync(snap.x, pos_, bytes, cudaMemcpyDeviceToDevice, stream_));
+  OMMB200_CK(cudaMemcpyAsync(snap.v, vel_, bytes, cudaMemcpyDeviceToDevice, stream_));
+  OMMB200_CK(cudaMemcpyAsync(&snap.rng, rng_step_, 8, cudaMemcpyDeviceToHost, stream_));
   if (learned_) {
-    OMMB200_CK(cudaMemcpyAsync(save_lr, lr_.params, 4 * kRadiiMlpParams, cudaMemcpyDeviceToDevice,
-                               stream_));
-    OMMB200_CK(cudaMemcpyAsync(save_lr + kRadiiMlpParams, lr_.moments, 8 * kRadiiMlpTrainable,
+    const size_t at = kRadiiMlpParams + 2 * kRadiiMlpTrainable;
+    OMMB200_CK(cudaMemcpyAsync(snap.lr, lr_.params, 4 * kRadiiMlpParams, cudaMemcpyDeviceToDevice, stream_));
+    OMMB200_CK(cudaMemcpyAsync(snap.lr + kRadiiMlpParams, lr_.moments, 8 * kRadiiMlpTrainable,
                                cudaMemcpyDeviceToDevice, stream_));
-    OMMB200_CK(cudaMemcpyAsync(save_lr + kRadiiMlpParams + 2 * kRadiiMlpTrainable, lr_.adam_t, 4,
+    OMMB200_CK(cudaMemcpyAsync(snap.lr + at, lr_.adam_t, 4, cudaMemcpyDeviceToDevice, stream_));
+    OMMB200_CK(cudaMemcpyAsync(snap.lr + at + 1, lr_.seg_offset, 4 * segments_.size(),
                                cudaMemcpyDeviceToDevice, stream_));
-    OMMB200_CK(cudaMemcpyAsync(save_lr + off_at, lr_.seg_offset, 4 * segments_.size(),
-                               cudaMemcpyDeviceToDevice, stream_));
-    OMMB200_CK(cudaMemcpyAsync(&save_state, lr_.state, sizeof(save_state), cudaMemcpyDeviceToHost,
+    OMMB200_CK(cudaMemcpyAsync(&snap.state, lr_.state, sizeof(snap.state), cudaMemcpyDeviceToHost,
                                stream_));
   }
   sync();
+}
+
+// Puts the saved state back and requests a neighbour-list rebuild from it.
+void Engine::restore_dynamic_state(const DynamicSnapshot& snap) {
+  const size_t bytes = 24 * (size_t)n_;
+  OMMB200_CK(cudaMemcpyAsync(pos_, snap.x, bytes, cudaMemcpyDeviceToDevice, stream_));
+  OMMB200_CK(cudaMemcpyAsync(vel_, snap.v, bytes, cudaMemcpyDeviceToDevice, stream_));
+  OMMB200_CK(cudaMemcpyAsync(rng_step_, &snap.rng, 8, cudaMemcpyHostToDevice, stream_));
+  const int one = 1;
+  OMMB200_CK(cudaMemcpyAsync(rebuild_, &one, sizeof(int), cudaMemcpyHostToDevice, stream_));
+  if (learned_) {
+    const size_t at = kRadiiMlpParams + 2 * kRadiiMlpTrainable;
+    OMMB200_CK(cudaMemcpyAsync(lr_.params, snap.lr, 4 * kRadiiMlpParams, cudaMemcpyDeviceToDevice, stream_));
+    OMMB200_CK(cudaMemcpyAsync(lr_.moments, snap.lr + kRadiiMlpParams, 8 * kRadiiMlpTrainable,
+                               cudaMemcpyDeviceToDevice, stream_));
+    OMMB200_CK(cudaMemcpyAsync(lr_.adam_t, snap.lr + at, 4, cudaMemcpyDeviceToDevice, stream_));
+    OMMB200_CK(cudaMemcpyAsync(lr_.seg_offset, snap.lr + at + 1, 4 * segments_.size(),
+                               cudaMemcpyDeviceToDevice, stream_));
+    OMMB200_CK(cudaMemcpyAsync(lr_.state, &snap.state, sizeof(snap.state), cudaMemcpyHostToDevice,
+                               stream_));
+  }
+  sync();
+}
+
+void Engine::autotune(int trial_steps, double* skin_out, int* ctas_out, double* ms_out) {
+  require(trial_steps > 0, "autotune needs a positive number of trial steps");
+  DynamicSnapshot saved;
+  save_dynamic_state(saved);
   const double time0 = time_;
   const int64_t steps0 = step_count_;
   const bool prof = profiling_;
@@ -1967,24 +2140,7 @@ void Engine::autotune(int trial_steps, double* skin_out, int* ctas_out, double* 
   OMMB200_CK(cudaEventCreate(&t0));
   OMMB200_CK(cudaEventCreate(&t1));
   auto restore = [&]() {
-    OMMB200_CK(cudaMemcpyAsync(pos_, save_x, bytes, cudaMemcpyDeviceToDevice, stream_));
-    OMMB200_CK(cudaMemcpyAsync(vel_, save_v, bytes, cudaMemcpyDeviceToDevice, stream_));
-    OMMB200_CK(cudaMemcpyAsync(rng_step_, &rng, 8, cudaMemcpyHostToDevice, stream_));
-    const int one = 1;
-    OMMB200_CK(cudaMemcpyAsync(rebuild_, &one, sizeof(int), cudaMemcpyHostToDevice, stream_));
-    if (learned_) {
-      OMMB200_CK(cudaMemcpyAsync(lr_.params, save_lr, 4 * kRadiiMlpParams,
-                                 cudaMemcpyDeviceToDevice, stream_));
-      OMMB200_CK(cudaMemcpyAsync(lr_.moments, save_lr + kRadiiMlpParams, 8 * kRadiiMlpTrainable,
-                                 cudaMemcpyDeviceToDevice, stream_));
-      OMMB200_CK(cudaMemcpyAsync(lr_.adam_t, save_lr + kRadiiMlpParams + 2 * kRadiiMlpTrainable,
-                                 4, cudaMemcpyDeviceToDevice, stream_));
-      OMMB200_CK(cudaMemcpyAsync(lr_.seg_offset, save_lr + off_at, 4 * segments_.size(),
-                                 cudaMemcpyDeviceToDevice, stream_));
-      OMMB200_CK(cudaMemcpyAsync(lr_.state, &save_state, sizeof(save_state),
-                                 cudaMemcpyHostToDevice, stream_));
-    }
-    sync();
+    restore_dynamic_state(saved);
     time_ = time0;
     step_count_ = steps0;
   };
@@ -2065,11 +2221,32 @@ void Engine::tuning(double* skin, int* pair_ctas_per_sm, int* tile_entries) cons
   if (tile_entries) *tile_entries = rect && nl_.halves ? 16 : 32;
 }
 
+void Engine::nlist_capacity(int* tile_capacity, int* column_capacity, int* regrows) const {
+  if (tile_capacity) *tile_capacity = nl_.tile_capacity;
+  if (column_capacity) *column_capacity = nb_periodic_ ? nl_.col_max : 0;
+  if (regrows) *regrows = regrows_;
+}
+
+void Engine::nlist_prune_stats(int* rebuild_tiles, int64_t* prunes, double* margin) {
+  int t = 0;
+  unsigned long long c = 0;
+  if (nb_ && nb_periodic_) {
+    OMMB200_CK(cudaMemcpyAsync(&t, nl_.n_tiles, 4, cudaMemcpyDeviceToHost, stream_));
+    OMMB200_CK(cudaMemcpyAsync(&c, prune_count_, 8, cudaMemcpyDeviceToHost, stream_));
+    sync();
+  }
+  if (rebuild_tiles) *rebuild_tiles = t;
+  if (prunes) *prunes = pruning() ? (int64_t)c : 0;
+  if (margin) *margin = pruning() ? kPruneMargin : 0.0;
+}
+
 void Engine::nlist_stats(int* tiles, int* blocks, int* masked, int64_t* rebuilds) {
   int v[3] = {0, 0, 0};
   unsigned long long r = 0;
   if (nb_) {
-    OMMB200_CK(cudaMemcpyAsync(&v[0], nl_.n_tiles, 4, cudaMemcpyDeviceToHost, stream_));
+    // the tiles the pair kernel evaluates: the pruned list's while pruning
+    OMMB200_CK(cudaMemcpyAsync(&v[0], pruning() ? prune_n_tiles_ : nl_.n_tiles, 4,
+                               cudaMemcpyDeviceToHost, stream_));
     OMMB200_CK(cudaMemcpyAsync(&v[1], nl_.n_blocks, 4, cudaMemcpyDeviceToHost, stream_));
     OMMB200_CK(cudaMemcpyAsync(&v[2], nl_.n_masks, 4, cudaMemcpyDeviceToHost, stream_));
     OMMB200_CK(cudaMemcpyAsync(&r, nl_.rebuild_count, 8, cudaMemcpyDeviceToHost, stream_));
@@ -2098,7 +2275,15 @@ int64_t Engine::debug_pair_list(int64_t max_pairs, int32_t* pairs) {
   OMMB200_CK(cudaMemsetAsync(dump_count_, 0, 8, stream_));
   dump_mode_ = true;
   try {
-    compute_forces(false, 0xffffffffu);
+    for (;;) {  // an overflowing list grows and the dump starts again
+      OMMB200_CK(cudaMemsetAsync(dump_count_, 0, 8, stream_));
+      compute_forces(false, 0xffffffffu);
+      sync();
+      const int st = take_status();
+      if (st == kStatusTileOverflow && grow_neighbor_capacity()) continue;
+      raise_status(st);
+      break;
+    }
   } catch (...) {
     dump_mode_ = false;
     throw;
@@ -2124,6 +2309,7 @@ struct CheckpointHeader {
   char magic[8];
   uint32_t version;
   int32_t n_atoms, n_segments, precision, learned, dynamic_list, rebuild_flag, pair_grid, halves;
+  int32_t prune_flag, unused;
   double time;
   int64_t step_count;
   double box[9];
@@ -2135,12 +2321,12 @@ struct CheckpointHeader {
   double bar_volume_scale, bar_pressure, bar_temperature;
 };
 constexpr char kCheckpointMagic[8] = {'O', 'M', 'B', '2', 'C', 'K', 'P', 'T'};
-constexpr uint32_t kCheckpointVersion = 4;
+constexpr uint32_t kCheckpointVersion = 5;
 }  // namespace
 
 size_t Engine::checkpoint_bytes() const {
   size_t b = sizeof(CheckpointHeader) + 2 * 24 * (size_t)n_;
-  if (nb_periodic_) b += 24 * (size_t)n_;
+  if (nb_periodic_) b += 2 * 24 * (size_t)n_;  // rebuild and prune reference positions
   if (learned_)
     b += 4 * (size_t)(kRadiiMlpParams + 2 * kRadiiMlpTrainable + 1 + segments_.size() + 1) +
          sizeof(LearnedState);
@@ -2175,9 +2361,11 @@ void Engine::save_checkpoint(uint8_t* out, size_t bytes) {
   h.bar_volume_scale = bar_volume_scale_;
   h.bar_pressure = bar_pressure_;
   h.bar_temperature = bar_temperature_;
-  int flag = 0;
+  int flag = 0, prune_flag = 0;
   OMMB200_CK(cudaMemcpyAsync(&h.rng_step, rng_step_, 8, cudaMemcpyDeviceToHost, stream_));
   OMMB200_CK(cudaMemcpyAsync(&flag, rebuild_, 4, cudaMemcpyDeviceToHost, stream_));
+  if (prune_flag_)
+    OMMB200_CK(cudaMemcpyAsync(&prune_flag, prune_flag_, 4, cudaMemcpyDeviceToHost, stream_));
   uint8_t* p = out + sizeof(CheckpointHeader);
   auto take = [&](const void* dev, size_t n) {
     OMMB200_CK(cudaMemcpyAsync(p, dev, n, cudaMemcpyDeviceToHost, stream_));
@@ -2185,7 +2373,10 @@ void Engine::save_checkpoint(uint8_t* out, size_t bytes) {
   };
   take(pos_, 24 * (size_t)n_);
   take(vel_, 24 * (size_t)n_);
-  if (nb_periodic_) take(nl_.pos_ref, 24 * (size_t)n_);
+  if (nb_periodic_) {
+    take(nl_.pos_ref, 24 * (size_t)n_);
+    take(pos_prune_, 24 * (size_t)n_);
+  }
   if (learned_) {
     take(lr_.params, 4 * kRadiiMlpParams);
     take(lr_.moments, 8 * kRadiiMlpTrainable);
@@ -2196,6 +2387,7 @@ void Engine::save_checkpoint(uint8_t* out, size_t bytes) {
   }
   sync();
   h.rebuild_flag = flag;
+  h.prune_flag = prune_flag;
   std::memcpy(out, &h, sizeof(h));
 }
 
@@ -2252,8 +2444,24 @@ void Engine::load_checkpoint(const uint8_t* in, size_t bytes) {
     const int one = 1;
     OMMB200_CK(cudaMemcpy(rebuild_, &one, 4, cudaMemcpyHostToDevice));
     launch_nlist_rebuild(from_ref, dp_, stream_);
+    // and the pruned list from the positions of the original run's last prune (its tiles hold
+    // the same entries, so every per-tile sum rounds the same)
+    put(pos_prune_, 24 * (size_t)n_);
+    if (pruning() && nb_) {
+      NlistArgs from_prune = nl_;
+      from_prune.pos = pos_prune_;
+      OMMB200_CK(cudaMemcpy(prune_flag_, &one, 4, cudaMemcpyHostToDevice));
+      if (dp_)
+        launch_pack<double>(n_slots_, nl_.sorted_atom, pos_prune_, nl_.image, nl_.block_center,
+                            qscaled_, half_sigma_, sqrt_eps_, posq_, ljp_, nl_.box, stream_);
+      else
+        launch_pack<float>(n_slots_, nl_.sorted_atom, pos_prune_, nl_.image, nl_.block_center,
+                           qscaled_, half_sigma_, sqrt_eps_, posq_, ljp_, nl_.box, stream_);
+      launch_nlist_prune(from_prune, prune_args(), dp_, stream_);
+    }
     sync();
     OMMB200_CK(cudaMemcpy(rebuild_, &h.rebuild_flag, 4, cudaMemcpyHostToDevice));
+    OMMB200_CK(cudaMemcpy(prune_flag_, &h.prune_flag, 4, cudaMemcpyHostToDevice));
   }
   if (learned_) {
     put(lr_.params, 4 * kRadiiMlpParams);

@@ -4,6 +4,7 @@
 
 #include <cufft.h>
 
+#include <functional>
 #include <memory>
 #include <string>
 #include <vector>
@@ -25,6 +26,11 @@ void nonbonded_forces_noalloc(int n, const double* pos, const double* q, const d
 constexpr double kTunedSkins[] = {0.06, 0.08, 0.1, 0.13, 0.16, 0.2};
 constexpr double kMaxTunedSkin = 0.2;
 constexpr int kTunedPairCtasPerSm[] = {4, 6, 7, 8, 9, 10, 11, 12};
+// Margin of the pruned pair list (nm): entries within cutoff + margin of their half block stay;
+// a particle that moves margin / 2 requests the next prune.  The allowance absorbs the FP32
+// rounding of the prune's distances.
+constexpr double kPruneMargin = 0.05;
+constexpr double kPruneAllowance = 1e-4;
 
 class DeviceArena {
  public:
@@ -45,6 +51,15 @@ struct EngineOptions {
   bool use_graph = true;
   double skin = 0.0;
   int steps_per_graph = 0;
+};
+
+// Device state that a re-run of MD steps starts from (Engine::save_dynamic_state).
+struct DynamicSnapshot {
+  double* x = nullptr;
+  double* v = nullptr;
+  float* lr = nullptr;  // learned radii: network, optimiser moments and step, system offsets
+  unsigned long long rng = 0;
+  LearnedState state{};
 };
 
 class Engine {
@@ -75,6 +90,8 @@ class Engine {
                  ommb200_state_info* info);
   void pme_parameters(double* alpha, int* nx, int* ny, int* nz) const;
   void nlist_stats(int* tiles, int* blocks, int* masked, int64_t* rebuilds);
+  void nlist_capacity(int* tile_capacity, int* column_capacity, int* regrows) const;
+  void nlist_prune_stats(int* rebuild_tiles, int64_t* prunes, double* margin);
   // current skin, pair-kernel CTAs per SM and neighbour entries per i-group (16: halves of
   // 32-particle blocks; 32: whole blocks)
   void tuning(double* skin, int* pair_ctas_per_sm, int* tile_entries) const;
@@ -119,9 +136,17 @@ class Engine {
   void update_box_dependents();
   void build_static_tiles();
   void enqueue_conditional_rebuild();
+  void enqueue_conditional_body(cudaGraphConditionalHandle handle,
+                                const std::function<void(cudaStream_t)>& body);
+  // The pair kernel runs on the pruned list: periodic rectangular boxes whose rebuild packs 16
+  // entries per half block (the builder that records each block's tiles).
+  bool pruning() const;
+  void alloc_pruned_list();
+  PruneArgs prune_args() const;
   // `in_step`: an MD step's evaluation (the learned radii may judge and train there);
   // `step_offset`: its position inside the captured group of steps.
   void compute_forces(bool energy, uint32_t groups, bool in_step = false, int step_offset = 0);
+  void compute_forces_checked(bool energy, uint32_t groups);
   void setup_learned(const LearnedRadiiDef& def);
   void upload_nonbonded_parameters(const NonbondedDef& nb);
   std::vector<long long> evaluate(bool energy, uint32_t groups, double* forces);
@@ -138,6 +163,14 @@ class Engine {
   // long-range corrections added to the fixed-point sums e[8] (energy, virial) of `groups`
   double assemble_energy(const long long e[8], uint32_t groups, double w[6]) const;
   void check_status();
+  // Reads and clears the device status word; raise_status throws its error (0: none).
+  int take_status();
+  void raise_status(int status);
+  // After a neighbour-list overflow: larger tile and mask arrays and per-column sort, and a
+  // rebuild requested; false when nothing can grow any more.
+  bool grow_neighbor_capacity();
+  void save_dynamic_state(DynamicSnapshot& snap);
+  void restore_dynamic_state(const DynamicSnapshot& snap);
   void sync();
   void destroy_graph();
   template <class Real>
@@ -230,6 +263,16 @@ class Engine {
   bool dump_mode_ = false;
   int pair_grid_ = 0;
   int sm_count_ = 148;
+  // pruned pair list (PruneArgs): inner tiles, entries, masks, exclusion columns, counters
+  int4* prune_tiles_ = nullptr;
+  void* prune_entries_ = nullptr;
+  uint32_t* prune_masks_ = nullptr;
+  uint32_t* prune_cols_ = nullptr;
+  int* prune_n_tiles_ = nullptr;
+  int prune_capacity_ = 0;
+  int* prune_flag_ = nullptr;
+  double* pos_prune_ = nullptr;
+  unsigned long long* prune_count_ = nullptr;
 
   // segments (independent systems) and the segment-padded slot order shared by the
   // non-periodic nonbonded tiles and GBSA: every segment starts on a 32-slot boundary
@@ -266,6 +309,9 @@ class Engine {
   int* cluster_atom_start_ = nullptr;
   int* cluster_atoms_ = nullptr;
   double skin_ = 0.0;
+
+  DynamicSnapshot step_snapshot_;  // start of the current run_steps batch (periodic systems)
+  int regrows_ = 0;                 // neighbour-list capacity increases so far
 
   // graph
   cudaGraph_t graph_ = nullptr;

@@ -154,6 +154,10 @@ __device__ __forceinline__ void check_rebuild(const IntegrateArgs& a, int atom, 
   const double dx = x[0] - a.pos_ref[3 * atom], dy = x[1] - a.pos_ref[3 * atom + 1],
                dz = x[2] - a.pos_ref[3 * atom + 2];
   if (dx * dx + dy * dy + dz * dz > a.half_skin2) *a.rebuild = 1;
+  if (!a.pos_prune) return;
+  const double px = x[0] - a.pos_prune[3 * atom], py = x[1] - a.pos_prune[3 * atom + 1],
+               pz = x[2] - a.pos_prune[3 * atom + 2];
+  if (px * px + py * py + pz * pz > a.half_margin2) *a.prune = 1;
 }
 
 // drift / thermostat / drift for one particle (langevin.rs:121-134 without the kick)

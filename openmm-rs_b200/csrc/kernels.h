@@ -63,9 +63,31 @@ struct NlistArgs {
   int col_max;        // largest column the per-column sort accepts
   int max_cand;       // candidate blocks one block can have (rectangular boxes), 0 = unknown
   int halves;         // rectangular boxes: 16 entries per half of a block (else 32 per block)
+  int* block_tiles;   // [2 * blocks] first tile and tile count of each block (halves builder)
+  int* prune;         // null, or set by every rebuild: the pruned list must be made again
+};
+
+// Pruned list: the rebuild's tiles cut down to the entries within cutoff + margin of a particle
+// of their half block at the current positions (the pair kernel's list while pruning is on).
+struct PruneArgs {
+  int4* tiles;          // [capacity] (I, flags, mask slot = tile index, 0)
+  void* entries;        // [32 * capacity] as the rebuild's entries
+  uint32_t* masks;      // [32 * capacity]
+  uint32_t* cols;       // [32 * capacity] scratch: exclusion column (bit per i-slot) per entry
+  int* n_tiles;         // tiles in use
+  int capacity;
+  int* prune;           // nonzero: prune before this evaluation's pair kernel
+  double* pos_prune;    // [3N] positions at the last prune
+  const void* posq;     // this evaluation's packed particles
+  double reach2;        // (cutoff + margin + a rounding allowance)^2
+  unsigned long long* prune_count;
 };
 
 void launch_nlist_rebuild(const NlistArgs& a, bool double_entries, cudaStream_t s);
+void launch_nlist_prune(const NlistArgs& a, const PruneArgs& p, bool double_entries,
+                        cudaStream_t s);
+// Sets `handle` to whether a prune is pending (the graph form of the early-exit prune kernels).
+void launch_prune_condition(const PruneArgs& p, cudaGraphConditionalHandle handle, cudaStream_t s);
 // Sets `handle` (a conditional graph node's condition) to whether a rebuild is pending.
 void launch_nlist_condition(const NlistArgs& a, cudaGraphConditionalHandle handle,
                             cudaStream_t s);
@@ -347,6 +369,9 @@ struct IntegrateArgs {
   double half_skin2;
   int* rebuild;
   int* status;
+  const double* pos_prune;        // positions at the last prune of the pair list (may be null)
+  double half_margin2;            // (margin / 2)^2: a particle moved farther requests a prune
+  int* prune;
 };
 void launch_integrate(const IntegrateArgs& a, cudaStream_t s);
 // Barostat volume move: positions scaled, per particle or per molecule (CSR lists of atoms)
@@ -376,6 +401,9 @@ void launch_mlp_infer(int n, const float* features, const float* params, float* 
 // snapshot rows (all of them in order when batch == n).  adam_m / adam_v hold the moments of
 // the trainable block, *adam_t the step count; grad_out (may be null) receives the gradient of
 // the last batch, loss_out[steps] (may be null) each batch's mean squared error.
+// Polls of the tensor-core kernels' MMA completion waits (polls < 0: the default, about a
+// millisecond); a smaller limit makes them give up, set the time-out status and return.
+void set_tensor_wait_limit(long long polls);
 void launch_mlp_train(int n, const float* features, const float* targets, float* params,
                       float* adam_m, float* adam_v, int* adam_t, int steps, int batch, float lr,
                       unsigned long long seed, float* grad_out, float* loss_out, int* status,

@@ -20,6 +20,8 @@
 //
 // Every kernel returns at once unless `rebuild` is set, so the sequence can sit in a CUDA
 // graph that is replayed every step.
+#include <type_traits>
+
 #include "kernels.h"
 
 namespace ommb200 {
@@ -749,6 +751,10 @@ __global__ void __launch_bounds__(32 * kCtaWarps, 4) nl_lists_cta(NlistArgs a) {
       }
       s_tile0 = t0;
       s_ntiles = nt;
+      if (a.block_tiles) {
+        a.block_tiles[2 * I] = t0;
+        a.block_tiles[2 * I + 1] = t0 < 0 ? 0 : nt;
+      }
     }
   }
   __syncthreads();
@@ -827,6 +833,204 @@ __global__ void nl_clear_flag(NlistArgs a) {
   if (*a.rebuild == 0) return;
   *a.rebuild = 0;
   *a.rebuild_count += 1;
+  if (a.prune) *a.prune = 1;  // the pruned list derives from the tiles just built
+}
+
+// ---- pruned list ---------------------------------------------------------------------------
+// The rebuild keeps every particle within cutoff + skin of a half block's box; between rebuilds
+// the pair kernel needs only those within cutoff of a particle of the half.  The prune keeps an
+// entry while it lies within cutoff + margin of some particle of its half at the current
+// positions and packs each half's kept entries, in their rebuild order, 16 to an inner tile; the
+// integrator asks for a new prune once a particle has moved more than margin / 2 since the last
+// one, so every pair within the cutoff until then stays listed (a pair approaches by less than
+// the margin, and it is among the rebuild's tiles while no particle moved skin / 2).  One CTA per
+// block I: pass 1 tests the entries of I's tiles (kept bits), a prefix over the tiles gives each
+// kept entry its place, pass 2 moves the entries with their exclusion columns (the bits of the
+// i-slots that exclude them), pass 3 writes each inner tile's masks (exclusions, padding) and
+// header.  Block I's self tile is copied.  A block with more tiles than the shared arrays hold
+// keeps all its entries (still a valid list).
+constexpr int kPruneMaxTiles = 256;
+constexpr int kPruneSharedCols = 64;  // inner tiles whose exclusion columns stay in shared memory
+
+template <bool kDouble>
+__global__ void __launch_bounds__(32 * kCtaWarps) nl_prune(const NlistArgs a, const PruneArgs p) {
+  if (*p.prune == 0) return;
+  using T4 = typename std::conditional<kDouble, double4, float4>::type;
+  using R = typename std::conditional<kDouble, double, float>::type;
+  __shared__ T4 s_i[32];
+  __shared__ int s_iatom[32];
+  __shared__ unsigned s_keep[kPruneMaxTiles];
+  __shared__ int s_pre[2][kPruneMaxTiles + 1];
+  __shared__ uint32_t s_cols[kPruneSharedCols][32];
+  __shared__ int s_t0, s_nt, s_img;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int I = blockIdx.x;
+  if (I >= *a.n_blocks) return;
+  const int t_out = a.block_tiles[2 * I], n_out = a.block_tiles[2 * I + 1];
+  if (t_out < 0 || n_out < 1 || t_out + n_out > a.tile_capacity) return;  // an overflowed build
+  const T4* posq = reinterpret_cast<const T4*>(p.posq);
+  const T4* ent = reinterpret_cast<const T4*>(a.entries);
+  T4* ent_in = reinterpret_cast<T4*>(p.entries);
+  const int n_nbr = n_out - 1;  // tile t_out is I's self tile
+  const bool all = n_nbr > kPruneMaxTiles;
+  if (w == 0) {
+    const int ai = a.sorted_atom[32 * I + lane];
+    s_iatom[lane] = ai;
+    s_i[lane] = posq[32 * I + lane];
+    if (ai >= 0)
+      for (int c = 0; c < 3; ++c) p.pos_prune[3 * ai + c] = a.pos[3 * ai + c];
+    if (lane == 0) s_img = 0;
+  }
+  __syncthreads();
+  // pass 1: an entry stays when it comes within reach of a particle of its half
+  const R reach2 = (R)p.reach2;
+  for (int k = w; k < (all ? 0 : n_nbr); k += kCtaWarps) {
+    const int t = t_out + 1 + k;
+    const T4 e = ent[32 * t + lane];
+    int slot;
+    if constexpr (kDouble) slot = (int)e.w;
+    else slot = __float_as_int(e.w);
+    bool keep = false;
+    if (slot >= 0) {
+      const T4 pj = posq[slot];
+      const R x = pj.x + e.x, y = pj.y + e.y, z = pj.z + e.z;
+      const int hb = lane & 16;
+      const bool image = (a.tiles[t].y & kTilePairImage) != 0;
+#pragma unroll 4
+      for (int q = 0; q < 16; ++q) {
+        const T4 pi = s_i[hb + q];
+        R dx = x - pi.x, dy = y - pi.y, dz = z - pi.z;
+        if (image) {
+          Box<R> b;
+          b.ax = (R)a.box.ax; b.bx = (R)a.box.bx; b.by = (R)a.box.by;
+          b.cx = (R)a.box.cx; b.cy = (R)a.box.cy; b.cz = (R)a.box.cz;
+          b.inv_ax = (R)a.box.inv_ax; b.inv_by = (R)a.box.inv_by; b.inv_cz = (R)a.box.inv_cz;
+          min_image_fast(dx, dy, dz, b);
+        }
+        keep = keep || (s_iatom[hb + q] >= 0 && dx * dx + dy * dy + dz * dz < reach2);
+      }
+    }
+    const unsigned kb = __ballot_sync(kFull, keep);
+    if (lane == 0) s_keep[k] = kb;
+  }
+  __syncthreads();
+  // prefix of the kept entries per half over I's tiles (warp h for half h)
+  if (w < 2) {
+    int carry = 0;
+    const int n_scan = all ? 0 : n_nbr;
+    for (int base = 0; base < n_scan; base += 32) {
+      const int k = base + lane;
+      const int v = k < n_scan ? __popc((s_keep[k] >> (16 * w)) & 0xffffu) : 0;
+      int incl = v;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += y;
+      }
+      if (k < n_scan) s_pre[w][k] = carry + incl - v;
+      carry += __shfl_sync(kFull, incl, 31);
+    }
+    if (lane == 0) s_pre[w][all ? 0 : n_nbr] = carry;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int longest = all ? 16 * n_nbr : max(s_pre[0][n_nbr], s_pre[1][n_nbr]);
+    const int nt = 1 + (longest + 15) / 16;
+    int t0 = atomicAdd(p.n_tiles, nt);
+    if (t0 + nt > p.capacity) {
+      report_status(a.status, kStatusTileOverflow);
+      t0 = -1;
+    }
+    s_t0 = t0;
+    s_nt = nt;
+  }
+  __syncthreads();
+  if (s_t0 < 0) return;
+  // exclusion columns of the inner neighbour tiles: shared memory, or the global scratch for a
+  // block with more tiles than that holds
+  const bool shared_cols = s_nt - 1 <= kPruneSharedCols;
+  uint32_t* cols = shared_cols ? &s_cols[0][0] : p.cols + 32 * (size_t)(s_t0 + 1);
+  // block I's self tile, unchanged (its mask slot becomes its tile index)
+  if (w == 0) {
+    int4 hdr = a.tiles[t_out];
+    const bool masked = (hdr.y & kTileHasMask) != 0 && hdr.z >= 0;
+    p.masks[32 * s_t0 + lane] = masked ? a.masks[32 * hdr.z + lane] : 0u;
+    hdr.z = s_t0;
+    if (!masked) hdr.y &= ~kTileHasMask;
+    if (lane == 0) p.tiles[s_t0] = hdr;
+  }
+  // pass 2: the kept entries to their inner places, with their exclusion columns
+  for (int k = w; k < n_nbr; k += kCtaWarps) {
+    const int t = t_out + 1 + k;
+    const int4 hdr = a.tiles[t];
+    if (lane == 0 && (hdr.y & kTilePairImage)) atomicOr(&s_img, kTilePairImage);
+    const T4 e = ent[32 * t + lane];
+    const unsigned kb = all ? kFull : s_keep[k];  // all: the tile as it is, padding included
+    uint32_t col = 0u;  // i-slots of this entry's half that exclude it
+    if ((hdr.y & kTileHasMask) && hdr.z >= 0) {
+      const uint32_t row = a.masks[32 * hdr.z + lane];
+      for (int q = 0; q < 32; ++q) {
+        const unsigned c = __ballot_sync(kFull, (row >> q) & 1u);
+        if (lane == q) col = c;
+      }
+    }
+    if ((kb >> lane) & 1u) {
+      const int half = lane >> 4;
+      const unsigned before = kb & ((1u << lane) - 1u) & (half ? 0xffff0000u : 0xffffu);
+      const int r = (all ? 16 * k : s_pre[half][k]) + __popc(before);
+      const int j = r / 16, q = 16 * half + (r & 15);
+      ent_in[32 * (s_t0 + 1 + j) + q] = e;
+      cols[32 * j + q] = col;
+    }
+  }
+  // padding places of each half's last tile
+  const int tot_a = all ? 16 * n_nbr : s_pre[0][n_nbr], tot_b = all ? 16 * n_nbr : s_pre[1][n_nbr];
+  for (int idx = threadIdx.x; idx < (s_nt - 1) * 32; idx += blockDim.x) {
+    const int j = idx >> 5, q = idx & 31, r = 16 * j + (q & 15);
+    if (r >= ((q & 16) ? tot_b : tot_a)) {
+      T4 pad;
+      pad.x = pad.y = pad.z = R(0);
+      if constexpr (kDouble) pad.w = -1.0;
+      else pad.w = __int_as_float(-1);
+      ent_in[32 * (s_t0 + 1 + j) + q] = pad;
+      cols[32 * j + q] = 0u;
+    }
+  }
+  __syncthreads();
+  // pass 3: masks (exclusions of the lane's i-slot among its half's entries, padding) and headers
+  const int ai = s_iatom[lane];
+  const int hb = lane & 16, tot = hb ? tot_b : tot_a;
+  for (int j = w; j < s_nt - 1; j += kCtaWarps) {
+    const int ti = s_t0 + 1 + j;
+    uint32_t m = 0u;
+    if (ai < 0) {
+      m = kFull;
+    } else {
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        const bool pad = 16 * j + q >= tot;
+        const bool excl = (cols[32 * j + hb + q] >> lane) & 1u;
+        if (pad || excl) m |= 1u << (hb + q);
+      }
+    }
+    p.masks[32 * ti + lane] = m;
+    const bool any = __any_sync(kFull, m != 0u);
+    if (lane == 0)
+      p.tiles[ti] = make_int4(I, kTileHalves | s_img | (any ? kTileHasMask : 0), ti, 0);
+  }
+}
+
+__global__ void nl_prune_begin(PruneArgs p) {
+  if (*p.prune) *p.n_tiles = 0;
+}
+
+__global__ void nl_prune_end(PruneArgs p) {
+  if (*p.prune == 0) return;
+  *p.prune = 0;
+  *p.prune_count += 1;
+}
+
+__global__ void nl_prune_condition(const int* prune, cudaGraphConditionalHandle handle) {
+  cudaGraphSetConditional(handle, *prune != 0 ? 1u : 0u);
 }
 
 }  // namespace
@@ -834,6 +1038,21 @@ __global__ void nl_clear_flag(NlistArgs a) {
 void launch_nlist_condition(const NlistArgs& a, cudaGraphConditionalHandle handle,
                             cudaStream_t s) {
   nl_set_condition<<<1, 1, 0, s>>>(a.rebuild, handle);
+}
+
+void launch_prune_condition(const PruneArgs& p, cudaGraphConditionalHandle handle, cudaStream_t s) {
+  nl_prune_condition<<<1, 1, 0, s>>>(p.prune, handle);
+}
+
+void launch_nlist_prune(const NlistArgs& a, const PruneArgs& p, bool double_entries,
+                        cudaStream_t s) {
+  const int block_cap = a.slot_capacity / 32;
+  nl_prune_begin<<<1, 1, 0, s>>>(p);
+  if (double_entries)
+    nl_prune<true><<<block_cap, 32 * kCtaWarps, 0, s>>>(a, p);
+  else
+    nl_prune<false><<<block_cap, 32 * kCtaWarps, 0, s>>>(a, p);
+  nl_prune_end<<<1, 1, 0, s>>>(p);
 }
 
 void launch_nlist_rebuild(const NlistArgs& a, bool double_entries, cudaStream_t s) {

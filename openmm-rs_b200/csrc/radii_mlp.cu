@@ -16,6 +16,8 @@
 // batches of particles): the weight gradients h1^T d2 and d1^T X of each 128-particle chunk
 // are one M = 128, N = 96, K = 128 MMA chain accumulated in tensor memory across the batch;
 // bias gradients are fixed-order block reductions, so a training step is deterministic.
+#include <atomic>
+
 #include "kernels.h"
 #include "tcgen05.cuh"
 
@@ -26,7 +28,12 @@ using bf16 = __nv_bfloat16;
 using namespace tc;
 
 constexpr int kNF = 32, kH = 64;
+// Polls of an mbarrier wait before a kernel gives up (about a millisecond).  The waits for a
+// round of MMAs take their limit from the launch (ommb200_set_tensor_core_wait_limit lowers it
+// to exercise the time-out path); the drain after a time-out always takes the full limit, so
+// no MMA still writes tensor memory when it is freed.
 constexpr uint32_t kWaitLimit = 1u << 22;
+std::atomic<uint32_t> g_wait_limit{kWaitLimit};
 
 // parameter block (floats)
 constexpr int kOffW1 = 0, kOffB1 = 2048, kOffW2 = 2112, kOffB2 = 6208, kOffW3 = 6272,
@@ -122,7 +129,8 @@ __global__ void __launch_bounds__(128) mlp_infer_kernel(int n, const float* __re
                                                         const float* __restrict__ P,
                                                         float* __restrict__ tail,
                                                         float* __restrict__ dtail,
-                                                        int* status, const int* gate) {
+                                                        int* status, const int* gate,
+                                                        uint32_t wait_limit) {
   if (gate && *gate == 0) return;
   extern __shared__ __align__(1024) uint8_t sm[];
   using L = InferSmem;
@@ -160,7 +168,7 @@ __global__ void __launch_bounds__(128) mlp_infer_kernel(int n, const float* __re
         mma_bf16(tmem + d, smem_desc(a + 256 * k, 128, sbo_a), smem_desc(b + 256 * k, 128, sbo_b),
                  idesc, k > 0);
       mma_commit(mbar);
-      s_ok = mbar_wait(mbar, phase, kWaitLimit) ? 1 : 0;
+      s_ok = mbar_wait(mbar, phase, wait_limit) ? 1 : 0;
     }
     __syncthreads();
     fence_after_sync();
@@ -288,7 +296,8 @@ __global__ void __launch_bounds__(128) mlp_train_kernel(int n, const float* __re
                                                         int* adam_t, int steps, int batch,
                                                         float lr, unsigned long long seed,
                                                         float* grad_out, float* loss_out,
-                                                        int* status, const int* gate) {
+                                                        int* status, const int* gate,
+                                                        uint32_t wait_limit) {
   if (gate && *gate == 0) return;
   extern __shared__ __align__(1024) uint8_t sm[];
   using L = TrainSmem;
@@ -326,7 +335,7 @@ __global__ void __launch_bounds__(128) mlp_train_kernel(int n, const float* __re
         mma_bf16(tmem + d, smem_desc(a + 256 * k, 128, sbo_a), smem_desc(b + 256 * k, 128, sbo_b),
                  idesc, accumulate || k > 0);
       mma_commit(mbar);
-      s_ok = mbar_wait(mbar, phase, kWaitLimit) ? 1 : 0;
+      s_ok = mbar_wait(mbar, phase, wait_limit) ? 1 : 0;
     }
     __syncthreads();
     fence_after_sync();
@@ -490,7 +499,7 @@ void launch_mlp_infer(int n, const float* features, const float* params, float* 
   const int tiles = (n + 127) / 128;
   const int grid = std::max(1, std::min(tiles, 2 * sm_count));
   mlp_infer_kernel<<<grid, 128, kInferSmemLaunch, s>>>(n, features, params, tail, dtail, status,
-                                                       gate);
+                                                       gate, g_wait_limit.load());
 }
 
 void launch_mlp_train(int n, const float* features, const float* targets, float* params,
@@ -502,7 +511,11 @@ void launch_mlp_train(int n, const float* features, const float* targets, float*
                        TrainSmem::bytes);
   mlp_train_kernel<<<1, 128, TrainSmem::bytes, s>>>(n, features, targets, params, adam_m, adam_v,
                                                     adam_t, steps, batch, lr, seed, grad_out,
-                                                    loss_out, status, gate);
+                                                    loss_out, status, gate, g_wait_limit.load());
+}
+
+void set_tensor_wait_limit(long long polls) {
+  g_wait_limit.store(polls < 0 ? kWaitLimit : (uint32_t)std::min<long long>(polls, kWaitLimit));
 }
 
 }  // namespace ommb200

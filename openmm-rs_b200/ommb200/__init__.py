@@ -47,7 +47,21 @@ class ConstraintError(OmmB200Error):
     pass
 
 
-_ERRORS = {ERR_INVALID_ARG: InvalidArgument, ERR_CONSTRAINT: ConstraintError}
+class NonfiniteError(OmmB200Error, FloatingPointError):
+    """A position or velocity became nonfinite during the steps."""
+
+
+class TimeoutError_(OmmB200Error, TimeoutError):
+    """A tensor-core kernel gave up waiting for its MMAs (OMMB200_ERR_TIMEOUT)."""
+
+
+class NeighborListOverflow(OmmB200Error):
+    """The neighbour list could not hold the pairs and could not grow any further."""
+
+
+_ERRORS = {ERR_INVALID_ARG: InvalidArgument, ERR_CONSTRAINT: ConstraintError,
+           ERR_NONFINITE: NonfiniteError, ERR_TIMEOUT: TimeoutError_,
+           ERR_NLIST_OVERFLOW: NeighborListOverflow}
 
 
 class Options(C.Structure):
@@ -131,6 +145,10 @@ def library() -> C.CDLL:
             "ommb200_context_apply_velocity_constraints": [P, D],
             "ommb200_context_step": [P, I],
             "ommb200_context_get_tuning": [P, C.POINTER(D), C.POINTER(I), C.POINTER(I)],
+            "ommb200_context_nlist_capacity": [P, C.POINTER(I), C.POINTER(I), C.POINTER(I)],
+            "ommb200_set_tensor_core_wait_limit": [C.c_longlong],
+            "ommb200_context_nlist_prune_stats": [P, C.POINTER(I), C.POINTER(C.c_int64),
+                                                  C.POINTER(D)],
             "ommb200_monte_carlo_barostat_create": [D, D, I, C.POINTER(P)],
             "ommb200_monte_carlo_barostat_set_default_pressure": [P, D],
             "ommb200_monte_carlo_barostat_get_default_pressure": [P, C.POINTER(D)],
@@ -726,12 +744,29 @@ class Context:
                 "tile_entries": width.value}
 
     def nlist_stats(self) -> dict:
-        """Neighbour-list state: tiles, blocks and masked tiles in use, rebuilds so far."""
+        """Neighbour-list state: tiles the pair kernel evaluates, blocks and masked tiles in
+        use, rebuilds so far."""
         t, b, m, r = C.c_int(), C.c_int(), C.c_int(), C.c_int64()
         _check(library().ommb200_context_nlist_stats(self._h, C.byref(t), C.byref(b), C.byref(m),
                                                      C.byref(r)))
         return {"tiles": t.value, "blocks": b.value, "masked_tiles": m.value,
                 "rebuilds": r.value}
+
+    def nlist_prune_stats(self) -> dict:
+        """Pruned pair list: the last rebuild's tiles, prunes so far, margin (nm; 0 = the pair
+        kernel reads the rebuild's tiles)."""
+        t, c, m = C.c_int(), C.c_int64(), C.c_double()
+        _check(library().ommb200_context_nlist_prune_stats(self._h, C.byref(t), C.byref(c),
+                                                           C.byref(m)))
+        return {"rebuild_tiles": t.value, "prunes": c.value, "margin_nm": m.value}
+
+    def nlist_capacity(self) -> dict:
+        """Neighbour-list capacities: tile slots, particles per x-y column, and how many times
+        an overflow made them grow."""
+        t, c, g = C.c_int(), C.c_int(), C.c_int()
+        _check(library().ommb200_context_nlist_capacity(self._h, C.byref(t), C.byref(c),
+                                                        C.byref(g)))
+        return {"tile_capacity": t.value, "column_capacity": c.value, "regrows": g.value}
 
     def stream_handle(self) -> int:
         """cudaStream_t (as an integer) that every kernel of this Context runs on."""
@@ -837,6 +872,12 @@ def _stream_of(t):
     import torch
 
     return torch.cuda.current_stream(t.device).cuda_stream
+
+
+def set_tensor_core_wait_limit(polls: int) -> None:
+    """Polls after which the tensor-core kernels give up waiting for their MMAs (a diagnostic
+    for the time-out path); polls < 0 restores the default."""
+    _check(library().ommb200_set_tensor_core_wait_limit(int(polls)))
 
 
 def radii_mlp_forward(features, params, with_gradient=True):

@@ -308,7 +308,7 @@ def test_autotune_keeps_the_trajectory():
         ctx.set_velocities_to_temperature(300.0, seed=6)
         if tune:
             t = ctx.autotune(40)
-            assert 0.05 < t["skin_nm"] <= 0.2 and t["pair_ctas_per_sm"] in (4, 6, 8, 12)
+            assert 0.05 < t["skin_nm"] <= 0.2 and t["pair_ctas_per_sm"] in range(4, 13)
         ctx.step(30)
         st = ctx.get_state(positions=True, velocities=True)
         out.append((st.positions, st.velocities, st.step_count))
