@@ -552,11 +552,11 @@ def main():
         # our kernels per MD step: rebuild condition 1, pack 1, prune condition 1 (pruned list),
         # pair 1, PME (spread, the three transform kernels, gather: 5; or spread, convert,
         # convolve, gather: 4 beside cuFFT), exceptions 1, integrate 1; the 8 rebuild kernels
-        # only on rebuild steps and the 3 prune kernels only on prune steps; one counter kernel
+        # only on rebuild steps and the 2 prune kernels only on prune steps; one counter kernel
         # per graph launch of 20 steps
         pruned = ctx.nlist_prune_stats()["margin_nm"] > 0
         per_md = 1 + 1 + (1 if pruned else 0) + 1 + (5 if "pme_transform" in times else 4) + 1 + 1
-        launches = (md_steps * per_md + 8 * rebuilds_timed + 3 * prunes_timed
+        launches = (md_steps * per_md + 8 * rebuilds_timed + 2 * prunes_timed
                     + args.steps * (args.segment // 20))
         extras["pairs_in_cutoff"] = pairs
         nl = ctx.nlist_stats()

@@ -67,6 +67,9 @@ typedef struct {
   int use_cuda_graph;         /* capture the step in a CUDA graph (default 1) */
   double neighbor_skin;       /* Verlet skin in nm; <= 0 picks the tuned default */
   int steps_per_graph;        /* steps captured per graph launch; <= 0 picks the default */
+  int pme_bricks;             /* brick-owned PME spread and gather (rectangular periodic boxes):
+                                 -1 when the grid has two bricks per SM or more (default), 0 never,
+                                 1 whenever the box allows; the forces are the same either way */
 } ommb200_options;
 
 typedef struct {
@@ -264,6 +267,10 @@ int ommb200_context_get_tuning(ommb200_context* ctx, double* skin, int* pair_cta
 /* PME parameters frozen at Context creation (nonbonded.rs:1078-1106). */
 int ommb200_context_get_pme_parameters(const ommb200_context* ctx, double* alpha, int* nx,
                                        int* ny, int* nz);
+/* Which PME spread/gather form runs (no reference counterpart): *bricks_in_use = 1 for the
+ * brick-owned form, 0 for the atomic one; *bricks = grid bricks of kBrickEdge^3 points (0 without
+ * PME).  Outputs may be NULL. */
+int ommb200_context_get_pme_layout(const ommb200_context* ctx, int* bricks_in_use, int* bricks);
 
 /* Learned-radii state of a Context whose GBSAOBCForce uses learned radii. */
 typedef struct {

@@ -130,6 +130,7 @@ void ommb200_default_options(ommb200_options* out) {
   out->use_cuda_graph = 1;
   out->neighbor_skin = 0.0;
   out->steps_per_graph = 0;
+  out->pme_bricks = -1;
 }
 
 // ---- System -----------------------------------------------------------------------------
@@ -535,12 +536,14 @@ static EngineOptions engine_options(const ommb200_options* options) {
   if (options) o = *options;
   require(o.precision == OMMB200_PRECISION_MIXED || o.precision == OMMB200_PRECISION_DOUBLE,
           "unknown precision");
+  require(o.pme_bricks >= -1 && o.pme_bricks <= 1, "pme_bricks must be -1, 0 or 1");
   EngineOptions eo;
   eo.precision = o.precision;
   eo.device = o.device;
   eo.use_graph = o.use_cuda_graph != 0;
   eo.skin = o.neighbor_skin;
   eo.steps_per_graph = o.steps_per_graph;
+  eo.pme_bricks = o.pme_bricks;
   return eo;
 }
 
@@ -696,6 +699,12 @@ int ommb200_context_get_pme_parameters(const ommb200_context* ctx, double* alpha
   return guarded([&] {
     require(ctx && ctx->engine && alpha && nx && ny && nz, "null argument");
     ctx->engine->pme_parameters(alpha, nx, ny, nz);
+  });
+}
+int ommb200_context_get_pme_layout(const ommb200_context* ctx, int* bricks_in_use, int* bricks) {
+  return guarded([&] {
+    require(ctx && ctx->engine, "null argument");
+    ctx->engine->pme_layout(bricks_in_use, bricks);
   });
 }
 

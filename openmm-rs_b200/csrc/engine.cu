@@ -438,6 +438,7 @@ void Engine::setup_nonbonded(const NonbondedDef& nb) {
     pos_prune_ = mem_.alloc<double>(3 * (size_t)n_);
     prune_count_ = mem_.alloc<unsigned long long>(1);
     prune_n_tiles_ = mem_.alloc<int>(1);
+    prune_done_ = mem_.alloc<unsigned>(1);
     a.prune = prune_flag_;
     alloc_pruned_list();
   }
@@ -532,6 +533,15 @@ void Engine::setup_nonbonded(const NonbondedDef& nb) {
       mod.insert(mod.end(), m.begin(), m.end());
     }
     OMMB200_CK(cudaMemcpy(moduli_, mod.data(), 8 * mod.size(), cudaMemcpyHostToDevice));
+    if (nb_periodic_ && nl_.n_cols > 0) {  // the brick form's slot ranges
+      for (int d = 0; d < 3; ++d) {
+        bricks_.grid[d] = grid_[d];
+        bricks_.nb[d] = (grid_[d] + kBrickEdge - 1) / kBrickEdge;
+      }
+      bricks_.n_col[0] = nl_.n_col[0];
+      bricks_.n_col[1] = nl_.n_col[1];
+      bricks_.ranges = mem_.alloc<int2>(2 * (size_t)nl_.n_cols * bricks_.nb[2]);
+    }
   }
   upload_nonbonded_parameters(nb);
 }
@@ -560,7 +570,12 @@ void Engine::upload_nonbonded_parameters(const NonbondedDef& nb) {
   dispersion_coeff_ =
       (nb_periodic_ && nb.use_dispersion_correction) ? dispersion_coefficient(nb) : 0.0;
   double q2 = 0.0;
-  for (double q : nb.charge) q2 += q * q;
+  max_abs_charge_ = 0.0;
+  for (double q : nb.charge) {
+    q2 += q * q;
+    max_abs_charge_ = std::max(max_abs_charge_, std::fabs(q));
+  }
+  if (volume_ > 0.0) update_bricks();  // after Context creation (the box is set)
   self_energy_ = nb_pme_ ? -kOne4PiEps0 * alpha_ / std::sqrt(kPiD) * q2 : 0.0;
   if (nb_pme_ && volume_ > 0.0) {  // after Context creation: the neutralising term
     double qt = 0.0;
@@ -1126,6 +1141,42 @@ void Engine::update_box_dependents() {
     for (double q : nb_->charge) qt += q;
     plasma_energy_ = kOne4PiEps0 * kPiD * qt * qt / (2.0 * alpha_ * alpha_ * volume_);
   }
+  update_bricks();
+}
+
+// Brick-owned PME (spread and gather of large grids in rectangular boxes): chosen while the box
+// is rectangular, every charge is below 16 e (the shared sums' bound), a brick's columns fit
+// kBrickMaxRanges and the grid has at least two bricks per SM (or the option asks for it).
+// A change of choice drops the captured graph and asks for a rebuild (the slot ranges are made
+// with the list); leaving the brick form zeroes the grid for the atomic spread.
+void Engine::update_bricks() {
+  const bool before = use_bricks_;
+  bool use = false;
+  if (bricks_.ranges && opt_.pme_bricks != 0 && box_[3] == 0.0 && box_[6] == 0.0 &&
+      box_[7] == 0.0 && max_abs_charge_ < 16.0) {
+    const double drift = 0.5 * std::max(skin_, kMaxTunedSkin), slack = 1e-3;
+    int cols[2] = {1, 1};
+    for (int d = 0; d < 3; ++d) {
+      bricks_.len[d] = box_[4 * d];
+      bricks_.cell[d] = box_[4 * d] / grid_[d];
+      bricks_.below[d] = 4.0 * bricks_.cell[d] + drift + slack;
+    }
+    bricks_.above = drift + slack;
+    for (int d = 0; d < 2; ++d) {
+      const double w = bricks_.len[d] / nl_.n_col[d];
+      const double span = kBrickEdge * bricks_.cell[d] + bricks_.below[d] + bricks_.above;
+      cols[d] = std::min(nl_.n_col[d], (int)std::floor(span / w) + 2);
+    }
+    const long long n = (long long)bricks_.nb[0] * bricks_.nb[1] * bricks_.nb[2];
+    use = 2 * cols[0] * cols[1] <= kBrickMaxRanges &&
+          (opt_.pme_bricks == 1 || n >= 2LL * sm_count_);
+  }
+  use_bricks_ = use;
+  if (use == before) return;
+  destroy_graph();
+  const int one = 1;
+  OMMB200_CK(cudaMemcpy(rebuild_, &one, 4, cudaMemcpyHostToDevice));
+  if (!use) OMMB200_CK(cudaMemset(pme_fixed_, 0, 8 * (size_t)grid_[0] * grid_[1] * grid_[2]));
 }
 
 void Engine::destroy_graph() {
@@ -1264,7 +1315,9 @@ void Engine::enqueue_conditional_rebuild() {
   cudaGraphConditionalHandle handle;
   OMMB200_CK(cudaGraphConditionalHandleCreate(&handle, cap, 0, cudaGraphCondAssignDefault));
   launch_nlist_condition(nl_, handle, stream_);
-  enqueue_conditional_body(handle, [&](cudaStream_t s) { launch_nlist_rebuild(nl_, dp_, s); });
+  enqueue_conditional_body(handle, [&](cudaStream_t s) {
+    launch_nlist_rebuild(nl_, dp_, s, use_bricks_ ? &bricks_ : nullptr);
+  });
 }
 
 // An IF node at the current point of the captured stream; its body is `body`'s launches,
@@ -1294,7 +1347,7 @@ void Engine::enqueue_conditional_body(cudaGraphConditionalHandle handle,
 }
 
 bool Engine::pruning() const {
-  return nb_periodic_ && nl_.block_tiles && nl_.halves && nl_.max_cand > 0 && box_[3] == 0.0 &&
+  return prune_margin_ > 0.0 && nb_periodic_ && nl_.block_tiles && nl_.halves && nl_.max_cand > 0 && box_[3] == 0.0 &&
          box_[6] == 0.0 && box_[7] == 0.0;
 }
 
@@ -1304,6 +1357,7 @@ void Engine::alloc_pruned_list() {
   prune_entries_ = mem_.alloc_bytes((size_t)(dp_ ? 32 : 16) * 32 * (size_t)prune_capacity_);
   prune_masks_ = mem_.alloc<uint32_t>(32 * (size_t)prune_capacity_);
   prune_cols_ = mem_.alloc<uint32_t>(32 * (size_t)prune_capacity_);
+  prune_keep_ = mem_.alloc<uint32_t>((size_t)prune_capacity_);
 }
 
 PruneArgs Engine::prune_args() const {
@@ -1312,12 +1366,15 @@ PruneArgs Engine::prune_args() const {
   p.entries = prune_entries_;
   p.masks = prune_masks_;
   p.cols = prune_cols_;
+  p.keep = prune_keep_;
+  p.done = prune_done_;
   p.n_tiles = prune_n_tiles_;
   p.capacity = prune_capacity_;
+  p.sm_count = sm_count_;
   p.prune = prune_flag_;
   p.pos_prune = pos_prune_;
   p.posq = posq_;
-  const double reach = nb_->cutoff + kPruneMargin + kPruneAllowance;
+  const double reach = nb_->cutoff + prune_margin_ + kPruneAllowance;
   p.reach2 = reach * reach;
   p.prune_count = prune_count_;
   return p;
@@ -1331,7 +1388,7 @@ void Engine::enqueue_nonbonded(bool energy, bool direct, bool reciprocal, bool d
     if (capturing_)
       enqueue_conditional_rebuild();
     else
-      launch_nlist_rebuild(nl_, dp_, stream_);
+      launch_nlist_rebuild(nl_, dp_, stream_, use_bricks_ ? &bricks_ : nullptr);
     prof_end();
   }
   // fork: PME on its own stream (serialised on the main stream while profiling, so that
@@ -1436,8 +1493,12 @@ void Engine::enqueue_nonbonded(bool energy, bool direct, bool reciprocal, bool d
     m.energy = energy_;
     m.alpha = alpha_;
     m.volume = volume_;
+    m.grid_stored = use_bricks_ ? 1 : 0;
     prof_begin("pme_spread");
-    launch_pme_spread<Real>(m, ps);
+    if (use_bricks_)
+      launch_pme_spread_bricks<Real>(m, bricks_, nl_, ps);
+    else
+      launch_pme_spread<Real>(m, ps);
     prof_end();
     if (own_fft_) {
       prof_begin("pme_transform");
@@ -1466,7 +1527,10 @@ void Engine::enqueue_nonbonded(bool energy, bool direct, bool reciprocal, bool d
     prof_end();
     }
     prof_begin("pme_gather");
-    launch_pme_gather<Real>(m, ps);
+    if (use_bricks_)
+      launch_pme_gather_bricks<Real>(m, bricks_, nl_, ps);
+    else
+      launch_pme_gather<Real>(m, ps);
     prof_end();
   }
   if (direct && n_exceptions_) {
@@ -1589,7 +1653,7 @@ IntegrateArgs Engine::integrate_args(int step_offset) const {
   a.status = status_;
   if (pruning() && a.pos_ref) {
     a.pos_prune = pos_prune_;
-    a.half_margin2 = 0.25 * kPruneMargin * kPruneMargin;
+    a.half_margin2 = 0.25 * prune_margin_ * prune_margin_;
     a.prune = prune_flag_;
   }
   return a;
@@ -2160,10 +2224,24 @@ void Engine::autotune(int trial_steps, double* skin_out, int* ctas_out, double* 
     OMMB200_CK(cudaEventElapsedTime(&ms, t0, t1));
     return (double)ms / trial_steps;
   };
-  double best_skin = skin_, best_ms = 1e30;
+  double best_skin = skin_, best_ms = 1e30, best_margin = prune_margin_;
   int best_ctas = pair_grid_ / std::max(1, sm_count_);
   int best_halves = nl_.halves;
+  // pruned-list margin (0 = no pruning), where the list builder records each block's tiles
+  auto tune_margin = [&]() {
+    if (!(nb_ && nb_periodic_ && nl_.block_tiles && nl_.max_cand > 0 && nl_.halves)) return;
+    for (double m : kTunedPruneMargins) {
+      prune_margin_ = m;
+      const double ms = trial(best_skin, best_ctas);
+      if (ms < best_ms) {
+        best_ms = ms;
+        best_margin = m;
+      }
+    }
+    prune_margin_ = best_margin;
+  };
   try {
+    tune_margin();
     if (nb_ && nb_periodic_) {
       for (double s : kTunedSkins) {
         const double ms = trial(s, best_ctas);
@@ -2185,6 +2263,7 @@ void Engine::autotune(int trial_steps, double* skin_out, int* ctas_out, double* 
       }
       nl_.halves = best_halves;
     }
+    tune_margin();  // again, for the chosen skin and tile width
     if (nb_) {
       for (int c : kTunedPairCtasPerSm) {
         const double ms = trial(best_skin, c);
@@ -2205,6 +2284,7 @@ void Engine::autotune(int trial_steps, double* skin_out, int* ctas_out, double* 
   skin_ = best_skin;
   nl_.skin = best_skin;
   nl_.halves = best_halves;
+  prune_margin_ = best_margin;
   pair_grid_ = sm_count_ * best_ctas;
   destroy_graph();
   restore();
@@ -2237,7 +2317,7 @@ void Engine::nlist_prune_stats(int* rebuild_tiles, int64_t* prunes, double* marg
   }
   if (rebuild_tiles) *rebuild_tiles = t;
   if (prunes) *prunes = pruning() ? (int64_t)c : 0;
-  if (margin) *margin = pruning() ? kPruneMargin : 0.0;
+  if (margin) *margin = pruning() ? prune_margin_ : 0.0;
 }
 
 void Engine::nlist_stats(int* tiles, int* blocks, int* masked, int64_t* rebuilds) {
@@ -2256,6 +2336,11 @@ void Engine::nlist_stats(int* tiles, int* blocks, int* masked, int64_t* rebuilds
   if (blocks) *blocks = v[1];
   if (masked) *masked = v[2];
   if (rebuilds) *rebuilds = (int64_t)r;
+}
+
+void Engine::pme_layout(int* bricks_in_use, int* bricks) const {
+  if (bricks_in_use) *bricks_in_use = use_bricks_ ? 1 : 0;
+  if (bricks) *bricks = bricks_.ranges ? bricks_.nb[0] * bricks_.nb[1] * bricks_.nb[2] : 0;
 }
 
 void Engine::pme_parameters(double* alpha, int* nx, int* ny, int* nz) const {
@@ -2315,13 +2400,14 @@ struct CheckpointHeader {
   double box[9];
   uint64_t seed, velocity_draws, rng_step;
   double skin;
+  double prune_margin;
   // barostat (zero without one): step counter, volume step and its window, totals, stream
   uint64_t bar_counter, bar_window_attempted, bar_window_accepted, bar_attempted, bar_accepted;
   uint64_t bar_seed, bar_draws;
   double bar_volume_scale, bar_pressure, bar_temperature;
 };
 constexpr char kCheckpointMagic[8] = {'O', 'M', 'B', '2', 'C', 'K', 'P', 'T'};
-constexpr uint32_t kCheckpointVersion = 5;
+constexpr uint32_t kCheckpointVersion = 6;
 }  // namespace
 
 size_t Engine::checkpoint_bytes() const {
@@ -2351,6 +2437,7 @@ void Engine::save_checkpoint(uint8_t* out, size_t bytes) {
   h.seed = seed_;
   h.velocity_draws = velocity_draws_;
   h.skin = skin_;
+  h.prune_margin = prune_margin_;
   h.bar_counter = bar_counter_;
   h.bar_window_attempted = bar_window_attempted_;
   h.bar_window_accepted = bar_window_accepted_;
@@ -2434,6 +2521,8 @@ void Engine::load_checkpoint(const uint8_t* in, size_t bytes) {
   if (nb_periodic_) {
     skin_ = h.skin;
     nl_.skin = h.skin;
+    prune_margin_ = h.prune_margin;
+    update_bricks();
     pair_grid_ = h.pair_grid;
     nl_.halves = h.halves;
     put(nl_.pos_ref, 24 * (size_t)n_);
@@ -2443,7 +2532,7 @@ void Engine::load_checkpoint(const uint8_t* in, size_t bytes) {
     from_ref.pos = nl_.pos_ref;
     const int one = 1;
     OMMB200_CK(cudaMemcpy(rebuild_, &one, 4, cudaMemcpyHostToDevice));
-    launch_nlist_rebuild(from_ref, dp_, stream_);
+    launch_nlist_rebuild(from_ref, dp_, stream_, use_bricks_ ? &bricks_ : nullptr);
     // and the pruned list from the positions of the original run's last prune (its tiles hold
     // the same entries, so every per-tile sum rounds the same)
     put(pos_prune_, 24 * (size_t)n_);

@@ -26,10 +26,13 @@ void nonbonded_forces_noalloc(int n, const double* pos, const double* q, const d
 constexpr double kTunedSkins[] = {0.06, 0.08, 0.1, 0.13, 0.16, 0.2};
 constexpr double kMaxTunedSkin = 0.2;
 constexpr int kTunedPairCtasPerSm[] = {4, 6, 7, 8, 9, 10, 11, 12};
-// Margin of the pruned pair list (nm): entries within cutoff + margin of their half block stay;
-// a particle that moves margin / 2 requests the next prune.  The allowance absorbs the FP32
-// rounding of the prune's distances.
-constexpr double kPruneMargin = 0.05;
+// Margins of the pruned pair list (nm) the autotuner tries: entries within cutoff + margin of
+// their half block stay, and a particle that moves margin / 2 requests the next prune, so a
+// wider margin prunes less often and leaves more pairs for the pair kernel; 0 turns pruning
+// off (the pair kernel reads the rebuild's list).  The allowance absorbs the FP32 rounding of
+// the prune's distances.
+constexpr double kTunedPruneMargins[] = {0.0, 0.05, 0.08, 0.12};
+constexpr double kDefaultPruneMargin = 0.08;
 constexpr double kPruneAllowance = 1e-4;
 
 class DeviceArena {
@@ -51,6 +54,7 @@ struct EngineOptions {
   bool use_graph = true;
   double skin = 0.0;
   int steps_per_graph = 0;
+  int pme_bricks = -1;  // brick-owned PME spread and gather: -1 by grid size, 0 off, 1 on
 };
 
 // Device state that a re-run of MD steps starts from (Engine::save_dynamic_state).
@@ -89,6 +93,7 @@ class Engine {
   void get_state(int flags, uint32_t groups, double* pos, double* vel, double* forces,
                  ommb200_state_info* info);
   void pme_parameters(double* alpha, int* nx, int* ny, int* nz) const;
+  void pme_layout(int* bricks_in_use, int* bricks) const;
   void nlist_stats(int* tiles, int* blocks, int* masked, int64_t* rebuilds);
   void nlist_capacity(int* tile_capacity, int* column_capacity, int* regrows) const;
   void nlist_prune_stats(int* rebuild_tiles, int64_t* prunes, double* margin);
@@ -134,6 +139,7 @@ class Engine {
   void build_static_layout();
   void setup_integrator();
   void update_box_dependents();
+  void update_bricks();
   void build_static_tiles();
   void enqueue_conditional_rebuild();
   void enqueue_conditional_body(cudaGraphConditionalHandle handle,
@@ -268,6 +274,12 @@ class Engine {
   void* prune_entries_ = nullptr;
   uint32_t* prune_masks_ = nullptr;
   uint32_t* prune_cols_ = nullptr;
+  uint32_t* prune_keep_ = nullptr;
+  double prune_margin_ = kDefaultPruneMargin;  // 0: no pruning
+  PmeBricks bricks_{};      // brick-owned PME geometry and slot ranges
+  bool use_bricks_ = false;
+  double max_abs_charge_ = 0.0;
+  unsigned* prune_done_ = nullptr;
   int* prune_n_tiles_ = nullptr;
   int prune_capacity_ = 0;
   int* prune_flag_ = nullptr;

@@ -74,8 +74,11 @@ struct PruneArgs {
   void* entries;        // [32 * capacity] as the rebuild's entries
   uint32_t* masks;      // [32 * capacity]
   uint32_t* cols;       // [32 * capacity] scratch: exclusion column (bit per i-slot) per entry
+  uint32_t* keep;       // [rebuild tile capacity] scratch: kept entries of each rebuild tile
+  unsigned* done;       // scratch: placement CTAs finished (the last one closes the prune)
   int* n_tiles;         // tiles in use
   int capacity;
+  int sm_count;         // grid of the keep pass
   int* prune;           // nonzero: prune before this evaluation's pair kernel
   double* pos_prune;    // [3N] positions at the last prune
   const void* posq;     // this evaluation's packed particles
@@ -83,7 +86,10 @@ struct PruneArgs {
   unsigned long long* prune_count;
 };
 
-void launch_nlist_rebuild(const NlistArgs& a, bool double_entries, cudaStream_t s);
+struct PmeBricks;
+// `bricks` (may be null): the brick-owned PME's slot ranges are remade with the list.
+void launch_nlist_rebuild(const NlistArgs& a, bool double_entries, cudaStream_t s,
+                          const PmeBricks* bricks = nullptr);
 void launch_nlist_prune(const NlistArgs& a, const PruneArgs& p, bool double_entries,
                         cudaStream_t s);
 // Sets `handle` to whether a prune is pending (the graph form of the early-exit prune kernels).
@@ -156,10 +162,37 @@ struct PmeArgs {
   long long* force;
   long long* energy;
   double alpha, volume;
+  int grid_stored;        // the spread stores every grid point: the transform leaves it as is
 };
 
 template <class Real>
 void launch_pme_spread(const PmeArgs<Real>& a, cudaStream_t s);
+
+// Brick-owned PME for rectangular boxes: the charge grid is cut into bricks of kBrickEdge^3
+// points (the last brick of an axis may be shorter) and one CTA owns each brick.  The atoms
+// that can touch a brick until the next neighbour-list rebuild are found through the rebuild's
+// x-y columns (z-sorted): for each column and z layer of bricks, the slot ranges (two where
+// the layer's reach wraps the box) of the atoms whose rebuild position lies within the
+// layer's reach, made at every rebuild.
+constexpr int kBrickEdge = 14;
+constexpr int kBrickMaxRanges = 256;  // slot ranges one brick gathers (columns x 2)
+struct PmeBricks {
+  int2* ranges;        // [n_cols * nb[2] * 2] (first slot, end slot)
+  int nb[3];           // bricks per axis
+  int grid[3];         // grid points per axis
+  int n_col[2];        // x-y columns of the neighbour-list sort
+  double len[3];       // box edge lengths (nm)
+  double cell[3];      // grid spacing (nm)
+  double below[3];     // reach of a brick below its lower faces: 4 cells + drift (plus slack)
+  double above;        // reach above its upper faces: drift (plus slack)
+};
+void launch_pme_brick_ranges(const NlistArgs& a, const PmeBricks& b, cudaStream_t s);
+template <class Real>
+void launch_pme_spread_bricks(const PmeArgs<Real>& a, const PmeBricks& b, const NlistArgs& nl,
+                              cudaStream_t s);
+template <class Real>
+void launch_pme_gather_bricks(const PmeArgs<Real>& a, const PmeBricks& b, const NlistArgs& nl,
+                              cudaStream_t s);
 // Influence table on the half spectrum for the current reciprocal box (device, f64 math).
 struct PmeRecip {
   double m[3][3];

@@ -843,21 +843,78 @@ __global__ void nl_clear_flag(NlistArgs a) {
 // positions and packs each half's kept entries, in their rebuild order, 16 to an inner tile; the
 // integrator asks for a new prune once a particle has moved more than margin / 2 since the last
 // one, so every pair within the cutoff until then stays listed (a pair approaches by less than
-// the margin, and it is among the rebuild's tiles while no particle moved skin / 2).  One CTA per
-// block I: pass 1 tests the entries of I's tiles (kept bits), a prefix over the tiles gives each
-// kept entry its place, pass 2 moves the entries with their exclusion columns (the bits of the
-// i-slots that exclude them), pass 3 writes each inner tile's masks (exclusions, padding) and
-// header.  Block I's self tile is copied.  A block with more tiles than the shared arrays hold
-// keeps all its entries (still a valid list).
+// the margin, and it is among the rebuild's tiles while no particle moved skin / 2).
+// Two kernels.  The keep pass gives every rebuild tile one warp over the whole list (two rounds
+// of loads: the tile, then its particles) and stores the kept bits of its 32 entries.  The
+// placement pass gives each block I one CTA: a prefix over I's tiles gives each kept entry its
+// place, the kept entries move with their exclusion columns (the bits of the i-slots that
+// exclude them), then each inner tile gets its masks (exclusions, padding) and header.  Block
+// I's self tile is copied.  A block with more tiles than the shared arrays hold keeps all its
+// entries (still a valid list).  The last placement CTA to finish closes the prune.
 constexpr int kPruneMaxTiles = 256;
 constexpr int kPruneSharedCols = 64;  // inner tiles whose exclusion columns stay in shared memory
+constexpr int kPruneKeepWarps = 8;
+constexpr int kPruneUnroll = 4;       // rebuild tiles a placement warp loads in one round
+constexpr int kPlaceWarps = 4;        // placement CTA: 128 threads, all blocks resident at once
 
 template <bool kDouble>
-__global__ void __launch_bounds__(32 * kCtaWarps) nl_prune(const NlistArgs a, const PruneArgs p) {
+__global__ void __launch_bounds__(32 * kPruneKeepWarps) nl_prune_keep(const NlistArgs a,
+                                                                     const PruneArgs p) {
   if (*p.prune == 0) return;
   using T4 = typename std::conditional<kDouble, double4, float4>::type;
   using R = typename std::conditional<kDouble, double, float>::type;
-  __shared__ T4 s_i[32];
+  __shared__ T4 s_i[kPruneKeepWarps][32];
+  __shared__ int s_ok[kPruneKeepWarps][32];
+  if (blockIdx.x == 0 && threadIdx.x == 0) {  // the placement pass allocates from zero
+    *p.n_tiles = 0;
+    *p.done = 0u;
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, hb = lane & 16;
+  const int n_t = min(*a.n_tiles, a.tile_capacity);
+  const T4* posq = reinterpret_cast<const T4*>(p.posq);
+  const T4* ent = reinterpret_cast<const T4*>(a.entries);
+  const R reach2 = (R)p.reach2;
+  Box<R> b;
+  b.ax = (R)a.box.ax; b.bx = (R)a.box.bx; b.by = (R)a.box.by;
+  b.cx = (R)a.box.cx; b.cy = (R)a.box.cy; b.cz = (R)a.box.cz;
+  b.inv_ax = (R)a.box.inv_ax; b.inv_by = (R)a.box.inv_by; b.inv_cz = (R)a.box.inv_cz;
+  for (int t = blockIdx.x * kPruneKeepWarps + w; t < n_t; t += gridDim.x * kPruneKeepWarps) {
+    const int4 hdr = a.tiles[t];
+    const T4 e = ent[32 * (size_t)t + lane];
+    const int ai = a.sorted_atom[32 * hdr.x + lane];
+    const T4 pi = posq[32 * hdr.x + lane];
+    int slot;
+    if constexpr (kDouble) slot = (int)e.w;
+    else slot = __float_as_int(e.w);
+    T4 pj = pi;
+    if (slot >= 0) pj = posq[slot];
+    __syncwarp();
+    s_i[w][lane] = pi;
+    s_ok[w][lane] = ai >= 0;
+    __syncwarp();
+    bool keep = false;
+    if (slot >= 0) {
+      const R x = pj.x + e.x, y = pj.y + e.y, z = pj.z + e.z;
+      const bool image = (hdr.y & kTilePairImage) != 0;
+#pragma unroll 4
+      for (int q = 0; q < 16; ++q) {
+        const T4 c = s_i[w][hb + q];
+        R dx = x - c.x, dy = y - c.y, dz = z - c.z;
+        if (image) min_image_fast(dx, dy, dz, b);
+        keep = keep || (s_ok[w][hb + q] && dx * dx + dy * dy + dz * dz < reach2);
+      }
+    }
+    const unsigned kb = __ballot_sync(kFull, keep);
+    if (lane == 0) p.keep[t] = kb;
+  }
+}
+
+template <bool kDouble>
+__global__ void __launch_bounds__(32 * kPlaceWarps) nl_prune_place(const NlistArgs a,
+                                                                const PruneArgs p) {
+  if (*p.prune == 0) return;
+  using T4 = typename std::conditional<kDouble, double4, float4>::type;
+  using R = typename std::conditional<kDouble, double, float>::type;
   __shared__ int s_iatom[32];
   __shared__ unsigned s_keep[kPruneMaxTiles];
   __shared__ int s_pre[2][kPruneMaxTiles + 1];
@@ -865,168 +922,162 @@ __global__ void __launch_bounds__(32 * kCtaWarps) nl_prune(const NlistArgs a, co
   __shared__ int s_t0, s_nt, s_img;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int I = blockIdx.x;
-  if (I >= *a.n_blocks) return;
-  const int t_out = a.block_tiles[2 * I], n_out = a.block_tiles[2 * I + 1];
-  if (t_out < 0 || n_out < 1 || t_out + n_out > a.tile_capacity) return;  // an overflowed build
-  const T4* posq = reinterpret_cast<const T4*>(p.posq);
-  const T4* ent = reinterpret_cast<const T4*>(a.entries);
-  T4* ent_in = reinterpret_cast<T4*>(p.entries);
-  const int n_nbr = n_out - 1;  // tile t_out is I's self tile
-  const bool all = n_nbr > kPruneMaxTiles;
-  if (w == 0) {
-    const int ai = a.sorted_atom[32 * I + lane];
-    s_iatom[lane] = ai;
-    s_i[lane] = posq[32 * I + lane];
-    if (ai >= 0)
-      for (int c = 0; c < 3; ++c) p.pos_prune[3 * ai + c] = a.pos[3 * ai + c];
-    if (lane == 0) s_img = 0;
+  int t_out = -1, n_out = 0;
+  if (I < *a.n_blocks) {
+    t_out = a.block_tiles[2 * I];
+    n_out = a.block_tiles[2 * I + 1];
   }
-  __syncthreads();
-  // pass 1: an entry stays when it comes within reach of a particle of its half
-  const R reach2 = (R)p.reach2;
-  for (int k = w; k < (all ? 0 : n_nbr); k += kCtaWarps) {
-    const int t = t_out + 1 + k;
-    const T4 e = ent[32 * t + lane];
-    int slot;
-    if constexpr (kDouble) slot = (int)e.w;
-    else slot = __float_as_int(e.w);
-    bool keep = false;
-    if (slot >= 0) {
-      const T4 pj = posq[slot];
-      const R x = pj.x + e.x, y = pj.y + e.y, z = pj.z + e.z;
-      const int hb = lane & 16;
-      const bool image = (a.tiles[t].y & kTilePairImage) != 0;
-#pragma unroll 4
-      for (int q = 0; q < 16; ++q) {
-        const T4 pi = s_i[hb + q];
-        R dx = x - pi.x, dy = y - pi.y, dz = z - pi.z;
-        if (image) {
-          Box<R> b;
-          b.ax = (R)a.box.ax; b.bx = (R)a.box.bx; b.by = (R)a.box.by;
-          b.cx = (R)a.box.cx; b.cy = (R)a.box.cy; b.cz = (R)a.box.cz;
-          b.inv_ax = (R)a.box.inv_ax; b.inv_by = (R)a.box.inv_by; b.inv_cz = (R)a.box.inv_cz;
-          min_image_fast(dx, dy, dz, b);
-        }
-        keep = keep || (s_iatom[hb + q] >= 0 && dx * dx + dy * dy + dz * dz < reach2);
-      }
-    }
-    const unsigned kb = __ballot_sync(kFull, keep);
-    if (lane == 0) s_keep[k] = kb;
-  }
-  __syncthreads();
-  // prefix of the kept entries per half over I's tiles (warp h for half h)
-  if (w < 2) {
-    int carry = 0;
+  // (a block of an overflowed build places nothing; the rebuild reported it)
+  if (t_out >= 0 && n_out >= 1 && t_out + n_out <= a.tile_capacity) {
+    const T4* ent = reinterpret_cast<const T4*>(a.entries);
+    T4* ent_in = reinterpret_cast<T4*>(p.entries);
+    const int n_nbr = n_out - 1;  // tile t_out is I's self tile
+    const bool all = n_nbr > kPruneMaxTiles;
     const int n_scan = all ? 0 : n_nbr;
-    for (int base = 0; base < n_scan; base += 32) {
-      const int k = base + lane;
-      const int v = k < n_scan ? __popc((s_keep[k] >> (16 * w)) & 0xffffu) : 0;
-      int incl = v;
-      for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(kFull, incl, o);
-        if (lane >= o) incl += y;
-      }
-      if (k < n_scan) s_pre[w][k] = carry + incl - v;
-      carry += __shfl_sync(kFull, incl, 31);
+    if (w == 0) {
+      const int ai = a.sorted_atom[32 * I + lane];
+      s_iatom[lane] = ai;
+      if (ai >= 0)
+        for (int c = 0; c < 3; ++c) p.pos_prune[3 * ai + c] = a.pos[3 * ai + c];
+      if (lane == 0) s_img = 0;
     }
-    if (lane == 0) s_pre[w][all ? 0 : n_nbr] = carry;
+    for (int k = threadIdx.x; k < n_scan; k += blockDim.x) s_keep[k] = p.keep[t_out + 1 + k];
+    __syncthreads();
+    // prefix of the kept entries per half over I's tiles (warp h for half h)
+    if (w < 2) {
+      int carry = 0;
+      for (int base = 0; base < n_scan; base += 32) {
+        const int k = base + lane;
+        const int v = k < n_scan ? __popc((s_keep[k] >> (16 * w)) & 0xffffu) : 0;
+        int incl = v;
+        for (int o = 1; o < 32; o <<= 1) {
+          const int y = __shfl_up_sync(kFull, incl, o);
+          if (lane >= o) incl += y;
+        }
+        if (k < n_scan) s_pre[w][k] = carry + incl - v;
+        carry += __shfl_sync(kFull, incl, 31);
+      }
+      if (lane == 0) s_pre[w][n_scan] = carry;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const int longest = all ? 16 * n_nbr : max(s_pre[0][n_nbr], s_pre[1][n_nbr]);
+      const int nt = 1 + (longest + 15) / 16;
+      int t0 = atomicAdd(p.n_tiles, nt);
+      if (t0 + nt > p.capacity) {
+        report_status(a.status, kStatusTileOverflow);
+        t0 = -1;
+      }
+      s_t0 = t0;
+      s_nt = nt;
+    }
+    __syncthreads();
+    if (s_t0 >= 0) {
+      // exclusion columns of the inner neighbour tiles: shared memory, or the global scratch
+      // for a block with more tiles than that holds
+      const bool shared_cols = s_nt - 1 <= kPruneSharedCols;
+      uint32_t* cols = shared_cols ? &s_cols[0][0] : p.cols + 32 * (size_t)(s_t0 + 1);
+      // block I's self tile, unchanged (its mask slot becomes its tile index)
+      if (w == 0) {
+        int4 hdr = a.tiles[t_out];
+        const bool masked = (hdr.y & kTileHasMask) != 0 && hdr.z >= 0;
+        p.masks[32 * s_t0 + lane] = masked ? a.masks[32 * hdr.z + lane] : 0u;
+        hdr.z = s_t0;
+        if (!masked) hdr.y &= ~kTileHasMask;
+        if (lane == 0) p.tiles[s_t0] = hdr;
+      }
+      // the kept entries to their inner places, with their exclusion columns; a warp loads
+      // kPruneUnroll tiles (headers, entries, then mask rows) before it moves them
+      for (int k0 = w; k0 < n_nbr; k0 += kPruneUnroll * kPlaceWarps) {
+        int4 hdr[kPruneUnroll];
+        T4 e[kPruneUnroll];
+        uint32_t row[kPruneUnroll];
+#pragma unroll
+        for (int u = 0; u < kPruneUnroll; ++u) {
+          const int k = k0 + u * kPlaceWarps;
+          hdr[u] = make_int4(0, 0, -1, 0);
+          if (k < n_nbr) {
+            hdr[u] = a.tiles[t_out + 1 + k];
+            e[u] = ent[32 * (size_t)(t_out + 1 + k) + lane];
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < kPruneUnroll; ++u)
+          row[u] = ((hdr[u].y & kTileHasMask) && hdr[u].z >= 0) ? a.masks[32 * hdr[u].z + lane]
+                                                                 : 0u;
+#pragma unroll
+        for (int u = 0; u < kPruneUnroll; ++u) {
+          const int k = k0 + u * kPlaceWarps;
+          if (k >= n_nbr) break;
+          if (lane == 0 && (hdr[u].y & kTilePairImage)) atomicOr(&s_img, kTilePairImage);
+          const unsigned kb = all ? kFull : s_keep[k];  // all: the tile as it is, padding too
+          uint32_t col = 0u;  // i-slots of this entry's half that exclude it
+          if ((hdr[u].y & kTileHasMask) && hdr[u].z >= 0) {
+            for (int q = 0; q < 32; ++q) {
+              const unsigned c = __ballot_sync(kFull, (row[u] >> q) & 1u);
+              if (lane == q) col = c;
+            }
+          }
+          if ((kb >> lane) & 1u) {
+            const int half = lane >> 4;
+            const unsigned before = kb & ((1u << lane) - 1u) & (half ? 0xffff0000u : 0xffffu);
+            const int r = (all ? 16 * k : s_pre[half][k]) + __popc(before);
+            const int j = r / 16, q = 16 * half + (r & 15);
+            ent_in[32 * (size_t)(s_t0 + 1 + j) + q] = e[u];
+            cols[32 * j + q] = col;
+          }
+        }
+      }
+      // padding places of each half's last tile
+      const int tot_a = all ? 16 * n_nbr : s_pre[0][n_nbr];
+      const int tot_b = all ? 16 * n_nbr : s_pre[1][n_nbr];
+      for (int idx = threadIdx.x; idx < (s_nt - 1) * 32; idx += blockDim.x) {
+        const int j = idx >> 5, q = idx & 31, r = 16 * j + (q & 15);
+        if (r >= ((q & 16) ? tot_b : tot_a)) {
+          T4 pad;
+          pad.x = pad.y = pad.z = R(0);
+          if constexpr (kDouble) pad.w = -1.0;
+          else pad.w = __int_as_float(-1);
+          ent_in[32 * (size_t)(s_t0 + 1 + j) + q] = pad;
+          cols[32 * j + q] = 0u;
+        }
+      }
+      __syncthreads();
+      // masks (exclusions of the lane's i-slot among its half's entries, padding) and headers
+      const int ai = s_iatom[lane];
+      const int hb = lane & 16, tot = hb ? tot_b : tot_a;
+      for (int j = w; j < s_nt - 1; j += kPlaceWarps) {
+        const int ti = s_t0 + 1 + j;
+        uint32_t m = 0u;
+        if (ai < 0) {
+          m = kFull;
+        } else {
+#pragma unroll
+          for (int q = 0; q < 16; ++q) {
+            const bool pad = 16 * j + q >= tot;
+            const bool excl = (cols[32 * j + hb + q] >> lane) & 1u;
+            if (pad || excl) m |= 1u << (hb + q);
+          }
+        }
+        p.masks[32 * (size_t)ti + lane] = m;
+        const bool any = __any_sync(kFull, m != 0u);
+        if (lane == 0)
+          p.tiles[ti] = make_int4(I, kTileHalves | s_img | (any ? kTileHasMask : 0), ti, 0);
+      }
+    }
   }
+  // the last CTA to finish: tile count within capacity, prune done
   __syncthreads();
   if (threadIdx.x == 0) {
-    const int longest = all ? 16 * n_nbr : max(s_pre[0][n_nbr], s_pre[1][n_nbr]);
-    const int nt = 1 + (longest + 15) / 16;
-    int t0 = atomicAdd(p.n_tiles, nt);
-    if (t0 + nt > p.capacity) {
-      report_status(a.status, kStatusTileOverflow);
-      t0 = -1;
-    }
-    s_t0 = t0;
-    s_nt = nt;
-  }
-  __syncthreads();
-  if (s_t0 < 0) return;
-  // exclusion columns of the inner neighbour tiles: shared memory, or the global scratch for a
-  // block with more tiles than that holds
-  const bool shared_cols = s_nt - 1 <= kPruneSharedCols;
-  uint32_t* cols = shared_cols ? &s_cols[0][0] : p.cols + 32 * (size_t)(s_t0 + 1);
-  // block I's self tile, unchanged (its mask slot becomes its tile index)
-  if (w == 0) {
-    int4 hdr = a.tiles[t_out];
-    const bool masked = (hdr.y & kTileHasMask) != 0 && hdr.z >= 0;
-    p.masks[32 * s_t0 + lane] = masked ? a.masks[32 * hdr.z + lane] : 0u;
-    hdr.z = s_t0;
-    if (!masked) hdr.y &= ~kTileHasMask;
-    if (lane == 0) p.tiles[s_t0] = hdr;
-  }
-  // pass 2: the kept entries to their inner places, with their exclusion columns
-  for (int k = w; k < n_nbr; k += kCtaWarps) {
-    const int t = t_out + 1 + k;
-    const int4 hdr = a.tiles[t];
-    if (lane == 0 && (hdr.y & kTilePairImage)) atomicOr(&s_img, kTilePairImage);
-    const T4 e = ent[32 * t + lane];
-    const unsigned kb = all ? kFull : s_keep[k];  // all: the tile as it is, padding included
-    uint32_t col = 0u;  // i-slots of this entry's half that exclude it
-    if ((hdr.y & kTileHasMask) && hdr.z >= 0) {
-      const uint32_t row = a.masks[32 * hdr.z + lane];
-      for (int q = 0; q < 32; ++q) {
-        const unsigned c = __ballot_sync(kFull, (row >> q) & 1u);
-        if (lane == q) col = c;
-      }
-    }
-    if ((kb >> lane) & 1u) {
-      const int half = lane >> 4;
-      const unsigned before = kb & ((1u << lane) - 1u) & (half ? 0xffff0000u : 0xffffu);
-      const int r = (all ? 16 * k : s_pre[half][k]) + __popc(before);
-      const int j = r / 16, q = 16 * half + (r & 15);
-      ent_in[32 * (s_t0 + 1 + j) + q] = e;
-      cols[32 * j + q] = col;
+    __threadfence();
+    if (atomicAdd(p.done, 1u) == gridDim.x - 1) {
+      __threadfence();
+      const int used = atomicAdd(p.n_tiles, 0);
+      if (used > p.capacity) *p.n_tiles = p.capacity;
+      *p.prune = 0;
+      *p.prune_count += 1;
     }
   }
-  // padding places of each half's last tile
-  const int tot_a = all ? 16 * n_nbr : s_pre[0][n_nbr], tot_b = all ? 16 * n_nbr : s_pre[1][n_nbr];
-  for (int idx = threadIdx.x; idx < (s_nt - 1) * 32; idx += blockDim.x) {
-    const int j = idx >> 5, q = idx & 31, r = 16 * j + (q & 15);
-    if (r >= ((q & 16) ? tot_b : tot_a)) {
-      T4 pad;
-      pad.x = pad.y = pad.z = R(0);
-      if constexpr (kDouble) pad.w = -1.0;
-      else pad.w = __int_as_float(-1);
-      ent_in[32 * (s_t0 + 1 + j) + q] = pad;
-      cols[32 * j + q] = 0u;
-    }
-  }
-  __syncthreads();
-  // pass 3: masks (exclusions of the lane's i-slot among its half's entries, padding) and headers
-  const int ai = s_iatom[lane];
-  const int hb = lane & 16, tot = hb ? tot_b : tot_a;
-  for (int j = w; j < s_nt - 1; j += kCtaWarps) {
-    const int ti = s_t0 + 1 + j;
-    uint32_t m = 0u;
-    if (ai < 0) {
-      m = kFull;
-    } else {
-#pragma unroll
-      for (int q = 0; q < 16; ++q) {
-        const bool pad = 16 * j + q >= tot;
-        const bool excl = (cols[32 * j + hb + q] >> lane) & 1u;
-        if (pad || excl) m |= 1u << (hb + q);
-      }
-    }
-    p.masks[32 * ti + lane] = m;
-    const bool any = __any_sync(kFull, m != 0u);
-    if (lane == 0)
-      p.tiles[ti] = make_int4(I, kTileHalves | s_img | (any ? kTileHasMask : 0), ti, 0);
-  }
-}
-
-__global__ void nl_prune_begin(PruneArgs p) {
-  if (*p.prune) *p.n_tiles = 0;
-}
-
-__global__ void nl_prune_end(PruneArgs p) {
-  if (*p.prune == 0) return;
-  *p.prune = 0;
-  *p.prune_count += 1;
 }
 
 __global__ void nl_prune_condition(const int* prune, cudaGraphConditionalHandle handle) {
@@ -1047,15 +1098,29 @@ void launch_prune_condition(const PruneArgs& p, cudaGraphConditionalHandle handl
 void launch_nlist_prune(const NlistArgs& a, const PruneArgs& p, bool double_entries,
                         cudaStream_t s) {
   const int block_cap = a.slot_capacity / 32;
-  nl_prune_begin<<<1, 1, 0, s>>>(p);
-  if (double_entries)
-    nl_prune<true><<<block_cap, 32 * kCtaWarps, 0, s>>>(a, p);
-  else
-    nl_prune<false><<<block_cap, 32 * kCtaWarps, 0, s>>>(a, p);
-  nl_prune_end<<<1, 1, 0, s>>>(p);
+  // the keep pass: as many CTAs as fit on the device at once, striding over the tiles
+  static int resident[2] = {0, 0};
+  int& r = resident[double_entries ? 1 : 0];
+  if (r == 0) {
+    if (double_entries)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, nl_prune_keep<true>, 32 * kPruneKeepWarps, 0);
+    else
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r, nl_prune_keep<false>, 32 * kPruneKeepWarps, 0);
+    r = std::max(r, 1);
+  }
+  const int keep_grid =
+      std::max(1, std::min(ceil_div(a.tile_capacity, kPruneKeepWarps), r * p.sm_count));
+  if (double_entries) {
+    nl_prune_keep<true><<<keep_grid, 32 * kPruneKeepWarps, 0, s>>>(a, p);
+    nl_prune_place<true><<<block_cap, 32 * kPlaceWarps, 0, s>>>(a, p);
+  } else {
+    nl_prune_keep<false><<<keep_grid, 32 * kPruneKeepWarps, 0, s>>>(a, p);
+    nl_prune_place<false><<<block_cap, 32 * kPlaceWarps, 0, s>>>(a, p);
+  }
 }
 
-void launch_nlist_rebuild(const NlistArgs& a, bool double_entries, cudaStream_t s) {
+void launch_nlist_rebuild(const NlistArgs& a, bool double_entries, cudaStream_t s,
+                          const PmeBricks* bricks) {
   const int tb = 256;
   const int ga = ceil_div(a.n_atoms, tb);
   const int block_cap = a.slot_capacity / 32;
@@ -1083,6 +1148,7 @@ void launch_nlist_rebuild(const NlistArgs& a, bool double_entries, cudaStream_t 
     else
       nl_lists<false><<<gl, 32 * kListWarps, 0, s>>>(a);
   }
+  if (bricks) launch_pme_brick_ranges(a, *bricks, s);
   nl_finish<<<std::max(1, std::min(ceil_div(a.n_cols, tb), 148 * 4)), tb, 0, s>>>(a);
   nl_clear_flag<<<1, 1, 0, s>>>(a);
 }

@@ -208,7 +208,7 @@ __global__ void convert_kernel(const PmeArgs<Real> a) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
        i += (long long)gridDim.x * blockDim.x) {
     a.grid_real[i] = (Real)((double)a.grid_fixed[i] * kGridScaleInv);
-    a.grid_fixed[i] = 0;
+    if (!a.grid_stored) a.grid_fixed[i] = 0;
   }
 }
 
@@ -600,7 +600,8 @@ __global__ void __launch_bounds__(kPlaneThreads) planes_forward(const PmeArgs<Re
         A[i] = v;
       });
   __syncthreads();
-  for (int i = threadIdx.x; i < ny * nz; i += blockDim.x) plane[i] = 0;  // ready for the next spread
+  if (!a.grid_stored)  // ready for the next atomic spread
+    for (int i = threadIdx.x; i < ny * nz; i += blockDim.x) plane[i] = 0;
   C2* r = stockham(A, B, twz, f, 2, nz, nyp);
   C2* o = r == A ? B : A;
   // split the two real rows' spectra: X_even = (Z_k + conj Z_-k)/2, X_odd = -i (Z_k - conj Z_-k)/2,
@@ -830,5 +831,354 @@ template void launch_pme_convolve<float>(const PmeArgs<float>&, bool, cudaStream
 template void launch_pme_convolve<double>(const PmeArgs<double>&, bool, cudaStream_t);
 template void launch_pme_gather<float>(const PmeArgs<float>&, cudaStream_t);
 template void launch_pme_gather<double>(const PmeArgs<double>&, cudaStream_t);
+
+// ---- brick-owned spreading and gathering -------------------------------------------------
+// For large grids in rectangular boxes.  One CTA per brick of kBrickEdge^3 grid points: it
+// collects the brick's candidate atoms from the per-rebuild slot ranges of the x-y columns in
+// reach, adds each candidate's stencil points that fall inside the brick (spread) or takes the
+// candidates whose stencil starts inside the brick (gather), and touches the global grid once
+// per point: the spread stores the brick's fixed-point sums, so the grid needs no zeroing and
+// no global atomics; the gather reads the brick and its 4-point halo into shared memory.  The
+// integer grid is the atomic spread's exactly (the same fixed-point contributions), and the
+// gather sums each atom's stencil planes in the order of the eight-lane kernel, so both paths
+// give the same forces.
+namespace {
+
+constexpr int kBrickThreads = 256;
+constexpr int kBrickCells = kBrickEdge * kBrickEdge * kBrickEdge;
+constexpr int kBrickCellsPerThread = (kBrickCells + kBrickThreads - 1) / kBrickThreads;
+constexpr int kBrickHalo = (kBrickEdge + 4) * (kBrickEdge + 4) * (kBrickEdge + 4);
+static_assert(kBrickMaxRanges <= kBrickThreads, "one range per thread when collecting");
+
+// first slot k in [s0, s0 + n) of a z-sorted column with zkey >= z (s0 + n if none)
+__device__ int column_lower(const NlistArgs& a, int s0, int n, float z) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (a.zkey[a.sorted_atom[s0 + mid]] < z)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return s0 + lo;
+}
+
+// One thread per (column, z layer of bricks): the slots of the column's atoms whose wrapped
+// rebuild z lies within the layer's reach, as one range or two (the reach wraps the box).
+__global__ void brick_ranges_kernel(const NlistArgs a, const PmeBricks b) {
+  if (*a.rebuild == 0) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.n_cols * b.nb[2]) return;
+  const int c = i % a.n_cols, bz = i / a.n_cols;
+  const int s0 = a.col_start[c];
+  const int n = min(a.col_scatter[c + 1] - a.col_scatter[c], a.col_max);
+  const double L = b.len[2];
+  const double z0 = bz * kBrickEdge * b.cell[2] - b.below[2];
+  const double z1 = min((bz + 1) * kBrickEdge, b.grid[2]) * b.cell[2] + b.above;
+  int2 r0 = make_int2(s0, s0), r1 = make_int2(s0, s0);
+  if (z1 - z0 >= L) {
+    r0.y = s0 + n;
+  } else if (z0 < 0.0) {
+    r0 = make_int2(column_lower(a, s0, n, (float)(z0 + L)), s0 + n);
+    r1 = make_int2(s0, column_lower(a, s0, n, (float)z1));
+  } else if (z1 > L) {
+    r0 = make_int2(column_lower(a, s0, n, (float)z0), s0 + n);
+    r1 = make_int2(s0, column_lower(a, s0, n, (float)(z1 - L)));
+  } else {
+    r0 = make_int2(column_lower(a, s0, n, (float)z0), column_lower(a, s0, n, (float)z1));
+  }
+  b.ranges[2 * i] = r0;
+  b.ranges[2 * i + 1] = r1;
+}
+
+// first grid point and extent of brick `id` along each axis
+__device__ __forceinline__ void brick_box(const PmeBricks& b, int id, int b0[3], int e[3],
+                                          int bi[3]) {
+  bi[0] = id % b.nb[0];
+  bi[1] = (id / b.nb[0]) % b.nb[1];
+  bi[2] = id / (b.nb[0] * b.nb[1]);
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    b0[d] = bi[d] * kBrickEdge;
+    e[d] = min(kBrickEdge, b.grid[d] - b0[d]);
+  }
+}
+
+// columns along axis d (0: x, 1: y) whose rebuild positions can reach brick index bd
+__device__ __forceinline__ void column_span(const PmeBricks& b, int d, int bd, int& c0, int& nc) {
+  const int ncol = b.n_col[d];
+  const double w = b.len[d] / ncol;
+  const double lo = bd * kBrickEdge * b.cell[d] - b.below[d];
+  const double hi = min((bd + 1) * kBrickEdge, b.grid[d]) * b.cell[d] + b.above;
+  c0 = (int)floor(lo / w);
+  nc = (int)floor(hi / w) - c0 + 1;
+  if (nc >= ncol) {
+    c0 = 0;
+    nc = ncol;
+  }
+}
+
+// The brick's candidate slot ranges into s_rng, their exclusive prefix into s_pre; returns the
+// number of ranges (the candidate count is s_pre[ranges]).  Block-wide, with barriers.
+__device__ int brick_candidates(const PmeBricks& b, const NlistArgs& nl, const int bi[3],
+                                int2* s_rng, int* s_pre, int* s_warp) {
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  int cx0, ncx, cy0, ncy;
+  column_span(b, 0, bi[0], cx0, ncx);
+  column_span(b, 1, bi[1], cy0, ncy);
+  const int nr = min(2 * ncx * ncy, kBrickMaxRanges);  // the host keeps 2 ncx ncy within
+  int len = 0;
+  if (t < nr) {
+    const int k = t >> 1, piece = t & 1;
+    int cx = (cx0 + k % ncx) % b.n_col[0];
+    int cy = (cy0 + k / ncx) % b.n_col[1];
+    cx += cx < 0 ? b.n_col[0] : 0;
+    cy += cy < 0 ? b.n_col[1] : 0;
+    const int col = cy * b.n_col[0] + cx;
+    const int2 r = b.ranges[2 * ((size_t)bi[2] * nl.n_cols + col) + piece];
+    s_rng[t] = r;
+    len = max(r.y - r.x, 0);
+  }
+  int incl = len;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) s_warp[w] = incl;
+  __syncthreads();
+  if (w == 0) {
+    int v = lane < kBrickThreads / 32 ? s_warp[lane] : 0, x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane < kBrickThreads / 32) s_warp[lane] = x - v;  // exclusive warp offsets
+  }
+  __syncthreads();
+  const int excl = incl - len + s_warp[w];
+  if (t < nr) s_pre[t] = excl;
+  if (t == nr - 1) s_pre[nr] = excl + len;
+  __syncthreads();
+  return nr;
+}
+
+// slot of candidate i: the last range whose prefix does not exceed i holds it
+__device__ __forceinline__ int candidate_slot(const int2* s_rng, const int* s_pre, int nr, int i) {
+  int lo = 0, hi = nr - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (s_pre[mid] <= i)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return s_rng[lo].x + (i - s_pre[lo]);
+}
+
+// in-brick points of a stencil along one axis: bit i for point base + i (periodic)
+__device__ __forceinline__ unsigned brick_points(int base, int n, int b0, int e) {
+  unsigned m = 0u;
+#pragma unroll
+  for (int i = 0; i < 5; ++i) {
+    int g = base + i;
+    g -= g >= n ? n : 0;
+    m |= ((unsigned)(g - b0) < (unsigned)e ? 1u : 0u) << i;
+  }
+  return m;
+}
+
+// Shared sums use 32-bit atomics on a split of each fixed-point contribution,
+// v = hi 2^22 + lo with 0 <= lo < 2^22 (|v| < 2^44 for |q| < 16 e).  Each round of the
+// candidate loop gives a point at most one contribution per thread (256), so both partial sums
+// stay inside 32 bits; after every round each thread folds its points into 64-bit registers.
+template <class Real>
+__global__ void __launch_bounds__(kBrickThreads) spread_bricks_kernel(const PmeArgs<Real> a,
+                                                                      const PmeBricks b,
+                                                                      const NlistArgs nl) {
+  __shared__ int c_hi[kBrickCells];
+  __shared__ unsigned int c_lo[kBrickCells];
+  __shared__ int2 s_rng[kBrickMaxRanges];
+  __shared__ int s_pre[kBrickMaxRanges + 1];
+  __shared__ int s_warp[kBrickThreads / 32];
+  int b0[3], e[3], bi[3];
+  brick_box(b, blockIdx.x, b0, e, bi);
+  for (int c = threadIdx.x; c < kBrickCells; c += kBrickThreads) {
+    c_hi[c] = 0;
+    c_lo[c] = 0u;
+  }
+  const int nr = brick_candidates(b, nl, bi, s_rng, s_pre, s_warp);
+  const int n_cand = s_pre[nr];
+  const int nc = e[0] * e[1] * e[2];
+  long long acc[kBrickCellsPerThread];
+#pragma unroll
+  for (int k = 0; k < kBrickCellsPerThread; ++k) acc[k] = 0;
+  const Real gscale = Real(kGridScale);
+  for (int i0 = 0; i0 < n_cand; i0 += kBrickThreads) {
+    const int i = i0 + threadIdx.x;
+    if (i < n_cand) {
+      const int atom = nl.sorted_atom[candidate_slot(s_rng, s_pre, nr, i)];
+      const double qd = atom >= 0 ? a.charge[atom] : 0.0;
+      int base[3];
+      Real frac[3];
+      if (qd != 0.0 && stencil(a, atom, base, frac)) {
+        const unsigned mx = brick_points(base[0], a.nx, b0[0], e[0]);
+        const unsigned my = brick_points(base[1], a.ny, b0[1], e[1]);
+        const unsigned mz = brick_points(base[2], a.nz, b0[2], e[2]);
+        if (mx && my && mz) {
+          Real w[3][5], dw[3][5];
+#pragma unroll
+          for (int d = 0; d < 3; ++d) spline5(frac[d], w[d], dw[d]);
+          const Real q = (Real)qd;
+#pragma unroll
+          for (int ix = 0; ix < 5; ++ix) {
+            if (!((mx >> ix) & 1u)) continue;
+            int gx = base[0] + ix;
+            gx -= gx >= a.nx ? a.nx : 0;
+            const Real qx = q * w[0][ix];
+#pragma unroll
+            for (int iy = 0; iy < 5; ++iy) {
+              if (!((my >> iy) & 1u)) continue;
+              int gy = base[1] + iy;
+              gy -= gy >= a.ny ? a.ny : 0;
+              const Real qxy = qx * w[1][iy];
+              const int row = ((gx - b0[0]) * e[1] + (gy - b0[1])) * e[2];
+#pragma unroll
+              for (int iz = 0; iz < 5; ++iz) {
+                if (!((mz >> iz) & 1u)) continue;
+                int gz = base[2] + iz;
+                gz -= gz >= a.nz ? a.nz : 0;
+                const long long v = to_fixed(qxy * w[2][iz], gscale);
+                const int cell = row + gz - b0[2];
+                atomicAdd(&c_hi[cell], (int)(v >> 22));
+                atomicAdd(&c_lo[cell], (unsigned int)(v & 0x3FFFFF));
+              }
+            }
+          }
+        }
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kBrickCellsPerThread; ++k) {
+      const int c = threadIdx.x + k * kBrickThreads;
+      if (c < nc) {
+        acc[k] += (long long)c_hi[c] * (1ll << 22) + (long long)c_lo[c];
+        c_hi[c] = 0;
+        c_lo[c] = 0u;
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int k = 0; k < kBrickCellsPerThread; ++k) {
+    const int c = threadIdx.x + k * kBrickThreads;
+    if (c < nc) {
+      const int cz = c % e[2], cy = (c / e[2]) % e[1], cx = c / (e[1] * e[2]);
+      a.grid_fixed[((long long)(b0[0] + cx) * a.ny + (b0[1] + cy)) * a.nz + b0[2] + cz] = acc[k];
+    }
+  }
+}
+
+template <class Real>
+__global__ void __launch_bounds__(kBrickThreads) gather_bricks_kernel(const PmeArgs<Real> a,
+                                                                      const PmeBricks b,
+                                                                      const NlistArgs nl) {
+  extern __shared__ __align__(16) unsigned char brick_smem[];
+  Real* phi = reinterpret_cast<Real*>(brick_smem);  // [(e0 + 4)(e1 + 4)(e2 + 4)]
+  __shared__ int2 s_rng[kBrickMaxRanges];
+  __shared__ int s_pre[kBrickMaxRanges + 1];
+  __shared__ int s_warp[kBrickThreads / 32];
+  int b0[3], e[3], bi[3];
+  brick_box(b, blockIdx.x, b0, e, bi);
+  const int h1 = e[1] + 4, h2 = e[2] + 4, nh = (e[0] + 4) * h1 * h2;
+  for (int c = threadIdx.x; c < nh; c += kBrickThreads) {
+    const int hz = c % h2, hy = (c / h2) % h1, hx = c / (h1 * h2);
+    int gx = b0[0] + hx, gy = b0[1] + hy, gz = b0[2] + hz;
+    gx -= gx >= a.nx ? a.nx : 0;
+    gy -= gy >= a.ny ? a.ny : 0;
+    gz -= gz >= a.nz ? a.nz : 0;
+    phi[c] = a.grid_real[((long long)gx * a.ny + gy) * a.nz + gz];
+  }
+  const int nr = brick_candidates(b, nl, bi, s_rng, s_pre, s_warp);  // barriers cover phi
+  const int n_cand = s_pre[nr];
+  for (int i = threadIdx.x; i < n_cand; i += kBrickThreads) {
+    const int atom = nl.sorted_atom[candidate_slot(s_rng, s_pre, nr, i)];
+    const double qd = atom >= 0 ? a.charge[atom] : 0.0;
+    int base[3];
+    Real frac[3];
+    if (qd == 0.0 || !stencil(a, atom, base, frac)) continue;
+    const int lx = base[0] - b0[0], ly = base[1] - b0[1], lz = base[2] - b0[2];
+    if ((unsigned)lx >= (unsigned)e[0] || (unsigned)ly >= (unsigned)e[1] ||
+        (unsigned)lz >= (unsigned)e[2])
+      continue;  // another brick's atom
+    Real w[3][5], dw[3][5];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) spline5(frac[d], w[d], dw[d]);
+    Real p0[5], p1[5], p2[5];  // stencil plane ix: the sums of lane ix of the eight-lane kernel
+#pragma unroll
+    for (int ix = 0; ix < 5; ++ix) {
+      Real g0 = 0, g1 = 0, g2 = 0;
+      const Real wx = w[0][ix], dwx = dw[0][ix];
+      for (int iy = 0; iy < 5; ++iy) {
+        const Real* row = phi + ((lx + ix) * h1 + (ly + iy)) * h2 + lz;
+        const Real wxy = wx * w[1][iy];
+        const Real dxy = dwx * w[1][iy];
+        const Real xdy = wx * dw[1][iy];
+#pragma unroll
+        for (int iz = 0; iz < 5; ++iz) {
+          const Real ph = row[iz];
+          g0 += ph * dxy * w[2][iz];
+          g1 += ph * xdy * w[2][iz];
+          g2 += ph * wxy * dw[2][iz];
+        }
+      }
+      p0[ix] = g0;
+      p1[ix] = g1;
+      p2[ix] = g2;
+    }
+    // the eight-lane kernel's xor tree (lanes 5-7 hold zeros)
+    const Real g0 = ((p0[0] + p0[4]) + p0[2]) + (p0[1] + p0[3]);
+    const Real g1 = ((p1[0] + p1[4]) + p1[2]) + (p1[1] + p1[3]);
+    const Real g2 = ((p2[0] + p2[4]) + p2[2]) + (p2[1] + p2[3]);
+    const double gd[3] = {(double)g0 * a.nx, (double)g1 * a.ny, (double)g2 * a.nz};
+    for (int c = 0; c < 3; ++c) {
+      const double f = -qd * (gd[0] * a.recip[0][c] + gd[1] * a.recip[1][c] + gd[2] * a.recip[2][c]);
+      add_fixed(a.force + (long long)c * a.n_atoms + atom, to_fixed(f, kForceScale));
+    }
+  }
+}
+
+}  // namespace
+
+void launch_pme_brick_ranges(const NlistArgs& a, const PmeBricks& b, cudaStream_t s) {
+  const int n = a.n_cols * b.nb[2];
+  brick_ranges_kernel<<<ceil_div(n, 128), 128, 0, s>>>(a, b);
+}
+
+template <class Real>
+void launch_pme_spread_bricks(const PmeArgs<Real>& a, const PmeBricks& b, const NlistArgs& nl,
+                              cudaStream_t s) {
+  spread_bricks_kernel<Real><<<b.nb[0] * b.nb[1] * b.nb[2], kBrickThreads, 0, s>>>(a, b, nl);
+}
+
+template <class Real>
+void launch_pme_gather_bricks(const PmeArgs<Real>& a, const PmeBricks& b, const NlistArgs& nl,
+                              cudaStream_t s) {
+  const int bytes = (int)(sizeof(Real) * kBrickHalo);  // the FP64 halo exceeds 48 KB with the rest
+  cudaFuncSetAttribute(gather_bricks_kernel<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       bytes);
+  gather_bricks_kernel<Real><<<b.nb[0] * b.nb[1] * b.nb[2], kBrickThreads, bytes, s>>>(a, b, nl);
+}
+
+template void launch_pme_spread_bricks<float>(const PmeArgs<float>&, const PmeBricks&,
+                                              const NlistArgs&, cudaStream_t);
+template void launch_pme_spread_bricks<double>(const PmeArgs<double>&, const PmeBricks&,
+                                               const NlistArgs&, cudaStream_t);
+template void launch_pme_gather_bricks<float>(const PmeArgs<float>&, const PmeBricks&,
+                                              const NlistArgs&, cudaStream_t);
+template void launch_pme_gather_bricks<double>(const PmeArgs<double>&, const PmeBricks&,
+                                               const NlistArgs&, cudaStream_t);
 
 }  // namespace ommb200

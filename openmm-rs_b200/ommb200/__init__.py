@@ -66,7 +66,8 @@ _ERRORS = {ERR_INVALID_ARG: InvalidArgument, ERR_CONSTRAINT: ConstraintError,
 
 class Options(C.Structure):
     _fields_ = [("precision", C.c_int), ("device", C.c_int), ("use_cuda_graph", C.c_int),
-                ("neighbor_skin", C.c_double), ("steps_per_graph", C.c_int)]
+                ("neighbor_skin", C.c_double), ("steps_per_graph", C.c_int),
+                ("pme_bricks", C.c_int)]
 
 
 class LearnedRadiiStats(C.Structure):
@@ -167,6 +168,7 @@ def library() -> C.CDLL:
                                           C.POINTER(D), C.POINTER(StateInfo)],
             "ommb200_context_get_pme_parameters": [P, C.POINTER(D), C.POINTER(I), C.POINTER(I),
                                                    C.POINTER(I)],
+            "ommb200_context_get_pme_layout": [P, C.POINTER(I), C.POINTER(I)],
             "ommb200_context_debug_pair_list": [P, C.c_int64, C.POINTER(C.c_int32),
                                                 C.POINTER(C.c_int64)],
             "ommb200_context_kernel_times": [P, I, C.c_char_p, I, C.POINTER(D), C.POINTER(I),
@@ -557,13 +559,15 @@ class State:
         return self.kinetic_energy
 
 
-def _options(precision, device, use_cuda_graph, neighbor_skin, steps_per_graph) -> "Options":
+def _options(precision, device, use_cuda_graph, neighbor_skin, steps_per_graph,
+             pme_bricks=-1) -> "Options":
     opt = Options()
     opt.precision = {"mixed": PRECISION_MIXED, "double": PRECISION_DOUBLE}[precision]
     opt.device = device
     opt.use_cuda_graph = int(use_cuda_graph)
     opt.neighbor_skin = neighbor_skin
     opt.steps_per_graph = steps_per_graph
+    opt.pme_bricks = pme_bricks
     return opt
 
 
@@ -572,9 +576,13 @@ class Context:
 
     def __init__(self, system: System, integrator: LangevinMiddleIntegrator, precision="mixed",
                  device: int = 0, use_cuda_graph: bool = True, neighbor_skin: float = 0.0,
-                 steps_per_graph: int = 0):
+                 steps_per_graph: int = 0, pme_bricks: int = -1):
+        """`pme_bricks`: brick-owned PME spread and gather in rectangular periodic boxes, -1 when
+        the grid has at least two bricks per SM, 0 never, 1 whenever the box allows (the forces
+        are the same either way)."""
         n = system.num_particles()
-        opt = _options(precision, device, use_cuda_graph, neighbor_skin, steps_per_graph)
+        opt = _options(precision, device, use_cuda_graph, neighbor_skin, steps_per_graph,
+                       pme_bricks)
         h = C.c_void_p()
         sys_h, int_h = system._take(), integrator._take()
         _check(library().ommb200_context_create(sys_h, int_h, C.byref(opt), C.byref(h)))
@@ -666,6 +674,12 @@ class Context:
                                                             C.byref(ny), C.byref(nz)))
         return a.value, (nx.value, ny.value, nz.value)
 
+    def pme_layout(self) -> dict:
+        """PME spread/gather form: brick-owned (`bricks_in_use`) or atomic; grid bricks."""
+        u, n = C.c_int(), C.c_int()
+        _check(library().ommb200_context_get_pme_layout(self._h, C.byref(u), C.byref(n)))
+        return {"bricks_in_use": bool(u.value), "bricks": n.value}
+
     def debug_pair_list(self, max_pairs: int | None = None) -> np.ndarray:
         """The interacting nonbonded pairs (i < j) as evaluated by the pair kernel."""
         count = C.c_int64()
@@ -726,13 +740,14 @@ class Context:
         _check(library().ommb200_context_set_profiling(self._h, int(enabled)))
 
     def autotune(self, trial_steps: int = 200) -> dict:
-        """Pick the Verlet skin and pair-kernel grid by timing `trial_steps` MD steps per
-        candidate; the state is restored afterwards."""
+        """Pick the Verlet skin, tile width, pruned-list margin and pair-kernel grid by timing
+        `trial_steps` MD steps per candidate; the state is restored afterwards."""
         skin, ctas, ms = C.c_double(), C.c_int(), C.c_double()
         _check(library().ommb200_context_autotune(self._h, int(trial_steps), C.byref(skin),
                                                   C.byref(ctas), C.byref(ms)))
         out = {"skin_nm": skin.value, "pair_ctas_per_sm": ctas.value, "ms_per_step": ms.value}
         out["tile_entries"] = self.tuning()["tile_entries"]
+        out["prune_margin_nm"] = self.nlist_prune_stats()["margin_nm"]
         return out
 
     def tuning(self) -> dict:
