@@ -67,9 +67,13 @@ typedef struct {
   int use_cuda_graph;         /* capture the step in a CUDA graph (default 1) */
   double neighbor_skin;       /* Verlet skin in nm; <= 0 picks the tuned default */
   int steps_per_graph;        /* steps captured per graph launch; <= 0 picks the default */
-  int pme_bricks;             /* brick-owned PME spread and gather (rectangular periodic boxes):
+  int pme_bricks;             /* brick-owned PME gather (rectangular periodic boxes):
                                  -1 when the grid has two bricks per SM or more (default), 0 never,
                                  1 whenever the box allows; the forces are the same either way */
+  double prune_margin;        /* nm, pruned pair list between rebuilds (periodic rectangular
+                                 boxes): entries beyond cutoff + margin of their half block are
+                                 dropped until a particle moves margin / 2; 0 = off; < 0 picks
+                                 the default (off; ommb200_context_autotune may turn it on) */
 } ommb200_options;
 
 typedef struct {
@@ -267,8 +271,8 @@ int ommb200_context_get_tuning(ommb200_context* ctx, double* skin, int* pair_cta
 /* PME parameters frozen at Context creation (nonbonded.rs:1078-1106). */
 int ommb200_context_get_pme_parameters(const ommb200_context* ctx, double* alpha, int* nx,
                                        int* ny, int* nz);
-/* Which PME spread/gather form runs (no reference counterpart): *bricks_in_use = 1 for the
- * brick-owned form, 0 for the atomic one; *bricks = grid bricks of kBrickEdge^3 points (0 without
+/* Which PME gather form runs (no reference counterpart): *bricks_in_use = 1 for the
+ * brick-owned form, 0 for the eight-lanes-per-particle one; *bricks = grid bricks of kBrickEdge^3 points (0 without
  * PME).  Outputs may be NULL. */
 int ommb200_context_get_pme_layout(const ommb200_context* ctx, int* bricks_in_use, int* bricks);
 

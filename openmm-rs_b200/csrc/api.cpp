@@ -131,6 +131,7 @@ void ommb200_default_options(ommb200_options* out) {
   out->neighbor_skin = 0.0;
   out->steps_per_graph = 0;
   out->pme_bricks = -1;
+  out->prune_margin = -1.0;
 }
 
 // ---- System -----------------------------------------------------------------------------
@@ -537,6 +538,8 @@ static EngineOptions engine_options(const ommb200_options* options) {
   require(o.precision == OMMB200_PRECISION_MIXED || o.precision == OMMB200_PRECISION_DOUBLE,
           "unknown precision");
   require(o.pme_bricks >= -1 && o.pme_bricks <= 1, "pme_bricks must be -1, 0 or 1");
+  require(std::isfinite(o.prune_margin) && o.prune_margin <= 0.5,
+          "prune_margin must be finite and at most 0.5 nm");
   EngineOptions eo;
   eo.precision = o.precision;
   eo.device = o.device;
@@ -544,6 +547,7 @@ static EngineOptions engine_options(const ommb200_options* options) {
   eo.skin = o.neighbor_skin;
   eo.steps_per_graph = o.steps_per_graph;
   eo.pme_bricks = o.pme_bricks;
+  eo.prune_margin = o.prune_margin;
   return eo;
 }
 

@@ -61,6 +61,18 @@ struct Box {
   Real inv_ax, inv_by, inv_cz;
 };
 
+// Position x of a particle relative to the centre c of its block, in the frame of the lattice
+// image n it was given at the last neighbour-list rebuild, with explicitly rounded operations
+// (the pack kernel and the integrator both write these and must agree bit for bit).
+__device__ __forceinline__ void block_local(const double x[3], double n0, double n1, double n2,
+                                            const double* c, const Box<double>& b, double o[3]) {
+  o[0] = __dsub_rn(__dsub_rn(x[0], __dadd_rn(__dadd_rn(__dmul_rn(n0, b.ax), __dmul_rn(n1, b.bx)),
+                                             __dmul_rn(n2, b.cx))),
+                   c[0]);
+  o[1] = __dsub_rn(__dsub_rn(x[1], __dadd_rn(__dmul_rn(n1, b.by), __dmul_rn(n2, b.cy))), c[1]);
+  o[2] = __dsub_rn(__dsub_rn(x[2], __dmul_rn(n2, b.cz)), c[2]);
+}
+
 // Minimum image in the reference's exact sequence (harmonic_bond.rs:152-159), computed
 // with explicitly rounded operations so that no fused multiply-add changes the result.
 __device__ __forceinline__ void min_image_exact(double& dx, double& dy, double& dz,

@@ -440,7 +440,8 @@ void Engine::setup_nonbonded(const NonbondedDef& nb) {
     prune_n_tiles_ = mem_.alloc<int>(1);
     prune_done_ = mem_.alloc<unsigned>(1);
     a.prune = prune_flag_;
-    alloc_pruned_list();
+    prune_margin_ = opt_.prune_margin >= 0.0 ? opt_.prune_margin : kDefaultPruneMargin;
+    if (prune_margin_ > 0.0) alloc_pruned_list();
   }
   posq_ = mem_.alloc_bytes((dp_ ? 32 : 16) * (size_t)n_slots_);
   ljp_ = mem_.alloc_bytes((dp_ ? 16 : 8) * (size_t)n_slots_);
@@ -541,6 +542,9 @@ void Engine::setup_nonbonded(const NonbondedDef& nb) {
       bricks_.n_col[0] = nl_.n_col[0];
       bricks_.n_col[1] = nl_.n_col[1];
       bricks_.ranges = mem_.alloc<int2>(2 * (size_t)nl_.n_cols * bricks_.nb[2]);
+      bricks_.n_slots = nl_.slot_capacity;
+      bricks_.base = mem_.alloc<int4>((size_t)nl_.slot_capacity);
+      bricks_.frac = mem_.alloc_bytes((dp_ ? 32 : 16) * (size_t)nl_.slot_capacity);
     }
   }
   upload_nonbonded_parameters(nb);
@@ -570,12 +574,7 @@ void Engine::upload_nonbonded_parameters(const NonbondedDef& nb) {
   dispersion_coeff_ =
       (nb_periodic_ && nb.use_dispersion_correction) ? dispersion_coefficient(nb) : 0.0;
   double q2 = 0.0;
-  max_abs_charge_ = 0.0;
-  for (double q : nb.charge) {
-    q2 += q * q;
-    max_abs_charge_ = std::max(max_abs_charge_, std::fabs(q));
-  }
-  if (volume_ > 0.0) update_bricks();  // after Context creation (the box is set)
+  for (double q : nb.charge) q2 += q * q;
   self_energy_ = nb_pme_ ? -kOne4PiEps0 * alpha_ / std::sqrt(kPiD) * q2 : 0.0;
   if (nb_pme_ && volume_ > 0.0) {  // after Context creation: the neutralising term
     double qt = 0.0;
@@ -607,6 +606,10 @@ void Engine::update_nonbonded(const NonbondedDef& src) {
   nb.epsilon = src.epsilon;
   nb.exceptions = src.exceptions;
   upload_nonbonded_parameters(nb);
+  if (packed_by_integrator()) {
+    pack_slots(pos_, stream_);
+    sync();
+  }
 }
 
 // context.rs:680-687 / gbsa_obc.rs:134-141: new charges, radii and scale factors.
@@ -1144,22 +1147,21 @@ void Engine::update_box_dependents() {
   update_bricks();
 }
 
-// Brick-owned PME (spread and gather of large grids in rectangular boxes): chosen while the box
-// is rectangular, every charge is below 16 e (the shared sums' bound), a brick's columns fit
-// kBrickMaxRanges and the grid has at least two bricks per SM (or the option asks for it).
-// A change of choice drops the captured graph and asks for a rebuild (the slot ranges are made
-// with the list); leaving the brick form zeroes the grid for the atomic spread.
+// Brick-owned PME gather (large grids in rectangular boxes): chosen while the box is rectangular,
+// a brick's columns fit kBrickMaxRanges and the grid has at least two bricks per SM (or the
+// option asks for it).  A change of choice drops the captured graph and asks for a rebuild (the
+// slot ranges are made with the list).
 void Engine::update_bricks() {
   const bool before = use_bricks_;
   bool use = false;
   if (bricks_.ranges && opt_.pme_bricks != 0 && box_[3] == 0.0 && box_[6] == 0.0 &&
-      box_[7] == 0.0 && max_abs_charge_ < 16.0) {
+      box_[7] == 0.0) {
     const double drift = 0.5 * std::max(skin_, kMaxTunedSkin), slack = 1e-3;
     int cols[2] = {1, 1};
     for (int d = 0; d < 3; ++d) {
       bricks_.len[d] = box_[4 * d];
       bricks_.cell[d] = box_[4 * d] / grid_[d];
-      bricks_.below[d] = 4.0 * bricks_.cell[d] + drift + slack;
+      bricks_.below[d] = drift + slack;  // a stencil starting in the brick: its base point
     }
     bricks_.above = drift + slack;
     for (int d = 0; d < 2; ++d) {
@@ -1176,7 +1178,6 @@ void Engine::update_bricks() {
   destroy_graph();
   const int one = 1;
   OMMB200_CK(cudaMemcpy(rebuild_, &one, 4, cudaMemcpyHostToDevice));
-  if (!use) OMMB200_CK(cudaMemset(pme_fixed_, 0, 8 * (size_t)grid_[0] * grid_[1] * grid_[2]));
 }
 
 void Engine::destroy_graph() {
@@ -1316,7 +1317,7 @@ void Engine::enqueue_conditional_rebuild() {
   OMMB200_CK(cudaGraphConditionalHandleCreate(&handle, cap, 0, cudaGraphCondAssignDefault));
   launch_nlist_condition(nl_, handle, stream_);
   enqueue_conditional_body(handle, [&](cudaStream_t s) {
-    launch_nlist_rebuild(nl_, dp_, s, use_bricks_ ? &bricks_ : nullptr);
+    launch_nlist_rebuild(nl_, dp_, s, with_new_list(nl_));
   });
 }
 
@@ -1347,8 +1348,12 @@ void Engine::enqueue_conditional_body(cudaGraphConditionalHandle handle,
 }
 
 bool Engine::pruning() const {
-  return prune_margin_ > 0.0 && nb_periodic_ && nl_.block_tiles && nl_.halves && nl_.max_cand > 0 && box_[3] == 0.0 &&
+  return prune_margin_ > 0.0 && prune_tiles_ && nb_periodic_ && nl_.block_tiles && nl_.halves && nl_.max_cand > 0 && box_[3] == 0.0 &&
          box_[6] == 0.0 && box_[7] == 0.0;
+}
+
+void Engine::ensure_pruned_list() {
+  if (!prune_tiles_ && nl_.block_tiles) alloc_pruned_list();
 }
 
 void Engine::alloc_pruned_list() {
@@ -1388,7 +1393,7 @@ void Engine::enqueue_nonbonded(bool energy, bool direct, bool reciprocal, bool d
     if (capturing_)
       enqueue_conditional_rebuild();
     else
-      launch_nlist_rebuild(nl_, dp_, stream_, use_bricks_ ? &bricks_ : nullptr);
+      launch_nlist_rebuild(nl_, dp_, stream_, with_new_list(nl_));
     prof_end();
   }
   // fork: PME on its own stream (serialised on the main stream while profiling, so that
@@ -1400,10 +1405,12 @@ void Engine::enqueue_nonbonded(bool energy, bool direct, bool reciprocal, bool d
     OMMB200_CK(cudaStreamWaitEvent(ps, fork_ev_, 0));
   }
   if (direct && pairs) {
-    prof_begin("pack");
-    launch_pack<Real>(n_slots_, nl_.sorted_atom, pos_, nl_.image, nl_.block_center, qscaled_,
-                      half_sigma_, sqrt_eps_, posq_, ljp_, nl_.box, stream_);
-    prof_end();
+    if (!packed_by_integrator()) {
+      prof_begin("pack");
+      launch_pack<Real>(n_slots_, nl_.sorted_atom, pos_, nl_.image, nl_.block_center, qscaled_,
+                        half_sigma_, sqrt_eps_, posq_, ljp_, nl_.box, stream_);
+      prof_end();
+    }
     const bool pruned = pruning();
     if (pruned) {  // a pending prune (after a rebuild, or once a particle moved margin / 2)
       const PruneArgs pa = prune_args();
@@ -1493,12 +1500,8 @@ void Engine::enqueue_nonbonded(bool energy, bool direct, bool reciprocal, bool d
     m.energy = energy_;
     m.alpha = alpha_;
     m.volume = volume_;
-    m.grid_stored = use_bricks_ ? 1 : 0;
     prof_begin("pme_spread");
-    if (use_bricks_)
-      launch_pme_spread_bricks<Real>(m, bricks_, nl_, ps);
-    else
-      launch_pme_spread<Real>(m, ps);
+    launch_pme_spread<Real>(m, ps);
     prof_end();
     if (own_fft_) {
       prof_begin("pme_transform");
@@ -1527,9 +1530,10 @@ void Engine::enqueue_nonbonded(bool energy, bool direct, bool reciprocal, bool d
     prof_end();
     }
     prof_begin("pme_gather");
-    if (use_bricks_)
+    if (use_bricks_) {
+      launch_pme_brick_stencils<Real>(m, bricks_, nl_, ps);
       launch_pme_gather_bricks<Real>(m, bricks_, nl_, ps);
-    else
+    } else
       launch_pme_gather<Real>(m, ps);
     prof_end();
   }
@@ -1558,9 +1562,12 @@ void Engine::enqueue_nonbonded(bool energy, bool direct, bool reciprocal, bool d
 }
 
 void Engine::compute_forces(bool energy, uint32_t groups, bool in_step, int step_offset) {
-  prof_begin("zero_forces");
-  OMMB200_CK(cudaMemsetAsync(force_, 0, sizeof(long long) * 3 * (size_t)n_, stream_));
-  prof_end();
+  // inside a captured group of steps the previous step's integrator left the forces zeroed
+  if (!(in_step && capturing_ && step_offset > 0)) {
+    prof_begin("zero_forces");
+    OMMB200_CK(cudaMemsetAsync(force_, 0, sizeof(long long) * 3 * (size_t)n_, stream_));
+    prof_end();
+  }
   gb_.fuse_nonbonded = 0;
   if (nb_) {
     const int g = nb_->force_group;
@@ -1661,9 +1668,41 @@ IntegrateArgs Engine::integrate_args(int step_offset) const {
 
 void Engine::enqueue_step(int step_offset) {
   compute_forces(false, integ_->integration_force_groups, true, step_offset);
+  IntegrateArgs a = integrate_args(step_offset);
+  a.zero_force = 1;
+  if (packed_by_integrator()) {
+    a.posq = posq_;
+    a.posq_double = dp_ ? 1 : 0;
+    a.atom_slot = nl_.atom_slot;
+    a.image = nl_.image;
+    a.block_center = nl_.block_center;
+    a.qscaled = qscaled_;
+    a.pbox = nl_.box;
+  }
   prof_begin("integrate");
-  launch_integrate(integrate_args(step_offset), stream_);
+  launch_integrate(a, stream_);
   prof_end();
+}
+
+// Periodic lists: the integrator writes the pair kernel's packed coordinates of the moved
+// particles, and the pack kernel runs only with a rebuild (new slots, images and centres) or
+// after new parameters or a checkpoint.  Every other change of the positions asks for a rebuild.
+bool Engine::packed_by_integrator() const { return nb_ && nb_periodic_ && segments_.size() <= 1; }
+
+std::function<void(cudaStream_t)> Engine::with_new_list(const NlistArgs& list) {
+  return [this, list](cudaStream_t s) {
+    if (use_bricks_) launch_pme_brick_ranges(list, bricks_, s);
+    if (packed_by_integrator()) pack_slots(list.pos, s, list.rebuild);
+  };
+}
+
+void Engine::pack_slots(const double* pos, cudaStream_t s, const int* only_after_rebuild) {
+  if (dp_)
+    launch_pack<double>(n_slots_, nl_.sorted_atom, pos, nl_.image, nl_.block_center, qscaled_,
+                        half_sigma_, sqrt_eps_, posq_, ljp_, nl_.box, s, only_after_rebuild);
+  else
+    launch_pack<float>(n_slots_, nl_.sorted_atom, pos, nl_.image, nl_.block_center, qscaled_,
+                       half_sigma_, sqrt_eps_, posq_, ljp_, nl_.box, s, only_after_rebuild);
 }
 
 void Engine::run_graph_steps(int launches) {
@@ -2231,6 +2270,7 @@ void Engine::autotune(int trial_steps, double* skin_out, int* ctas_out, double* 
   auto tune_margin = [&]() {
     if (!(nb_ && nb_periodic_ && nl_.block_tiles && nl_.max_cand > 0 && nl_.halves)) return;
     for (double m : kTunedPruneMargins) {
+      if (m > 0.0) ensure_pruned_list();
       prune_margin_ = m;
       const double ms = trial(best_skin, best_ctas);
       if (ms < best_ms) {
@@ -2522,6 +2562,7 @@ void Engine::load_checkpoint(const uint8_t* in, size_t bytes) {
     skin_ = h.skin;
     nl_.skin = h.skin;
     prune_margin_ = h.prune_margin;
+    if (prune_margin_ > 0.0) ensure_pruned_list();
     update_bricks();
     pair_grid_ = h.pair_grid;
     nl_.halves = h.halves;
@@ -2532,7 +2573,7 @@ void Engine::load_checkpoint(const uint8_t* in, size_t bytes) {
     from_ref.pos = nl_.pos_ref;
     const int one = 1;
     OMMB200_CK(cudaMemcpy(rebuild_, &one, 4, cudaMemcpyHostToDevice));
-    launch_nlist_rebuild(from_ref, dp_, stream_, use_bricks_ ? &bricks_ : nullptr);
+    launch_nlist_rebuild(from_ref, dp_, stream_, with_new_list(from_ref));
     // and the pruned list from the positions of the original run's last prune (its tiles hold
     // the same entries, so every per-tile sum rounds the same)
     put(pos_prune_, 24 * (size_t)n_);
@@ -2548,6 +2589,7 @@ void Engine::load_checkpoint(const uint8_t* in, size_t bytes) {
                            qscaled_, half_sigma_, sqrt_eps_, posq_, ljp_, nl_.box, stream_);
       launch_nlist_prune(from_prune, prune_args(), dp_, stream_);
     }
+    if (packed_by_integrator() && nb_) pack_slots(pos_, stream_);  // the saved run's last step wrote these
     sync();
     OMMB200_CK(cudaMemcpy(rebuild_, &h.rebuild_flag, 4, cudaMemcpyHostToDevice));
     OMMB200_CK(cudaMemcpy(prune_flag_, &h.prune_flag, 4, cudaMemcpyHostToDevice));

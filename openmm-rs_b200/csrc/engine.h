@@ -32,7 +32,7 @@ constexpr int kTunedPairCtasPerSm[] = {4, 6, 7, 8, 9, 10, 11, 12};
 // off (the pair kernel reads the rebuild's list).  The allowance absorbs the FP32 rounding of
 // the prune's distances.
 constexpr double kTunedPruneMargins[] = {0.0, 0.05, 0.08, 0.12};
-constexpr double kDefaultPruneMargin = 0.08;
+constexpr double kDefaultPruneMargin = 0.0;
 constexpr double kPruneAllowance = 1e-4;
 
 class DeviceArena {
@@ -54,7 +54,8 @@ struct EngineOptions {
   bool use_graph = true;
   double skin = 0.0;
   int steps_per_graph = 0;
-  int pme_bricks = -1;  // brick-owned PME spread and gather: -1 by grid size, 0 off, 1 on
+  int pme_bricks = -1;  // brick-owned PME gather: -1 by grid size, 0 off, 1 on
+  double prune_margin = -1.0;  // nm; 0 off, < 0 the default
 };
 
 // Device state that a re-run of MD steps starts from (Engine::save_dynamic_state).
@@ -140,6 +141,10 @@ class Engine {
   void setup_integrator();
   void update_box_dependents();
   void update_bricks();
+  bool packed_by_integrator() const;
+  // the launches that follow a neighbour-list build of `list` (brick ranges, gated pack)
+  std::function<void(cudaStream_t)> with_new_list(const NlistArgs& list);
+  void pack_slots(const double* pos, cudaStream_t s, const int* only_after_rebuild = nullptr);
   void build_static_tiles();
   void enqueue_conditional_rebuild();
   void enqueue_conditional_body(cudaGraphConditionalHandle handle,
@@ -148,6 +153,7 @@ class Engine {
   // entries per half block (the builder that records each block's tiles).
   bool pruning() const;
   void alloc_pruned_list();
+  void ensure_pruned_list();  // the pruned list's arrays, allocated on first use
   PruneArgs prune_args() const;
   // `in_step`: an MD step's evaluation (the learned radii may judge and train there);
   // `step_offset`: its position inside the captured group of steps.
@@ -276,9 +282,8 @@ class Engine {
   uint32_t* prune_cols_ = nullptr;
   uint32_t* prune_keep_ = nullptr;
   double prune_margin_ = kDefaultPruneMargin;  // 0: no pruning
-  PmeBricks bricks_{};      // brick-owned PME geometry and slot ranges
+  PmeBricks bricks_{};      // brick-owned PME gather: geometry, slot ranges, stencils
   bool use_bricks_ = false;
-  double max_abs_charge_ = 0.0;
   unsigned* prune_done_ = nullptr;
   int* prune_n_tiles_ = nullptr;
   int prune_capacity_ = 0;

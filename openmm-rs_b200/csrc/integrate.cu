@@ -32,6 +32,32 @@ __device__ __forceinline__ void force3(const long long* f, int n, int i, double 
   o[1] = (double)f[n + i] * kForceScaleInv;
   o[2] = (double)f[2 * n + i] * kForceScaleInv;
 }
+// The force of `atom` for this step's kick; zeroed behind the read when the step owns the
+// clearing for the next evaluation.
+__device__ __forceinline__ void consume_force(const IntegrateArgs& a, int n, int atom, double o[3]) {
+  force3(a.force, n, atom, o);
+  if (a.zero_force) {
+    a.force[atom] = 0;
+    a.force[n + atom] = 0;
+    a.force[2 * n + atom] = 0;
+  }
+}
+
+// The pair kernel's packed coordinates of `atom` at its new position x (periodic lists; the
+// same block-local arithmetic as the pack kernel).
+__device__ __forceinline__ void write_packed(const IntegrateArgs& a, int atom, const double x[3]) {
+  if (!a.posq) return;
+  const int s = a.atom_slot[atom];
+  double r[3];
+  block_local(x, a.image[3 * atom], a.image[3 * atom + 1], a.image[3 * atom + 2],
+              a.block_center + 3 * (s >> 5), a.pbox, r);
+  if (a.posq_double)
+    reinterpret_cast<double4*>(a.posq)[s] = make_double4(r[0], r[1], r[2], a.qscaled[atom]);
+  else
+    reinterpret_cast<float4*>(a.posq)[s] =
+        make_float4((float)r[0], (float)r[1], (float)r[2], (float)a.qscaled[atom]);
+}
+
 __device__ __forceinline__ double dot(const double* a, const double* b) {
   return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
 }
@@ -202,7 +228,7 @@ __device__ void water_step_lanes(const IntegrateArgs& a, int w, int k, uint64_t 
     ld3(a.pos, atom, rk);
     ld3(a.vel, atom, vk);
     double f[3];
-    force3(a.force, n, atom, f);
+    consume_force(a, n, atom, f);
     for (int c = 0; c < 3; ++c) vk[c] += f[c] * imk * a.dt;
   }
   double r[3][3], v[3][3], x[3][3];
@@ -226,6 +252,7 @@ __device__ void water_step_lanes(const IntegrateArgs& a, int w, int k, uint64_t 
   if (!(finite3(xo) && finite3(wk))) report_status(a.status, kStatusNonfinite);
   st3(a.pos, atom, xo);
   st3(a.vel, atom, wk);
+  write_packed(a, atom, xo);
   check_rebuild(a, atom, xo);
 }
 
@@ -234,12 +261,13 @@ __device__ void free_step(const IntegrateArgs& a, int atom, uint64_t step, int n
   double x[3], v[3], f[3];
   ld3(a.pos, atom, x);
   ld3(a.vel, atom, v);
-  force3(a.force, n, atom, f);
+  consume_force(a, n, atom, f);
   for (int c = 0; c < 3; ++c) v[c] += f[c] * im * a.dt;
   ou_update(a, atom, im, step, x, v);
   if (!(finite3(x) && finite3(v))) report_status(a.status, kStatusNonfinite);
   st3(a.pos, atom, x);
   st3(a.vel, atom, v);
+  write_packed(a, atom, x);
   check_rebuild(a, atom, x);
 }
 
@@ -297,9 +325,9 @@ __device__ void cluster_step(const IntegrateArgs& a, int c, uint64_t step, int n
   for (int s = s0; s < s1; ++s) {
     const int atom = a.cluster_atoms[s];
     const double im = a.inv_mass[atom];
-    if (im == 0.0) continue;
     double f[3];
-    force3(a.force, n, atom, f);
+    consume_force(a, n, atom, f);
+    if (im == 0.0) continue;
     for (int q = 0; q < 3; ++q) a.vel[3 * atom + q] += f[q] * im * a.dt;
   }
   bool ok = cluster_solve(a, c, a.pos, a.vel, true, nullptr);
@@ -323,6 +351,7 @@ __device__ void cluster_step(const IntegrateArgs& a, int c, uint64_t step, int n
     ld3(a.pos, atom, x);
     ld3(a.vel, atom, v);
     if (!(finite3(x) && finite3(v))) report_status(a.status, kStatusNonfinite);
+    write_packed(a, atom, x);
     check_rebuild(a, atom, x);
   }
 }

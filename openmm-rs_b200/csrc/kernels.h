@@ -3,6 +3,7 @@
 #pragma once
 
 #include <algorithm>
+#include <functional>
 #include <cuda_runtime.h>
 #include <cufft.h>
 #include <stdint.h>
@@ -86,10 +87,11 @@ struct PruneArgs {
   unsigned long long* prune_count;
 };
 
-struct PmeBricks;
-// `bricks` (may be null): the brick-owned PME's slot ranges are remade with the list.
+// `with_list` (may be empty) enqueues launches that need the new list and must run only on a
+// rebuild: it is called after the list is built and before the rebuild flag clears, so its
+// kernels can gate on the flag (the brick gather's slot ranges, the pack of the new slots).
 void launch_nlist_rebuild(const NlistArgs& a, bool double_entries, cudaStream_t s,
-                          const PmeBricks* bricks = nullptr);
+                          const std::function<void(cudaStream_t)>& with_list = {});
 void launch_nlist_prune(const NlistArgs& a, const PruneArgs& p, bool double_entries,
                         cudaStream_t s);
 // Sets `handle` to whether a prune is pending (the graph form of the early-exit prune kernels).
@@ -137,12 +139,14 @@ template <class Real>
 void launch_pair(const PairArgs<Real>& a, int elec, bool energy, bool dump, int grid,
                  cudaStream_t s);
 
-// Per-step packing of block-local coordinates and LJ parameters into the sorted slots.
+// Packing of block-local coordinates and LJ parameters into the sorted slots; with
+// `only_after_rebuild` set, only when that rebuild flag is set (between rebuilds of a periodic
+// list the integrator writes the packed coordinates).
 template <class Real>
 void launch_pack(int n_slots, const int* sorted_atom, const double* pos, const int* image,
                  const double* block_center, const double* qscaled, const double* half_sigma,
                  const double* two_sqrt_eps, void* posq, void* ljp, const Box<double>& box,
-                 cudaStream_t s);
+                 cudaStream_t s, const int* only_after_rebuild = nullptr);
 
 // ---- PME -------------------------------------------------------------------------------
 template <class Real>
@@ -162,34 +166,37 @@ struct PmeArgs {
   long long* force;
   long long* energy;
   double alpha, volume;
-  int grid_stored;        // the spread stores every grid point: the transform leaves it as is
 };
 
 template <class Real>
 void launch_pme_spread(const PmeArgs<Real>& a, cudaStream_t s);
 
-// Brick-owned PME for rectangular boxes: the charge grid is cut into bricks of kBrickEdge^3
-// points (the last brick of an axis may be shorter) and one CTA owns each brick.  The atoms
-// that can touch a brick until the next neighbour-list rebuild are found through the rebuild's
-// x-y columns (z-sorted): for each column and z layer of bricks, the slot ranges (two where
-// the layer's reach wraps the box) of the atoms whose rebuild position lies within the
-// layer's reach, made at every rebuild.
+// Brick-owned PME gather for rectangular boxes: the grid is cut into bricks of kBrickEdge^3
+// points (the last brick of an axis may be shorter) and one CTA gathers the particles whose
+// stencil starts in its brick.  The particles that can reach a brick until the next
+// neighbour-list rebuild are found through the rebuild's x-y columns (z-sorted): for each
+// column and z layer of bricks, the slot ranges (two where the layer's reach wraps the box) of
+// the particles whose rebuild position lies within the layer's reach, made at every rebuild.
 constexpr int kBrickEdge = 14;
 constexpr int kBrickMaxRanges = 256;  // slot ranges one brick gathers (columns x 2)
 struct PmeBricks {
   int2* ranges;        // [n_cols * nb[2] * 2] (first slot, end slot)
+  int4* base;          // [slots] this step's stencil base point per axis, w = 1 for a charged
+                       //   particle with a finite position (0: it touches no grid point)
+  void* frac;          // [slots] Real4: stencil fractions per axis, w = the charge as Real
+  int n_slots;
   int nb[3];           // bricks per axis
   int grid[3];         // grid points per axis
   int n_col[2];        // x-y columns of the neighbour-list sort
   double len[3];       // box edge lengths (nm)
   double cell[3];      // grid spacing (nm)
-  double below[3];     // reach of a brick below its lower faces: 4 cells + drift (plus slack)
+  double below[3];     // reach of a brick below its lower faces: drift (plus slack)
   double above;        // reach above its upper faces: drift (plus slack)
 };
 void launch_pme_brick_ranges(const NlistArgs& a, const PmeBricks& b, cudaStream_t s);
 template <class Real>
-void launch_pme_spread_bricks(const PmeArgs<Real>& a, const PmeBricks& b, const NlistArgs& nl,
-                              cudaStream_t s);
+void launch_pme_brick_stencils(const PmeArgs<Real>& a, const PmeBricks& b, const NlistArgs& nl,
+                               cudaStream_t s);
 template <class Real>
 void launch_pme_gather_bricks(const PmeArgs<Real>& a, const PmeBricks& b, const NlistArgs& nl,
                               cudaStream_t s);
@@ -391,7 +398,7 @@ struct IntegrateArgs {
   double* pos;
   double* vel;
   double* scratch;                // [3N] SHAKE reference / proposal buffer
-  const long long* force;
+  long long* force;
   const double* inv_mass;
   double dt, decay, noise_var;    // noise_var = kT (1 - decay^2)
   double tolerance;
@@ -405,6 +412,17 @@ struct IntegrateArgs {
   const double* pos_prune;        // positions at the last prune of the pair list (may be null)
   double half_margin2;            // (margin / 2)^2: a particle moved farther requests a prune
   int* prune;
+  // MD steps only: the step zeroes every force it consumed (the next step's evaluation needs
+  // no clearing), and, where `posq` is set (periodic lists), writes each moved particle's new
+  // block-local position and charge into its slot of the pair kernel's packed coordinates
+  int zero_force;
+  void* posq;                     // float4 or double4 per slot
+  int posq_double;
+  const int* atom_slot;
+  const int* image;               // lattice image of each particle at the last rebuild
+  const double* block_center;
+  const double* qscaled;
+  Box<double> pbox;
 };
 void launch_integrate(const IntegrateArgs& a, cudaStream_t s);
 // Barostat volume move: positions scaled, per particle or per molecule (CSR lists of atoms)

@@ -1120,7 +1120,7 @@ void launch_nlist_prune(const NlistArgs& a, const PruneArgs& p, bool double_entr
 }
 
 void launch_nlist_rebuild(const NlistArgs& a, bool double_entries, cudaStream_t s,
-                          const PmeBricks* bricks) {
+                          const std::function<void(cudaStream_t)>& with_list) {
   const int tb = 256;
   const int ga = ceil_div(a.n_atoms, tb);
   const int block_cap = a.slot_capacity / 32;
@@ -1148,7 +1148,7 @@ void launch_nlist_rebuild(const NlistArgs& a, bool double_entries, cudaStream_t 
     else
       nl_lists<false><<<gl, 32 * kListWarps, 0, s>>>(a);
   }
-  if (bricks) launch_pme_brick_ranges(a, *bricks, s);
+  if (with_list) with_list(s);
   nl_finish<<<std::max(1, std::min(ceil_div(a.n_cols, tb), 148 * 4)), tb, 0, s>>>(a);
   nl_clear_flag<<<1, 1, 0, s>>>(a);
 }

@@ -422,12 +422,15 @@ __global__ void __launch_bounds__(32 * kPairWarps, 6) pair_kernel_x2(const PairA
   }
 }
 
+// `only_after_rebuild` (may be null): pack only when that rebuild flag is set (the integrator
+// writes the packed coordinates of the other steps).
 template <class Real>
 __global__ void pack_kernel(int n_slots, const int* sorted_atom, const double* pos,
                             const int* image, const double* block_center, const double* qscaled,
                             const double* half_sigma, const double* two_sqrt_eps,
                             typename V4<Real>::T4* posq, typename V4<Real>::T2* ljp,
-                            Box<double> b) {
+                            Box<double> b, const int* only_after_rebuild) {
+  if (only_after_rebuild && *only_after_rebuild == 0) return;
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n_slots) return;
   const int a = sorted_atom[s];
@@ -437,11 +440,13 @@ __global__ void pack_kernel(int n_slots, const int* sorted_atom, const double* p
     out.x = out.y = out.z = out.w = Real(0);
     lj.x = lj.y = Real(0);
   } else {
-    const double n0 = image[3 * a], n1 = image[3 * a + 1], n2 = image[3 * a + 2];
-    const double* c = block_center + 3 * (s >> 5);
-    out.x = (Real)(pos[3 * a] - (n0 * b.ax + n1 * b.bx + n2 * b.cx) - c[0]);
-    out.y = (Real)(pos[3 * a + 1] - (n1 * b.by + n2 * b.cy) - c[1]);
-    out.z = (Real)(pos[3 * a + 2] - n2 * b.cz - c[2]);
+    const double x[3] = {pos[3 * a], pos[3 * a + 1], pos[3 * a + 2]};
+    double r[3];
+    block_local(x, image[3 * a], image[3 * a + 1], image[3 * a + 2], block_center + 3 * (s >> 5),
+                b, r);
+    out.x = (Real)r[0];
+    out.y = (Real)r[1];
+    out.z = (Real)r[2];
     out.w = (Real)qscaled[a];
     lj.x = (Real)half_sigma[a];
     lj.y = (Real)two_sqrt_eps[a];
@@ -489,20 +494,20 @@ template <class Real>
 void launch_pack(int n_slots, const int* sorted_atom, const double* pos, const int* image,
                  const double* block_center, const double* qscaled, const double* half_sigma,
                  const double* two_sqrt_eps, void* posq, void* ljp, const Box<double>& box,
-                 cudaStream_t s) {
+                 cudaStream_t s, const int* only_after_rebuild) {
   pack_kernel<Real><<<ceil_div(n_slots, 256), 256, 0, s>>>(
       n_slots, sorted_atom, pos, image, block_center, qscaled, half_sigma, two_sqrt_eps,
       reinterpret_cast<typename V4<Real>::T4*>(posq), reinterpret_cast<typename V4<Real>::T2*>(ljp),
-      box);
+      box, only_after_rebuild);
 }
 
 template void launch_pair<float>(const PairArgs<float>&, int, bool, bool, int, cudaStream_t);
 template void launch_pair<double>(const PairArgs<double>&, int, bool, bool, int, cudaStream_t);
 template void launch_pack<float>(int, const int*, const double*, const int*, const double*,
                                  const double*, const double*, const double*, void*, void*,
-                                 const Box<double>&, cudaStream_t);
+                                 const Box<double>&, cudaStream_t, const int*);
 template void launch_pack<double>(int, const int*, const double*, const int*, const double*,
                                   const double*, const double*, const double*, void*, void*,
-                                  const Box<double>&, cudaStream_t);
+                                  const Box<double>&, cudaStream_t, const int*);
 
 }  // namespace ommb200

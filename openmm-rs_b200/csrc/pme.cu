@@ -208,7 +208,7 @@ __global__ void convert_kernel(const PmeArgs<Real> a) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
        i += (long long)gridDim.x * blockDim.x) {
     a.grid_real[i] = (Real)((double)a.grid_fixed[i] * kGridScaleInv);
-    if (!a.grid_stored) a.grid_fixed[i] = 0;
+    a.grid_fixed[i] = 0;
   }
 }
 
@@ -600,8 +600,7 @@ __global__ void __launch_bounds__(kPlaneThreads) planes_forward(const PmeArgs<Re
         A[i] = v;
       });
   __syncthreads();
-  if (!a.grid_stored)  // ready for the next atomic spread
-    for (int i = threadIdx.x; i < ny * nz; i += blockDim.x) plane[i] = 0;
+  for (int i = threadIdx.x; i < ny * nz; i += blockDim.x) plane[i] = 0;  // ready for the next spread
   C2* r = stockham(A, B, twz, f, 2, nz, nyp);
   C2* o = r == A ? B : A;
   // split the two real rows' spectra: X_even = (Z_k + conj Z_-k)/2, X_odd = -i (Z_k - conj Z_-k)/2,
@@ -832,21 +831,19 @@ template void launch_pme_convolve<double>(const PmeArgs<double>&, bool, cudaStre
 template void launch_pme_gather<float>(const PmeArgs<float>&, cudaStream_t);
 template void launch_pme_gather<double>(const PmeArgs<double>&, cudaStream_t);
 
-// ---- brick-owned spreading and gathering -------------------------------------------------
-// For large grids in rectangular boxes.  One CTA per brick of kBrickEdge^3 grid points: it
-// collects the brick's candidate atoms from the per-rebuild slot ranges of the x-y columns in
-// reach, adds each candidate's stencil points that fall inside the brick (spread) or takes the
-// candidates whose stencil starts inside the brick (gather), and touches the global grid once
-// per point: the spread stores the brick's fixed-point sums, so the grid needs no zeroing and
-// no global atomics; the gather reads the brick and its 4-point halo into shared memory.  The
-// integer grid is the atomic spread's exactly (the same fixed-point contributions), and the
-// gather sums each atom's stencil planes in the order of the eight-lane kernel, so both paths
-// give the same forces.
+// ---- brick-owned gathering --------------------------------------------------------------
+// For large grids in rectangular boxes.  A first kernel stores every slot's stencil (base point,
+// fractions, charge).  Then one CTA per brick of kBrickEdge^3 grid points reads the brick and
+// its 4-point halo of the potential grid into shared memory once, collects its candidates from
+// the per-rebuild slot ranges of the x-y columns in reach (one 16-byte stencil load each), and
+// takes those whose stencil starts inside the brick, so every particle is gathered by one CTA
+// from shared memory instead of by eight lanes from L2.  Each atom's stencil planes are summed
+// in the order of the eight-lane kernel, so both forms give the same forces.  (A brick-owned
+// spread, storing each brick's sums once, measured slower than the atomic spread on the 196^3
+// grid: its shared-memory sums cost more than the global atomics they replace.)
 namespace {
 
 constexpr int kBrickThreads = 256;
-constexpr int kBrickCells = kBrickEdge * kBrickEdge * kBrickEdge;
-constexpr int kBrickCellsPerThread = (kBrickCells + kBrickThreads - 1) / kBrickThreads;
 constexpr int kBrickHalo = (kBrickEdge + 4) * (kBrickEdge + 4) * (kBrickEdge + 4);
 static_assert(kBrickMaxRanges <= kBrickThreads, "one range per thread when collecting");
 
@@ -977,114 +974,44 @@ __device__ __forceinline__ int candidate_slot(const int2* s_rng, const int* s_pr
   return s_rng[lo].x + (i - s_pre[lo]);
 }
 
-// in-brick points of a stencil along one axis: bit i for point base + i (periodic)
-__device__ __forceinline__ unsigned brick_points(int base, int n, int b0, int e) {
-  unsigned m = 0u;
-#pragma unroll
-  for (int i = 0; i < 5; ++i) {
-    int g = base + i;
-    g -= g >= n ? n : 0;
-    m |= ((unsigned)(g - b0) < (unsigned)e ? 1u : 0u) << i;
-  }
-  return m;
-}
-
-// Shared sums use 32-bit atomics on a split of each fixed-point contribution,
-// v = hi 2^22 + lo with 0 <= lo < 2^22 (|v| < 2^44 for |q| < 16 e).  Each round of the
-// candidate loop gives a point at most one contribution per thread (256), so both partial sums
-// stay inside 32 bits; after every round each thread folds its points into 64-bit registers.
 template <class Real>
-__global__ void __launch_bounds__(kBrickThreads) spread_bricks_kernel(const PmeArgs<Real> a,
-                                                                      const PmeBricks b,
-                                                                      const NlistArgs nl) {
-  __shared__ int c_hi[kBrickCells];
-  __shared__ unsigned int c_lo[kBrickCells];
-  __shared__ int2 s_rng[kBrickMaxRanges];
-  __shared__ int s_pre[kBrickMaxRanges + 1];
-  __shared__ int s_warp[kBrickThreads / 32];
-  int b0[3], e[3], bi[3];
-  brick_box(b, blockIdx.x, b0, e, bi);
-  for (int c = threadIdx.x; c < kBrickCells; c += kBrickThreads) {
-    c_hi[c] = 0;
-    c_lo[c] = 0u;
-  }
-  const int nr = brick_candidates(b, nl, bi, s_rng, s_pre, s_warp);
-  const int n_cand = s_pre[nr];
-  const int nc = e[0] * e[1] * e[2];
-  long long acc[kBrickCellsPerThread];
-#pragma unroll
-  for (int k = 0; k < kBrickCellsPerThread; ++k) acc[k] = 0;
-  const Real gscale = Real(kGridScale);
-  for (int i0 = 0; i0 < n_cand; i0 += kBrickThreads) {
-    const int i = i0 + threadIdx.x;
-    if (i < n_cand) {
-      const int atom = nl.sorted_atom[candidate_slot(s_rng, s_pre, nr, i)];
-      const double qd = atom >= 0 ? a.charge[atom] : 0.0;
-      int base[3];
-      Real frac[3];
-      if (qd != 0.0 && stencil(a, atom, base, frac)) {
-        const unsigned mx = brick_points(base[0], a.nx, b0[0], e[0]);
-        const unsigned my = brick_points(base[1], a.ny, b0[1], e[1]);
-        const unsigned mz = brick_points(base[2], a.nz, b0[2], e[2]);
-        if (mx && my && mz) {
-          Real w[3][5], dw[3][5];
-#pragma unroll
-          for (int d = 0; d < 3; ++d) spline5(frac[d], w[d], dw[d]);
-          const Real q = (Real)qd;
-#pragma unroll
-          for (int ix = 0; ix < 5; ++ix) {
-            if (!((mx >> ix) & 1u)) continue;
-            int gx = base[0] + ix;
-            gx -= gx >= a.nx ? a.nx : 0;
-            const Real qx = q * w[0][ix];
-#pragma unroll
-            for (int iy = 0; iy < 5; ++iy) {
-              if (!((my >> iy) & 1u)) continue;
-              int gy = base[1] + iy;
-              gy -= gy >= a.ny ? a.ny : 0;
-              const Real qxy = qx * w[1][iy];
-              const int row = ((gx - b0[0]) * e[1] + (gy - b0[1])) * e[2];
-#pragma unroll
-              for (int iz = 0; iz < 5; ++iz) {
-                if (!((mz >> iz) & 1u)) continue;
-                int gz = base[2] + iz;
-                gz -= gz >= a.nz ? a.nz : 0;
-                const long long v = to_fixed(qxy * w[2][iz], gscale);
-                const int cell = row + gz - b0[2];
-                atomicAdd(&c_hi[cell], (int)(v >> 22));
-                atomicAdd(&c_lo[cell], (unsigned int)(v & 0x3FFFFF));
-              }
-            }
-          }
-        }
-      }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < kBrickCellsPerThread; ++k) {
-      const int c = threadIdx.x + k * kBrickThreads;
-      if (c < nc) {
-        acc[k] += (long long)c_hi[c] * (1ll << 22) + (long long)c_lo[c];
-        c_hi[c] = 0;
-        c_lo[c] = 0u;
-      }
-    }
-    __syncthreads();
-  }
-#pragma unroll
-  for (int k = 0; k < kBrickCellsPerThread; ++k) {
-    const int c = threadIdx.x + k * kBrickThreads;
-    if (c < nc) {
-      const int cz = c % e[2], cy = (c / e[2]) % e[1], cx = c / (e[1] * e[2]);
-      a.grid_fixed[((long long)(b0[0] + cx) * a.ny + (b0[1] + cy)) * a.nz + b0[2] + cz] = acc[k];
-    }
-  }
+struct Real4Of;
+template <>
+struct Real4Of<float> {
+  using T = float4;
+};
+template <>
+struct Real4Of<double> {
+  using T = double4;
+};
+
+// This step's stencil of every sorted slot (the spread and the gather of the brick form read it
+// once per candidate instead of recomputing it from the position): base point per axis and the
+// fractions, as `stencil` gives them, and the charge as Real.
+template <class Real>
+__global__ void brick_stencils_kernel(const PmeArgs<Real> a, const PmeBricks b, const NlistArgs nl) {
+  using R4 = typename Real4Of<Real>::T;
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= b.n_slots) return;
+  const int atom = nl.sorted_atom[s];
+  const double qd = atom >= 0 ? a.charge[atom] : 0.0;
+  int base[3] = {0, 0, 0};
+  Real frac[3] = {Real(0), Real(0), Real(0)};
+  const bool ok = qd != 0.0 && stencil(a, atom, base, frac);
+  b.base[s] = make_int4(base[0], base[1], base[2], ok ? 1 : 0);
+  R4 f;
+  f.x = frac[0];
+  f.y = frac[1];
+  f.z = frac[2];
+  f.w = (Real)qd;
+  reinterpret_cast<R4*>(b.frac)[s] = f;
 }
 
 template <class Real>
 __global__ void __launch_bounds__(kBrickThreads) gather_bricks_kernel(const PmeArgs<Real> a,
                                                                       const PmeBricks b,
                                                                       const NlistArgs nl) {
+  using R4 = typename Real4Of<Real>::T;
   extern __shared__ __align__(16) unsigned char brick_smem[];
   Real* phi = reinterpret_cast<Real*>(brick_smem);  // [(e0 + 4)(e1 + 4)(e2 + 4)]
   __shared__ int2 s_rng[kBrickMaxRanges];
@@ -1104,18 +1031,19 @@ __global__ void __launch_bounds__(kBrickThreads) gather_bricks_kernel(const PmeA
   const int nr = brick_candidates(b, nl, bi, s_rng, s_pre, s_warp);  // barriers cover phi
   const int n_cand = s_pre[nr];
   for (int i = threadIdx.x; i < n_cand; i += kBrickThreads) {
-    const int atom = nl.sorted_atom[candidate_slot(s_rng, s_pre, nr, i)];
-    const double qd = atom >= 0 ? a.charge[atom] : 0.0;
-    int base[3];
-    Real frac[3];
-    if (qd == 0.0 || !stencil(a, atom, base, frac)) continue;
-    const int lx = base[0] - b0[0], ly = base[1] - b0[1], lz = base[2] - b0[2];
-    if ((unsigned)lx >= (unsigned)e[0] || (unsigned)ly >= (unsigned)e[1] ||
+    const int slot = candidate_slot(s_rng, s_pre, nr, i);
+    const int4 sb = b.base[slot];
+    const int lx = sb.x - b0[0], ly = sb.y - b0[1], lz = sb.z - b0[2];
+    if (!sb.w || (unsigned)lx >= (unsigned)e[0] || (unsigned)ly >= (unsigned)e[1] ||
         (unsigned)lz >= (unsigned)e[2])
-      continue;  // another brick's atom
+      continue;  // uncharged, or another brick's particle
+    const R4 sf = reinterpret_cast<const R4*>(b.frac)[slot];
+    const int atom = nl.sorted_atom[slot];
+    const double qd = a.charge[atom];
     Real w[3][5], dw[3][5];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) spline5(frac[d], w[d], dw[d]);
+    spline5(sf.x, w[0], dw[0]);
+    spline5(sf.y, w[1], dw[1]);
+    spline5(sf.z, w[2], dw[2]);
     Real p0[5], p1[5], p2[5];  // stencil plane ix: the sums of lane ix of the eight-lane kernel
 #pragma unroll
     for (int ix = 0; ix < 5; ++ix) {
@@ -1158,10 +1086,14 @@ void launch_pme_brick_ranges(const NlistArgs& a, const PmeBricks& b, cudaStream_
 }
 
 template <class Real>
-void launch_pme_spread_bricks(const PmeArgs<Real>& a, const PmeBricks& b, const NlistArgs& nl,
-                              cudaStream_t s) {
-  spread_bricks_kernel<Real><<<b.nb[0] * b.nb[1] * b.nb[2], kBrickThreads, 0, s>>>(a, b, nl);
+void launch_pme_brick_stencils(const PmeArgs<Real>& a, const PmeBricks& b, const NlistArgs& nl,
+                               cudaStream_t s) {
+  brick_stencils_kernel<Real><<<ceil_div(b.n_slots, 256), 256, 0, s>>>(a, b, nl);
 }
+template void launch_pme_brick_stencils<float>(const PmeArgs<float>&, const PmeBricks&,
+                                               const NlistArgs&, cudaStream_t);
+template void launch_pme_brick_stencils<double>(const PmeArgs<double>&, const PmeBricks&,
+                                                const NlistArgs&, cudaStream_t);
 
 template <class Real>
 void launch_pme_gather_bricks(const PmeArgs<Real>& a, const PmeBricks& b, const NlistArgs& nl,
@@ -1172,10 +1104,6 @@ void launch_pme_gather_bricks(const PmeArgs<Real>& a, const PmeBricks& b, const 
   gather_bricks_kernel<Real><<<b.nb[0] * b.nb[1] * b.nb[2], kBrickThreads, bytes, s>>>(a, b, nl);
 }
 
-template void launch_pme_spread_bricks<float>(const PmeArgs<float>&, const PmeBricks&,
-                                              const NlistArgs&, cudaStream_t);
-template void launch_pme_spread_bricks<double>(const PmeArgs<double>&, const PmeBricks&,
-                                               const NlistArgs&, cudaStream_t);
 template void launch_pme_gather_bricks<float>(const PmeArgs<float>&, const PmeBricks&,
                                               const NlistArgs&, cudaStream_t);
 template void launch_pme_gather_bricks<double>(const PmeArgs<double>&, const PmeBricks&,

@@ -67,7 +67,7 @@ _ERRORS = {ERR_INVALID_ARG: InvalidArgument, ERR_CONSTRAINT: ConstraintError,
 class Options(C.Structure):
     _fields_ = [("precision", C.c_int), ("device", C.c_int), ("use_cuda_graph", C.c_int),
                 ("neighbor_skin", C.c_double), ("steps_per_graph", C.c_int),
-                ("pme_bricks", C.c_int)]
+                ("pme_bricks", C.c_int), ("prune_margin", C.c_double)]
 
 
 class LearnedRadiiStats(C.Structure):
@@ -560,7 +560,7 @@ class State:
 
 
 def _options(precision, device, use_cuda_graph, neighbor_skin, steps_per_graph,
-             pme_bricks=-1) -> "Options":
+             pme_bricks=-1, prune_margin=-1.0) -> "Options":
     opt = Options()
     opt.precision = {"mixed": PRECISION_MIXED, "double": PRECISION_DOUBLE}[precision]
     opt.device = device
@@ -568,6 +568,7 @@ def _options(precision, device, use_cuda_graph, neighbor_skin, steps_per_graph,
     opt.neighbor_skin = neighbor_skin
     opt.steps_per_graph = steps_per_graph
     opt.pme_bricks = pme_bricks
+    opt.prune_margin = prune_margin
     return opt
 
 
@@ -576,13 +577,14 @@ class Context:
 
     def __init__(self, system: System, integrator: LangevinMiddleIntegrator, precision="mixed",
                  device: int = 0, use_cuda_graph: bool = True, neighbor_skin: float = 0.0,
-                 steps_per_graph: int = 0, pme_bricks: int = -1):
-        """`pme_bricks`: brick-owned PME spread and gather in rectangular periodic boxes, -1 when
+                 steps_per_graph: int = 0, pme_bricks: int = -1, prune_margin: float = -1.0):
+        """`pme_bricks`: brick-owned PME gather in rectangular periodic boxes, -1 when
         the grid has at least two bricks per SM, 0 never, 1 whenever the box allows (the forces
-        are the same either way)."""
+        are the same either way).  `prune_margin` (nm): the pruned pair list between rebuilds
+        (0 off, < 0 the default: off until `autotune` picks a margin)."""
         n = system.num_particles()
         opt = _options(precision, device, use_cuda_graph, neighbor_skin, steps_per_graph,
-                       pme_bricks)
+                       pme_bricks, prune_margin)
         h = C.c_void_p()
         sys_h, int_h = system._take(), integrator._take()
         _check(library().ommb200_context_create(sys_h, int_h, C.byref(opt), C.byref(h)))
@@ -675,7 +677,8 @@ class Context:
         return a.value, (nx.value, ny.value, nz.value)
 
     def pme_layout(self) -> dict:
-        """PME spread/gather form: brick-owned (`bricks_in_use`) or atomic; grid bricks."""
+        """PME gather form: brick-owned (`bricks_in_use`) or eight lanes per particle; grid
+        bricks."""
         u, n = C.c_int(), C.c_int()
         _check(library().ommb200_context_get_pme_layout(self._h, C.byref(u), C.byref(n)))
         return {"bricks_in_use": bool(u.value), "bricks": n.value}

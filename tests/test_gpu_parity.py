@@ -397,18 +397,28 @@ def test_pme_grid_shapes_match_oracle(grid, precision, bound):
 
 
 def test_nve_energy_is_conserved():
-    # friction 0, temperature 0: LangevinMiddle reduces to velocity Verlet with SETTLE
+    """friction 0, temperature 0: LangevinMiddle reduces to velocity Verlet with SETTLE.  At the
+    production 2 fs step over 40 ps (after 10 ps without the thermostat): the total energy
+    fluctuates by well under 1 % of the kinetic energy, and its drift is below 0.1 kJ/mol/ns
+    per degree of freedom (6 per rigid
+    water; a thermostat-free run that heats or cools at that rate changes its temperature by
+    about 12 K per ns; the 100 ps drift of the 23,958-atom box measured by bench.py is
+    0.0002 +- 0.002)."""
     w, x, v = equilibrated_water()
-    integ = ommb200.LangevinMiddleIntegrator(0.0, 0.0, 0.001)
+    integ = ommb200.LangevinMiddleIntegrator(0.0, 0.0, 0.002)
     ctx = ommb200.Context(systems.water_system(w), integ, precision="mixed")
     ctx.set_positions(x)
     ctx.set_velocities(v)
-    e = []
-    for _ in range(20):
-        ctx.step(100)
+    ctx.step(5000)  # let the thermostat-free state settle
+    t, e = [], []
+    for k in range(201):
         st = ctx.get_state(energy=True)
+        t.append(0.2 * k)  # ps
         e.append(st.potential_energy + st.kinetic_energy)
-    e = np.array(e)
+        ctx.step(100)
+    t, e = np.array(t), np.array(e)
     ke = ctx.get_state(energy=True).kinetic_energy
-    # fluctuation well below 1% of the kinetic energy over 2 ps
     assert np.abs(e - e.mean()).max() < 0.01 * ke, (e.max() - e.min(), ke)
+    dof = 6 * w.n_waters
+    slope = np.polyfit(t, e, 1)[0] * 1000.0 / dof  # kJ/mol/ns per degree of freedom
+    assert abs(slope) < 0.1, slope

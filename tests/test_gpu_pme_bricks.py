@@ -1,10 +1,10 @@
-"""Brick-owned PME spread and gather against the atomic form.
+"""Brick-owned PME gather against the eight-lanes-per-particle gather.
 
-The brick form gives each CTA one brick of grid points and stores the brick's fixed-point sums
-once; the atomic form adds every stencil point into the global grid.  Both add the same
-fixed-point contributions (an integer sum, independent of order) and the gather sums each
-atom's stencil planes in the same order, so the forces, the energy and whole trajectories must
-be bit-identical between the two, and equal the oracle's (pme.rs:141-425) within the usual
+The brick form gives each CTA one brick of grid points, reads the brick and its halo of the
+potential grid into shared memory and gathers the particles whose stencil starts in it; the
+other form gathers each particle with eight lanes from L2.  Both sum each particle's stencil
+planes in the same order, so the forces, the energy and whole trajectories must be
+bit-identical between the two, and equal the oracle's (pme.rs:141-425) within the usual
 tolerance.  Cases: the 23,958-atom cube (56^3 grid: four bricks per axis) and a rectangular,
 non-cubic box whose grid leaves shorter bricks at the high end of every axis.
 """
@@ -88,21 +88,17 @@ def nonbonded_copy(w, charges):
     return nb
 
 
-def test_brick_form_leaves_and_returns_with_the_charge_bound():
-    """A charge of 16 e or more (the bound of the brick form's 32-bit shared sums) switches the
-    Context to the atomic form; charges back below it switch the brick form on again."""
+def test_parameter_updates_keep_the_forms_equal():
+    """A live parameter update (new charges, one of 20 e) reaches both gather forms alike."""
     w = synth.water_preset("water-1944")
-    ctx = context(w, "mixed", 1)
-    f0 = ctx.get_state(forces=True).forces
     big = w.charges().copy()
-    big[0] = 20.0
-    ctx.update_nonbonded_parameters(nonbonded_copy(w, big))
-    assert not ctx.pme_layout()["bricks_in_use"]
-    ref = context(w, "mixed", 0)
-    ref.update_nonbonded_parameters(nonbonded_copy(w, big))
-    assert np.array_equal(ctx.get_state(forces=True).forces, ref.get_state(forces=True).forces)
-    ctx.update_nonbonded_parameters(nonbonded_copy(w, w.charges()))
-    assert ctx.pme_layout()["bricks_in_use"]
-    assert np.array_equal(ctx.get_state(forces=True).forces, f0)
-    ctx.close()
-    ref.close()
+    big[0], big[1] = 20.0, -19.0
+    got = []
+    for bricks in (1, 0):
+        ctx = context(w, "mixed", bricks)
+        assert ctx.pme_layout()["bricks_in_use"] == bool(bricks)
+        ctx.update_nonbonded_parameters(nonbonded_copy(w, big))
+        got.append(ctx.get_state(forces=True, energy=True))
+        ctx.close()
+    assert np.array_equal(got[0].forces, got[1].forces)
+    assert got[0].potential_energy == got[1].potential_energy

@@ -24,7 +24,7 @@ def pair_keys(p):
 def test_pair_set_between_prunes_is_the_reference_pair_set(precision):
     w = synth.water_preset("water-1944")
     ctx = ommb200.Context(systems.water_system(w), systems.langevin(temperature=400.0, seed=13),
-                          precision=precision)
+                          precision=precision, prune_margin=0.05)
     ctx.set_positions(w.positions)
     ctx.set_velocities_to_temperature(400.0, seed=6)
     excl = [e[:2] for e in w.exceptions()]
@@ -47,7 +47,8 @@ def test_pair_set_between_prunes_is_the_reference_pair_set(precision):
 
 def test_pruned_list_is_smaller_and_forces_match_oracle():
     w = synth.water_preset("water-1944")
-    ctx = ommb200.Context(systems.water_system(w), systems.langevin(seed=17), precision="mixed")
+    ctx = ommb200.Context(systems.water_system(w), systems.langevin(seed=17), precision="mixed",
+                          prune_margin=0.08)
     ctx.set_positions(w.positions)
     ctx.set_velocities_to_temperature(300.0, seed=8)
     ctx.step(45)
@@ -62,3 +63,14 @@ def test_pruned_list_is_smaller_and_forces_match_oracle():
     assert err < 5e-6
     assert abs(st.potential_energy - e_ref) < 2e-6 * abs(e_ref) + 1e-6 * w.n_atoms
     ctx.close()
+
+
+def test_pruning_is_off_by_default_and_margin_zero():
+    w = synth.water_preset("water-1944")
+    for kw in ({}, {"prune_margin": 0.0}):
+        ctx = ommb200.Context(systems.water_system(w), systems.langevin(), **kw)
+        ctx.set_positions(w.positions)
+        ctx.step(5)
+        assert ctx.nlist_prune_stats()["margin_nm"] == 0.0
+        assert ctx.nlist_prune_stats()["prunes"] == 0
+        ctx.close()

@@ -11,15 +11,19 @@ from ommb200 import synth, systems
 pytestmark = pytest.mark.gpu
 
 
-def water_ctx(w, seed=3, **kw):
-    ctx = ommb200.Context(systems.water_system(w, **kw), systems.langevin(seed=seed))
+def water_ctx(w, seed=3, prune_margin=-1.0, **kw):
+    ctx = ommb200.Context(systems.water_system(w, **kw), systems.langevin(seed=seed),
+                          prune_margin=prune_margin)
     ctx.set_positions(w.positions)
     return ctx
 
 
-def test_checkpoint_continues_water_bit_for_bit():
+@pytest.mark.parametrize("margin", [0.0, 0.05])
+def test_checkpoint_continues_water_bit_for_bit(margin):
+    """With the pruned list (margin 0.05 nm) too: the loading Context starts without one and
+    takes the margin, the prune positions and the pending-prune flag from the checkpoint."""
     w = synth.water_preset("water-1944")
-    a = water_ctx(w)
+    a = water_ctx(w, prune_margin=margin)
     a.set_velocities_to_temperature(300.0, seed=5)
     a.step(150)
     ck = a.create_checkpoint()
@@ -37,6 +41,7 @@ def test_checkpoint_continues_water_bit_for_bit():
     assert sa.step_count == sb.step_count == 320
     assert abs(sa.time - sb.time) < 1e-12
     assert stats_a["tiles"] == b.nlist_stats()["tiles"]
+    assert a.nlist_prune_stats()["margin_nm"] == b.nlist_prune_stats()["margin_nm"] == margin
 
 
 def test_checkpoint_continues_learned_radii_batch_bit_for_bit():
