@@ -483,7 +483,8 @@ void Engine::setup_nonbonded(const NonbondedDef& nb) {
       };
       auto block = [](int want, int lo, int hi) { return std::min(hi, std::max(lo, (want + 31) / 32 * 32)); };
       // plane kernels: a third of a plane's elements per thread pass (copies), at least one
-      // butterfly per thread in every stage; x pass: at least the butterflies of a stage
+      // butterfly per thread in every stage (256-thread CTAs, which would fit beside the pair
+      // kernel's CTAs, measured slower); x pass: at least the butterflies of a stage
       fft_.threads[0] = fft_.threads[2] =
           block(std::max(std::max(items(2, nyp), items(1, nzh)), nzh * ny / 3), 128, 512);
       fft_.threads[1] = block(std::max(items(0, fft_.pencils_x), fft_.pencils_x * grid_[0] / 4), 64, 256);
@@ -1404,6 +1405,26 @@ void Engine::enqueue_nonbonded(bool energy, bool direct, bool reciprocal, bool d
     OMMB200_CK(cudaEventRecord(fork_ev_, stream_));
     OMMB200_CK(cudaStreamWaitEvent(ps, fork_ev_, 0));
   }
+  // the exclusion corrections first: a small kernel that leaves SMs free while the reciprocal
+  // chain starts beside it, before the pair kernel fills every SM
+  if (direct && n_exceptions_) {
+    ExceptionArgs e{};
+    e.n = n_exceptions_;
+    e.pairs = exc_pairs_;
+    e.params = exc_params_;
+    e.pos = pos_;
+    e.force = force_;
+    e.energy = energy_;
+    e.atom_segment = segments_.size() > 1 ? d_atom_segment_ : nullptr;
+    e.box = nl_.box;
+    e.use_pbc = nb_periodic_ && nb.exceptions_use_pbc;
+    e.ewald = nb_pme_;
+    e.alpha = alpha_;
+    e.n_atoms_for_force = n_;
+    prof_begin("exceptions");
+    launch_exceptions(e, energy, stream_);
+    prof_end();
+  }
   if (direct && pairs) {
     if (!packed_by_integrator()) {
       prof_begin("pack");
@@ -1535,24 +1556,6 @@ void Engine::enqueue_nonbonded(bool energy, bool direct, bool reciprocal, bool d
       launch_pme_gather_bricks<Real>(m, bricks_, nl_, ps);
     } else
       launch_pme_gather<Real>(m, ps);
-    prof_end();
-  }
-  if (direct && n_exceptions_) {
-    ExceptionArgs e{};
-    e.n = n_exceptions_;
-    e.pairs = exc_pairs_;
-    e.params = exc_params_;
-    e.pos = pos_;
-    e.force = force_;
-    e.energy = energy_;
-    e.atom_segment = segments_.size() > 1 ? d_atom_segment_ : nullptr;
-    e.box = nl_.box;
-    e.use_pbc = nb_periodic_ && nb.exceptions_use_pbc;
-    e.ewald = nb_pme_;
-    e.alpha = alpha_;
-    e.n_atoms_for_force = n_;
-    prof_begin("exceptions");
-    launch_exceptions(e, energy, stream_);
     prof_end();
   }
   if (ps != stream_) {  // join

@@ -43,20 +43,6 @@ __device__ __forceinline__ void consume_force(const IntegrateArgs& a, int n, int
   }
 }
 
-// The pair kernel's packed coordinates of `atom` at its new position x (periodic lists; the
-// same block-local arithmetic as the pack kernel).
-__device__ __forceinline__ void write_packed(const IntegrateArgs& a, int atom, const double x[3]) {
-  if (!a.posq) return;
-  const int s = a.atom_slot[atom];
-  double r[3];
-  block_local(x, a.image[3 * atom], a.image[3 * atom + 1], a.image[3 * atom + 2],
-              a.block_center + 3 * (s >> 5), a.pbox, r);
-  if (a.posq_double)
-    reinterpret_cast<double4*>(a.posq)[s] = make_double4(r[0], r[1], r[2], a.qscaled[atom]);
-  else
-    reinterpret_cast<float4*>(a.posq)[s] =
-        make_float4((float)r[0], (float)r[1], (float)r[2], (float)a.qscaled[atom]);
-}
 
 __device__ __forceinline__ double dot(const double* a, const double* b) {
   return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
@@ -175,15 +161,49 @@ __device__ __forceinline__ bool finite3(const double a[3]) {
   return isfinite(a[0]) && isfinite(a[1]) && isfinite(a[2]);
 }
 
-__device__ __forceinline__ void check_rebuild(const IntegrateArgs& a, int atom, const double x[3]) {
+// What a particle's end-of-step bookkeeping reads (neighbour-list and prune reference
+// positions, slot, lattice image, block centre), loaded at the start of the step so that the
+// loads overlap the arithmetic instead of following the stores of x and v.
+struct StepTail {
+  double ref[3], prune_ref[3], img[3];
+  const double* center;
+  int slot;
+};
+
+__device__ __forceinline__ void load_tail(const IntegrateArgs& a, int atom, StepTail& t) {
+  if (a.pos_ref) ld3(a.pos_ref, atom, t.ref);
+  if (a.pos_prune) ld3(a.pos_prune, atom, t.prune_ref);
+  if (a.posq) {
+    t.slot = a.atom_slot[atom];
+    t.img[0] = a.image[3 * atom];
+    t.img[1] = a.image[3 * atom + 1];
+    t.img[2] = a.image[3 * atom + 2];
+    t.center = a.block_center + 3 * (t.slot >> 5);
+  }
+}
+
+__device__ __forceinline__ void check_rebuild(const IntegrateArgs& a, const StepTail& t,
+                                              const double x[3]) {
   if (!a.pos_ref) return;
-  const double dx = x[0] - a.pos_ref[3 * atom], dy = x[1] - a.pos_ref[3 * atom + 1],
-               dz = x[2] - a.pos_ref[3 * atom + 2];
+  const double dx = x[0] - t.ref[0], dy = x[1] - t.ref[1], dz = x[2] - t.ref[2];
   if (dx * dx + dy * dy + dz * dz > a.half_skin2) *a.rebuild = 1;
   if (!a.pos_prune) return;
-  const double px = x[0] - a.pos_prune[3 * atom], py = x[1] - a.pos_prune[3 * atom + 1],
-               pz = x[2] - a.pos_prune[3 * atom + 2];
+  const double px = x[0] - t.prune_ref[0], py = x[1] - t.prune_ref[1], pz = x[2] - t.prune_ref[2];
   if (px * px + py * py + pz * pz > a.half_margin2) *a.prune = 1;
+}
+
+// The pair kernel's packed coordinates of `atom` at its new position x (periodic lists; the
+// same block-local arithmetic as the pack kernel); `q` = its scaled charge.
+__device__ __forceinline__ void write_packed(const IntegrateArgs& a, const StepTail& t, double q,
+                                             const double x[3]) {
+  if (!a.posq) return;
+  double r[3];
+  block_local(x, t.img[0], t.img[1], t.img[2], t.center, a.pbox, r);
+  if (a.posq_double)
+    reinterpret_cast<double4*>(a.posq)[t.slot] = make_double4(r[0], r[1], r[2], q);
+  else
+    reinterpret_cast<float4*>(a.posq)[t.slot] =
+        make_float4((float)r[0], (float)r[1], (float)r[2], (float)q);
 }
 
 // drift / thermostat / drift for one particle (langevin.rs:121-134 without the kick)
@@ -224,9 +244,13 @@ __device__ void water_step_lanes(const IntegrateArgs& a, int w, int k, uint64_t 
   const double im[3] = {1.0 / a.geom.m_o, 1.0 / a.geom.m_h, 1.0 / a.geom.m_h};
   const double imk = k == 0 ? im[0] : im[1];
   double rk[3] = {0, 0, 0}, vk[3] = {0, 0, 0};
+  StepTail tail{};
+  double qk = 0.0;
   if (k < 3) {
     ld3(a.pos, atom, rk);
     ld3(a.vel, atom, vk);
+    load_tail(a, atom, tail);
+    if (a.posq) qk = a.qscaled[atom];
     double f[3];
     consume_force(a, n, atom, f);
     for (int c = 0; c < 3; ++c) vk[c] += f[c] * imk * a.dt;
@@ -252,8 +276,8 @@ __device__ void water_step_lanes(const IntegrateArgs& a, int w, int k, uint64_t 
   if (!(finite3(xo) && finite3(wk))) report_status(a.status, kStatusNonfinite);
   st3(a.pos, atom, xo);
   st3(a.vel, atom, wk);
-  write_packed(a, atom, xo);
-  check_rebuild(a, atom, xo);
+  write_packed(a, tail, qk, xo);
+  check_rebuild(a, tail, xo);
 }
 
 __device__ void free_step(const IntegrateArgs& a, int atom, uint64_t step, int n) {
@@ -261,14 +285,17 @@ __device__ void free_step(const IntegrateArgs& a, int atom, uint64_t step, int n
   double x[3], v[3], f[3];
   ld3(a.pos, atom, x);
   ld3(a.vel, atom, v);
+  StepTail tail{};
+  load_tail(a, atom, tail);
+  const double q = a.posq ? a.qscaled[atom] : 0.0;
   consume_force(a, n, atom, f);
   for (int c = 0; c < 3; ++c) v[c] += f[c] * im * a.dt;
   ou_update(a, atom, im, step, x, v);
   if (!(finite3(x) && finite3(v))) report_status(a.status, kStatusNonfinite);
   st3(a.pos, atom, x);
   st3(a.vel, atom, v);
-  write_packed(a, atom, x);
-  check_rebuild(a, atom, x);
+  write_packed(a, tail, q, x);
+  check_rebuild(a, tail, x);
 }
 
 // constraints.rs:81-156 restricted to one cluster.  `values` are positions (velocities=false,
@@ -351,8 +378,10 @@ __device__ void cluster_step(const IntegrateArgs& a, int c, uint64_t step, int n
     ld3(a.pos, atom, x);
     ld3(a.vel, atom, v);
     if (!(finite3(x) && finite3(v))) report_status(a.status, kStatusNonfinite);
-    write_packed(a, atom, x);
-    check_rebuild(a, atom, x);
+    StepTail tail{};
+    load_tail(a, atom, tail);
+    write_packed(a, tail, a.posq ? a.qscaled[atom] : 0.0, x);
+    check_rebuild(a, tail, x);
   }
 }
 

@@ -845,6 +845,7 @@ namespace {
 
 constexpr int kBrickThreads = 256;
 constexpr int kBrickHalo = (kBrickEdge + 4) * (kBrickEdge + 4) * (kBrickEdge + 4);
+constexpr int kBrickOwnChunk = 2048;  // candidates tested before their owners are gathered
 static_assert(kBrickMaxRanges <= kBrickThreads, "one range per thread when collecting");
 
 // first slot k in [s0, s0 + n) of a z-sorted column with zkey >= z (s0 + n if none)
@@ -1017,6 +1018,8 @@ __global__ void __launch_bounds__(kBrickThreads) gather_bricks_kernel(const PmeA
   __shared__ int2 s_rng[kBrickMaxRanges];
   __shared__ int s_pre[kBrickMaxRanges + 1];
   __shared__ int s_warp[kBrickThreads / 32];
+  __shared__ int s_own[kBrickOwnChunk];
+  __shared__ int s_nown;
   int b0[3], e[3], bi[3];
   brick_box(b, blockIdx.x, b0, e, bi);
   const int h1 = e[1] + 4, h2 = e[2] + 4, nh = (e[0] + 4) * h1 * h2;
@@ -1030,13 +1033,35 @@ __global__ void __launch_bounds__(kBrickThreads) gather_bricks_kernel(const PmeA
   }
   const int nr = brick_candidates(b, nl, bi, s_rng, s_pre, s_warp);  // barriers cover phi
   const int n_cand = s_pre[nr];
-  for (int i = threadIdx.x; i < n_cand; i += kBrickThreads) {
-    const int slot = candidate_slot(s_rng, s_pre, nr, i);
+  // The candidates are tested in chunks; the owners (stencil starting in this brick, about a
+  // third) are listed in shared memory and then gathered one per thread, so that the 125-point
+  // sums run on full warps.  The order of the list does not matter: each particle's force is
+  // its own sum, added in fixed point.
+  for (int i0 = 0; i0 < n_cand; i0 += kBrickOwnChunk) {
+    if (threadIdx.x == 0) s_nown = 0;
+    __syncthreads();
+    const int i1 = min(i0 + kBrickOwnChunk, n_cand);
+    for (int i = i0 + threadIdx.x; i < i1; i += kBrickThreads) {
+      const int slot = candidate_slot(s_rng, s_pre, nr, i);
+      const int4 sb = b.base[slot];
+      const bool own = sb.w && (unsigned)(sb.x - b0[0]) < (unsigned)e[0] &&
+                       (unsigned)(sb.y - b0[1]) < (unsigned)e[1] &&
+                       (unsigned)(sb.z - b0[2]) < (unsigned)e[2];
+      const unsigned m = __ballot_sync(__activemask(), own);
+      if (own) {
+        const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+        int at = 0;
+        if (lane == leader) at = atomicAdd(&s_nown, __popc(m));
+        at = __shfl_sync(m, at, leader) + __popc(m & ((1u << lane) - 1u));
+        s_own[at] = slot;
+      }
+    }
+    __syncthreads();
+    const int n_own = s_nown;
+    for (int o = threadIdx.x; o < n_own; o += kBrickThreads) {
+    const int slot = s_own[o];
     const int4 sb = b.base[slot];
     const int lx = sb.x - b0[0], ly = sb.y - b0[1], lz = sb.z - b0[2];
-    if (!sb.w || (unsigned)lx >= (unsigned)e[0] || (unsigned)ly >= (unsigned)e[1] ||
-        (unsigned)lz >= (unsigned)e[2])
-      continue;  // uncharged, or another brick's particle
     const R4 sf = reinterpret_cast<const R4*>(b.frac)[slot];
     const int atom = nl.sorted_atom[slot];
     const double qd = a.charge[atom];
@@ -1075,6 +1100,8 @@ __global__ void __launch_bounds__(kBrickThreads) gather_bricks_kernel(const PmeA
       const double f = -qd * (gd[0] * a.recip[0][c] + gd[1] * a.recip[1][c] + gd[2] * a.recip[2][c]);
       add_fixed(a.force + (long long)c * a.n_atoms + atom, to_fixed(f, kForceScale));
     }
+    }
+    __syncthreads();  // the list is refilled by the next chunk
   }
 }
 
