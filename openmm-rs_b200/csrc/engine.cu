@@ -1117,13 +1117,22 @@ void Engine::update_box_dependents() {
   nl_.max_cand = 0;
   if (nb_periodic_ && box_[3] == 0.0 && box_[6] == 0.0 && box_[7] == 0.0) {
     // candidate blocks of one block in the column-neighbourhood kernel, for the largest skin
-    // the autotuner may pick: every column in reach times the most blocks a column can hold
+    // the autotuner may pick.  At most every block of every column in reach; expected, per
+    // column the blocks (each ~32 / (density * column area) tall) whose z-extent comes within
+    // reach of I's, twice over.  The kernel keeps its candidates in shared memory, so the
+    // expected count (not the bound) sets how many of its CTAs share an SM; a block with more
+    // candidates reports an overflow and the list grows (`cand_scale_`).
     const double reach = nb_->cutoff + std::max(skin_, kMaxTunedSkin);
     const int nx = nl_.n_col[0], ny = nl_.n_col[1];
     const int kx = (int)std::floor(reach * nx / box_[0] + 1e-6) + 1;
     const int ky = (int)std::floor(reach * ny / box_[4] + 1e-6) + 1;
     const long long cols = (long long)std::min(nx, 2 * kx + 1) * std::min(ny, 2 * ky + 1);
-    const long long cand = cols * (nl_.col_max / 32 + 1);
+    const long long bound = cols * (nl_.col_max / 32 + 1);
+    const double column_area = (box_[0] / nx) * (box_[4] / ny);
+    const double block_height = 32.0 / (n_ / volume_ * column_area);
+    const double per_column = (2.0 * reach + 2.0 * block_height) / block_height + 2.0;
+    const long long expected = (long long)std::ceil(2.0 * cand_scale_ * cols * per_column);
+    const long long cand = std::min(bound, expected);
     if (cand * 48 <= 200 * 1024) nl_.max_cand = (int)cand;
   }
   for (auto& L : bonded_) L.args.box = make_box(box_);
@@ -1249,6 +1258,10 @@ bool Engine::grow_neighbor_capacity() {
   if (want_masks > a.mask_capacity) {
     a.mask_capacity = (int)want_masks;
     a.masks = mem_.alloc<uint32_t>(32 * (size_t)a.mask_capacity);
+    grew = true;
+  }
+  if (nl_.max_cand > 0 && cand_scale_ < 64) {  // the builder's candidate arrays
+    cand_scale_ *= 2;
     grew = true;
   }
   if (!grew) return false;

@@ -282,6 +282,7 @@ class Engine {
   uint32_t* prune_cols_ = nullptr;
   uint32_t* prune_keep_ = nullptr;
   double prune_margin_ = kDefaultPruneMargin;  // 0: no pruning
+  int cand_scale_ = 1;  // growth of the list builder's candidate arrays after overflows
   PmeBricks bricks_{};      // brick-owned PME gather: geometry, slot ranges, stencils
   bool use_bricks_ = false;
   unsigned* prune_done_ = nullptr;
