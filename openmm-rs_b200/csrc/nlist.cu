@@ -546,6 +546,7 @@ __global__ void __launch_bounds__(32 * kListWarps) nl_lists(NlistArgs a) {
 // atomic, so they are contiguous.  The selected particles and their order are a function of
 // the rebuild positions alone, so the tile contents are deterministic.
 constexpr int kCtaWarps = 8;
+constexpr int kStageRegs = 2;  // staged candidates per lane when phase A packs its regions
 
 template <bool kDouble>
 __global__ void __launch_bounds__(32 * kCtaWarps, 4) nl_lists_cta(NlistArgs a) {
@@ -558,7 +559,7 @@ __global__ void __launch_bounds__(32 * kCtaWarps, 4) nl_lists_cta(NlistArgs a) {
   uint32_t* c_mask = reinterpret_cast<uint32_t*>(c_un + cap);        // [2][cap] per half of I
   int* c_pre = reinterpret_cast<int*>(c_mask + 2 * (size_t)cap);     // [2][cap + 1]
   __shared__ int s_wcount[kCtaWarps], s_wbase[kCtaWarps + 1];
-  __shared__ int s_tile0, s_ntiles;
+  __shared__ int s_tile0, s_ntiles, s_spill;
   __shared__ int s_slots[kCtaWarps][32];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int nb = *a.n_blocks;
@@ -628,8 +629,14 @@ __global__ void __launch_bounds__(32 * kCtaWarps, 4) nl_lists_cta(NlistArgs a) {
     }
     return gap2 < reach2;
   };
-  // phase A: two passes over this warp's columns
-  for (int pass = 0; pass < 2; ++pass) {
+  // phase A: the warps split I's columns.  In one pass each warp stages its candidates, in
+  // test order, in its own region of the candidate arrays; the regions are then packed in
+  // warp order (through registers, so no region is overwritten before it is read).  A warp
+  // with more candidates than its region holds makes the CTA test again, placing every
+  // candidate at its final offset.  Either way candidate c of warp w lands at
+  // s_wbase[w] + c, the same order whichever way it was placed.
+  const int region = min(cap / kCtaWarps, 32 * kStageRegs);
+  auto scan_columns = [&](bool staged) {
     int n = 0;
     for (int q = w; q < n_colq; q += kCtaWarps) {
       const int oy = q / nx_iter, ox = q % nx_iter;
@@ -643,8 +650,9 @@ __global__ void __launch_bounds__(32 * kCtaWarps, 4) nl_lists_cta(NlistArgs a) {
         bool unsafe = false, cand = false;
         if (J < j1) cand = test(J, d, &unsafe);
         const unsigned m = __ballot_sync(kFull, cand);
-        if (pass == 1 && cand) {
-          const int k = s_wbase[w] + n + __popc(m & ((1u << lane) - 1u));
+        if (cand) {
+          const int r = n + __popc(m & ((1u << lane) - 1u));
+          const int k = staged ? (r < region ? w * region + r : cap) : s_wbase[w] + r;
           if (k < cap) {
             c_J[k] = J;
             c_un[k] = unsafe ? 1 : 0;
@@ -656,18 +664,55 @@ __global__ void __launch_bounds__(32 * kCtaWarps, 4) nl_lists_cta(NlistArgs a) {
         n += __popc(m);
       }
     }
-    if (pass == 0) {
-      if (lane == 0) s_wcount[w] = n;
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        int t = 0;
-        for (int u = 0; u < kCtaWarps; ++u) {
-          s_wbase[u] = t;
-          t += s_wcount[u];
-        }
-        s_wbase[kCtaWarps] = t;
+    return n;
+  };
+  if (threadIdx.x == 0) s_spill = 0;
+  __syncthreads();
+  {
+    const int n = scan_columns(true);
+    if (lane == 0) {
+      s_wcount[w] = n;
+      if (n > region) s_spill = 1;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int u = 0; u < kCtaWarps; ++u) {
+      s_wbase[u] = t;
+      t += s_wcount[u];
+    }
+    s_wbase[kCtaWarps] = t;
+  }
+  __syncthreads();
+  if (s_spill) {
+    scan_columns(false);
+  } else {
+    const int nw = s_wcount[w];
+    int rJ[kStageRegs], run[kStageRegs];
+    double rd[kStageRegs][3];
+#pragma unroll
+    for (int u = 0; u < kStageRegs; ++u) {
+      const int i = lane + 32 * u, k = w * region + i;
+      if (i < nw) {
+        rJ[u] = c_J[k];
+        run[u] = c_un[k];
+        rd[u][0] = c_d[k];
+        rd[u][1] = c_d[cap + k];
+        rd[u][2] = c_d[2 * cap + k];
       }
-      __syncthreads();
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < kStageRegs; ++u) {
+      const int i = lane + 32 * u, k = s_wbase[w] + i;
+      if (i < nw && k < cap) {
+        c_J[k] = rJ[u];
+        c_un[k] = run[u];
+        c_d[k] = rd[u][0];
+        c_d[cap + k] = rd[u][1];
+        c_d[2 * cap + k] = rd[u][2];
+      }
     }
   }
   __syncthreads();
