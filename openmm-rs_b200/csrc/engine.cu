@@ -1418,6 +1418,66 @@ void Engine::enqueue_nonbonded(bool energy, bool direct, bool reciprocal, bool d
     OMMB200_CK(cudaEventRecord(fork_ev_, stream_));
     OMMB200_CK(cudaStreamWaitEvent(ps, fork_ev_, 0));
   }
+  // the reciprocal chain is enqueued first, so its kernels reach the GPU ahead of the direct
+  // chain's (the two orders measured within run-to-run spread of each other)
+  if (reciprocal && nb_pme_) {
+    PmeArgs<Real> m{};
+    m.n_atoms = n_;
+    m.order = nl_.sorted_atom;
+    m.n_order = n_slots_;
+    m.pos = pos_;
+    m.charge = charge_;
+    m.nx = grid_[0];
+    m.ny = grid_[1];
+    m.nz = grid_[2];
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) m.recip[r][c] = recip_[r][c];
+    m.grid_fixed = pme_fixed_;
+    m.grid_real = static_cast<Real*>(pme_real_);
+    m.grid_k = pme_k_;
+    m.influence = static_cast<const Real*>(influence_);
+    m.moduli = moduli_;
+    m.force = force_;
+    m.energy = energy_;
+    m.alpha = alpha_;
+    m.volume = volume_;
+    prof_begin("pme_spread");
+    launch_pme_spread<Real>(m, ps);
+    prof_end();
+    if (own_fft_) {
+      prof_begin("pme_transform");
+      launch_pme_transform<Real>(m, fft_, energy, ps);
+      prof_end();
+    } else {
+    prof_begin("pme_convert");
+    launch_pme_convert<Real>(m, ps);
+    prof_end();
+    OMMB200_CKFFT(cufftSetStream(fft_fwd_, ps));
+    OMMB200_CKFFT(cufftSetStream(fft_inv_, ps));
+    prof_begin("pme_fft_forward");
+    if (dp_)
+      OMMB200_CKFFT(cufftExecD2Z(fft_fwd_, (cufftDoubleReal*)pme_real_, (cufftDoubleComplex*)pme_k_));
+    else
+      OMMB200_CKFFT(cufftExecR2C(fft_fwd_, (cufftReal*)pme_real_, (cufftComplex*)pme_k_));
+    prof_end();
+    prof_begin("pme_convolve");
+    launch_pme_convolve<Real>(m, energy, ps);
+    prof_end();
+    prof_begin("pme_fft_inverse");
+    if (dp_)
+      OMMB200_CKFFT(cufftExecZ2D(fft_inv_, (cufftDoubleComplex*)pme_k_, (cufftDoubleReal*)pme_real_));
+    else
+      OMMB200_CKFFT(cufftExecC2R(fft_inv_, (cufftComplex*)pme_k_, (cufftReal*)pme_real_));
+    prof_end();
+    }
+    prof_begin("pme_gather");
+    if (use_bricks_) {
+      launch_pme_brick_stencils<Real>(m, bricks_, nl_, ps);
+      launch_pme_gather_bricks<Real>(m, bricks_, nl_, ps);
+    } else
+      launch_pme_gather<Real>(m, ps);
+    prof_end();
+  }
   // the exclusion corrections first: a small kernel that leaves SMs free while the reciprocal
   // chain starts beside it, before the pair kernel fills every SM
   if (direct && n_exceptions_) {
@@ -1511,64 +1571,6 @@ void Engine::enqueue_nonbonded(bool energy, bool direct, bool reciprocal, bool d
     p.pair_capacity = dump_capacity_;
     prof_begin("pair");
     launch_pair<Real>(p, elec_, energy, dump, pair_grid_, stream_);
-    prof_end();
-  }
-  if (reciprocal && nb_pme_) {
-    PmeArgs<Real> m{};
-    m.n_atoms = n_;
-    m.order = nl_.sorted_atom;
-    m.n_order = n_slots_;
-    m.pos = pos_;
-    m.charge = charge_;
-    m.nx = grid_[0];
-    m.ny = grid_[1];
-    m.nz = grid_[2];
-    for (int r = 0; r < 3; ++r)
-      for (int c = 0; c < 3; ++c) m.recip[r][c] = recip_[r][c];
-    m.grid_fixed = pme_fixed_;
-    m.grid_real = static_cast<Real*>(pme_real_);
-    m.grid_k = pme_k_;
-    m.influence = static_cast<const Real*>(influence_);
-    m.moduli = moduli_;
-    m.force = force_;
-    m.energy = energy_;
-    m.alpha = alpha_;
-    m.volume = volume_;
-    prof_begin("pme_spread");
-    launch_pme_spread<Real>(m, ps);
-    prof_end();
-    if (own_fft_) {
-      prof_begin("pme_transform");
-      launch_pme_transform<Real>(m, fft_, energy, ps);
-      prof_end();
-    } else {
-    prof_begin("pme_convert");
-    launch_pme_convert<Real>(m, ps);
-    prof_end();
-    OMMB200_CKFFT(cufftSetStream(fft_fwd_, ps));
-    OMMB200_CKFFT(cufftSetStream(fft_inv_, ps));
-    prof_begin("pme_fft_forward");
-    if (dp_)
-      OMMB200_CKFFT(cufftExecD2Z(fft_fwd_, (cufftDoubleReal*)pme_real_, (cufftDoubleComplex*)pme_k_));
-    else
-      OMMB200_CKFFT(cufftExecR2C(fft_fwd_, (cufftReal*)pme_real_, (cufftComplex*)pme_k_));
-    prof_end();
-    prof_begin("pme_convolve");
-    launch_pme_convolve<Real>(m, energy, ps);
-    prof_end();
-    prof_begin("pme_fft_inverse");
-    if (dp_)
-      OMMB200_CKFFT(cufftExecZ2D(fft_inv_, (cufftDoubleComplex*)pme_k_, (cufftDoubleReal*)pme_real_));
-    else
-      OMMB200_CKFFT(cufftExecC2R(fft_inv_, (cufftComplex*)pme_k_, (cufftReal*)pme_real_));
-    prof_end();
-    }
-    prof_begin("pme_gather");
-    if (use_bricks_) {
-      launch_pme_brick_stencils<Real>(m, bricks_, nl_, ps);
-      launch_pme_gather_bricks<Real>(m, bricks_, nl_, ps);
-    } else
-      launch_pme_gather<Real>(m, ps);
     prof_end();
   }
   if (ps != stream_) {  // join
