@@ -507,13 +507,19 @@ def main():
     launches = None
     if rank == 0 and not args.skip_extras:
         prof_steps = 100
+        cull0 = ctx.pair_cull_stats()
         times = kernel_profile(ctx, prof_steps)
+        cull1 = ctx.pair_cull_stats()
         pairs = ctx.count_pairs()
         pair_ms, pair_n = times.get("pair", (0.0, 1))
         t_pair = pair_ms / max(pair_n, 1) / 1000.0
         fp32_peak = ommb200.measure_fp32_peak(local)
         achieved = pairs * FLOPS_PER_PAIR / t_pair / 1e12 if t_pair > 0 else None
-        roofline = {"bound": "fp32", "kernel": "pair_kernel_x2<Ewald> (packed FP32)",
+        culled = cull1["cull_tiles"] > 0
+        kernel = ("pair_kernel_cull<Ewald> (packed FP32, entries culled at the current "
+                  "positions, runs of %d tiles)" % cull1["cull_tiles"] if culled
+                  else "pair_kernel_x2<Ewald> (packed FP32)")
+        roofline = {"bound": "fp32", "kernel": kernel,
                     "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                     "frac": (achieved / fp32_peak) if achieved else None,
                     "peak_source": "measured FP32 FMA throughput of this GPU "
@@ -521,8 +527,9 @@ def main():
                                    "FP32 figure",
                     "algorithmic": f"{pairs} in-cutoff pairs x {FLOPS_PER_PAIR} flops per launch",
                     "avg_launch_ms": 1000.0 * t_pair,
-                    "traffic": None, "traffic_source": "profiles/pair_kernel_water-23958.md "
-                                                      "(one ncu capture, scaled by tiles)"}
+                    "traffic": None,
+                    "traffic_source": "profiles/%s_%s.md (one ncu capture, scaled by tiles)"
+                                      % ("pair_kernel_cull" if culled else "pair_kernel", WORKLOAD)}
         peaks = measured_peaks()
         hbm = peaks.get("hbm_gbs")
         integ_ms, integ_n = times.get("integrate", (0.0, 1))
@@ -569,11 +576,16 @@ def main():
                     + 2 * prunes_timed + args.steps * (args.segment // 20))
         extras["pairs_in_cutoff"] = pairs
         nl = ctx.nlist_stats()
-        roofline["traffic"] = profiled_traffic(f"pair_kernel_{WORKLOAD}", nl["tiles"])
+        roofline["traffic"] = profiled_traffic(
+            ("pair_kernel_cull_" if culled else "pair_kernel_") + WORKLOAD, nl["tiles"])
         # self tiles are 32 x 32 pair slots, neighbour tiles 2 x 16 x 16 (halves of block I)
         # or 32 x 32 (whole blocks), as the autotuner chose
         per_tile = 512 if ctx.tuning()["tile_entries"] == 16 else 1024
         slots = nl["blocks"] * 1024 + (nl["tiles"] - nl["blocks"]) * per_tile
+        if culled:  # the slots the culling kernel evaluated: 512 per round
+            nl["listed_pair_efficiency"] = pairs / max(1, slots)
+            nl["cull_rounds_per_launch"] = (cull1["rounds"] - cull0["rounds"]) / max(1, pair_n)
+            slots = 512 * nl["cull_rounds_per_launch"]
         nl["pair_efficiency"] = pairs / max(1, slots)
         nl["md_steps_per_rebuild"] = md_steps / max(1, rebuilds_timed)  # timed region only
         nl.update(ctx.nlist_prune_stats())

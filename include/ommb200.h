@@ -74,6 +74,13 @@ typedef struct {
                                  boxes): entries beyond cutoff + margin of their half block are
                                  dropped until a particle moves margin / 2; 0 = off; < 0 picks
                                  the default (off; ommb200_context_autotune may turn it on) */
+  int pair_cull;              /* mixed precision, periodic rectangular boxes without a pruned
+                                 list: the pair kernel drops, at every evaluation, the entries
+                                 beyond the cutoff of their half block's current bounding box
+                                 and packs the rest into full rounds; a warp takes runs of this
+                                 many tiles of one block.  0 = off (every listed entry is
+                                 evaluated); < 0 picks the default (8); at most 64.  The pair set
+                                 is the same either way */
 } ommb200_options;
 
 typedef struct {
@@ -380,6 +387,11 @@ int ommb200_context_nlist_capacity(ommb200_context* ctx, int* tile_capacity, int
  * tiles directly). */
 int ommb200_context_nlist_prune_stats(ommb200_context* ctx, int* rebuild_tiles, int64_t* prunes,
                                       double* margin);
+/* The culling pair kernel (ommb200_options.pair_cull; no reference counterpart): tiles per
+ * warp run as this Context uses it now (0 when the pair kernel evaluates every listed entry),
+ * and the rounds it has run since the Context was created, each 2 x 16 x 16 pair slots (a self
+ * tile runs two).  Either output may be NULL. */
+int ommb200_context_get_pair_cull(ommb200_context* ctx, int* tiles_per_run, int64_t* rounds);
 /* The cudaStream_t every kernel of this Context is launched on (for CUDA-event timing). */
 int ommb200_context_get_stream(ommb200_context* ctx, void** stream);
 /* Diagnostics (no reference counterpart): the number of polls after which the tensor-core

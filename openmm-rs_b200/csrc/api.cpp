@@ -132,6 +132,7 @@ void ommb200_default_options(ommb200_options* out) {
   out->steps_per_graph = 0;
   out->pme_bricks = -1;
   out->prune_margin = -1.0;
+  out->pair_cull = -1;
 }
 
 // ---- System -----------------------------------------------------------------------------
@@ -540,6 +541,7 @@ static EngineOptions engine_options(const ommb200_options* options) {
   require(o.pme_bricks >= -1 && o.pme_bricks <= 1, "pme_bricks must be -1, 0 or 1");
   require(std::isfinite(o.prune_margin) && o.prune_margin <= 0.5,
           "prune_margin must be finite and at most 0.5 nm");
+  require(o.pair_cull >= -1 && o.pair_cull <= 64, "pair_cull must be -1, 0 or 1-64 tiles");
   EngineOptions eo;
   eo.precision = o.precision;
   eo.device = o.device;
@@ -548,6 +550,7 @@ static EngineOptions engine_options(const ommb200_options* options) {
   eo.steps_per_graph = o.steps_per_graph;
   eo.pme_bricks = o.pme_bricks;
   eo.prune_margin = o.prune_margin;
+  eo.pair_cull = o.pair_cull;
   return eo;
 }
 
@@ -889,6 +892,12 @@ int ommb200_context_nlist_prune_stats(ommb200_context* ctx, int* rebuild_tiles, 
   return guarded([&] {
     OMMB200_CTX;
     E.nlist_prune_stats(rebuild_tiles, prunes, margin);
+  });
+}
+int ommb200_context_get_pair_cull(ommb200_context* ctx, int* tiles_per_run, int64_t* rounds) {
+  return guarded([&] {
+    OMMB200_CTX;
+    E.pair_cull_stats(tiles_per_run, rounds);
   });
 }
 int ommb200_context_get_stream(ommb200_context* ctx, void** stream) {

@@ -372,6 +372,9 @@ void Engine::setup_nonbonded(const NonbondedDef& nb) {
       a.n_col[d] = std::max(1, std::min(4096, (int)std::floor(box_[4 * d] / width)));
     a.n_cols = a.n_col[0] * a.n_col[1];
     const double col_area = (box_[0] / a.n_col[0]) * (box_[4] / a.n_col[1]);
+    list_density_ = density;
+    list_col_w_[0] = box_[0] / a.n_col[0];
+    list_col_w_[1] = box_[4] / a.n_col[1];
     const double expected = density * col_area * box_[8];
     a.col_max = std::max(64, (int)std::min(4096.0, 2.5 * expected + 64));
     a.slot_capacity = ((n_ + 31 * a.n_cols) + 31) / 32 * 32;
@@ -442,6 +445,11 @@ void Engine::setup_nonbonded(const NonbondedDef& nb) {
     a.prune = prune_flag_;
     prune_margin_ = opt_.prune_margin >= 0.0 ? opt_.prune_margin : kDefaultPruneMargin;
     if (prune_margin_ > 0.0) alloc_pruned_list();
+    cull_tiles_ = opt_.pair_cull >= 0 ? opt_.pair_cull : kDefaultCullTiles;
+    cull_work_ = mem_.alloc<int>(2);
+    OMMB200_CK(cudaMemset(cull_work_, 0, 2 * sizeof(int)));
+    cull_rounds_ = mem_.alloc<unsigned long long>(1);
+    OMMB200_CK(cudaMemset(cull_rounds_, 0, sizeof(unsigned long long)));
   }
   posq_ = mem_.alloc_bytes((dp_ ? 32 : 16) * (size_t)n_slots_);
   ljp_ = mem_.alloc_bytes((dp_ ? 16 : 8) * (size_t)n_slots_);
@@ -1361,6 +1369,26 @@ void Engine::enqueue_conditional_body(cudaGraphConditionalHandle handle,
   OMMB200_CK(cudaStreamEndCapture(aux_stream_, &done));
 }
 
+bool Engine::culling() const {
+  return cull_tiles_ > 0 && !dp_ && !pruning() && nb_periodic_ && nl_.block_tiles && nl_.halves &&
+         nl_.max_cand > 0 && elec_ != kElecCoulomb && segments_.size() <= 1 && box_[3] == 0.0 &&
+         box_[6] == 0.0 && box_[7] == 0.0;
+}
+
+int Engine::cull_chunks() const {
+  // entries per half block: particles within cutoff + skin of a wx x wy x hz/2 box (its
+  // Minkowski sum with that sphere).  A block lists only the blocks after it, so the first
+  // blocks of the order hold all of them (twice the mean); the sub-chunks cover that with a
+  // margin, so the last one, which takes whatever is left, stays short
+  const double a = list_col_w_[0], b = list_col_w_[1];
+  const double c = 16.0 / std::max(1e-9, list_density_ * a * b);
+  const double r = nb_->cutoff + skin_;
+  const double vol = a * b * c + 2.0 * (a * b + b * c + c * a) * r + kPiD * (a + b + c) * r * r +
+                     4.0 / 3.0 * kPiD * r * r * r;
+  const double tiles_max = 1.0 + list_density_ * vol / 16.0;
+  return std::max(1, (int)std::ceil(1.25 * tiles_max / std::max(1, cull_tiles_)));
+}
+
 bool Engine::pruning() const {
   return prune_margin_ > 0.0 && prune_tiles_ && nb_periodic_ && nl_.block_tiles && nl_.halves && nl_.max_cand > 0 && box_[3] == 0.0 &&
          box_[6] == 0.0 && box_[7] == 0.0;
@@ -1569,6 +1597,17 @@ void Engine::enqueue_nonbonded(bool energy, bool direct, bool reciprocal, bool d
     p.pair_dump = dump_pairs_;
     p.pair_count = dump_count_;
     p.pair_capacity = dump_capacity_;
+    if (culling()) {
+      p.cull_tiles = cull_tiles_;
+      p.cull_chunks = cull_chunks();
+      // pairs at r^2 >= rc^2 + band are outside whatever the f64 decision says; the factor
+      // covers the rounding of the sum
+      p.cull2 = (Real)((rc * rc + (double)p.band) * (1.0 + 1e-5));
+      p.n_blocks = nl_.n_blocks;
+      p.block_tiles = nl_.block_tiles;
+      p.cull_work = cull_work_;
+      p.cull_rounds = cull_rounds_;
+    }
     prof_begin("pair");
     launch_pair<Real>(p, elec_, energy, dump, pair_grid_, stream_);
     prof_end();
@@ -2284,6 +2323,22 @@ void Engine::autotune(int trial_steps, double* skin_out, int* ctas_out, double* 
   double best_skin = skin_, best_ms = 1e30, best_margin = prune_margin_;
   int best_ctas = pair_grid_ / std::max(1, sm_count_);
   int best_halves = nl_.halves;
+  int best_cull = cull_tiles_;
+  // culling pair kernel: tiles per warp run (0 = off); it runs only without a pruned list
+  auto tune_cull = [&]() {
+    if (!(nb_ && nb_periodic_ && nl_.block_tiles && nl_.max_cand > 0 && nl_.halves) || dp_ ||
+        prune_margin_ > 0.0)
+      return;
+    for (int c : kTunedCullTiles) {
+      cull_tiles_ = c;
+      const double ms = trial(best_skin, best_ctas);
+      if (ms < best_ms) {
+        best_ms = ms;
+        best_cull = c;
+      }
+    }
+    cull_tiles_ = best_cull;
+  };
   // pruned-list margin (0 = no pruning), where the list builder records each block's tiles
   auto tune_margin = [&]() {
     if (!(nb_ && nb_periodic_ && nl_.block_tiles && nl_.max_cand > 0 && nl_.halves)) return;
@@ -2299,6 +2354,7 @@ void Engine::autotune(int trial_steps, double* skin_out, int* ctas_out, double* 
     prune_margin_ = best_margin;
   };
   try {
+    tune_cull();
     tune_margin();
     if (nb_ && nb_periodic_) {
       for (double s : kTunedSkins) {
@@ -2322,6 +2378,7 @@ void Engine::autotune(int trial_steps, double* skin_out, int* ctas_out, double* 
       nl_.halves = best_halves;
     }
     tune_margin();  // again, for the chosen skin and tile width
+    tune_cull();
     if (nb_) {
       for (int c : kTunedPairCtasPerSm) {
         const double ms = trial(best_skin, c);
@@ -2343,6 +2400,7 @@ void Engine::autotune(int trial_steps, double* skin_out, int* ctas_out, double* 
   nl_.skin = best_skin;
   nl_.halves = best_halves;
   prune_margin_ = best_margin;
+  cull_tiles_ = best_cull;
   pair_grid_ = sm_count_ * best_ctas;
   destroy_graph();
   restore();
@@ -2363,6 +2421,16 @@ void Engine::nlist_capacity(int* tile_capacity, int* column_capacity, int* regro
   if (tile_capacity) *tile_capacity = nl_.tile_capacity;
   if (column_capacity) *column_capacity = nb_periodic_ ? nl_.col_max : 0;
   if (regrows) *regrows = regrows_;
+}
+
+void Engine::pair_cull_stats(int* tiles_per_run, int64_t* rounds) {
+  unsigned long long r = 0;
+  if (cull_rounds_) {
+    OMMB200_CK(cudaMemcpyAsync(&r, cull_rounds_, 8, cudaMemcpyDeviceToHost, stream_));
+    sync();
+  }
+  if (tiles_per_run) *tiles_per_run = culling() ? cull_tiles_ : 0;
+  if (rounds) *rounds = (int64_t)r;
 }
 
 void Engine::nlist_prune_stats(int* rebuild_tiles, int64_t* prunes, double* margin) {
@@ -2452,7 +2520,7 @@ struct CheckpointHeader {
   char magic[8];
   uint32_t version;
   int32_t n_atoms, n_segments, precision, learned, dynamic_list, rebuild_flag, pair_grid, halves;
-  int32_t prune_flag, unused;
+  int32_t prune_flag, cull_tiles;
   double time;
   int64_t step_count;
   double box[9];
@@ -2465,7 +2533,7 @@ struct CheckpointHeader {
   double bar_volume_scale, bar_pressure, bar_temperature;
 };
 constexpr char kCheckpointMagic[8] = {'O', 'M', 'B', '2', 'C', 'K', 'P', 'T'};
-constexpr uint32_t kCheckpointVersion = 6;
+constexpr uint32_t kCheckpointVersion = 7;
 }  // namespace
 
 size_t Engine::checkpoint_bytes() const {
@@ -2496,6 +2564,7 @@ void Engine::save_checkpoint(uint8_t* out, size_t bytes) {
   h.velocity_draws = velocity_draws_;
   h.skin = skin_;
   h.prune_margin = prune_margin_;
+  h.cull_tiles = cull_tiles_;
   h.bar_counter = bar_counter_;
   h.bar_window_attempted = bar_window_attempted_;
   h.bar_window_accepted = bar_window_accepted_;
@@ -2580,6 +2649,7 @@ void Engine::load_checkpoint(const uint8_t* in, size_t bytes) {
     skin_ = h.skin;
     nl_.skin = h.skin;
     prune_margin_ = h.prune_margin;
+    cull_tiles_ = h.cull_tiles;
     if (prune_margin_ > 0.0) ensure_pruned_list();
     update_bricks();
     pair_grid_ = h.pair_grid;

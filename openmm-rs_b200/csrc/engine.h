@@ -34,6 +34,11 @@ constexpr int kTunedPairCtasPerSm[] = {4, 6, 7, 8, 9, 10, 11, 12};
 constexpr double kTunedPruneMargins[] = {0.0, 0.05, 0.08, 0.12};
 constexpr double kDefaultPruneMargin = 0.0;
 constexpr double kPruneAllowance = 1e-4;
+// Culling pair kernel (FP32, periodic rectangular boxes, no pruned list): a warp takes a
+// sub-chunk of this many consecutive tiles of one block; 0 reads every tile's entries as they
+// are (pair_kernel_x2).  The autotuner tries the values below.
+constexpr int kDefaultCullTiles = 8;
+constexpr int kTunedCullTiles[] = {0, 4, 8, 16, 32, 64};
 
 class DeviceArena {
  public:
@@ -56,6 +61,7 @@ struct EngineOptions {
   int steps_per_graph = 0;
   int pme_bricks = -1;  // brick-owned PME gather: -1 by grid size, 0 off, 1 on
   double prune_margin = -1.0;  // nm; 0 off, < 0 the default
+  int pair_cull = -1;  // culling pair kernel: tiles per sub-chunk; 0 off, < 0 the default
 };
 
 // Device state that a re-run of MD steps starts from (Engine::save_dynamic_state).
@@ -98,6 +104,9 @@ class Engine {
   void nlist_stats(int* tiles, int* blocks, int* masked, int64_t* rebuilds);
   void nlist_capacity(int* tile_capacity, int* column_capacity, int* regrows) const;
   void nlist_prune_stats(int* rebuild_tiles, int64_t* prunes, double* margin);
+  // tiles per warp run of the culling pair kernel (0 when it does not run) and the rounds it
+  // has run so far (each 2 x 16 x 16 pair slots)
+  void pair_cull_stats(int* tiles_per_run, int64_t* rounds);
   // current skin, pair-kernel CTAs per SM and neighbour entries per i-group (16: halves of
   // 32-particle blocks; 32: whole blocks)
   void tuning(double* skin, int* pair_ctas_per_sm, int* tile_entries) const;
@@ -152,6 +161,10 @@ class Engine {
   // The pair kernel runs on the pruned list: periodic rectangular boxes whose rebuild packs 16
   // entries per half block (the builder that records each block's tiles).
   bool pruning() const;
+  // whether the culling pair kernel runs, and its sub-chunks per block (tiles per block
+  // estimated from the density, the column widths and the cutoff + skin)
+  bool culling() const;
+  int cull_chunks() const;
   void alloc_pruned_list();
   void ensure_pruned_list();  // the pruned list's arrays, allocated on first use
   PruneArgs prune_args() const;
@@ -282,6 +295,10 @@ class Engine {
   uint32_t* prune_cols_ = nullptr;
   uint32_t* prune_keep_ = nullptr;
   double prune_margin_ = kDefaultPruneMargin;  // 0: no pruning
+  int cull_tiles_ = kDefaultCullTiles;  // culling pair kernel's sub-chunk (0: off)
+  int* cull_work_ = nullptr;  // its work counters (zero between launches)
+  unsigned long long* cull_rounds_ = nullptr;  // its rounds so far
+  double list_density_ = 0.0, list_col_w_[2] = {0.0, 0.0};  // for the tiles-per-block estimate
   int cand_scale_ = 1;  // growth of the list builder's candidate arrays after overflows
   PmeBricks bricks_{};      // brick-owned PME gather: geometry, slot ranges, stencils
   bool use_bricks_ = false;

@@ -133,6 +133,16 @@ struct PairArgs {
   int32_t* pair_dump;   // diagnostics
   unsigned long long* pair_count;
   long long pair_capacity;
+  // culling form (FP32, periodic halves-tile lists from the CTA builder): cull_tiles > 0 runs
+  // pair_kernel_cull over sub-chunks of cull_tiles tiles, cull_chunks per block (the last
+  // takes the rest); entries farther than sqrt(cull2) from their half block's box are dropped
+  int cull_tiles;
+  int cull_chunks;
+  Real cull2;
+  const int* n_blocks;     // device: blocks in use
+  const int* block_tiles;  // [2 * blocks] first tile and tile count of each block
+  int* cull_work;          // [2] zero between launches: next sub-chunk, warps finished
+  unsigned long long* cull_rounds;  // rounds run (each 2 x 16 x 16 pair slots), accumulated
 };
 
 template <class Real>

@@ -67,7 +67,7 @@ _ERRORS = {ERR_INVALID_ARG: InvalidArgument, ERR_CONSTRAINT: ConstraintError,
 class Options(C.Structure):
     _fields_ = [("precision", C.c_int), ("device", C.c_int), ("use_cuda_graph", C.c_int),
                 ("neighbor_skin", C.c_double), ("steps_per_graph", C.c_int),
-                ("pme_bricks", C.c_int), ("prune_margin", C.c_double)]
+                ("pme_bricks", C.c_int), ("prune_margin", C.c_double), ("pair_cull", C.c_int)]
 
 
 class LearnedRadiiStats(C.Structure):
@@ -150,6 +150,7 @@ def library() -> C.CDLL:
             "ommb200_set_tensor_core_wait_limit": [C.c_longlong],
             "ommb200_context_nlist_prune_stats": [P, C.POINTER(I), C.POINTER(C.c_int64),
                                                   C.POINTER(D)],
+            "ommb200_context_get_pair_cull": [P, C.POINTER(I), C.POINTER(C.c_int64)],
             "ommb200_monte_carlo_barostat_create": [D, D, I, C.POINTER(P)],
             "ommb200_monte_carlo_barostat_set_default_pressure": [P, D],
             "ommb200_monte_carlo_barostat_get_default_pressure": [P, C.POINTER(D)],
@@ -560,7 +561,7 @@ class State:
 
 
 def _options(precision, device, use_cuda_graph, neighbor_skin, steps_per_graph,
-             pme_bricks=-1, prune_margin=-1.0) -> "Options":
+             pme_bricks=-1, prune_margin=-1.0, pair_cull=-1) -> "Options":
     opt = Options()
     opt.precision = {"mixed": PRECISION_MIXED, "double": PRECISION_DOUBLE}[precision]
     opt.device = device
@@ -569,6 +570,7 @@ def _options(precision, device, use_cuda_graph, neighbor_skin, steps_per_graph,
     opt.steps_per_graph = steps_per_graph
     opt.pme_bricks = pme_bricks
     opt.prune_margin = prune_margin
+    opt.pair_cull = pair_cull
     return opt
 
 
@@ -577,14 +579,17 @@ class Context:
 
     def __init__(self, system: System, integrator: LangevinMiddleIntegrator, precision="mixed",
                  device: int = 0, use_cuda_graph: bool = True, neighbor_skin: float = 0.0,
-                 steps_per_graph: int = 0, pme_bricks: int = -1, prune_margin: float = -1.0):
+                 steps_per_graph: int = 0, pme_bricks: int = -1, prune_margin: float = -1.0,
+                 pair_cull: int = -1):
         """`pme_bricks`: brick-owned PME gather in rectangular periodic boxes, -1 when
         the grid has at least two bricks per SM, 0 never, 1 whenever the box allows (the forces
         are the same either way).  `prune_margin` (nm): the pruned pair list between rebuilds
-        (0 off, < 0 the default: off until `autotune` picks a margin)."""
+        (0 off, < 0 the default: off until `autotune` picks a margin).  `pair_cull`: tiles per
+        warp run of the culling pair kernel, which drops entries beyond the cutoff of their half
+        block at every evaluation (0 off, < 0 the default)."""
         n = system.num_particles()
         opt = _options(precision, device, use_cuda_graph, neighbor_skin, steps_per_graph,
-                       pme_bricks, prune_margin)
+                       pme_bricks, prune_margin, pair_cull)
         h = C.c_void_p()
         sys_h, int_h = system._take(), integrator._take()
         _check(library().ommb200_context_create(sys_h, int_h, C.byref(opt), C.byref(h)))
@@ -751,15 +756,24 @@ class Context:
         out = {"skin_nm": skin.value, "pair_ctas_per_sm": ctas.value, "ms_per_step": ms.value}
         out["tile_entries"] = self.tuning()["tile_entries"]
         out["prune_margin_nm"] = self.nlist_prune_stats()["margin_nm"]
+        out["cull_tiles"] = self.tuning()["cull_tiles"]
         return out
 
     def tuning(self) -> dict:
-        """Current skin, pair-kernel CTAs per SM and neighbour entries per i-group."""
+        """Current skin, pair-kernel CTAs per SM, neighbour entries per i-group and tiles per
+        warp run of the culling pair kernel (0: off)."""
         skin, ctas, width = C.c_double(), C.c_int(), C.c_int()
         _check(library().ommb200_context_get_tuning(self._h, C.byref(skin), C.byref(ctas),
                                                     C.byref(width)))
         return {"skin_nm": skin.value, "pair_ctas_per_sm": ctas.value,
-                "tile_entries": width.value}
+                "tile_entries": width.value, "cull_tiles": self.pair_cull_stats()["cull_tiles"]}
+
+    def pair_cull_stats(self) -> dict:
+        """Culling pair kernel: tiles per warp run (0: not in use) and the rounds it has run
+        so far, each 2 x 16 x 16 pair slots."""
+        t, r = C.c_int(), C.c_int64()
+        _check(library().ommb200_context_get_pair_cull(self._h, C.byref(t), C.byref(r)))
+        return {"cull_tiles": t.value, "rounds": r.value}
 
     def nlist_stats(self) -> dict:
         """Neighbour-list state: tiles the pair kernel evaluates, blocks and masked tiles in

@@ -146,13 +146,15 @@ def test_batch_validation_happens_before_the_device():
 
 def test_default_options_and_option_validation():
     """ommb200_default_options fills the layout options (pme_bricks -1: by grid size;
-    prune_margin -1: the default, no pruned list), and out-of-range values are refused before
-    any device work, with or without a GPU."""
+    prune_margin -1: the default, no pruned list; pair_cull -1: the default run length of the
+    culling pair kernel), and out-of-range values are refused before any device work, with or
+    without a GPU."""
     opt = ommb200.Options()
     ommb200.library().ommb200_default_options(C.byref(opt))
     assert opt.use_cuda_graph == 1 and opt.steps_per_graph == 0
-    assert opt.pme_bricks == -1 and opt.prune_margin == -1.0
+    assert opt.pme_bricks == -1 and opt.prune_margin == -1.0 and opt.pair_cull == -1
     w = synth.water_box(8, 1.9, (2, 2, 2), seed=1)
-    for kw in ({"pme_bricks": 2}, {"prune_margin": 0.8}, {"prune_margin": float("nan")}):
+    for kw in ({"pme_bricks": 2}, {"prune_margin": 0.8}, {"prune_margin": float("nan")},
+               {"pair_cull": -2}, {"pair_cull": 65}):
         with pytest.raises(ommb200.InvalidArgument):
             ommb200.Context(systems.water_system(w), systems.langevin(), **kw)
