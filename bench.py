@@ -65,6 +65,12 @@ def parse():
     p.add_argument("--systems", type=int, default=16,
                    help="chains-learned: number of chains (small cases for profiler captures)")
     p.add_argument("--atoms", type=int, default=5000, help="chains-learned: atoms per chain")
+    p.add_argument("--pair-cull", type=int, default=-1,
+                   help="water boxes without the autotuner (--no-equilibrate): tiles per warp "
+                        "run of the culling pair kernel (0 off, -1 the default)")
+    p.add_argument("--skin", type=float, default=0.0,
+                   help="water boxes without the autotuner (--no-equilibrate): Verlet skin in "
+                        "nm (0: the default)")
     return p.parse_args()
 
 
@@ -204,7 +210,8 @@ def build_context(precision, seed, device):
 
     w, x, v = equilibrate(seed, device)
     ctx = ommb200.Context(systems.water_system(w), systems.langevin(seed=seed),
-                          precision=precision, device=device, use_cuda_graph=USE_GRAPH)
+                          precision=precision, device=device, use_cuda_graph=USE_GRAPH,
+                          pair_cull=PAIR_CULL, neighbor_skin=SKIN)
     ctx.set_positions(x)
     ctx.set_velocities(v)
     TUNED[precision] = ctx.autotune(200) if TUNE else None
@@ -214,6 +221,8 @@ def build_context(precision, seed, device):
 TUNE = True
 TUNED = {}
 USE_GRAPH = True
+PAIR_CULL = -1
+SKIN = 0.0
 
 
 def time_segments(ctx, torch, segments, md_steps, flush):
@@ -442,8 +451,9 @@ def run_reference(args):
 
 def main():
     args = parse()
-    global EQUILIBRATION_STEPS, TUNE, WORKLOAD, USE_GRAPH
+    global EQUILIBRATION_STEPS, TUNE, WORKLOAD, USE_GRAPH, PAIR_CULL, SKIN
     USE_GRAPH = not args.no_graph
+    PAIR_CULL, SKIN = args.pair_cull, args.skin
     if args.workload.startswith("water"):
         WORKLOAD = args.workload
     if args.no_equilibrate:

@@ -79,8 +79,10 @@ typedef struct {
                                  beyond the cutoff of their half block's current bounding box
                                  and packs the rest into full rounds; a warp takes runs of this
                                  many tiles of one block.  0 = off (every listed entry is
-                                 evaluated); < 0 picks the default (8); at most 64.  The pair set
-                                 is the same either way */
+                                 evaluated); < 0 picks by size (64 when the list gives each
+                                 resident warp about 40 tiles or more, else off;
+                                 ommb200_context_autotune may change it); at most 64.  The pair
+                                 set is the same either way */
 } ommb200_options;
 
 typedef struct {

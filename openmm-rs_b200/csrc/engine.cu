@@ -445,7 +445,7 @@ void Engine::setup_nonbonded(const NonbondedDef& nb) {
     a.prune = prune_flag_;
     prune_margin_ = opt_.prune_margin >= 0.0 ? opt_.prune_margin : kDefaultPruneMargin;
     if (prune_margin_ > 0.0) alloc_pruned_list();
-    cull_tiles_ = opt_.pair_cull >= 0 ? opt_.pair_cull : kDefaultCullTiles;
+    cull_tiles_ = opt_.pair_cull >= 0 ? opt_.pair_cull : 0;  // < 0: set by size below
     cull_work_ = mem_.alloc<int>(2);
     OMMB200_CK(cudaMemset(cull_work_, 0, 2 * sizeof(int)));
     cull_rounds_ = mem_.alloc<unsigned long long>(1);
@@ -458,6 +458,11 @@ void Engine::setup_nonbonded(const NonbondedDef& nb) {
   cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, opt_.device);
   sm_count_ = dev_sms;
   pair_grid_ = dev_sms * 8;
+  if (nb_periodic_ && opt_.pair_cull < 0) {  // by size: runs pay off with many tiles per warp
+    const double tiles = 0.5 * tiles_per_block_max() * n_ / 32.0;
+    const double warps = dev_sms * 5.0 * 4.0;  // resident warps of the culling kernel
+    cull_tiles_ = tiles / warps >= kCullMinTilesPerWarp ? kDefaultCullTiles : 0;
+  }
 
   if (nb_pme_) {
     const long long g = (long long)grid_[0] * grid_[1] * grid_[2];
@@ -1375,18 +1380,22 @@ bool Engine::culling() const {
          box_[6] == 0.0 && box_[7] == 0.0;
 }
 
-int Engine::cull_chunks() const {
+double Engine::tiles_per_block_max() const {
   // entries per half block: particles within cutoff + skin of a wx x wy x hz/2 box (its
   // Minkowski sum with that sphere).  A block lists only the blocks after it, so the first
-  // blocks of the order hold all of them (twice the mean); the sub-chunks cover that with a
-  // margin, so the last one, which takes whatever is left, stays short
+  // blocks of the order hold all of them, twice the mean
   const double a = list_col_w_[0], b = list_col_w_[1];
   const double c = 16.0 / std::max(1e-9, list_density_ * a * b);
   const double r = nb_->cutoff + skin_;
   const double vol = a * b * c + 2.0 * (a * b + b * c + c * a) * r + kPiD * (a + b + c) * r * r +
                      4.0 / 3.0 * kPiD * r * r * r;
-  const double tiles_max = 1.0 + list_density_ * vol / 16.0;
-  return std::max(1, (int)std::ceil(1.25 * tiles_max / std::max(1, cull_tiles_)));
+  return 1.0 + list_density_ * vol / 16.0;
+}
+
+int Engine::cull_chunks() const {
+  // runs cover the largest block with a margin, so the last one, which takes whatever is
+  // left, stays short
+  return std::max(1, (int)std::ceil(1.25 * tiles_per_block_max() / std::max(1, cull_tiles_)));
 }
 
 bool Engine::pruning() const {

@@ -34,10 +34,13 @@ constexpr int kTunedPairCtasPerSm[] = {4, 6, 7, 8, 9, 10, 11, 12};
 constexpr double kTunedPruneMargins[] = {0.0, 0.05, 0.08, 0.12};
 constexpr double kDefaultPruneMargin = 0.0;
 constexpr double kPruneAllowance = 1e-4;
-// Culling pair kernel (FP32, periodic rectangular boxes, no pruned list): a warp takes a
-// sub-chunk of this many consecutive tiles of one block; 0 reads every tile's entries as they
-// are (pair_kernel_x2).  The autotuner tries the values below.
-constexpr int kDefaultCullTiles = 8;
+// Culling pair kernel (FP32, periodic rectangular boxes, no pruned list): a warp takes a run
+// of this many consecutive tiles of one block; 0 reads every tile's entries as they are
+// (pair_kernel_x2).  By default it runs with kDefaultCullTiles when the list gives a resident
+// warp about kCullMinTilesPerWarp tiles or more (below that each tile's loads are exposed);
+// the autotuner tries the values below.
+constexpr int kDefaultCullTiles = 64;
+constexpr double kCullMinTilesPerWarp = 40.0;
 constexpr int kTunedCullTiles[] = {0, 4, 8, 16, 32, 64};
 
 class DeviceArena {
@@ -165,6 +168,7 @@ class Engine {
   // estimated from the density, the column widths and the cutoff + skin)
   bool culling() const;
   int cull_chunks() const;
+  double tiles_per_block_max() const;  // estimate from the density and the cutoff + skin
   void alloc_pruned_list();
   void ensure_pruned_list();  // the pruned list's arrays, allocated on first use
   PruneArgs prune_args() const;
@@ -295,7 +299,7 @@ class Engine {
   uint32_t* prune_cols_ = nullptr;
   uint32_t* prune_keep_ = nullptr;
   double prune_margin_ = kDefaultPruneMargin;  // 0: no pruning
-  int cull_tiles_ = kDefaultCullTiles;  // culling pair kernel's sub-chunk (0: off)
+  int cull_tiles_ = 0;  // culling pair kernel's run length in tiles (0: off)
   int* cull_work_ = nullptr;  // its work counters (zero between launches)
   unsigned long long* cull_rounds_ = nullptr;  // its rounds so far
   double list_density_ = 0.0, list_col_w_[2] = {0.0, 0.0};  // for the tiles-per-block estimate

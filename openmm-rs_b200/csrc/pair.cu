@@ -819,10 +819,10 @@ __global__ void __launch_bounds__(32 * kPairWarps, 5) pair_kernel_cull(const Pai
     add_fixed(a.energy, e_fixed);
     for (int c = 0; c < 6; ++c) add_fixed(a.energy + 1 + c, w_fixed[c]);
   }
-  // every warp has taken its last sub-chunk index before it counts itself, so the last one to
-  // count may reset both counters
+  // a warp counts itself only after its last fetch returned (the fetch's value decided the
+  // loop's exit), so when the last warp counts itself no fetch is left and it may reset both
+  // counters for the next launch
   if (lane == 0) {
-    __threadfence();
     if (atomicAdd(a.cull_work + 1, 1) == nwarps - 1) {
       a.cull_work[0] = 0;
       a.cull_work[1] = 0;

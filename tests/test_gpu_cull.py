@@ -116,4 +116,5 @@ def test_culling_applies_to_the_mixed_form_without_a_pruned_list_only():
     w = box("water-1944")[0]
     assert context(w, 8, precision="double").tuning()["cull_tiles"] == 0
     assert context(w, 8, prune_margin=0.05).tuning()["cull_tiles"] == 0
-    assert context(w, -1).tuning()["cull_tiles"] > 0  # on by default
+    # by size: a 1,944-atom list gives each warp a fraction of a tile, so it stays off
+    assert context(w, -1).tuning()["cull_tiles"] == 0
