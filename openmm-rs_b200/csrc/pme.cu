@@ -99,14 +99,20 @@ __global__ void spread_kernel(const PmeArgs<Real> a) {
 // x-y column, z-sorted), two threads per atom, and adds the atoms' 125-point stencils into a
 // shared-memory copy of the grid box they touch, then adds that box to the global grid, so
 // each grid point receives one global atomic per CTA instead of one per stencil.  Shared
-// accumulation uses native 32-bit atomics on a split of each 64-bit fixed-point value,
-// v = hi 2^20 + lo with 0 <= lo < 2^20: at most 64 contributions per cell keep both partial
-// sums inside 32 bits (for |q| < 16 e), and hi_sum 2^20 + lo_sum recovers the exact 64-bit
-// total, so the integer grid is identical to direct spreading.  A CTA whose box exceeds
-// kSpreadCells (it straddles a periodic edge of the column order) or that holds a larger
-// charge spreads directly.
+// accumulation uses native 32-bit integer atomics (64-bit shared atomics measured 1.5-1.8x
+// slower).  FP64 form: a split of each 2^-40 fixed-point value, v = hi 2^20 + lo with
+// 0 <= lo < 2^20; at most 64 contributions per cell keep both partial sums inside 32 bits (for
+// |q| < 16 e), and hi_sum 2^20 + lo_sum recovers the exact 64-bit total.  FP32 form: one atomic
+// per point, each contribution (a float product) rounded to 2^-26 e, which keeps 64 of them
+// inside 32 bits for |q| < 2 e (the order-5 B-spline peaks at 115/192 per axis, so a point gets
+// at most 0.22 |q| from an atom); the box is added to the 2^-40 global grid scaled by 2^14,
+// exactly.  Either way the sums are exact integers, so the grid does not depend on the order
+// of the additions.  A CTA whose box exceeds kSpreadCells (it straddles a periodic edge of the
+// column order) or that holds a larger charge spreads directly.
 constexpr int kSpreadAtoms = 64;
 constexpr int kSpreadCells = 4096;
+constexpr float kSpreadScale32 = 67108864.f;           // 2^26 (FP32 form, staged)
+constexpr long long kSpreadWiden32 = 1ll << 14;        // 2^40 / 2^26
 
 template <class Real>
 __global__ void __launch_bounds__(2 * kSpreadAtoms) spread_staged_kernel(const PmeArgs<Real> a) {
@@ -132,7 +138,8 @@ __global__ void __launch_bounds__(2 * kSpreadAtoms) spread_staged_kernel(const P
       atomicMin(&s_lo[d], base[d]);
       atomicMax(&s_hi[d], base[d]);
     }
-    if (fabs(qd) >= 16.0) s_big = 1;  // the 32-bit partial sums need |q| < 16 e
+    // the 32-bit partial sums need |q| < 2 e (FP32 form) or |q| < 16 e (FP64 form)
+    if (fabs(qd) >= (sizeof(Real) == 4 ? 2.0 : 16.0)) s_big = 1;
   }
   __syncthreads();
   if (s_hi[0] < 0) return;  // no charged atom in this CTA (uniform)
@@ -171,7 +178,7 @@ __global__ void __launch_bounds__(2 * kSpreadAtoms) spread_staged_kernel(const P
   const int nc = (int)n_cells;
   for (int c = tid; c < nc; c += 2 * kSpreadAtoms) {
     c_hi[c] = 0;
-    c_lo[c] = 0u;
+    if constexpr (sizeof(Real) == 8) c_lo[c] = 0u;
   }
   __syncthreads();
   if (ok) {
@@ -182,16 +189,21 @@ __global__ void __launch_bounds__(2 * kSpreadAtoms) spread_staged_kernel(const P
         const int row = ((base[0] - lo0 + ix) * ey + (base[1] - lo1 + iy)) * ez + (base[2] - lo2);
 #pragma unroll
         for (int iz = 0; iz < 5; ++iz) {
-          const long long v = to_fixed(qxy * w[2][iz], gscale);
-          atomicAdd(&c_hi[row + iz], (int)(v >> 20));
-          atomicAdd(&c_lo[row + iz], (unsigned int)(v & 0xFFFFF));
+          if constexpr (sizeof(Real) == 4) {
+            atomicAdd(&c_hi[row + iz], __float2int_rn(qxy * w[2][iz] * kSpreadScale32));
+          } else {
+            const long long v = to_fixed(qxy * w[2][iz], gscale);
+            atomicAdd(&c_hi[row + iz], (int)(v >> 20));
+            atomicAdd(&c_lo[row + iz], (unsigned int)(v & 0xFFFFF));
+          }
         }
       }
     }
   }
   __syncthreads();
   for (int c = tid; c < nc; c += 2 * kSpreadAtoms) {
-    const long long v = (long long)c_hi[c] * (1ll << 20) + (long long)c_lo[c];
+    const long long v = sizeof(Real) == 4 ? (long long)c_hi[c] * kSpreadWiden32
+                                          : (long long)c_hi[c] * (1ll << 20) + (long long)c_lo[c];
     if (v == 0) continue;
     const int cz = c % ez, cy = (c / ez) % ey, cx = c / (ez * ey);
     int gx = lo0 + cx, gy = lo1 + cy, gz = lo2 + cz;
