@@ -2387,15 +2387,26 @@ void Engine::autotune(int trial_steps, double* skin_out, int* ctas_out, double* 
       nl_.halves = best_halves;
     }
     tune_margin();  // again, for the chosen skin and tile width
-    tune_cull();
+    // pair-kernel grid, jointly with the culling kernel's run length: its warps stay resident
+    // until the work runs out, so a smaller grid leaves SMs to the reciprocal chain beside it
     if (nb_) {
-      for (int c : kTunedPairCtasPerSm) {
-        const double ms = trial(best_skin, c);
-        if (ms < best_ms) {
-          best_ms = ms;
-          best_ctas = c;
+      const bool cull_ok = nb_periodic_ && nl_.block_tiles && nl_.max_cand > 0 && nl_.halves &&
+                           !dp_ && best_margin == 0.0;
+      const std::vector<int> culls = cull_ok ? std::vector<int>(std::begin(kTunedCullTiles),
+                                                                std::end(kTunedCullTiles))
+                                             : std::vector<int>{cull_tiles_};
+      for (int k : culls) {
+        cull_tiles_ = k;
+        for (int c : kTunedPairCtasPerSm) {
+          const double ms = trial(best_skin, c);
+          if (ms < best_ms) {
+            best_ms = ms;
+            best_ctas = c;
+            best_cull = k;
+          }
         }
       }
+      cull_tiles_ = best_cull;
     }
   } catch (...) {
     cudaEventDestroy(t0);

@@ -25,7 +25,7 @@ void nonbonded_forces_noalloc(int n, const double* pos, const double* q, const d
 // Verlet skins and pair-kernel CTAs per SM the autotuner tries.
 constexpr double kTunedSkins[] = {0.06, 0.08, 0.1, 0.13, 0.16, 0.2};
 constexpr double kMaxTunedSkin = 0.2;
-constexpr int kTunedPairCtasPerSm[] = {4, 6, 7, 8, 9, 10, 11, 12};
+constexpr int kTunedPairCtasPerSm[] = {2, 3, 4, 6, 7, 8, 9, 10, 11, 12};
 // Margins of the pruned pair list (nm) the autotuner tries: entries within cutoff + margin of
 // their half block stay, and a particle that moves margin / 2 requests the next prune, so a
 // wider margin prunes less often and leaves more pairs for the pair kernel; 0 turns pruning
