@@ -308,12 +308,14 @@ def test_autotune_keeps_the_trajectory():
         ctx.set_velocities_to_temperature(300.0, seed=6)
         if tune:
             t = ctx.autotune(40)
-            assert 0.05 < t["skin_nm"] <= 0.2 and t["pair_ctas_per_sm"] in range(4, 13)
+            assert 0.05 < t["skin_nm"] <= 0.2 and t["pair_ctas_per_sm"] in range(2, 13)
+            assert t["cull_tiles"] in (0, 4, 8, 16, 32, 64)
         ctx.step(30)
         st = ctx.get_state(positions=True, velocities=True)
         out.append((st.positions, st.velocities, st.step_count))
-    # the skin changes how pairs are grouped into tiles (so float summation order), never
-    # which pairs interact or the random stream: the trajectories agree to rounding
+    # the skin and the pair kernel's form change how pairs are grouped into tiles and rounds
+    # (so float summation order), never which pairs interact or the random stream: the
+    # trajectories agree to rounding
     assert np.abs(out[0][0] - out[1][0]).max() < 1e-6
     assert np.abs(out[0][1] - out[1][1]).max() < 1e-3
     assert out[0][2] == out[1][2] == 30
