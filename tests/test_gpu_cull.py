@@ -118,3 +118,49 @@ def test_culling_applies_to_the_mixed_form_without_a_pruned_list_only():
     assert context(w, 8, prune_margin=0.05).tuning()["cull_tiles"] == 0
     # by size: a 1,944-atom list gives each warp a fraction of a tile, so it stays off
     assert context(w, -1).tuning()["cull_tiles"] == 0
+
+
+@pytest.mark.parametrize("name", ["water-1944", "sparse"])
+def test_culled_reaction_field_with_switching_matches_oracle(name):
+    """The reaction-field form with an LJ switching function (nonbonded.rs:888-900,
+    1222-1243) through the culling kernel: the same pairs, the same forces as the oracle."""
+    w = box(name)[0]
+    f_ref, e_ref = O.nonbonded(w.positions, w.charges(), w.sigmas(), w.epsilons(),
+                               w.exceptions(), method="CutoffPeriodic", cutoff=0.9, box=w.box,
+                               use_switching=True, switching_distance=0.8, threads=8)
+    ref_pairs = O.pair_set(w.positions, 0.9, box=w.box,
+                           exclusions=[e[:2] for e in w.exceptions()])
+    for k in (0, 1, 8):
+        ctx = ommb200.Context(systems.water_system(w, method="CutoffPeriodic",
+                                                   switching_distance=0.8),
+                              systems.langevin(seed=7), pair_cull=k)
+        ctx.set_positions(w.positions)
+        assert ctx.tuning()["cull_tiles"] == k
+        st = ctx.get_state(forces=True, energy=True)
+        assert rms_rel(st.forces, f_ref) < MIXED_FORCE_RMS, k
+        # the reaction-field total is small (~1 kJ/mol per atom) beside the pair energies
+        # it sums, so its FP32 error is bounded per atom rather than relative to the total
+        assert abs(st.potential_energy - e_ref) < 2e-5 * w.n_atoms, k
+        got = ctx.debug_pair_list()
+        assert np.array_equal(pair_keys(got), pair_keys(ref_pairs)), k
+
+
+def test_culled_checkpoint_continues_bit_for_bit():
+    """The checkpoint carries the run length, so a Context created without culling continues a
+    culled trajectory bit for bit."""
+    w = box("sparse")[0]
+    a = context(w, 8)
+    a.set_velocities_to_temperature(300.0, seed=5)
+    a.step(80)
+    ck = a.create_checkpoint()
+    a.step(60)
+    sa = a.get_state(positions=True, velocities=True, forces=True, energy=True)
+    b = context(w, 0)
+    b.load_checkpoint(ck)
+    assert b.tuning()["cull_tiles"] == 8
+    b.step(60)
+    sb = b.get_state(positions=True, velocities=True, forces=True, energy=True)
+    assert np.array_equal(sa.positions, sb.positions)
+    assert np.array_equal(sa.velocities, sb.velocities)
+    assert np.array_equal(sa.forces, sb.forces)
+    assert sa.potential_energy == sb.potential_energy

@@ -59,9 +59,10 @@ def rms_rel(a, b):
     return float(np.sqrt(((a - b) ** 2).sum() / (b ** 2).sum()))
 
 
-def test_overflowing_neighbor_list_grows_and_matches_the_oracle():
+@pytest.mark.parametrize("pair_cull", [0, 8])
+def test_overflowing_neighbor_list_grows_and_matches_the_oracle(pair_cull):
     sysm, pos, q = dense_column_system()
-    ctx = ommb200.Context(sysm, systems.langevin(), precision="mixed")
+    ctx = ommb200.Context(sysm, systems.langevin(), precision="mixed", pair_cull=pair_cull)
     before = ctx.nlist_capacity()
     ctx.set_positions(pos)
     st = ctx.get_state(forces=True, energy=True)
@@ -74,15 +75,20 @@ def test_overflowing_neighbor_list_grows_and_matches_the_oracle():
     assert abs(st.potential_energy - e_ref) < 1e-5 * abs(e_ref) + 1e-3
 
 
-def test_steps_that_overflow_rerun_to_the_grown_list_trajectory():
+@pytest.mark.parametrize("pair_cull", [0, 8])
+def test_steps_that_overflow_rerun_to_the_grown_list_trajectory(pair_cull):
+    """Also with the culling pair kernel: its runs are fixed slices of each block's own tiles,
+    which do not depend on the list's capacity."""
     sysm, pos, q = dense_column_system()
-    grown = ommb200.Context(sysm, systems.langevin(step_size=0.001, seed=9), precision="mixed")
+    grown = ommb200.Context(sysm, systems.langevin(step_size=0.001, seed=9), precision="mixed",
+                            pair_cull=pair_cull)
     grown.set_positions(pos)
     grown.set_velocities_to_temperature(300.0, seed=4)  # evaluates forces: the list grows here
     assert grown.nlist_capacity()["regrows"] >= 1
     v0 = grown.get_state(velocities=True).velocities
     sysm, _, _ = dense_column_system()  # a Context takes its System over
-    fresh = ommb200.Context(sysm, systems.langevin(step_size=0.001, seed=9), precision="mixed")
+    fresh = ommb200.Context(sysm, systems.langevin(step_size=0.001, seed=9), precision="mixed",
+                            pair_cull=pair_cull)
     fresh.set_positions(pos)
     fresh.set_velocities(v0)  # no force evaluation before the steps
     assert fresh.nlist_capacity()["regrows"] == 0
