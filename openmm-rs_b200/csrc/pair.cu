@@ -438,12 +438,12 @@ __global__ void __launch_bounds__(32 * kPairWarps, 5) pair_kernel_x2(const PairA
 // are committed once.  Sub-chunks are fixed runs of a block's own tiles, whose order the
 // builder fixes, so rounds, float sums and forces are the same run to run, whichever warp
 // takes them: warps fetch sub-chunks from a counter (all blocks' first sub-chunks, then the
-// second ones, ...), and the last warp to finish resets the counter for the next launch
-// (no warp waits for another).  Self tiles and
-// tiles that need a per-pair minimum image are staged and run directly, after the queue is
-// drained; a self tile runs as two rounds (each half's i-slots with the entries of its own
-// half, then of the other half).  Exclusion words are kept over all 32 i-slots of block I,
-// an entry of a tile holding only its own half's bits.
+// second ones, ...), and the last warp to finish resets the counter for the next launch (no
+// warp waits for another).  Self tiles and tiles that need a per-pair minimum image are staged
+// and run directly, after the queue is drained; a self tile runs as two rounds (each half's
+// i-slots with the entries of its own half, then of the other half).  Exclusion words are kept
+// over all 32 i-slots of block I, an entry of a tile holding only its own half's bits.  The
+// next tile's header, entry and mask word are loaded one tile ahead.
 constexpr int kRing = 64;  // queued entries per half of block I, per warp (a power of two)
 
 // 32 x 32 bit transpose across the warp: lane r holds row r (bit c = M[r][c]); the result in
