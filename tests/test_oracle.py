@@ -2,7 +2,8 @@
 
 The reference commits no golden output vectors for this path, so these restated tests (each
 citing the reference test it mirrors) are what ties the oracle to the reference's behaviour.
-CPU only.
+Closed forms from outside the reference pin the PME sum further: a direct Ewald sum and the
+Madelung energies of rock salt and cesium chloride.  CPU only.
 """
 import math
 
@@ -164,6 +165,45 @@ def test_pme_agrees_with_direct_ewald():
     fe, ee = O.ewald_reciprocal(pos, q, box, alpha, 12)
     assert abs(ep - ee) < 1e-6 * abs(ee)
     assert np.sqrt(((fp - fe) ** 2).sum() / (fe ** 2).sum()) < 1e-5
+
+
+def _rock_salt(cells, a):
+    """Conventional rock-salt cells (4 cation + 4 anion sites each), a cubic periodic box."""
+    g = np.arange(2 * cells) * (a / 2)
+    x, y, z = np.meshgrid(g, g, g, indexing="ij")
+    pos = np.stack([x, y, z], -1).reshape(-1, 3) + 0.01
+    idx = np.stack(np.meshgrid(*[np.arange(2 * cells)] * 3, indexing="ij"), -1).reshape(-1, 3)
+    q = np.where(idx.sum(1) % 2 == 0, 1.0, -1.0)
+    return pos, q, np.eye(3) * cells * a
+
+
+def _cesium_chloride(cells, a):
+    """Simple-cubic cations with anions at the cube centres, a cubic periodic box."""
+    g = np.arange(cells) * a
+    c = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    pos = np.vstack([c, c + a / 2]) + 0.01
+    q = np.concatenate([np.ones(len(c)), -np.ones(len(c))])
+    return pos, q, np.eye(3) * cells * a
+
+
+@pytest.mark.parametrize("lattice,cells,a,madelung,r0_per_a", [
+    ("rock salt", 4, 0.5628, 1.74756459463, 0.5),
+    ("cesium chloride", 5, 0.4123, 1.76267477307, math.sqrt(3) / 2),
+])
+def test_pme_reproduces_madelung_energies(lattice, cells, a, madelung, r0_per_a):
+    """An analytic pin of the whole PME sum (direct, reciprocal and self terms,
+    nonbonded.rs:771-1042, pme.rs:141-425): for a neutral ionic crystal whose periodic cell has
+    no dipole, the Ewald energy with conducting boundaries is the Madelung lattice energy,
+    -(N/2) M k_e q^2 / r0 (r0 the nearest-neighbour distance), and by symmetry no ion feels a
+    force."""
+    pos, q, box = (_rock_salt if lattice == "rock salt" else _cesium_chloride)(cells, a)
+    n = len(q)
+    f, e = O.nonbonded(pos, q, np.full(n, 0.1), np.zeros(n), [], method="PME", cutoff=1.0,
+                       ewald_tolerance=1e-6, box=box, use_dispersion_correction=False,
+                       threads=8)
+    exact = -(n / 2) * madelung * K / (r0_per_a * a)
+    assert abs(e - exact) < 3e-6 * abs(exact), (e, exact)
+    assert np.abs(f).max() < 1e-2  # against pair forces of K / r0^2 ~ 1,700 kJ/mol/nm
 
 
 # --- virial = -dU/d(strain) ---------------------------------------------------------------
