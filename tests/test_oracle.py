@@ -206,6 +206,22 @@ def test_pme_reproduces_madelung_energies(lattice, cells, a, madelung, r0_per_a)
     assert np.abs(f).max() < 1e-2  # against pair forces of K / r0^2 ~ 1,700 kJ/mol/nm
 
 
+def test_dispersion_correction_is_the_lj_tail_integral():
+    """nonbonded.rs:660-719 for identical particles: the correction is the LJ energy beyond the
+    cutoff of a uniform fluid, (N^2 / 2V) int_rc^inf 4 pi r^2 4 eps [(s/r)^12 - (s/r)^6] dr =
+    8 pi N^2 eps / V [s^12 / (9 rc^9) - s^6 / (3 rc^3)], whatever the positions."""
+    box_len, n_side, sig, eps, rc = 3.0, 5, 0.3, 0.5, 1.0
+    g = (np.arange(n_side) + 0.5) * box_len / n_side
+    pos = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    n = len(pos)
+    args = (pos, np.zeros(n), np.full(n, sig), np.full(n, eps), [])
+    kw = dict(method="CutoffPeriodic", cutoff=rc, box=np.eye(3) * box_len)
+    _, with_tail = O.nonbonded(*args, use_dispersion_correction=True, **kw)
+    _, without = O.nonbonded(*args, use_dispersion_correction=False, **kw)
+    tail = 8 * math.pi * n * n * eps / box_len**3 * (sig**12 / (9 * rc**9) - sig**6 / (3 * rc**3))
+    assert abs((with_tail - without) - tail) < 1e-12 * abs(tail)
+
+
 # --- virial = -dU/d(strain) ---------------------------------------------------------------
 def test_virial_matches_strain_derivative():
     w = synth.water_box(40, 1.9, (4, 4, 3), seed=5)
