@@ -206,6 +206,43 @@ def test_pme_reproduces_madelung_energies(lattice, cells, a, madelung, r0_per_a)
     assert np.abs(f).max() < 1e-2  # against pair forces of K / r0^2 ~ 1,700 kJ/mol/nm
 
 
+@pytest.mark.parametrize("method", ["CutoffNonPeriodic", "CutoffPeriodic"])
+def test_reaction_field_pair_closed_form(method):
+    """nonbonded.rs:1222-1243: a pair inside the cutoff has E = k q1 q2 (1/r + k_rf r^2 - c_rf)
+    with k_rf = (e_rf - 1) / ((2 e_rf + 1) rc^3), c_rf = 3 e_rf / ((2 e_rf + 1) rc), and the
+    force along the pair k q1 q2 (1/r^2 - 2 k_rf r)."""
+    r, rc, e_rf, q1, q2 = 0.5, 1.0, 78.3, 0.7, -0.4
+    kw = dict(method=method, cutoff=rc, reaction_field_dielectric=e_rf,
+              use_dispersion_correction=False)
+    if method == "CutoffPeriodic":
+        kw["box"] = np.eye(3) * 3.0
+    f, e = O.nonbonded([[0, 0, 0], [r, 0, 0]], [q1, q2], [0.1, 0.1], [0, 0], [], **kw)
+    krf = (e_rf - 1) / ((2 * e_rf + 1) * rc**3)
+    crf = 3 * e_rf / ((2 * e_rf + 1) * rc)
+    assert abs(e - K * q1 * q2 * (1 / r + krf * r * r - crf)) < 1e-12
+    assert abs(f[1, 0] - K * q1 * q2 * (1 / r**2 - 2 * krf * r)) < 1e-11
+    assert abs(f[0, 0] + f[1, 0]) < 1e-12
+
+
+@pytest.mark.parametrize("r", [0.85, 0.95])
+def test_lj_switching_closed_form(r):
+    """nonbonded.rs:888-900: between the switching distance and the cutoff the LJ energy is
+    multiplied by S(t) = 1 - 10 t^3 + 15 t^4 - 6 t^5, t = (r - rs) / (rc - rs), and the force is
+    -(dU/dr S + U dS/dr)."""
+    sig, eps, rs, rc = 0.3, 0.6, 0.8, 1.0
+    f, e = O.nonbonded([[0, 0, 0], [r, 0, 0]], [0, 0], [sig, sig], [eps, eps], [],
+                       method="CutoffNonPeriodic", cutoff=rc, use_switching=True,
+                       switching_distance=rs, use_dispersion_correction=False)
+    t = (r - rs) / (rc - rs)
+    s = 1 - 10 * t**3 + 15 * t**4 - 6 * t**5
+    ds = (-30 * t**2 + 60 * t**3 - 30 * t**4) / (rc - rs)
+    sr6 = (sig / r) ** 6
+    u = 4 * eps * (sr6 * sr6 - sr6)
+    du = 4 * eps * (-12 * sr6 * sr6 + 6 * sr6) / r
+    assert abs(e - u * s) < 1e-15
+    assert abs(f[1, 0] + (du * s + u * ds)) < 1e-14
+
+
 def test_dispersion_correction_is_the_lj_tail_integral():
     """nonbonded.rs:660-719 for identical particles: the correction is the LJ energy beyond the
     cutoff of a uniform fluid, (N^2 / 2V) int_rc^inf 4 pi r^2 4 eps [(s/r)^12 - (s/r)^6] dr =
