@@ -10,6 +10,8 @@ oracle or engine output is written here), citing the test each case comes from:
 * nonbonded.rs:1497-1515  test_exclusions
 * tests/gbsa_obc.rs:24-58 isolated_gbsa_matches_born_and_surface_energies
 * tests/integrator_compatibility.rs:38-58 langevin_middle_matches_reference_zero_temperature_update
+* harmonic_bond.rs:187-228  test_bonds, test_periodic
+* harmonic_angle.rs:212-259 test_equilibrium, test_displaced_angle, test_conservation
 * Random123 kat_vectors for philox4x32_10 (Salmon et al., SC'11)
 
 Run:  python tests/golden/make_known_answers.py
@@ -64,6 +66,28 @@ def main():
         temperature=0.0, friction=2.0, step_size=0.1, position=[1.0, 0.0, 0.0],
         velocity=[0.3, 0.0, 0.0], force=[4.0, 0.0, 0.0], mass=2.0, expected_velocity_x=v,
         expected_position_x=1.0 + 0.05 * (0.5 + v), tolerance=2e-7)
+    # harmonic_bond.rs:187-208: bonds (0, 1, 1.5, 0.8) and (1, 2, 1.2, 0.7) (i, j, length, k)
+    cases["harmonic_bonds"] = dict(
+        positions=[[0.0, 2.0, 0.0], [0.0, 0.0, 0.0], [1.0, 0.0, 0.0]],
+        bonds=[[0, 1, 1.5, 0.8], [1, 2, 1.2, 0.7]],
+        expected_force0_y=-0.8 * 0.5, expected_force2_x=0.7 * 0.2,
+        expected_energy=0.5 * 0.8 * 0.25 + 0.5 * 0.7 * 0.04, tolerance=1e-5)
+    # harmonic_bond.rs:210-228: the minimum image across a 3 nm cubic box
+    cases["harmonic_bond_periodic"] = dict(
+        positions=[[0.0, 2.0, 0.0], [0.0, 0.0, 0.0]], bonds=[[0, 1, 1.2, 0.8]],
+        box=[[3.0, 0.0, 0.0], [0.0, 3.0, 0.0], [0.0, 0.0, 3.0]],
+        expected_energy=0.5 * 0.8 * 0.04, tolerance=1e-5)
+    # harmonic_angle.rs:212-259 (i, j, k, theta0, k_theta)
+    cases["harmonic_angles"] = dict(
+        equilibrium=dict(positions=[[1.0, 0.0, 0.0], [0.0, 0.0, 0.0], [0.0, 1.0, 0.0]],
+                         angles=[[0, 1, 2, math.pi / 2, 1.0]], expected_energy=0.0,
+                         energy_tolerance=1e-5, force_tolerance=1e-4),
+        displaced=dict(positions=[[1.0, 0.0, 0.0], [0.0, 0.0, 0.0], [1.0, 1.0, 0.0]],
+                       angles=[[0, 1, 2, math.pi / 2, 2.0]],
+                       expected_energy=0.5 * 2.0 * (math.pi / 4 - math.pi / 2) ** 2,
+                       energy_tolerance=1e-5),
+        conservation=dict(positions=[[1.2, 0.3, 0.0], [0.0, 0.0, 0.0], [0.4, 1.1, 0.0]],
+                          angles=[[0, 1, 2, math.pi / 2, 1.5]], force_sum_tolerance=1e-4))
     # Random123 philox4x32_10 known-answer vectors
     cases["philox4x32_10"] = [
         dict(ctr=[0, 0, 0, 0], key=[0, 0],

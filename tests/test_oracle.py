@@ -60,6 +60,33 @@ def test_lfmiddle_zero_temperature_known_answer(known_answers):
     assert abs(x[0, 0] - c["expected_position_x"]) < c["tolerance"]
 
 
+def test_harmonic_bond_known_answers(known_answers):
+    c = known_answers["harmonic_bonds"]  # harmonic_bond.rs:187-208
+    f, e = O.harmonic_bonds(c["positions"], [tuple(b) for b in c["bonds"]])
+    assert abs(f[0, 1] - c["expected_force0_y"]) < c["tolerance"]
+    assert abs(f[2, 0] - c["expected_force2_x"]) < c["tolerance"]
+    assert abs(f[1, 0] + f[0, 0] + f[2, 0]) < c["tolerance"]
+    assert abs(e - c["expected_energy"]) < c["tolerance"]
+    c = known_answers["harmonic_bond_periodic"]  # harmonic_bond.rs:210-228
+    _, e = O.harmonic_bonds(c["positions"], [tuple(b) for b in c["bonds"]], use_pbc=True,
+                            box=np.array(c["box"]))
+    assert abs(e - c["expected_energy"]) < c["tolerance"]
+
+
+def test_harmonic_angle_known_answers(known_answers):
+    c = known_answers["harmonic_angles"]  # harmonic_angle.rs:212-259
+    eq = c["equilibrium"]
+    f, e = O.harmonic_angles(eq["positions"], [tuple(a) for a in eq["angles"]])
+    assert abs(e - eq["expected_energy"]) < eq["energy_tolerance"]
+    assert np.abs(f).max() < eq["force_tolerance"]
+    d = c["displaced"]
+    _, e = O.harmonic_angles(d["positions"], [tuple(a) for a in d["angles"]])
+    assert abs(e - d["expected_energy"]) < d["energy_tolerance"]
+    cons = c["conservation"]
+    f, _ = O.harmonic_angles(cons["positions"], [tuple(a) for a in cons["angles"]])
+    assert np.abs(f.sum(0)).max() < cons["force_sum_tolerance"]
+
+
 def test_philox_known_answer_vectors(known_answers):
     for case in known_answers["philox4x32_10"]:
         assert list(O.philox(case["ctr"], case["key"])) == case["out"]
