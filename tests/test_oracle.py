@@ -390,6 +390,26 @@ def test_equipartition_free_particles():
     assert abs(ek / 2000 - expected) < 0.12 * expected
 
 
+def test_lfmiddle_one_step_variances_and_moments():
+    """tests/stochastic.rs:173-216 for LangevinMiddle: from rest with no force, one step gives
+    velocities of variance kT/m (1 - exp(-2 gamma dt)) for each mass, positions v dt/2
+    exactly, and normalized velocities with the Gaussian moments 0, 1, 3 (within six standard
+    errors)."""
+    count, temperature, friction, dt = 60000, 310.0, 2.1, 0.003
+    masses = np.array([[1.0, 4.0, 9.0][i % 3] for i in range(count)])
+    zero = np.zeros((count, 3))
+    rc, x, v = O.lfmiddle_step(zero, zero, zero, masses, dt, temperature, friction,
+                               O.gaussian_noise(371, 0, 0, count))
+    assert rc == 0
+    assert np.abs(x - v * dt / 2).max() < 1e-15
+    kb = 1.380649e-23 * 6.02214076e23 / 1000.0
+    for group in range(3):
+        var = kb * temperature / masses[group] * -np.expm1(-2.0 * friction * dt)
+        z = (v[group::3] / np.sqrt(var)).reshape(-1)
+        for moment, target, spread in [(1, 0.0, 1.0), (2, 1.0, 2.0), (4, 3.0, 96.0)]:
+            assert abs((z ** moment).mean() - target) < 6.0 * np.sqrt(spread / z.size), moment
+
+
 def test_gaussian_stream_moments():
     z = O.gaussian_noise(123, 0, 7, 200000).reshape(-1)
     assert abs(z.mean()) < 0.01
