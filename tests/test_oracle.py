@@ -270,6 +270,22 @@ def test_lj_switching_closed_form(r):
     assert abs(f[1, 0] + (du * s + u * ds)) < 1e-14
 
 
+def test_direct_and_reciprocal_parts_sum_to_the_whole():
+    """tests/force_groups.rs:55-96 (the PME case): the direct-space part and the
+    reciprocal-space part (each with the corrections it owns) add up to the complete
+    NonbondedForce, energies to 1e-10 and forces to rounding."""
+    pos = [[0.1, 0.2, 0.3], [0.6, 0.4, 0.2], [2.8, 0.7, 0.4]]
+    args = (pos, [0.4, -0.3, 0.1], [0.3, 0.32, 0.34], [0.5, 0.6, 0.7],
+            [(0, 2, -0.02, 0.32, 0.4)])
+    kw = dict(method="PME", cutoff=1.0, box=np.eye(3) * 3.0)
+    f_all, e_all = O.nonbonded(*args, **kw)
+    f_dir, e_dir = O.nonbonded(*args, include_reciprocal=False, **kw)
+    f_rec, e_rec = O.nonbonded(*args, include_direct=False, **kw)
+    assert abs(e_all - e_dir - e_rec) < 1e-10
+    assert np.abs(f_all - f_dir - f_rec).max() < 1e-10
+    assert e_dir != 0.0 and e_rec != 0.0
+
+
 def test_dispersion_correction_is_the_lj_tail_integral():
     """nonbonded.rs:660-719 for identical particles: the correction is the LJ energy beyond the
     cutoff of a uniform fluid, (N^2 / 2V) int_rc^inf 4 pi r^2 4 eps [(s/r)^12 - (s/r)^6] dr =
